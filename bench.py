@@ -1,0 +1,353 @@
+"""Benchmark of the matrix-free PA operator path on B200.
+
+Default workload (N=1): the scale-up configuration 128^3 Q2 hex mesh on the
+unit cube (257^3 = 16,974,593 DOFs, 3^3 Gauss points), lognormal kappa
+(sigma^2 = 1, correlation length 0.1, seeded), FP64.
+
+A step is one application of the constrained FP64 PA diffusion operator
+(y = A x, sum-factorised apply + deterministic scatter) to a device-resident
+vector; `value` is whole-job GDOF/s (DOFs of all ranks x steps / max-over-ranks
+device time).  `e2e` is the same metric through the public C ABI call
+(fg_op_apply on pinned host buffers: H2D copy of x, apply, D2H copy of y each
+step).  `solve` reports time to FP64 true relative residual 1e-8 of plain FP64
+PCG (Chebyshev(4) on D^-1 A, and Jacobi).
+
+--impl reference times the reference's algorithm (the oracle port of
+crates/assembly/src/partial.rs's element loop with the Hex8 isoparametric
+Jacobian) on the host cores, on a z-slab sample of the same workload.
+
+Multi-GPU: one independent instance per rank (its own seeded kappa), no
+data-path collective; scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "fem-rs_b200"))
+
+METRIC = "time to 1e-8 FP64 residual & PA GDOF/s on 1 B200: chosen vs plain FP64 PCG"
+WORKLOADS = {
+    # name: (n elements per direction, order)
+    "c1a": (128, 2),   # 128^3 Q2, 17.0M DOFs (headline)
+    "c1b": (64, 3),    # 64^3 Q3, 7.2M DOFs
+    "c4": (128, 1),    # 128^3 Q1, 2.15M DOFs
+    "small": (64, 2),  # 64^3 Q2, 2.15M DOFs (profiling case, qdata 340 MB > L2)
+}
+
+
+def canonical_bytes(n, p):
+    """Algorithmic bytes of one FP64 diffusion apply: 6 symmetric qdata
+    components per quadrature point, an int32 element-to-DOF map, x read and
+    y written once."""
+    E = n ** 3
+    q3 = (p + 1) ** 3
+    N = (n * p + 1) ** 3
+    return 6 * q3 * E * 8 + q3 * E * 4 + 2 * N * 8, 6 * q3 * E * 8 + 2 * N * 8
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """Per-launch DRAM bytes of the apply kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch_full_size:"):
+                return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [s.strip() for s in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_apply_sample(n, p, kq_full, reps=2, layers=None):
+    """Oracle (reference-algorithm port) apply on a z-slab of the workload, all
+    host threads.  Returns (GDOF/s, threads, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    nzs = layers or max(1, n // 8)
+    q3 = (p + 1) ** 3
+    kq = np.ascontiguousarray(kq_full[: n * n * nzs * q3])
+    mesh = O.Mesh(n, n, nzs, p)
+    coef = O.Coef(O.DIFF, kappa_q=kq)
+    x = np.random.default_rng(1).standard_normal(mesh.ndofs)
+    y = np.zeros(mesh.ndofs)
+    O.pa_apply(mesh, coef, x, y)  # warm
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.pa_apply(mesh, coef, x, y)
+    dt = (time.perf_counter() - t0) / reps
+    cores = os.cpu_count()
+    desc = (f"oracle port of the reference PA element loop (partial.rs:154-208 + assembler.rs:96-143), "
+            f"{n}x{n}x{nzs} Q{p} z-slab of the workload ({mesh.ndofs} DOFs), {reps} applies, "
+            f"OpenMP {cores} threads")
+    return mesh.ndofs / dt / 1e9, cores, desc
+
+
+def run_reference(args, n, p):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from femgpu.fields import lognormal_kappa_q
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    nzs = max(1, n // 32)
+    q3 = (p + 1) ** 3
+    kq = lognormal_kappa_q(n, n, n, p, seed=0)[: n * n * nzs * q3].copy()
+    mesh = O.Mesh(n, n, nzs, p)
+    coef = O.Coef(O.DIFF, kappa_q=kq)
+    x = np.random.default_rng(1).standard_normal(mesh.ndofs)
+    y = np.zeros(mesh.ndofs)
+    for _ in range(args.warmup):
+        O.pa_apply(mesh, coef, x, y)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.pa_apply(mesh, coef, x, y)
+    dt = time.perf_counter() - t0
+    val = mesh.ndofs * args.steps / dt / 1e9
+    cores = os.cpu_count()
+    out = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "GDOF/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: lognormal kappa GRF (sigma2=1, ell=0.1, seed 0) at Gauss points, x ~ N(0,1)",
+        "config": {"workload": f"{n}^3 Q{p} FP64 PA diffusion apply (sample: {n}x{n}x{nzs} z-slab)",
+                   "order": p, "n_elem_1d": n, "l2": "inputs larger than L2 not applicable on CPU"},
+        "cpu_baseline": {"value": val, "unit": "GDOF/s", "cores": cores, "kind": "port",
+                         "sample": f"{n}x{n}x{nzs} Q{p} z-slab ({mesh.ndofs} DOFs) per step, OpenMP {cores} threads; "
+                                   "the reference (Rust) cannot be built here, so this is the C restatement of its algorithm"},
+        "e2e": {"value": val, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c1a", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    n, p = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, n, p)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import femgpu
+    from femgpu.fields import lognormal_kappa_q, sin_nodal
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    kq = lognormal_kappa_q(n, n, n, p, sigma2=1.0, ell=0.1, seed=rank)
+    op = femgpu.PADiffusionOperator((n, n, n), p, kappa=kq)
+    stream = torch.cuda.current_stream(dev)
+    op.set_stream(stream.cuda_stream)
+    N = op.n_dofs()
+    gen = np.random.default_rng(1000 + rank)
+    x = torch.from_numpy(op.to_native(gen.standard_normal(N))).to(dev)
+    y = torch.zeros_like(x)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        op.apply_native(x.data_ptr(), y.data_ptr(), accumulate=False, constrained=True)
+    torch.cuda.synchronize()
+    op.check()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        op.apply_native(x.data_ptr(), y.data_ptr(), accumulate=False, constrained=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t_ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    if world > 1:
+        tt = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    op.check()
+    per_apply_s = t_ms / 1e3 / args.steps
+    value = world * N * args.steps / (t_ms / 1e3) / 1e9
+    bytes_canon, bytes_nomap = canonical_bytes(n, p)
+    peak, peak_kind = measured_peak()
+    achieved = bytes_canon / per_apply_s / 1e9
+    tr = profile_traffic(f"pa_apply_fp64_q{p}_{n}.txt")
+    launches_per_apply = 2 if (op.nx > 32 or op.ny > 4 or op.nz > 1) else 1
+
+    # e2e through the public C ABI with pinned host buffers
+    xh = torch.from_numpy(gen.standard_normal(N)).pin_memory()
+    yh = torch.zeros(N, dtype=torch.float64).pin_memory()
+    k_e2e = max(3, min(args.steps, 20))
+    for _ in range(2):
+        op.apply_zero(xh, yh, constrained=True)
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(k_e2e):
+        op.apply_zero(xh, yh, constrained=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    te_ms = f0.elapsed_time(f1)
+    if world > 1:
+        tt = torch.tensor([te_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te_ms = float(tt.item())
+    e2e_val = world * N * k_e2e / (te_ms / 1e3) / 1e9
+    _ = float(yh[0])
+
+    solve = None
+    if not args.no_solve:
+        solve = {}
+        mass = femgpu.PAMassOperator((n, n, n), p)
+        mass.set_stream(stream.cuda_stream)
+        b = np.zeros(N)
+        mass.apply_zero(sin_nodal(n, n, n, p), b, constrained=False)
+        # homogeneous Dirichlet: zero boundary rows of the RHS
+        bb = b.reshape(op.NK, op.NJ, op.NI)
+        bb[0], bb[-1], bb[:, 0], bb[:, -1], bb[:, :, 0], bb[:, :, -1] = 0, 0, 0, 0, 0, 0
+        mass.close()
+        for name, pc in (("plain_fp64_chebyshev4", femgpu.PC_CHEBYSHEV), ("plain_fp64_jacobi", femgpu.PC_JACOBI)):
+            xs = np.zeros(N)
+            cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4)
+            r = op.pcg(b, xs, cfg, pc)
+            solve[name] = {"iterations": r.iterations, "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual,
+                           "converged": r.converged, "applies": r.applies,
+                           "lmax": r.lmax if pc == femgpu.PC_CHEBYSHEV else None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            v, cores, desc = cpu_apply_sample(n, p, kq)
+            cpu = {"value": v, "unit": "GDOF/s", "cores": cores, "kind": "port", "sample": desc}
+        except Exception as exc:  # keep the bench line even if the oracle is unavailable
+            cpu = {"value": None, "unit": "GDOF/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "GDOF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: lognormal kappa GRF (sigma2=1, ell=0.1, seed=rank) at Gauss points, x ~ N(0,1)",
+            "config": {"workload": f"{n}^3 Q{p} unit-cube hex, FP64 PA diffusion apply (constrained), "
+                                   f"{N} DOFs per rank", "order": p, "n_elem_1d": n,
+                       "l2": "inputs larger than L2 (qdata %.2f GB per apply)" % (6 * (p + 1) ** 3 * n ** 3 * 8 / 1e9),
+                       "parallelism": f"{world} independent instances"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": tr,
+                         "bytes_per_apply_canonical": bytes_canon, "bytes_per_apply_no_map": bytes_nomap,
+                         "frac_no_map": bytes_nomap / per_apply_s / 1e9 / peak, "peak_kind": peak_kind,
+                         "kernel": "pa_apply_kernel + fixup_kernel (timed together per apply)"},
+            "e2e": {"value": e2e_val, "unit": "GDOF/s", "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
+                    "steps": k_e2e},
+            "gpu_launches": launches_per_apply * args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "solve": solve,
+        }
+        print(json.dumps(out), flush=True)
+    op.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,775 @@
+// femgpu.cu -- host side of libfemgpu.so: the C ABI of include/femgpu.h over
+// the sm_100a kernels of pa_kernels.cuh and vec_kernels.cuh.
+//
+// There is no CPU fallback: every numeric entry point runs on the GPU and
+// fails with FG_CUDA_ERROR when no usable device is present.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/femgpu.h"
+#include "fg_common.cuh"
+#include "pa_kernels.cuh"
+#include "vec_kernels.cuh"
+
+
+using namespace fg;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local int t_last_status = FG_OK;
+static thread_local std::string t_last_msg;
+
+static int fail(int status, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_last_status = status;
+    t_last_msg = buf;
+    return status;
+}
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(FG_CUDA_ERROR, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                               \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// 1-D tables: Gauss-Legendre (crates/element/src/quadrature.rs:12-32) and
+// equispaced Lagrange polynomials (quad.rs:92-105, seg.rs:119-121 conventions).
+// ---------------------------------------------------------------------------
+static void gauss_legendre(int n, double *x, double *w) {
+    switch (n) {
+    case 1: x[0] = 0.0; w[0] = 2.0; break;
+    case 2: { double a = 1.0 / std::sqrt(3.0); x[0] = -a; x[1] = a; w[0] = w[1] = 1.0; } break;
+    case 3: {
+        double a = std::sqrt(3.0 / 5.0);
+        x[0] = -a; x[1] = 0.0; x[2] = a;
+        w[0] = 5.0 / 9.0; w[1] = 8.0 / 9.0; w[2] = 5.0 / 9.0;
+    } break;
+    default: {
+        double a = std::sqrt(3.0 / 7.0 - 2.0 / 7.0 * std::sqrt(6.0 / 5.0));
+        double b = std::sqrt(3.0 / 7.0 + 2.0 / 7.0 * std::sqrt(6.0 / 5.0));
+        double wa = (18.0 + std::sqrt(30.0)) / 36.0, wb = (18.0 - std::sqrt(30.0)) / 36.0;
+        x[0] = -b; x[1] = -a; x[2] = a; x[3] = b;
+        w[0] = wb; w[1] = wa; w[2] = wa; w[3] = wb;
+    } break;
+    }
+}
+
+static void lagrange1d(int p, double xi, double *phi, double *dphi) {
+    double nodes[FG_MAXP + 1];
+    for (int k = 0; k <= p; ++k) nodes[k] = -1.0 + 2.0 * k / p;
+    for (int i = 0; i <= p; ++i) {
+        double v = 1.0, dv = 0.0;
+        for (int j = 0; j <= p; ++j) {
+            if (j == i) continue;
+            double den = nodes[i] - nodes[j];
+            double prod = 1.0 / den;
+            for (int m = 0; m <= p; ++m) {
+                if (m == i || m == j) continue;
+                prod *= (xi - nodes[m]) / (nodes[i] - nodes[m]);
+            }
+            dv += prod;
+            v *= (xi - nodes[j]) / den;
+        }
+        phi[i] = v;
+        dphi[i] = dv;
+    }
+}
+
+static std::mutex g_init_mu;
+static bool g_tables_ready[64];
+
+static int ensure_tables(int dev) {
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    if (dev < 0 || dev >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", dev);
+    if (g_tables_ready[dev]) return FG_OK;
+    double B[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {}, G[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {};
+    float Bf[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {}, Gf[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {};
+    for (int p = 1; p <= FG_MAXP; ++p) {
+        double x[4], w[4];
+        gauss_legendre(p + 1, x, w);
+        for (int q = 0; q <= p; ++q) {
+            double phi[4], dphi[4];
+            lagrange1d(p, x[q], phi, dphi);
+            for (int d = 0; d <= p; ++d) {
+                B[p - 1][q][d] = phi[d];
+                G[p - 1][q][d] = dphi[d];
+                Bf[p - 1][q][d] = (float)phi[d];
+                Gf[p - 1][q][d] = (float)dphi[d];
+            }
+        }
+    }
+    CK(cudaMemcpyToSymbol(c_B64, B, sizeof B));
+    CK(cudaMemcpyToSymbol(c_G64, G, sizeof G));
+    CK(cudaMemcpyToSymbol(c_B32, Bf, sizeof Bf));
+    CK(cudaMemcpyToSymbol(c_G32, Gf, sizeof Gf));
+    g_tables_ready[dev] = true;
+    return FG_OK;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static int ensure_encode() {
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    if (g_encode) return FG_OK;
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !fn)
+        return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled entry point not found");
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return FG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernel configurations per order
+// ---------------------------------------------------------------------------
+template <int P> struct KCfg;
+template <> struct KCfg<1> { static constexpr int WY = 4, S = 4, MINB = 3; };
+template <> struct KCfg<2> { static constexpr int WY = 4, S = 3, MINB = 2; };
+template <> struct KCfg<3> { static constexpr int WY = 2, S = 2, MINB = 1; };
+
+static int cfg_wy(int p) { return p == 1 ? KCfg<1>::WY : p == 2 ? KCfg<2>::WY : KCfg<3>::WY; }
+
+// ---------------------------------------------------------------------------
+// the operator handle
+// ---------------------------------------------------------------------------
+struct fg_op {
+    std::mutex mu;
+    int device = 0;
+    Grid g{};
+    int ess_tags = 0, kind = 0, p = 0;
+    int64_t N = 0, Nn = 0;
+    double *qd = nullptr, *face = nullptr;
+    double *xs = nullptr, *ys = nullptr;
+    double *dinv = nullptr, *ones = nullptr;
+    bool have_dinv = false;
+    double lmax_est = 0.0;
+    bool have_lmax = false;
+    double *r = nullptr, *z = nullptr, *pv = nullptr, *ap = nullptr, *xw = nullptr, *bw = nullptr;
+    double *cres = nullptr, *cd = nullptr, *ct = nullptr;
+    double *partials = nullptr;
+    SolverState *st = nullptr;
+    int *d_err = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static void free_op(fg_op *op) {
+    if (!op) return;
+    cudaSetDevice(op->device);
+    if (op->stream) cudaStreamSynchronize(op->stream);
+    double *bufs[] = {op->qd, op->face, op->xs, op->ys, op->dinv, op->ones, op->r, op->z, op->pv, op->ap,
+                      op->xw, op->bw, op->cres, op->cd, op->ct, op->partials};
+    for (double *b : bufs)
+        if (b) cudaFree(b);
+    if (op->st) cudaFree(op->st);
+    if (op->d_err) cudaFree(op->d_err);
+    if (op->ev0) cudaEventDestroy(op->ev0);
+    if (op->ev1) cudaEventDestroy(op->ev1);
+    if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
+    delete op;
+}
+
+static int alloc_vec(double **p, int64_t n) {
+    CK(cudaMalloc(p, sizeof(double) * std::max<int64_t>(n, 1)));
+    CK(cudaMemset(*p, 0, sizeof(double) * std::max<int64_t>(n, 1)));
+    return FG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <int P, int OPK>
+static int launch_apply_t(fg_op *op, const Grid &g, const double *x, double *y, int accumulate,
+                          const int *skip) {
+    using C = KCfg<P>;
+    using SM = ApplySmem<P, double, C::WY, C::S, NComp<OPK>::v>;
+    static bool attr_set[64] = {};
+    auto kern = pa_apply_kernel<P, OPK, double, C::WY, C::S, C::MINB>;
+    if (!attr_set[op->device]) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
+        attr_set[op->device] = true;
+    }
+    CUtensorMap tmap;
+    cuuint64_t gdim[3] = {(cuuint64_t)g.NI, (cuuint64_t)g.NJ, (cuuint64_t)g.NK};
+    cuuint64_t gstr[2] = {(cuuint64_t)g.NIp * sizeof(double),
+                          (cuuint64_t)g.NIp * g.NJ * sizeof(double)};
+    cuuint32_t box[3] = {(cuuint32_t)SM::XW, (cuuint32_t)SM::RY, (cuuint32_t)(P + 1)};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult cr = g_encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(x), gdim,
+                           gstr, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
+    ApplyArgs<double> A{g, op->qd, y, op->face, accumulate, op->d_err, skip};
+    kern<<<g.n_items(), C::WY * 32, SM::bytes, op->stream>>>(tmap, A);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+template <int P>
+static int launch_apply_p(fg_op *op, const Grid &g, const double *x, double *y, int accumulate,
+                          const int *skip) {
+    switch (op->kind) {
+    case FG_MASS: return launch_apply_t<P, 1>(op, g, x, y, accumulate, skip);
+    case FG_DIFF: return launch_apply_t<P, 2>(op, g, x, y, accumulate, skip);
+    default: return launch_apply_t<P, 3>(op, g, x, y, accumulate, skip);
+    }
+}
+
+static int launch_fixup(fg_op *op, const Grid &g, double *y, const int *skip) {
+    const int64_t total = (int64_t)(g.ntx - 1) * g.NJ * g.NK + (int64_t)(g.nty - 1) * g.NI * g.NK +
+                          (int64_t)(g.ntz - 1) * g.NI * g.NJ;
+    if (total <= 0) return FG_OK;
+    const int threads = 256;
+    const int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 16);
+    fixup_kernel<double><<<blocks, threads, 0, op->stream>>>(g, y, op->face, skip);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+static int apply_native(fg_op *op, const double *x, double *y, int accumulate, int constrained,
+                        const int *skip) {
+    Grid g = op->g;
+    g.ess = constrained ? op->ess_tags : 0;
+    int rc;
+    switch (op->p) {
+    case 1: rc = launch_apply_p<1>(op, g, x, y, accumulate, skip); break;
+    case 2: rc = launch_apply_p<2>(op, g, x, y, accumulate, skip); break;
+    default: rc = launch_apply_p<3>(op, g, x, y, accumulate, skip); break;
+    }
+    if (rc) return rc;
+    return launch_fixup(op, g, y, skip);
+}
+
+template <int P, int OPK> static int launch_diag_t(fg_op *op, const Grid &g, double *y) {
+    constexpr int WY = KCfg<P>::WY;
+    ApplyArgs<double> A{g, op->qd, y, op->face, 0, op->d_err, nullptr};
+    pa_diag_kernel<P, OPK, double, WY><<<g.n_items(), WY * 32, 0, op->stream>>>(A);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+template <int P> static int launch_diag_p(fg_op *op, const Grid &g, double *y) {
+    switch (op->kind) {
+    case FG_MASS: return launch_diag_t<P, 1>(op, g, y);
+    case FG_DIFF: return launch_diag_t<P, 2>(op, g, y);
+    default: return launch_diag_t<P, 3>(op, g, y);
+    }
+}
+static int diag_native(fg_op *op, double *y, int constrained) {
+    Grid g = op->g;
+    g.ess = constrained ? op->ess_tags : 0;
+    int rc;
+    switch (op->p) {
+    case 1: rc = launch_diag_p<1>(op, g, y); break;
+    case 2: rc = launch_diag_p<2>(op, g, y); break;
+    default: rc = launch_diag_p<3>(op, g, y); break;
+    }
+    if (rc) return rc;
+    return launch_fixup(op, g, y, nullptr);
+}
+
+template <int P, int OPK>
+static int launch_setup_t(fg_op *op, SetupArgs &S) {
+    const int64_t total = (int64_t)op->g.nx * op->g.ny * op->g.nz * (P + 1) * (P + 1) * (P + 1);
+    const int threads = 256;
+    const int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 32);
+    qdata_setup_kernel<P, OPK, double><<<blocks, threads, 0, op->stream>>>(S, op->qd);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+template <int P> static int launch_setup_p(fg_op *op, SetupArgs &S, int64_t *qsize) {
+    switch (op->kind) {
+    case FG_MASS: *qsize = qd_size<P, 1>(op->g); break;
+    case FG_DIFF: *qsize = qd_size<P, 2>(op->g); break;
+    default: *qsize = qd_size<P, 3>(op->g); break;
+    }
+    if (!op->qd) {
+        int rc = alloc_vec(&op->qd, *qsize);
+        if (rc) return rc;
+        return FG_OK;
+    }
+    switch (op->kind) {
+    case FG_MASS: return launch_setup_t<P, 1>(op, S);
+    case FG_DIFF: return launch_setup_t<P, 2>(op, S);
+    default: return launch_setup_t<P, 3>(op, S);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+FG_API void fg_cfg_default(fg_cfg *c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof *c);
+    c->rtol = 1e-8;
+    c->atol = 0.0;
+    c->max_iter = 1000;
+    c->print_level = 0;
+    c->precond = FG_PC_JACOBI;
+    c->cheb_degree = 4;
+    c->precision = FG_FP64;
+    c->power_iters = 20;
+    c->lmax = 0.0;
+    c->lmin_ratio = 30.0;
+    c->lmax_safety = 1.1;
+    c->inner_rtol = 1e-4;
+    c->check_interval = 10;
+}
+
+FG_API int fg_last_error(char *buf, size_t n) {
+    if (buf && n) {
+        std::strncpy(buf, t_last_msg.c_str(), n - 1);
+        buf[n - 1] = 0;
+    }
+    return t_last_status;
+}
+
+FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, double c_mass,
+                        double c_diff, const double *kappa_q, double kappa_const,
+                        const double *rho_q, double rho_const, int ess_tags, fg_op **out) {
+    t_last_status = FG_OK;
+    if (!out) return fail(FG_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!mesh || mesh->nx < 1 || mesh->ny < 1 || mesh->nz < 1)
+        return fail(FG_INVALID_ARGUMENT, "mesh must have at least one element per direction");
+    if (order < 1 || order > FG_MAXP)
+        return fail(FG_UNSUPPORTED, "unsupported order %d (supported: 1..%d)", order, FG_MAXP);
+    if (nq1d != order + 1)
+        return fail(FG_UNSUPPORTED, "nq1d must be order+1 (hex_rule(2p+1)), got %d", nq1d);
+    if (kind < 1 || kind > 3) return fail(FG_INVALID_ARGUMENT, "bad operator kind %d", kind);
+    if (ess_tags < 0 || ess_tags > 63) return fail(FG_INVALID_ARGUMENT, "bad ess_tags %d", ess_tags);
+    const int64_t NI = (int64_t)mesh->nx * order + 1, NJ = (int64_t)mesh->ny * order + 1,
+                  NK = (int64_t)mesh->nz * order + 1;
+    if (NI * NJ * NK > ((int64_t)1 << 40) || NI > (1 << 20) || NJ > (1 << 20) || NK > (1 << 20))
+        return fail(FG_INVALID_ARGUMENT, "mesh too large");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    int rc = ensure_tables(dev);
+    if (rc) return rc;
+    if ((rc = ensure_encode())) return rc;
+
+    fg_op *op = new fg_op();
+    op->device = dev;
+    op->kind = kind;
+    op->p = order;
+    op->ess_tags = ess_tags;
+    Grid &g = op->g;
+    g.nx = mesh->nx; g.ny = mesh->ny; g.nz = mesh->nz; g.p = order;
+    g.NI = (int)NI; g.NJ = (int)NJ; g.NK = (int)NK;
+    g.NIp = round_up((int)NI, 4);
+    g.WY = cfg_wy(order);
+    g.ntx = (g.nx + 31) / 32;
+    g.nty = (g.ny + g.WY - 1) / g.WY;
+    // layers per item: as many as keep >= 4 items per SM slot on a 148-SM part
+    int TZ = 8;
+    while (TZ > 1 && (int64_t)g.ntx * g.nty * ((g.nz + TZ - 1) / TZ) < 148 * 4) TZ /= 2;
+    g.TZ = TZ;
+    g.ntz = (g.nz + TZ - 1) / TZ;
+    g.ess = 0;
+    op->N = NI * NJ * NK;
+    op->Nn = (int64_t)g.NIp * NJ * NK;
+
+    auto bail = [&](int s) { free_op(op); return s; };
+    if (cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(FG_CUDA_ERROR, "cudaStreamCreate failed"));
+    op->own_stream = true;
+    if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)))
+        return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
+    if (cudaMalloc(&op->st, sizeof(SolverState)) != cudaSuccess ||
+        cudaMemset(op->st, 0, sizeof(SolverState)) != cudaSuccess)
+        return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
+    if ((rc = alloc_vec(&op->face, (int64_t)g.n_items() * g.face_stride()))) return bail(rc);
+    if ((rc = alloc_vec(&op->xs, op->Nn)) || (rc = alloc_vec(&op->ys, op->Nn))) return bail(rc);
+    if ((rc = alloc_vec(&op->partials, VEC_GRID * 4))) return bail(rc);
+    cudaEventCreate(&op->ev0);
+    cudaEventCreate(&op->ev1);
+
+    // inputs for the quadrature-data build
+    const int64_t E = (int64_t)g.nx * g.ny * g.nz;
+    const int Q3 = (order + 1) * (order + 1) * (order + 1);
+    double *d_vc = nullptr, *d_kq = nullptr, *d_rq = nullptr;
+    auto cleanup_in = [&]() {
+        if (d_vc) cudaFree(d_vc);
+        if (d_kq) cudaFree(d_kq);
+        if (d_rq) cudaFree(d_rq);
+    };
+    if (mesh->vcoord) {
+        const size_t nb = sizeof(double) * 3 * (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+        if (cudaMalloc(&d_vc, nb) || cudaMemcpy(d_vc, mesh->vcoord, nb, cudaMemcpyHostToDevice)) {
+            cleanup_in();
+            return bail(fail(FG_CUDA_ERROR, "vertex upload failed"));
+        }
+    }
+    if (kappa_q) {
+        const size_t nb = sizeof(double) * E * Q3;
+        if (cudaMalloc(&d_kq, nb) || cudaMemcpy(d_kq, kappa_q, nb, cudaMemcpyHostToDevice)) {
+            cleanup_in();
+            return bail(fail(FG_CUDA_ERROR, "kappa upload failed"));
+        }
+    }
+    if (rho_q) {
+        const size_t nb = sizeof(double) * E * Q3;
+        if (cudaMalloc(&d_rq, nb) || cudaMemcpy(d_rq, rho_q, nb, cudaMemcpyHostToDevice)) {
+            cleanup_in();
+            return bail(fail(FG_CUDA_ERROR, "rho upload failed"));
+        }
+    }
+    SetupArgs S{};
+    S.g = g;
+    S.vcoord = d_vc;
+    S.kappa_q = d_kq;
+    S.rho_q = d_rq;
+    S.kappa_c = kappa_const;
+    S.rho_c = rho_const;
+    S.c_m = c_mass;
+    S.c_k = c_diff;
+    gauss_legendre(order + 1, S.gx, S.gw);
+    S.err = op->d_err;
+    int64_t qsize = 0;
+    for (int pass = 0; pass < 2 && !rc; ++pass) {  // pass 0 allocates, pass 1 launches
+        switch (order) {
+        case 1: rc = launch_setup_p<1>(op, S, &qsize); break;
+        case 2: rc = launch_setup_p<2>(op, S, &qsize); break;
+        default: rc = launch_setup_p<3>(op, S, &qsize); break;
+        }
+    }
+    if (!rc && cudaStreamSynchronize(op->stream) != cudaSuccess)
+        rc = fail(FG_CUDA_ERROR, "qdata setup failed: %s", cudaGetErrorString(cudaGetLastError()));
+    cleanup_in();
+    if (rc) return bail(rc);
+    int herr = 0;
+    cudaMemcpy(&herr, op->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (herr & FG_DERR_BOUNDS) return bail(fail(FG_BOUNDS, "degenerate element (det J = 0)"));
+    *out = op;
+    return FG_OK;
+}
+
+FG_API void fg_op_destroy(fg_op *op) { free_op(op); }
+
+FG_API int64_t fg_op_ndofs(const fg_op *op) { return op ? op->N : -1; }
+
+FG_API int64_t fg_op_native_len(const fg_op *op) { return op ? op->Nn : -1; }
+
+FG_API int fg_op_layout(const fg_op *op, int64_t dims[4]) {
+    if (!op || !dims) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    dims[0] = op->g.NI; dims[1] = op->g.NJ; dims[2] = op->g.NK; dims[3] = op->g.NIp;
+    return FG_OK;
+}
+
+FG_API int fg_op_set_stream(fg_op *op, void *stream) {
+    if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    CK(cudaStreamSynchronize(op->stream));
+    if (op->own_stream) cudaStreamDestroy(op->stream);
+    op->own_stream = false;
+    op->stream = reinterpret_cast<cudaStream_t>(stream);
+    return FG_OK;
+}
+
+static int check_device_error(fg_op *op) {
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, op->d_err, sizeof(int), cudaMemcpyDeviceToHost, op->stream));
+    CK(cudaStreamSynchronize(op->stream));
+    if (herr) {
+        cudaMemsetAsync(op->d_err, 0, sizeof(int), op->stream);
+        if (herr & FG_DERR_TIMEOUT) return fail(FG_DEVICE_TIMEOUT, "device-side wait timed out");
+        return fail(FG_BOUNDS, "device-side bounds error");
+    }
+    return FG_OK;
+}
+
+FG_API int fg_op_check(fg_op *op) {
+    if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    return check_device_error(op);
+}
+
+static int to_native(fg_op *op, double *dst, const double *src, int mem) {
+    const Grid &g = op->g;
+    CK(cudaMemcpy2DAsync(dst, sizeof(double) * g.NIp, src, sizeof(double) * g.NI,
+                         sizeof(double) * g.NI, (size_t)g.NJ * g.NK,
+                         mem == FG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                         op->stream));
+    return FG_OK;
+}
+static int from_native(fg_op *op, double *dst, const double *src, int mem) {
+    const Grid &g = op->g;
+    CK(cudaMemcpy2DAsync(dst, sizeof(double) * g.NI, src, sizeof(double) * g.NIp,
+                         sizeof(double) * g.NI, (size_t)g.NJ * g.NK,
+                         mem == FG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                         op->stream));
+    return FG_OK;
+}
+
+FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, int constrained,
+                       int mem) {
+    if (!op || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    int rc;
+    if ((rc = to_native(op, op->xs, x, mem))) return rc;
+    if (accumulate && (rc = to_native(op, op->ys, y, mem))) return rc;
+    if ((rc = apply_native(op, op->xs, op->ys, accumulate, constrained, nullptr))) return rc;
+    if ((rc = from_native(op, y, op->ys, mem))) return rc;
+    return check_device_error(op);
+}
+
+FG_API int fg_op_apply_native(fg_op *op, const double *x, double *y, int accumulate,
+                              int constrained) {
+    if (!op || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (x == y) return fail(FG_INVALID_ARGUMENT, "x and y must not alias");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    return apply_native(op, x, y, accumulate, constrained, nullptr);
+}
+
+FG_API int fg_op_diagonal(fg_op *op, double *d, int constrained, int mem) {
+    if (!op || !d) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    int rc;
+    if ((rc = diag_native(op, op->ys, constrained))) return rc;
+    if ((rc = from_native(op, d, op->ys, mem))) return rc;
+    return check_device_error(op);
+}
+
+// ---------------------------------------------------------------------------
+// PCG
+// ---------------------------------------------------------------------------
+static int ensure_solver_buffers(fg_op *op, bool cheb) {
+    int rc;
+    double **v[] = {&op->r, &op->z, &op->pv, &op->ap, &op->xw, &op->bw};
+    for (double **b : v)
+        if (!*b && (rc = alloc_vec(b, op->Nn))) return rc;
+    if (cheb) {
+        double **c[] = {&op->cres, &op->cd, &op->ct};
+        for (double **b : c)
+            if (!*b && (rc = alloc_vec(b, op->Nn))) return rc;
+    }
+    return FG_OK;
+}
+
+static int ensure_dinv(fg_op *op) {
+    if (op->have_dinv) return FG_OK;
+    int rc;
+    if (!op->dinv && (rc = alloc_vec(&op->dinv, op->Nn))) return rc;
+    if ((rc = diag_native(op, op->ys, 1))) return rc;
+    k_invert_diag<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->g, op->ys, op->dinv);
+    CK(cudaGetLastError());
+    op->have_dinv = true;
+    return FG_OK;
+}
+
+static int read_state(fg_op *op, SolverState *h) {
+    CK(cudaMemcpyAsync(h, op->st, sizeof(SolverState), cudaMemcpyDeviceToHost, op->stream));
+    CK(cudaStreamSynchronize(op->stream));
+    return FG_OK;
+}
+
+// lambda_max(D^-1 A) by power iteration from the hashed start vector
+static int estimate_lmax(fg_op *op, int iters, double *out) {
+    int rc;
+    const int64_t n = op->Nn;
+    k_hash_vector<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->g, op->cd, op->partials, op->st);
+    k_scale_by_rho<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->cd, op->cd, op->st);
+    CK(cudaGetLastError());
+    for (int it = 0; it < iters; ++it) {
+        if ((rc = apply_native(op, op->cd, op->ct, 0, 1, nullptr))) return rc;
+        k_dinv_norm<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->ct, op->dinv, op->partials, op->st);
+        k_scale_by_rho<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->ct, op->cd, op->st);
+        CK(cudaGetLastError());
+    }
+    SolverState h;
+    if ((rc = read_state(op, &h))) return rc;
+    *out = h.rho;
+    return FG_OK;
+}
+
+struct ChebCoef {
+    double inv_theta;
+    std::vector<double> c1, c2;
+};
+static ChebCoef cheb_coefs(double lmin, double lmax, int k) {
+    ChebCoef c;
+    const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+    const double sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    c.inv_theta = 1.0 / theta;
+    for (int s = 1; s < k; ++s) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        c.c1.push_back(rn * rho);
+        c.c2.push_back(2.0 * rn / delta);
+        rho = rn;
+    }
+    return c;
+}
+
+// z = Chebyshev(D^-1 A) r (Saad Alg. 12.1, zero start, k sweeps)
+static int cheb_apply(fg_op *op, const ChebCoef &cc, const double *r, double *z, const int *skip,
+                      int64_t *applies) {
+    const int64_t n = op->Nn;
+    const SolverState *sst = skip ? op->st : nullptr;
+    k_cheb_first<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, r, op->dinv, op->cres, op->cd, z,
+                                                           cc.inv_theta, sst);
+    CK(cudaGetLastError());
+    for (size_t s = 0; s < cc.c1.size(); ++s) {
+        int rc = apply_native(op, op->cd, op->ct, 0, 1, skip);
+        if (rc) return rc;
+        ++*applies;
+        k_cheb_step<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->ct, op->dinv, op->cres, op->cd,
+                                                              z, cc.c1[s], cc.c2[s], sst);
+        CK(cudaGetLastError());
+    }
+    return FG_OK;
+}
+
+FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, fg_result *res,
+                  int mem) {
+    if (!op || !b || !x) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    fg_cfg cfg;
+    if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
+    if (cfg.max_iter < 0) return fail(FG_INVALID_ARGUMENT, "max_iter < 0");
+    if (cfg.precision != FG_FP64) return fail(FG_UNSUPPORTED, "precision %d not available", cfg.precision);
+    if (cfg.precond < 0 || cfg.precond > 2) return fail(FG_INVALID_ARGUMENT, "bad precond");
+    if (cfg.precond == FG_PC_CHEBYSHEV && cfg.cheb_degree < 1)
+        return fail(FG_INVALID_ARGUMENT, "cheb_degree must be >= 1");
+    if (cfg.check_interval < 1) cfg.check_interval = 10;
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    const bool cheb = cfg.precond == FG_PC_CHEBYSHEV;
+    int rc;
+    if ((rc = ensure_solver_buffers(op, true))) return rc;
+    double *dinv_use = op->dinv;
+    if (cfg.precond == FG_PC_NONE) {
+        // operator CG: z = r, i.e. Jacobi with an identity diagonal (pads zero)
+        if (!op->ones) {
+            if ((rc = alloc_vec(&op->ones, op->Nn))) return rc;
+            k_invert_diag<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->g, op->ones, op->ones);
+            CK(cudaGetLastError());
+        }
+        dinv_use = op->ones;
+    } else if ((rc = ensure_dinv(op))) {
+        return rc;
+    } else {
+        dinv_use = op->dinv;
+    }
+    double lmax = 0.0, lmin = 0.0;
+    int64_t applies = 0;
+    if (cheb) {
+        if (cfg.lmax > 0) {
+            lmax = cfg.lmax;
+        } else {
+            if (!op->have_lmax) {
+                if ((rc = estimate_lmax(op, cfg.power_iters > 0 ? cfg.power_iters : 20, &op->lmax_est)))
+                    return rc;
+                op->have_lmax = true;
+            }
+            lmax = (cfg.lmax_safety > 0 ? cfg.lmax_safety : 1.1) * op->lmax_est;
+        }
+        lmin = lmax / (cfg.lmin_ratio > 0 ? cfg.lmin_ratio : 30.0);
+    }
+    const ChebCoef cc = cheb ? cheb_coefs(lmin, lmax, cfg.cheb_degree) : ChebCoef{};
+    if ((rc = to_native(op, op->bw, b, mem)) || (rc = to_native(op, op->xw, x, mem))) return rc;
+    SolverState h{};
+    h.rtol = cfg.rtol;
+    h.atol = cfg.atol;
+    h.max_iter = cfg.max_iter;
+    CK(cudaMemcpyAsync(op->st, &h, sizeof h, cudaMemcpyHostToDevice, op->stream));
+    CK(cudaEventRecord(op->ev0, op->stream));
+    const int64_t n = op->Nn;
+    const int *skip = &op->st->done;
+    // r0 = b - A x0
+    if ((rc = apply_native(op, op->xw, op->ap, 0, 1, nullptr))) return rc;
+    ++applies;
+    k_pcg_init<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, dinv_use, op->r, op->z,
+                                                         op->pv, cheb ? 0 : 1, op->partials, op->st);
+    CK(cudaGetLastError());
+    if (cheb) {
+        if ((rc = cheb_apply(op, cc, op->r, op->z, skip, &applies))) return rc;
+        k_pcg_rz<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r, op->z, op->partials, op->st, 1);
+        k_pcg_pupdate<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z, op->pv, op->st, 1);
+        CK(cudaGetLastError());
+    }
+    int iters_launched = 0;
+    while (iters_launched < cfg.max_iter) {
+        const int chunk = std::min(cfg.check_interval, cfg.max_iter - iters_launched);
+        for (int k = 0; k < chunk; ++k) {
+            if ((rc = apply_native(op, op->pv, op->ap, 0, 1, skip))) return rc;
+            k_pcg_pap<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->pv, op->ap, op->partials, op->st);
+            k_pcg_update<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->xw, op->r, op->pv, op->ap,
+                                                                   dinv_use, op->z, cheb ? 0 : 1,
+                                                                   op->partials, op->st);
+            if (cheb) {
+                if ((rc = cheb_apply(op, cc, op->r, op->z, skip, &applies))) return rc;
+                k_pcg_rz<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r, op->z, op->partials, op->st, 0);
+            }
+            k_pcg_pupdate<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z, op->pv, op->st, 0);
+            CK(cudaGetLastError());
+        }
+        iters_launched += chunk;
+        if ((rc = read_state(op, &h))) return rc;
+        if (h.done) break;
+    }
+    CK(cudaEventRecord(op->ev1, op->stream));
+    if ((rc = read_state(op, &h))) return rc;
+    // applies actually executed: initial residual (+ initial smoother), one per
+    // iteration started, and the smoother after every update that left the solve running
+    const int km1 = cheb ? cfg.cheb_degree - 1 : 0;
+    const bool stopped_by_update = h.converged || (!h.breakdown && h.iter >= cfg.max_iter);
+    int64_t done_applies = 1;
+    if (!(h.iter == 0 && h.done && !h.breakdown)) done_applies += km1;
+    done_applies += h.iter + (h.breakdown ? 1 : 0);
+    done_applies += (int64_t)km1 * (h.iter - (stopped_by_update ? 1 : 0));
+    // true residual in FP64
+    if ((rc = apply_native(op, op->xw, op->ap, 0, 1, nullptr))) return rc;
+    k_true_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->partials, op->st);
+    CK(cudaGetLastError());
+    if ((rc = from_native(op, x, op->xw, mem))) return rc;
+    SolverState h2;
+    if ((rc = read_state(op, &h2))) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, op->ev0, op->ev1);
+    if ((rc = check_device_error(op))) return rc;
+    int status = h.converged ? FG_OK : (h.breakdown ? FG_BREAKDOWN : FG_CONVERGENCE_FAILED);
+    if (res) {
+        res->converged = h.converged;
+        res->iterations = h.converged ? h.iter : (h.breakdown ? h.iter : cfg.max_iter);
+        res->final_residual = h.res;
+        res->true_residual = h2.tmp[0];
+        res->status = status;
+        res->outer_iterations = 1;
+        res->applies = done_applies;
+        res->lmax = lmax;
+        res->solve_ms = ms;
+    }
+    if (cfg.print_level >= 1)
+        fprintf(stderr, "fg_pcg: %s after %d iterations, residual %.3e (true %.3e)\n",
+                h.converged ? "converged" : "not converged", h.iter, h.res, h2.tmp[0]);
+    if (status == FG_OK) t_last_status = FG_OK;
+    else if (status == FG_BREAKDOWN) fail(status, "CG breakdown: p^T A p is near zero");
+    else fail(status, "solver did not converge in %d iterations (residual = %.3e)", cfg.max_iter, h.res);
+    return status;
+}
+
+}  // extern "C"

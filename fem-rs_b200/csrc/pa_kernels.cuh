@@ -1,0 +1,654 @@
+// pa_kernels.cuh -- partial-assembly (PA) mass / diffusion operator on a
+// structured hex mesh of order P (Q = P+1 Gauss points per direction),
+// hand-written for sm_100a.
+//
+// It computes the same operator as the reference's element loop
+// (crates/assembly/src/partial.rs:85-130 mass, :154-208 diffusion, with the
+// Hex8 isoparametric geometry of crates/assembly/src/assembler.rs:96-143),
+// factored libCEED-style as E^T B^T D B E:
+//   E    gather of the element DOFs from the L-vector (a TMA tile load of x),
+//   B    sum-factorised interpolation / gradient to the quadrature points,
+//   D    the quadrature data: 6 symmetric components w|detJ| kappa J^-1 J^-T
+//        (diffusion) and/or w|detJ| rho (mass), precomputed once,
+//   B^T  the transposed contractions,
+//   E^T  a deterministic scatter with no floating-point atomics.
+//
+// Work decomposition.  A CTA owns an "item": a tile of 32 elements in x
+// (one warp, one element per lane) by WY element rows in y (one warp per row),
+// and sweeps TZ element layers in z.  Each thread keeps its element's
+// contractions in registers.  Contributions of neighbouring elements to the
+// DOFs they share are summed in a fixed order: across x by a warp shuffle,
+// across y through shared memory between the row warps, across z by carrying
+// the top DOF plane of a layer in shared memory into the next layer.  DOFs on
+// the three upper faces of an item that belong to a neighbouring item are
+// written to a per-item face buffer; fixup_kernel then adds them to the owner
+// values in a fixed order.  The result is bit-identical from run to run.
+//
+// Streams into shared memory: the quadrature data of each warp is laid out in
+// HBM in exactly the order the warp consumes it (one contiguous block per
+// element column of quadrature points), and is streamed with 1-D bulk async
+// copies (cp.async.bulk) into an S-deep ring of stages per warp.  The x tile
+// of each layer is a 3-D TMA tensor load (cp.async.bulk.tensor, no multicast)
+// into a double buffer.
+#pragma once
+#include "fg_common.cuh"
+
+namespace fg {
+
+template <int OPK> struct NComp { static constexpr int v = OPK == 1 ? 1 : (OPK == 2 ? 6 : 7); };
+
+// Quadrature-data layout: [item][warp][layer][col=(qy,qx)][qz][comp][lane].
+template <int P, int OPK>
+__host__ __device__ inline int64_t qd_index(const Grid &g, int item, int w, int lz, int col,
+                                            int qz, int comp, int lane) {
+    constexpr int Q = P + 1, NC = NComp<OPK>::v;
+    return (((((int64_t)item * g.WY + w) * g.TZ + lz) * (Q * Q) + col) * Q + qz) * (NC * 32) +
+           comp * 32 + lane;
+}
+template <int P, int OPK>
+__host__ __device__ inline int64_t qd_size(const Grid &g) {
+    constexpr int Q = P + 1, NC = NComp<OPK>::v;
+    return (int64_t)g.n_items() * g.WY * g.TZ * Q * Q * Q * NC * 32;
+}
+
+template <typename T> struct ApplyArgs {
+    Grid g;
+    const T *qd;      // quadrature data (layout above)
+    T *y;             // native-layout output
+    T *face;          // per-item face slots (scratch)
+    int accumulate;   // 1: y += A x, 0: y = A x
+    int *err;         // device error word
+    const int *skip;  // if non-null and *skip != 0 the kernel returns at once
+};
+
+// Shared-memory plan of the apply kernel (bytes).
+template <int P, typename T, int WY, int S, int NC> struct ApplySmem {
+    static constexpr int D = P + 1, Q = P + 1;
+    static constexpr int XW = round_up(32 * P + 1, 16 / (int)sizeof(T));
+    static constexpr int RY = WY * P + 1;
+    static constexpr int XTILE = (P + 1) * RY * XW;               // elements
+    static constexpr int XB = round_up(XTILE * (int)sizeof(T), 128);
+    static constexpr int STAGE = Q * NC * 32;                     // elements
+    static constexpr int QB = STAGE * (int)sizeof(T);
+    static constexpr int off_q = 2 * XB;
+    static constexpr int off_y = off_q + WY * S * QB;
+    static constexpr int off_c = off_y + WY * D * D * 32 * (int)sizeof(T);
+    static constexpr int off_b = round_up(off_c + D * D * WY * 32 * (int)sizeof(T), 8);
+    static constexpr int bytes = off_b + (2 + WY * S) * 8;
+};
+
+// ---------------------------------------------------------------------------
+// Merge of neighbouring element contributions and the scatter.  `out` holds
+// the element result [c][b][a]; after this call every DOF of the item box is
+// either stored into y (owned), or into the face slot of the item (owned by a
+// neighbour item).  `essval(c,b,a)` returns the value written on essential
+// DOFs (x for the constrained apply, 1 for the diagonal).
+// ---------------------------------------------------------------------------
+template <int P, typename T, int WY, class EssVal>
+__device__ __forceinline__ void merge_and_store(T (&out)[P + 1][P + 1][P + 1], const Grid &g,
+                                                T *ybuf, T *carry, int lz, int nl, int tz,
+                                                int warp, int lane, int item, bool valid,
+                                                int lane_last, int w_last, bool fx0, bool fx1,
+                                                bool fy0, bool fy1, bool fz0, bool fz1, T *y,
+                                                T *face, int accumulate, EssVal essval) {
+    constexpr int D = P + 1;
+    constexpr int NT = WY * 32;
+    // x: lane l receives the a=P face of lane l-1 into its a=0 face
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+#pragma unroll
+        for (int b = 0; b < D; ++b) {
+            T v = __shfl_up_sync(0xffffffffu, out[c][b][P], 1);
+            if (lane > 0) out[c][b][0] += v;
+        }
+    // y: row warp w receives the b=P row of warp w-1 into its b=0 row
+    T *yb = ybuf + warp * (D * D * 32);
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+#pragma unroll
+        for (int a = 0; a < D; ++a) yb[(c * D + a) * 32 + lane] = out[c][P][a];
+    __syncthreads();
+    if (warp > 0) {
+        const T *yp = ybuf + (warp - 1) * (D * D * 32);
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+#pragma unroll
+            for (int a = 0; a < D; ++a) out[c][0][a] += yp[(c * D + a) * 32 + lane];
+    }
+    // z: layer lz receives the c=P plane of layer lz-1 into its c=0 plane
+    const int tid = warp * 32 + lane;
+    if (lz > 0) {
+#pragma unroll
+        for (int b = 0; b < D; ++b)
+#pragma unroll
+            for (int a = 0; a < D; ++a) out[0][b][a] += carry[(b * D + a) * NT + tid];
+    }
+    if (lz + 1 < nl) {
+#pragma unroll
+        for (int b = 0; b < D; ++b)
+#pragma unroll
+            for (int a = 0; a < D; ++a) carry[(b * D + a) * NT + tid] = out[P][b][a];
+    }
+    if (!valid) return;
+    const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty;
+    const int I0 = tx * 32 * P, J0 = ty * WY * P, K0 = tz * g.TZ * P;
+    const int ex = tx * 32 + lane, ey = ty * WY + warp, ez = tz * g.TZ + lz;
+    const int SX = 32 * P + 1, SY = WY * P + 1;
+    T *fxp = face + (int64_t)item * g.face_stride();
+    T *fyp = fxp + g.fx();
+    T *fzp = fyp + g.fy();
+    const bool last_layer = (lz == nl - 1);
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+        if (c == P && !last_layer) continue;
+        const int K = K0 + P * lz + c;
+        const bool zhi = (c == P) && (ez != g.nz - 1);
+#pragma unroll
+        for (int b = 0; b < D; ++b) {
+            if (b == P && warp != w_last) continue;
+            const int J = J0 + P * warp + b;
+            const bool yhi = (b == P) && (ey != g.ny - 1);
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                if (a == P && lane != lane_last) continue;
+                const int I = I0 + P * lane + a;
+                const bool xhi = (a == P) && (ex != g.nx - 1);
+                T v = out[c][b][a];
+                if (xhi) {
+                    fxp[(K - K0) * SY + (J - J0)] = v;
+                } else if (yhi) {
+                    fyp[(K - K0) * SX + (I - I0)] = v;
+                } else if (zhi) {
+                    fzp[(J - J0) * SX + (I - I0)] = v;
+                } else {
+                    const bool e = (a == 0 && fx0) || (a == P && fx1) || (b == 0 && fy0) ||
+                                   (b == P && fy1) || (c == 0 && fz0) || (c == P && fz1);
+                    if (e) v = essval(c, b, a);
+                    const int64_t d = g.dof(I, J, K);
+                    y[d] = accumulate ? y[d] + v : v;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The apply kernel.
+// ---------------------------------------------------------------------------
+template <int P, int OPK, typename T, int WY, int S, int MINB>
+__global__ void __launch_bounds__(WY * 32, MINB)
+    pa_apply_kernel(const __grid_constant__ CUtensorMap xmap, const ApplyArgs<T> A) {
+    constexpr int D = P + 1, Q = P + 1, NC = NComp<OPK>::v;
+    constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
+    constexpr int COLS = Q * Q;
+    using SM = ApplySmem<P, T, WY, S, NC>;
+    constexpr int STAGE = SM::STAGE, XW = SM::XW, RY = SM::RY;
+    using TB = Tab<T>;
+
+    if (A.skip && *A.skip) return;
+    const Grid g = A.g;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T *xs = reinterpret_cast<T *>(smem_raw);
+    T *qs = reinterpret_cast<T *>(smem_raw + SM::off_q);
+    T *ybuf = reinterpret_cast<T *>(smem_raw + SM::off_y);
+    T *carry = reinterpret_cast<T *>(smem_raw + SM::off_c);
+    uint64_t *xbar = reinterpret_cast<uint64_t *>(smem_raw + SM::off_b);
+    uint64_t *qbar = xbar + 2;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int item = blockIdx.x;
+    const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty, tz = item / (g.ntx * g.nty);
+    const int nl = min(g.TZ, g.nz - tz * g.TZ);
+    const int ex = tx * 32 + lane, ey = ty * WY + warp;
+    const bool valid = ex < g.nx && ey < g.ny;
+    const int lane_last = min(31, g.nx - 1 - tx * 32);
+    const int w_last = min(WY - 1, g.ny - 1 - ty * WY);
+    const int I0 = tx * 32 * P, J0 = ty * WY * P, K0 = tz * g.TZ * P;
+    const int total_cols = nl * COLS;
+    const T *qdw = A.qd + (int64_t)(item * WY + warp) * g.TZ * COLS * STAGE;
+    T *qsw = qs + warp * S * STAGE;
+    uint64_t *qbw = qbar + warp * S;
+    constexpr uint32_t XBYTES = (uint32_t)(SM::XTILE * sizeof(T));
+    constexpr uint32_t QBYTES = (uint32_t)SM::QB;
+
+    if (threadIdx.x == 0) {
+        prefetch_tmap(&xmap);
+        mbar_init(&xbar[0], 1);
+        mbar_init(&xbar[1], 1);
+        for (int i = 0; i < WY * S; ++i) mbar_init(&qbar[i], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    int x_issued = 0, q_issued = 0;  // thread 0 / lane 0 bookkeeping
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&xbar[0], XBYTES);
+        tma_load_3d(xs, &xmap, I0, J0, K0, &xbar[0]);
+        x_issued = 1;
+    }
+    if (lane == 0) {
+        for (int j = 0; j < S && j < total_cols; ++j) {
+            mbar_arrive_expect_tx(&qbw[j], QBYTES);
+            bulk_g2s(qsw + j * STAGE, qdw + (int64_t)j * STAGE, QBYTES, &qbw[j]);
+            q_issued = j + 1;
+        }
+    }
+    const int ess = g.ess;
+    const bool fx0 = (ess & 16) && ex == 0, fx1 = (ess & 32) && ex == g.nx - 1;
+    const bool fy0 = (ess & 4) && ey == 0, fy1 = (ess & 8) && ey == g.ny - 1;
+    bool ok = true;
+    int x_waited = 0, q_waited = 0;
+
+    for (int lz = 0; lz < nl; ++lz) {
+        const int ez = tz * g.TZ + lz;
+        const bool fz0 = (ess & 1) && ez == 0, fz1 = (ess & 2) && ez == g.nz - 1;
+        const int xb = lz & 1;
+        if (threadIdx.x == 0 && ok && lz + 1 < nl) {
+            // buffer (lz+1)&1 was last read in layer lz-1, before the end-of-layer barrier
+            fence_proxy_async();
+            mbar_arrive_expect_tx(&xbar[(lz + 1) & 1], XBYTES);
+            tma_load_3d(reinterpret_cast<unsigned char *>(xs) + ((lz + 1) & 1) * SM::XB, &xmap, I0,
+                        J0, K0 + (lz + 1) * P, &xbar[(lz + 1) & 1]);
+            x_issued = lz + 2;
+        }
+        if (ok && !mbar_wait(&xbar[xb], (lz >> 1) & 1, A.err)) ok = false;
+        x_waited = lz + 1;
+        const T *xt = reinterpret_cast<const T *>(reinterpret_cast<const unsigned char *>(xs) +
+                                                  xb * SM::XB);
+
+        // ---- gather (E) with essential-DOF masking -------------------------
+        T u[D][D][D];
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+#pragma unroll
+            for (int b = 0; b < D; ++b)
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    const T v = xt[(c * RY + warp * P + b) * XW + lane * P + a];
+                    const bool e = (a == 0 && fx0) || (a == P && fx1) || (b == 0 && fy0) ||
+                                   (b == P && fy1) || (c == 0 && fz0) || (c == P && fz1);
+                    u[c][b][a] = e ? T(0) : v;
+                }
+        // ---- B: contractions in x then y ----------------------------------
+        T C0[D][Q][Q], C1[D][Q][Q], C2[D][Q][Q];  // [c][qy][qx]
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            T A0[D][Q], A1[D][Q];
+#pragma unroll
+            for (int b = 0; b < D; ++b)
+#pragma unroll
+                for (int qx = 0; qx < Q; ++qx) {
+                    T s0 = 0, s1 = 0;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        s0 += TB::B(P, qx, a) * u[c][b][a];
+                        if (HK) s1 += TB::G(P, qx, a) * u[c][b][a];
+                    }
+                    A0[b][qx] = s0;
+                    A1[b][qx] = s1;
+                }
+#pragma unroll
+            for (int qy = 0; qy < Q; ++qy)
+#pragma unroll
+                for (int qx = 0; qx < Q; ++qx) {
+                    T s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+                    for (int b = 0; b < D; ++b) {
+                        s0 += TB::B(P, qy, b) * A0[b][qx];
+                        if (HK) {
+                            s1 += TB::G(P, qy, b) * A0[b][qx];
+                            s2 += TB::B(P, qy, b) * A1[b][qx];
+                        }
+                    }
+                    C0[c][qy][qx] = s0;
+                    C1[c][qy][qx] = s1;
+                    C2[c][qy][qx] = s2;
+                }
+        }
+        // ---- per quadrature column: B in z, D, B^T in z (in place) --------
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy)
+#pragma unroll
+            for (int qx = 0; qx < Q; ++qx) {
+                const int col = qy * Q + qx;
+                const int j = lz * COLS + col;
+                const int s = j % S;
+                if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+                q_waited = j + 1;
+                const T *qc = qsw + s * STAGE;
+                T vx[Q], vy[Q], vz[Q], vu[Q];
+#pragma unroll
+                for (int qz = 0; qz < Q; ++qz) {
+                    T gx = 0, gy = 0, gz = 0, ui = 0;
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        if (HK) {
+                            gx += TB::B(P, qz, c) * C2[c][qy][qx];
+                            gy += TB::B(P, qz, c) * C1[c][qy][qx];
+                            gz += TB::G(P, qz, c) * C0[c][qy][qx];
+                        }
+                        if (HM) ui += TB::B(P, qz, c) * C0[c][qy][qx];
+                    }
+                    const T *qq = qc + qz * (NC * 32) + lane;
+                    if (HK) {
+                        const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128],
+                                d5 = qq[160];
+                        vx[qz] = d0 * gx + d1 * gy + d2 * gz;
+                        vy[qz] = d1 * gx + d3 * gy + d4 * gz;
+                        vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                    }
+                    if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
+                }
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    T e0 = 0, e1 = 0, e2 = 0;
+#pragma unroll
+                    for (int qz = 0; qz < Q; ++qz) {
+                        if (HK) {
+                            e2 += TB::B(P, qz, c) * vx[qz];
+                            e1 += TB::B(P, qz, c) * vy[qz];
+                            e0 += TB::G(P, qz, c) * vz[qz];
+                        }
+                        if (HM) e0 += TB::B(P, qz, c) * vu[qz];
+                    }
+                    C0[c][qy][qx] = e0;
+                    C1[c][qy][qx] = e1;
+                    C2[c][qy][qx] = e2;
+                }
+                __syncwarp();
+                if (lane == 0 && ok && j + S < total_cols) {
+                    fence_proxy_async();
+                    mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                    bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                    q_issued = j + S + 1;
+                }
+            }
+        // ---- B^T: contractions in y then x --------------------------------
+        T out[D][D][D];
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            T F0[D][Q], F1[D][Q];
+#pragma unroll
+            for (int b = 0; b < D; ++b)
+#pragma unroll
+                for (int qx = 0; qx < Q; ++qx) {
+                    T s0 = 0, s1 = 0;
+#pragma unroll
+                    for (int qy = 0; qy < Q; ++qy) {
+                        if (HK) {
+                            s0 += TB::G(P, qy, b) * C1[c][qy][qx];
+                            s1 += TB::B(P, qy, b) * C2[c][qy][qx];
+                        }
+                        s0 += TB::B(P, qy, b) * C0[c][qy][qx];
+                    }
+                    F0[b][qx] = s0;
+                    F1[b][qx] = s1;
+                }
+#pragma unroll
+            for (int b = 0; b < D; ++b)
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    T s = 0;
+#pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+                        s += TB::B(P, qx, a) * F0[b][qx];
+                        if (HK) s += TB::G(P, qx, a) * F1[b][qx];
+                    }
+                    out[c][b][a] = s;
+                }
+        }
+        // ---- E^T: merge + store --------------------------------------------
+        merge_and_store<P, T, WY>(
+            out, g, ybuf, carry, lz, nl, tz, warp, lane, item, valid, lane_last, w_last, fx0, fx1,
+            fy0, fy1, fz0, fz1, A.y, A.face, A.accumulate,
+            [&](int c, int b, int a) { return xt[(c * RY + warp * P + b) * XW + lane * P + a]; });
+        __syncthreads();
+    }
+    // Drain copies still in flight after a timeout (bounded waits).
+    if (!ok) {
+        if (lane == 0)
+            for (int j = q_waited; j < q_issued; ++j)
+                mbar_wait(&qbw[j % S], (j / S) & 1, nullptr, 100000000ull);
+        if (threadIdx.x == 0)
+            for (int j = x_waited; j < x_issued; ++j)
+                mbar_wait(&xbar[j & 1], (j >> 1) & 1, nullptr, 100000000ull);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal of the operator (Jacobi).  Same item decomposition and scatter; the
+// element diagonal sum_q g_i^T D_q g_i (+ m_q phi_i^2) is formed directly from
+// the quadrature data in global memory (a setup-time kernel).
+// ---------------------------------------------------------------------------
+template <int P, int OPK, typename T, int WY>
+__global__ void __launch_bounds__(WY * 32) pa_diag_kernel(const ApplyArgs<T> A) {
+    constexpr int D = P + 1, Q = P + 1, NC = NComp<OPK>::v;
+    constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
+    using TB = Tab<T>;
+    const Grid g = A.g;
+    __shared__ T ybuf[WY * D * D * 32];
+    __shared__ T carry[D * D * WY * 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int item = blockIdx.x;
+    const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty, tz = item / (g.ntx * g.nty);
+    const int nl = min(g.TZ, g.nz - tz * g.TZ);
+    const int ex = tx * 32 + lane, ey = ty * WY + warp;
+    const bool valid = ex < g.nx && ey < g.ny;
+    const int lane_last = min(31, g.nx - 1 - tx * 32);
+    const int w_last = min(WY - 1, g.ny - 1 - ty * WY);
+    const int ess = g.ess;
+    const bool fx0 = (ess & 16) && ex == 0, fx1 = (ess & 32) && ex == g.nx - 1;
+    const bool fy0 = (ess & 4) && ey == 0, fy1 = (ess & 8) && ey == g.ny - 1;
+    for (int lz = 0; lz < nl; ++lz) {
+        const int ez = tz * g.TZ + lz;
+        const bool fz0 = (ess & 1) && ez == 0, fz1 = (ess & 2) && ez == g.nz - 1;
+        T out[D][D][D];
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+#pragma unroll
+            for (int b = 0; b < D; ++b)
+#pragma unroll
+                for (int a = 0; a < D; ++a) out[c][b][a] = 0;
+        for (int qz = 0; qz < Q; ++qz)
+            for (int qy = 0; qy < Q; ++qy)
+#pragma unroll
+                for (int qx = 0; qx < Q; ++qx) {
+                    const T *qq = A.qd + qd_index<P, OPK>(g, item, warp, lz, qy * Q + qx, qz, 0, lane);
+                    T d[7];
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) d[k] = qq[k * 32];
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+#pragma unroll
+                        for (int b = 0; b < D; ++b)
+#pragma unroll
+                            for (int a = 0; a < D; ++a) {
+                                const T Bx = TB::B(P, qx, a), By = TB::B(P, qy, b), Bz = TB::B(P, qz, c);
+                                T s = 0;
+                                if (HK) {
+                                    const T gx = TB::G(P, qx, a) * By * Bz;
+                                    const T gy = Bx * TB::G(P, qy, b) * Bz;
+                                    const T gz = Bx * By * TB::G(P, qz, c);
+                                    s = d[0] * gx * gx + d[3] * gy * gy + d[5] * gz * gz +
+                                        T(2) * (d[1] * gx * gy + d[2] * gx * gz + d[4] * gy * gz);
+                                }
+                                if (HM) {
+                                    const T ph = Bx * By * Bz;
+                                    s += d[HK ? 6 : 0] * ph * ph;
+                                }
+                                out[c][b][a] += s;
+                            }
+                }
+        merge_and_store<P, T, WY>(out, g, ybuf, carry, lz, nl, tz, warp, lane, item, valid,
+                                  lane_last, w_last, fx0, fx1, fy0, fy1, fz0, fz1, A.y, A.face, 0,
+                                  [](int, int, int) { return T(1); });
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fix-up: for every DOF on an item's lower face that a neighbour item also
+// touches, add the neighbours' face-slot partials to the owner's value, in a
+// fixed (dz, dy, dx) order.  One thread per candidate DOF; the three plane
+// families are enumerated once each (x-planes own their DOFs, y-planes skip
+// DOFs on x-planes, z-planes skip DOFs on x- or y-planes).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void fixup_kernel(const Grid g, T *__restrict__ y, const T *__restrict__ face,
+                             const int *skip) {
+    if (skip && *skip) return;
+    const int P = g.p;
+    const int SXe = 32 * P, SYe = g.WY * P, SZe = g.TZ * P;
+    const int64_t nX = (int64_t)(g.ntx - 1) * g.NJ * g.NK;
+    const int64_t nY = (int64_t)(g.nty - 1) * g.NI * g.NK;
+    const int64_t nZ = (int64_t)(g.ntz - 1) * g.NI * g.NJ;
+    const int64_t total = nX + nY + nZ;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        int I, J, K;
+        if (t < nX) {
+            const int64_t per = (int64_t)g.NJ * g.NK;
+            const int k = (int)(t / per) + 1;
+            const int64_t r = t % per;
+            J = (int)(r % g.NJ);
+            K = (int)(r / g.NJ);
+            I = k * SXe;
+        } else if (t < nX + nY) {
+            const int64_t u = t - nX, per = (int64_t)g.NI * g.NK;
+            const int k = (int)(u / per) + 1;
+            const int64_t r = u % per;
+            I = (int)(r % g.NI);
+            K = (int)(r / g.NI);
+            J = k * SYe;
+            if (I > 0 && I % SXe == 0 && I < g.NI - 1) continue;
+        } else {
+            const int64_t u = t - nX - nY, per = (int64_t)g.NI * g.NJ;
+            const int k = (int)(u / per) + 1;
+            const int64_t r = u % per;
+            I = (int)(r % g.NI);
+            J = (int)(r / g.NI);
+            K = k * SZe;
+            if (I > 0 && I % SXe == 0 && I < g.NI - 1) continue;
+            if (J > 0 && J % SYe == 0 && J < g.NJ - 1) continue;
+        }
+        if (g.is_ess(I, J, K)) continue;  // final value written by the owner item
+        const int sx = (I > 0 && I % SXe == 0 && I < g.NI - 1);
+        const int sy = (J > 0 && J % SYe == 0 && J < g.NJ - 1);
+        const int sz = (K > 0 && K % SZe == 0 && K < g.NK - 1);
+        const int tx = min(I / SXe, g.ntx - 1), ty = min(J / SYe, g.nty - 1),
+                  tz = min(K / SZe, g.ntz - 1);
+        const int64_t d = g.dof(I, J, K);
+        T sum = y[d];
+        const int fs = g.face_stride(), fxs = g.fx(), fys = g.fy();
+        for (int dz = 0; dz <= sz; ++dz)
+            for (int dy = 0; dy <= sy; ++dy)
+                for (int dx = 0; dx <= sx; ++dx) {
+                    if (!(dx | dy | dz)) continue;
+                    const int nx_ = tx - dx, ny_ = ty - dy, nz_ = tz - dz;
+                    const int nb = (nz_ * g.nty + ny_) * g.ntx + nx_;
+                    const int I0 = nx_ * SXe, J0 = ny_ * SYe, K0 = nz_ * SZe;
+                    const T *fb = face + (int64_t)nb * fs;
+                    if (dx)
+                        sum += fb[(K - K0) * (SYe + 1) + (J - J0)];
+                    else if (dy)
+                        sum += fb[fxs + (K - K0) * (SXe + 1) + (I - I0)];
+                    else
+                        sum += fb[fxs + fys + (J - J0) * (SXe + 1) + (I - I0)];
+                }
+        y[d] = sum;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Quadrature-data setup: one thread per (element, quadrature point).
+// Trilinear geometry from the 8 element vertices (HexQ1 node order of
+// crates/element/src/lagrange/hex.rs:27-36), J_id = sum_k x_k[i] dphi_k/dxi_d
+// (assembler.rs:96-123), D = w |detJ| kappa c_k J^-1 J^-T, m = w |detJ| rho c_m.
+// ---------------------------------------------------------------------------
+struct SetupArgs {
+    Grid g;
+    const double *vcoord;   // (nx+1)(ny+1)(nz+1)*3 or null (uniform unit cube)
+    const double *kappa_q;  // [E][qz][qy][qx] or null
+    const double *rho_q;
+    double kappa_c, rho_c, c_m, c_k;
+    double gx[4], gw[4];    // Gauss rule for Q = p+1 points
+    int *err;
+};
+
+template <int P, int OPK, typename T>
+__global__ void qdata_setup_kernel(const SetupArgs S, T *__restrict__ qd) {
+    constexpr int Q = P + 1, NC = NComp<OPK>::v;
+    constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
+    const Grid &g = S.g;
+    const int64_t E = (int64_t)g.nx * g.ny * g.nz;
+    const int64_t total = E * Q * Q * Q;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int q = (int)(t % (Q * Q * Q));
+        const int64_t e = t / (Q * Q * Q);
+        const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
+        const int ex = (int)(e % g.nx), ey = (int)((e / g.nx) % g.ny), ez = (int)(e / ((int64_t)g.nx * g.ny));
+        const double xi[3] = {S.gx[qx], S.gx[qy], S.gx[qz]};
+        const double w = S.gw[qx] * S.gw[qy] * S.gw[qz];
+        const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                               {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+        double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int k = 0; k < 8; ++k) {
+            const double sx = off[k][0] ? 1.0 : -1.0, sy = off[k][1] ? 1.0 : -1.0,
+                         sz = off[k][2] ? 1.0 : -1.0;
+            const double fx = 1.0 + sx * xi[0], fy = 1.0 + sy * xi[1], fz = 1.0 + sz * xi[2];
+            const double gr[3] = {0.125 * sx * fy * fz, 0.125 * sy * fx * fz, 0.125 * sz * fx * fy};
+            const int vi = ex + off[k][0], vj = ey + off[k][1], vk = ez + off[k][2];
+            double xv[3];
+            if (S.vcoord) {
+                const int64_t id = ((int64_t)vk * (g.ny + 1) + vj) * (g.nx + 1) + vi;
+                xv[0] = S.vcoord[3 * id];
+                xv[1] = S.vcoord[3 * id + 1];
+                xv[2] = S.vcoord[3 * id + 2];
+            } else {
+                xv[0] = (double)vi / g.nx;
+                xv[1] = (double)vj / g.ny;
+                xv[2] = (double)vk / g.nz;
+            }
+            for (int i = 0; i < 3; ++i)
+                for (int d = 0; d < 3; ++d) J[i][d] += xv[i] * gr[d];
+        }
+        const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                           J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+        if (!(fabs(det) > 0.0)) {
+            if (S.err) atomicOr(S.err, FG_DERR_BOUNDS);
+        }
+        const double wd = w * fabs(det);
+        const int tx = ex / 32, lane = ex % 32, ty = ey / g.WY, wy = ey % g.WY, tz = ez / g.TZ,
+                  lz = ez % g.TZ;
+        const int item = (tz * g.nty + ty) * g.ntx + tx;
+        T *dst = qd + qd_index<P, OPK>(g, item, wy, lz, qy * Q + qx, qz, 0, lane);
+        if (HK) {
+            double inv[3][3];
+            inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+            inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+            inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+            inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+            inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+            inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+            inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+            inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+            inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+            const double kap = S.kappa_q ? S.kappa_q[e * (Q * Q * Q) + q] : S.kappa_c;
+            const double s = wd * kap * S.c_k;
+            const int mi[6] = {0, 0, 0, 1, 1, 2}, ni[6] = {0, 1, 2, 1, 2, 2};
+            for (int k = 0; k < 6; ++k) {
+                const int m = mi[k], n = ni[k];
+                const double v = inv[m][0] * inv[n][0] + inv[m][1] * inv[n][1] + inv[m][2] * inv[n][2];
+                dst[k * 32] = (T)(s * v);
+            }
+        }
+        if (HM) {
+            const double rho = S.rho_q ? S.rho_q[e * (Q * Q * Q) + q] : S.rho_c;
+            dst[(HK ? 6 : 0) * 32] = (T)(wd * rho * S.c_m);
+        }
+        (void)NC;
+    }
+}
+
+}  // namespace fg

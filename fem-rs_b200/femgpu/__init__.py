@@ -1,0 +1,379 @@
+"""femgpu -- Python front end of libfemgpu.so (the sm_100a PA operator + PCG).
+
+Mirrors the fem-rs operator / solver surface on top of the C ABI in
+include/femgpu.h:
+
+  * ``PADiffusionOperator`` / ``PAMassOperator`` / ``PAMassDiffusionOperator``
+    with ``apply`` (y += A x), ``apply_zero`` (y = A x) and ``n_dofs``
+    (crates/assembly/src/partial.rs:45-57, 65-208);
+  * ``SolverConfig`` / ``SolveResult`` / ``SolverError`` and its variants
+    (crates/solver/src/lib.rs:46-142);
+  * ``solve_cg_operator``, ``solve_pcg_jacobi`` and ``solve_pcg_chebyshev``
+    (crates/solver/src/lib.rs:198-297, crates/parallel/src/par_solver.rs:262-342).
+
+There is no CPU fallback: importing works anywhere the shared library exists,
+and every numeric call runs on the GPU or raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libfemgpu.so")
+
+FG_OK, FG_CONVERGENCE_FAILED, FG_DIMENSION_MISMATCH, FG_BREAKDOWN = 0, 1, 2, 3
+FG_UNSUPPORTED, FG_DEVICE_TIMEOUT, FG_BOUNDS, FG_CUDA_ERROR, FG_INVALID_ARGUMENT = 4, 5, 6, 7, 8
+MASS, DIFF, MASS_DIFF = 1, 2, 3
+HOST, DEVICE = 0, 1
+PC_NONE, PC_JACOBI, PC_CHEBYSHEV = 0, 1, 2
+FP64, FP32_IR = 0, 1
+TAG_ALL = 63
+
+# every symbol include/femgpu.h declares
+EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "fg_op_ndofs",
+           "fg_op_layout", "fg_op_native_len", "fg_op_set_stream", "fg_op_apply",
+           "fg_op_apply_native", "fg_op_diagonal", "fg_pcg", "fg_op_check")
+
+
+class FgMesh(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("vcoord", C.c_void_p)]
+
+
+class FgCfg(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_iter", C.c_int32),
+                ("print_level", C.c_int32), ("precond", C.c_int32), ("cheb_degree", C.c_int32),
+                ("precision", C.c_int32), ("power_iters", C.c_int32), ("lmax", C.c_double),
+                ("lmin_ratio", C.c_double), ("lmax_safety", C.c_double), ("inner_rtol", C.c_double),
+                ("check_interval", C.c_int32), ("reserved", C.c_int32)]
+
+
+class FgResult(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("final_residual", C.c_double),
+                ("true_residual", C.c_double), ("status", C.c_int32), ("outer_iterations", C.c_int32),
+                ("applies", C.c_int64), ("lmax", C.c_double), ("solve_ms", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libfemgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libfemgpu.so not built ({LIB_PATH}); run `make -C fem-rs_b200`")
+        L = C.CDLL(LIB_PATH)
+        vp, i, d, i64 = C.c_void_p, C.c_int, C.c_double, C.c_int64
+        L.fg_cfg_default.argtypes = [vp]
+        L.fg_last_error.argtypes = [C.c_char_p, C.c_size_t]
+        L.fg_op_create.argtypes = [vp, i, i, i, d, d, vp, d, vp, d, i, C.POINTER(vp)]
+        L.fg_op_destroy.argtypes = [vp]
+        L.fg_op_destroy.restype = None
+        L.fg_op_ndofs.argtypes = [vp]
+        L.fg_op_ndofs.restype = i64
+        L.fg_op_native_len.argtypes = [vp]
+        L.fg_op_native_len.restype = i64
+        L.fg_op_layout.argtypes = [vp, vp]
+        L.fg_op_set_stream.argtypes = [vp, vp]
+        L.fg_op_apply.argtypes = [vp, vp, vp, i, i, i]
+        L.fg_op_apply_native.argtypes = [vp, vp, vp, i, i]
+        L.fg_op_diagonal.argtypes = [vp, vp, i, i]
+        L.fg_pcg.argtypes = [vp, vp, vp, vp, vp, i]
+        L.fg_op_check.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(512)
+    lib().fg_last_error(buf, 512)
+    return buf.value.decode()
+
+
+# --------------------------------------------------------------------------
+# errors (crates/solver/src/lib.rs:46-54)
+# --------------------------------------------------------------------------
+class SolverError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(msg)
+        self.status = status
+
+
+class ConvergenceFailed(SolverError):
+    pass
+
+
+class DimensionMismatch(SolverError):
+    pass
+
+
+class Breakdown(SolverError):
+    """SolverError::Linger("CG operator breakdown: p^T A p is near zero")."""
+
+
+class DeviceError(SolverError):
+    pass
+
+
+def _check(rc):
+    if rc == FG_OK:
+        return
+    msg = last_error()
+    cls = {FG_CONVERGENCE_FAILED: ConvergenceFailed, FG_DIMENSION_MISMATCH: DimensionMismatch,
+           FG_BREAKDOWN: Breakdown}.get(rc, DeviceError)
+    raise cls(rc, f"femgpu status {rc}: {msg}")
+
+
+# --------------------------------------------------------------------------
+# config / result (crates/solver/src/lib.rs:70-142)
+# --------------------------------------------------------------------------
+@dataclass
+class SolverConfig:
+    rtol: float = 1e-8
+    atol: float = 0.0
+    max_iter: int = 1000
+    verbose: bool = False
+    print_level: int = 0
+    cheb_degree: int = 4
+    power_iters: int = 20
+    lmax: float = 0.0
+    lmin_ratio: float = 30.0
+    lmax_safety: float = 1.1
+    precision: int = FP64
+    inner_rtol: float = 1e-4
+    check_interval: int = 10
+
+    def to_c(self, precond):
+        c = FgCfg()
+        lib().fg_cfg_default(C.byref(c))
+        c.rtol, c.atol, c.max_iter = self.rtol, self.atol, self.max_iter
+        c.print_level = self.print_level or (2 if self.verbose else 0)
+        c.precond, c.cheb_degree, c.precision = precond, self.cheb_degree, self.precision
+        c.power_iters, c.lmax, c.lmin_ratio = self.power_iters, self.lmax, self.lmin_ratio
+        c.lmax_safety, c.inner_rtol, c.check_interval = self.lmax_safety, self.inner_rtol, self.check_interval
+        return c
+
+
+@dataclass
+class SolveResult:
+    converged: bool
+    iterations: int
+    final_residual: float
+    true_residual: float = 0.0
+    applies: int = 0
+    lmax: float = 0.0
+    solve_ms: float = 0.0
+    outer_iterations: int = 1
+    status: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+# --------------------------------------------------------------------------
+# operators
+# --------------------------------------------------------------------------
+def _as_f64(a):
+    """(pointer, mem, keepalive) for a numpy array or a CUDA torch tensor."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise TypeError("expected a C-contiguous float64 array")
+        return a.ctypes.data, HOST
+    mod = type(a).__module__
+    if mod.startswith("torch"):
+        if a.dtype.__repr__() != "torch.float64" or not a.is_contiguous():
+            raise TypeError("expected a contiguous float64 tensor")
+        return a.data_ptr(), (DEVICE if a.is_cuda else HOST)
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+class PAOperator:
+    """Matrix-free PA operator on a structured hex box (sm_100a kernels).
+
+    ``mesh``: (nx, ny, nz) or dict(nx=, ny=, nz=, vcoord=array((nx+1)(ny+1)(nz+1), 3)).
+    ``kappa`` / ``rho``: scalar or per-quadrature-point array [E][qz][qy][qx].
+    ``ess_tags``: Dirichlet boundary tags (bit t-1 = tag t) for the constrained form.
+    """
+
+    def __init__(self, mesh, order, kind=DIFF, kappa=1.0, rho=1.0, c_mass=1.0, c_diff=1.0,
+                 ess_tags=TAG_ALL, quad_order=None):
+        if isinstance(mesh, dict):
+            nx, ny, nz, vc = mesh["nx"], mesh["ny"], mesh["nz"], mesh.get("vcoord")
+        else:
+            (nx, ny, nz), vc = mesh, None
+        self.nx, self.ny, self.nz, self.order, self.kind = int(nx), int(ny), int(nz), int(order), kind
+        nq = order + 1 if quad_order is None else (int(quad_order) + 2) // 2
+        self._vc = None if vc is None else np.ascontiguousarray(vc, dtype=np.float64)
+        m = FgMesh(self.nx, self.ny, self.nz, None if self._vc is None else self._vc.ctypes.data)
+        kq = None if np.isscalar(kappa) else np.ascontiguousarray(kappa, dtype=np.float64)
+        rq = None if np.isscalar(rho) else np.ascontiguousarray(rho, dtype=np.float64)
+        E = self.nx * self.ny * self.nz
+        for arr in (kq, rq):
+            if arr is not None and arr.size != E * nq ** 3:
+                raise DimensionMismatch(FG_DIMENSION_MISMATCH, "coefficient array has wrong size")
+        h = C.c_void_p()
+        rc = lib().fg_op_create(C.byref(m), self.order, nq, kind, float(c_mass), float(c_diff),
+                                None if kq is None else kq.ctypes.data,
+                                float(kappa) if kq is None else 0.0,
+                                None if rq is None else rq.ctypes.data,
+                                float(rho) if rq is None else 0.0, int(ess_tags), C.byref(h))
+        _check(rc)
+        self._h = h
+        dims = (C.c_int64 * 4)()
+        lib().fg_op_layout(self._h, dims)
+        self.NI, self.NJ, self.NK, self.NIp = (int(v) for v in dims)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fg_op_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # MatFreeOperator
+    def n_dofs(self):
+        return int(lib().fg_op_ndofs(self._h))
+
+    @property
+    def native_len(self):
+        return int(lib().fg_op_native_len(self._h))
+
+    def _apply(self, x, y, accumulate, constrained):
+        n = self.n_dofs()
+        if len(x) != n or len(y) != n:
+            raise DimensionMismatch(FG_DIMENSION_MISMATCH, f"operator is {n}x{n}, vectors {len(x)}/{len(y)}")
+        px, mx = _as_f64(x)
+        py, my = _as_f64(y)
+        if mx != my:
+            raise TypeError("x and y must live in the same memory space")
+        _check(lib().fg_op_apply(self._h, px, py, int(accumulate), int(constrained), mx))
+        return y
+
+    def apply(self, x, y, constrained=False):
+        """y += A x (does not zero y first), partial.rs:46-47."""
+        return self._apply(x, y, True, constrained)
+
+    def apply_zero(self, x, y, constrained=False):
+        """y = A x, partial.rs:50-53."""
+        return self._apply(x, y, False, constrained)
+
+    def matvec(self, x, constrained=False):
+        y = np.zeros(self.n_dofs())
+        return self.apply_zero(np.ascontiguousarray(x, dtype=np.float64), y, constrained)
+
+    def apply_native(self, x_ptr, y_ptr, accumulate=False, constrained=True):
+        """Device pointers in the native (padded) layout; asynchronous."""
+        _check(lib().fg_op_apply_native(self._h, x_ptr, y_ptr, int(accumulate), int(constrained)))
+
+    def diagonal(self, constrained=True):
+        d = np.zeros(self.n_dofs())
+        _check(lib().fg_op_diagonal(self._h, d.ctypes.data, int(constrained), HOST))
+        return d
+
+    def check(self):
+        _check(lib().fg_op_check(self._h))
+
+    def set_stream(self, stream_ptr):
+        _check(lib().fg_op_set_stream(self._h, stream_ptr))
+
+    # native layout helpers
+    def to_native(self, v):
+        out = np.zeros((self.NK, self.NJ, self.NIp))
+        out[:, :, :self.NI] = np.asarray(v).reshape(self.NK, self.NJ, self.NI)
+        return out.ravel()
+
+    def from_native(self, v):
+        return np.asarray(v).reshape(self.NK, self.NJ, self.NIp)[:, :, :self.NI].ravel()
+
+    # solver
+    def pcg(self, b, x, cfg: SolverConfig, precond) -> SolveResult:
+        n = self.n_dofs()
+        if len(b) != n or len(x) != n:
+            raise DimensionMismatch(FG_DIMENSION_MISMATCH, f"matrix is {n}x{n}, rhs has length {len(b)}")
+        pb, mb = _as_f64(b)
+        px, mx = _as_f64(x)
+        if mb != mx:
+            raise TypeError("b and x must live in the same memory space")
+        c = cfg.to_c(precond)
+        r = FgResult()
+        rc = lib().fg_pcg(self._h, pb, px, C.byref(c), C.byref(r), mb)
+        res = SolveResult(bool(r.converged), int(r.iterations), float(r.final_residual),
+                          float(r.true_residual), int(r.applies), float(r.lmax), float(r.solve_ms),
+                          int(r.outer_iterations), int(r.status))
+        if rc not in (FG_OK, FG_CONVERGENCE_FAILED):
+            _check(rc)
+        return res
+
+
+class PADiffusionOperator(PAOperator):
+    """PADiffusionOperator::new(space, kappa, quad_order) (partial.rs:138-149)."""
+
+    def __init__(self, mesh, order, kappa=1.0, quad_order=None, ess_tags=TAG_ALL):
+        super().__init__(mesh, order, DIFF, kappa=kappa, quad_order=quad_order, ess_tags=ess_tags)
+
+
+class PAMassOperator(PAOperator):
+    """PAMassOperator::new(space, rho, quad_order) (partial.rs:65-80)."""
+
+    def __init__(self, mesh, order, rho=1.0, quad_order=None, ess_tags=TAG_ALL):
+        super().__init__(mesh, order, MASS, rho=rho, quad_order=quad_order, ess_tags=ess_tags)
+
+
+class PAMassDiffusionOperator(PAOperator):
+    """c_mass M + c_diff K in one apply (the SDIRK stage matrix M + gamma dt K of
+    examples/mfem_ex10_heat_equation.rs:141-156, matrix-free)."""
+
+    def __init__(self, mesh, order, c_mass, c_diff, kappa=1.0, rho=1.0, ess_tags=TAG_ALL):
+        super().__init__(mesh, order, MASS_DIFF, kappa=kappa, rho=rho, c_mass=c_mass,
+                         c_diff=c_diff, ess_tags=ess_tags)
+
+
+# --------------------------------------------------------------------------
+# solver entry points
+# --------------------------------------------------------------------------
+def _finish(res: SolveResult, cfg: SolverConfig, raise_on_fail: bool):
+    if raise_on_fail and not res.converged:
+        if res.status == FG_BREAKDOWN:
+            raise Breakdown(FG_BREAKDOWN, "CG operator breakdown: p^T A p is near zero")
+        raise ConvergenceFailed(FG_CONVERGENCE_FAILED,
+                                f"solver did not converge in {cfg.max_iter} iterations "
+                                f"(residual = {res.final_residual:.3e})")
+    return res
+
+
+def solve_cg_operator(nrows, ncols, op: PAOperator, b, x, cfg=None):
+    """Unpreconditioned CG over the constrained operator (lib.rs:198-278);
+    raises ConvergenceFailed / Breakdown like the reference's Err variants."""
+    cfg = cfg or SolverConfig()
+    if nrows != ncols or len(b) != nrows or len(x) != ncols or op.n_dofs() != nrows:
+        raise DimensionMismatch(FG_DIMENSION_MISMATCH,
+                                f"dimension mismatch: matrix is {nrows}x{ncols}, rhs has length {len(b)}")
+    return _finish(op.pcg(b, x, cfg, PC_NONE), cfg, True)
+
+
+def solve_pcg_jacobi(op: PAOperator, b, x, cfg=None):
+    """PCG + Jacobi (lib.rs:281-297, par_solver.rs:262-342): returns a
+    SolveResult with converged=False instead of raising on non-convergence."""
+    cfg = cfg or SolverConfig()
+    return op.pcg(b, x, cfg, PC_JACOBI)
+
+
+def solve_pcg_chebyshev(op: PAOperator, b, x, cfg=None):
+    """PCG with a Chebyshev(D^-1 A) preconditioner of cfg.cheb_degree sweeps."""
+    cfg = cfg or SolverConfig()
+    return op.pcg(b, x, cfg, PC_CHEBYSHEV)
+
+
+def unit_cube_vertices(nx, ny, nz):
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    return np.stack([i / nx, j / ny, k / nz], axis=-1).reshape(-1, 3).astype(np.float64)

@@ -1,0 +1,179 @@
+/*
+ * femgpu.h -- C ABI of the B200 (sm_100a) partial-assembly operator + PCG
+ * library (libfemgpu.so).  Plain pointers and sizes only.
+ *
+ * This is the drop-in boundary for fem-rs's matrix-free operator path.  Each
+ * entry point names the reference interface it replaces (paths inside the
+ * fem-rs workspace):
+ *
+ *   MatFreeOperator { apply (y += A x), apply_zero (y = A x), n_dofs }
+ *       crates/assembly/src/partial.rs:45-57
+ *   PAMassOperator / PADiffusionOperator ::new + ::apply
+ *       crates/assembly/src/partial.rs:65-130, 138-208
+ *   LinearOperator { nrows, ncols, apply (y = A x) }
+ *       crates/assembly/src/backend.rs:39-46
+ *   CsrMatrix::diagonal (Jacobi)          crates/linalg/src/csr.rs:245-252
+ *   boundary_dofs + apply_dirichlet       crates/space/src/constraints.rs:31-120
+ *   solve_cg_operator                     crates/solver/src/lib.rs:198-278
+ *   solve_pcg_jacobi / par_solve_pcg_jacobi
+ *       crates/solver/src/lib.rs:281-297, crates/parallel/src/par_solver.rs:262-342
+ *   SolverConfig / SolveResult / SolverError
+ *       crates/solver/src/lib.rs:46-142
+ *   chebyshev_smooth / estimate_spectral_radius
+ *       crates/amg/src/lib.rs:53-123 (textbook Chebyshev on D^-1 A instead)
+ *
+ * Meshes are structured hexahedral boxes (nx*ny*nz elements) with trilinear
+ * geometry from arbitrary vertex positions; order p = 1..3 with p+1 Gauss
+ * points per direction (hex_rule(2p+1), crates/element/src/quadrature.rs:405-419).
+ * DOFs are numbered lexicographically on the (nx*p+1)(ny*p+1)(nz*p+1) grid,
+ * I fastest (for p = 1 this is unit_cube_tet's node numbering,
+ * crates/mesh/src/simplex.rs:608-610).
+ *
+ * Thread safety: calls on one handle serialise on the handle's mutex and run
+ * on its CUDA stream; distinct handles are independent.
+ */
+#ifndef FEMGPU_H
+#define FEMGPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define FG_API __attribute__((visibility("default")))
+#else
+#define FG_API
+#endif
+
+/* Status codes; they map 1:1 onto SolverError / FemCeedError variants
+ * (crates/solver/src/lib.rs:46-54, crates/assembly/src/reed/context.rs:305-312). */
+enum fg_status {
+    FG_OK = 0,
+    FG_CONVERGENCE_FAILED = 1, /* SolverError::ConvergenceFailed */
+    FG_DIMENSION_MISMATCH = 2, /* SolverError::DimensionMismatch */
+    FG_BREAKDOWN = 3,          /* SolverError::Linger("...breakdown...") */
+    FG_UNSUPPORTED = 4,        /* ref_elem panic on unsupported element/order */
+    FG_DEVICE_TIMEOUT = 5,     /* a bounded device-side wait ran out */
+    FG_BOUNDS = 6,             /* degenerate element / bad index */
+    FG_CUDA_ERROR = 7,
+    FG_INVALID_ARGUMENT = 8
+};
+
+/* Operator kinds: A = c_mass*M + c_diff*K restricted to the chosen terms. */
+enum fg_kind { FG_MASS = 1, FG_DIFF = 2, FG_MASS_DIFF = 3 };
+
+/* Where the caller's vectors live. */
+enum fg_mem { FG_HOST = 0, FG_DEVICE = 1 };
+
+/* Preconditioners and precisions of fg_pcg. */
+enum fg_precond { FG_PC_NONE = 0, FG_PC_JACOBI = 1, FG_PC_CHEBYSHEV = 2 };
+enum fg_precision { FG_FP64 = 0, FG_FP32_IR = 1 };
+
+/* Boundary tags (simplex.rs:650-679 order): bit t-1 selects tag t. */
+enum fg_tag {
+    FG_TAG_Z0 = 1, FG_TAG_Z1 = 2, FG_TAG_Y0 = 4, FG_TAG_Y1 = 8, FG_TAG_X0 = 16, FG_TAG_X1 = 32,
+    FG_TAG_ALL = 63
+};
+
+typedef struct fg_op fg_op;
+
+typedef struct {
+    int32_t nx, ny, nz;    /* elements per direction */
+    const double *vcoord;  /* host, (nx+1)(ny+1)(nz+1)*3 vertex coordinates,
+                              lexicographic i fastest; NULL = unit cube */
+} fg_mesh;
+
+typedef struct {
+    double rtol;           /* converge when ||r||/||b|| < rtol (default 1e-8) */
+    double atol;           /* ... or ||r|| < atol */
+    int32_t max_iter;      /* default 1000 */
+    int32_t print_level;   /* PrintLevel: 0 silent, 1 summary, 2 iterations */
+    int32_t precond;       /* fg_precond */
+    int32_t cheb_degree;   /* Chebyshev sweeps (first sweep from zero needs no apply) */
+    int32_t precision;     /* fg_precision */
+    int32_t power_iters;   /* power iterations on D^-1 A for lambda_max (default 20) */
+    double lmax;           /* <= 0: estimate; lambda_max = lmax_safety * estimate */
+    double lmin_ratio;     /* lambda_min = lambda_max / lmin_ratio (default 30) */
+    double lmax_safety;    /* default 1.1 */
+    double inner_rtol;     /* FP32_IR: inner relative tolerance (default 1e-4) */
+    int32_t check_interval;/* iterations between host polls of the device flag */
+    int32_t reserved;
+} fg_cfg;
+
+typedef struct {
+    int32_t converged;
+    int32_t iterations;      /* PCG iterations (inner iterations summed for FP32_IR) */
+    double final_residual;   /* ||r||/||b|| of the recurrence residual */
+    double true_residual;    /* ||b - A x||/||b|| recomputed in FP64 at exit */
+    int32_t status;          /* fg_status */
+    int32_t outer_iterations;/* FP32_IR refinement steps */
+    int64_t applies;         /* operator applications */
+    double lmax;             /* Chebyshev upper bound used */
+    double solve_ms;         /* device time of the solve */
+} fg_result;
+
+/* Defaults of SolverConfig::default() (crates/solver/src/lib.rs:116-120). */
+FG_API void fg_cfg_default(fg_cfg *cfg);
+
+/* Build the operator: uploads the mesh, computes the quadrature data
+ * (PAMassOperator::new / PADiffusionOperator::new + the libCEED-style
+ * qdata build of crates/assembly/src/reed/qfunction.rs:155-192 in 3-D).
+ * kappa_q / rho_q: host arrays [E][qz][qy][qx] (E = nx*ny*nz, element index
+ * (ez*ny + ey)*nx + ex) of per-quadrature-point coefficients, or NULL for the
+ * constants.  nq1d must be order+1.  ess_tags: Dirichlet boundary tags used
+ * when a call asks for the constrained operator. */
+FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, double c_mass,
+                        double c_diff, const double *kappa_q, double kappa_const,
+                        const double *rho_q, double rho_const, int ess_tags, fg_op **out);
+FG_API void fg_op_destroy(fg_op *op);
+
+/* MatFreeOperator::n_dofs / LinearOperator::{nrows,ncols}. */
+FG_API int64_t fg_op_ndofs(const fg_op *op);
+
+/* dims = {NI, NJ, NK, NIp}: DOF grid and the native row pitch of device
+ * vectors used by the *_native entry points (pads must hold zeros). */
+FG_API int fg_op_layout(const fg_op *op, int64_t dims[4]);
+FG_API int64_t fg_op_native_len(const fg_op *op);
+
+/* Run on the caller's CUDA stream (cudaStream_t) instead of the handle's own. */
+FG_API int fg_op_set_stream(fg_op *op, void *stream);
+
+/* MatFreeOperator::apply (accumulate = 1: y += A x) and apply_zero
+ * (accumulate = 0: y = A x); LinearOperator::apply is accumulate = 0.
+ * constrained = 1 applies the Dirichlet elimination of the ess_tags DOFs
+ * (rows and columns of essential DOFs replaced by the identity), the form the
+ * solver uses.  x, y: plain lexicographic vectors of n_dofs doubles in host
+ * (mem = FG_HOST) or device (FG_DEVICE) memory.  Synchronous. */
+FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, int constrained,
+                       int mem);
+
+/* Same on device vectors in the native layout (fg_op_layout); asynchronous
+ * on the handle's stream, no host synchronisation. */
+FG_API int fg_op_apply_native(fg_op *op, const double *x, double *y, int accumulate,
+                              int constrained);
+
+/* Diagonal of the (constrained) operator, 1 on essential DOFs (the Jacobi
+ * diagonal CsrMatrix::diagonal gives after apply_dirichlet). */
+FG_API int fg_op_diagonal(fg_op *op, double *d, int constrained, int mem);
+
+/* Preconditioned CG on the constrained operator (solve_pcg_jacobi /
+ * solve_cg_operator semantics): x holds the initial guess on entry and the
+ * solution on exit.  Stopping rule of par_solve_pcg_jacobi, checked every
+ * iteration on the device.  Returns FG_OK, FG_CONVERGENCE_FAILED or
+ * FG_BREAKDOWN (res->status carries the same code). */
+FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg, fg_result *res,
+                  int mem);
+
+/* Synchronise the handle's stream and report device-side errors
+ * (FG_DEVICE_TIMEOUT, FG_BOUNDS). */
+FG_API int fg_op_check(fg_op *op);
+
+/* Message of the last failing call on this thread; returns its status. */
+FG_API int fg_last_error(char *buf, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
