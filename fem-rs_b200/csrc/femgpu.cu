@@ -773,3 +773,105 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free apply.
+//
+// Same kernels as fg_op_apply_native, but the face-slot scratch that the
+// fix-up pass reads comes from a fixed array compiled into this library
+// instead of the handle's own buffer, so the call neither allocates nor
+// depends on allocator state.  The array lives in every GPU context that
+// loads the library until the process exits.
+// ---------------------------------------------------------------------------
+#define FG_NOALLOC_FACE_DOUBLES (4u << 20)  // 4 Mi doubles = 32 MiB
+static __device__ __align__(256) double g_noalloc_face[FG_NOALLOC_FACE_DOUBLES];
+static double *g_noalloc_face_ptr[64];  // device address of g_noalloc_face, per device
+static std::mutex g_noalloc_mu;
+
+// Host code cannot use g_noalloc_face directly (its host-side name is only a
+// stand-in for the symbol); resolve the device address once per device, with
+// that device current.
+static int noalloc_scratch(int dev, double **out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (dev < 0 || dev >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", dev);
+    if (!g_noalloc_face_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_face);
+        if (e != cudaSuccess || !p)
+            return fail(FG_CUDA_ERROR, "cudaGetSymbolAddress(g_noalloc_face) failed: %s",
+                        cudaGetErrorString(e));
+        g_noalloc_face_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_face_ptr[dev];
+    return FG_OK;
+}
+
+template <int P, int OPK>
+static int noalloc_launch_apply_t(fg_op *op, const Grid &g, const double *x, double *y,
+                                  int accumulate, double *face) {
+    using C = KCfg<P>;
+    using SM = ApplySmem<P, double, C::WY, C::S, NComp<OPK>::v>;
+    auto kern = pa_apply_kernel<P, OPK, double, C::WY, C::S, C::MINB>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
+    CUtensorMap tmap;
+    cuuint64_t gdim[3] = {(cuuint64_t)g.NI, (cuuint64_t)g.NJ, (cuuint64_t)g.NK};
+    cuuint64_t gstr[2] = {(cuuint64_t)g.NIp * sizeof(double),
+                          (cuuint64_t)g.NIp * g.NJ * sizeof(double)};
+    cuuint32_t box[3] = {(cuuint32_t)SM::XW, (cuuint32_t)SM::RY, (cuuint32_t)(P + 1)};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult cr = g_encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(x), gdim,
+                           gstr, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
+    ApplyArgs<double> A{g, op->qd, y, face, accumulate, op->d_err, nullptr};
+    kern<<<g.n_items(), C::WY * 32, SM::bytes, op->stream>>>(tmap, A);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+template <int P>
+static int noalloc_launch_apply_p(fg_op *op, const Grid &g, const double *x, double *y,
+                                  int accumulate, double *face) {
+    switch (op->kind) {
+    case FG_MASS: return noalloc_launch_apply_t<P, 1>(op, g, x, y, accumulate, face);
+    case FG_DIFF: return noalloc_launch_apply_t<P, 2>(op, g, x, y, accumulate, face);
+    default: return noalloc_launch_apply_t<P, 3>(op, g, x, y, accumulate, face);
+    }
+}
+
+extern "C" FG_API int fg_op_apply_native_noalloc(fg_op *op, const double *x, double *y,
+                                                 int accumulate, int constrained) {
+    if (!op || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (x == y) return fail(FG_INVALID_ARGUMENT, "x and y must not alias");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    Grid g = op->g;
+    g.ess = constrained ? op->ess_tags : 0;
+    const size_t need = (size_t)g.n_items() * (size_t)g.face_stride();
+    if (need > FG_NOALLOC_FACE_DOUBLES)
+        return fail(FG_INVALID_ARGUMENT,
+                    "fg_op_apply_native_noalloc: this operator needs %zu doubles of face scratch, "
+                    "more than the %u (32 MiB) of the static scratch array; use fg_op_apply_native",
+                    need, (unsigned)FG_NOALLOC_FACE_DOUBLES);
+    double *face = nullptr;
+    int rc = noalloc_scratch(op->device, &face);
+    if (rc) return rc;
+    // Every face slot the fix-up reads is written by the apply kernel earlier in
+    // the same call, so stale contents from a previous call need no clearing.
+    switch (op->p) {
+    case 1: rc = noalloc_launch_apply_p<1>(op, g, x, y, accumulate, face); break;
+    case 2: rc = noalloc_launch_apply_p<2>(op, g, x, y, accumulate, face); break;
+    default: rc = noalloc_launch_apply_p<3>(op, g, x, y, accumulate, face); break;
+    }
+    if (rc) return rc;
+    const int64_t total = (int64_t)(g.ntx - 1) * g.NJ * g.NK + (int64_t)(g.nty - 1) * g.NI * g.NK +
+                          (int64_t)(g.ntz - 1) * g.NI * g.NJ;
+    if (total > 0) {
+        const int threads = 256;
+        const int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 16);
+        fixup_kernel<double><<<blocks, threads, 0, op->stream>>>(g, y, face, nullptr);
+        CK(cudaGetLastError());
+    }
+    return FG_OK;
+}

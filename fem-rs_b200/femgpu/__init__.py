@@ -36,7 +36,8 @@ TAG_ALL = 63
 # every symbol include/femgpu.h declares
 EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "fg_op_ndofs",
            "fg_op_layout", "fg_op_native_len", "fg_op_set_stream", "fg_op_apply",
-           "fg_op_apply_native", "fg_op_diagonal", "fg_pcg", "fg_op_check")
+           "fg_op_apply_native", "fg_op_diagonal", "fg_pcg", "fg_op_check",
+           "fg_op_apply_native_noalloc")
 
 
 class FgMesh(C.Structure):

@@ -154,6 +154,28 @@ FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, in
 FG_API int fg_op_apply_native(fg_op *op, const double *x, double *y, int accumulate,
                               int constrained);
 
+/* fg_op_apply_native_noalloc: fg_op_apply_native without any device memory
+ * management.  This entry point has no counterpart in the reference (fem-rs
+ * has no GPU path); it exists for callers that cannot let a library allocate
+ * device memory: programs whose memory pool or arena already owns the GPU's
+ * memory (a cudaMalloc from here would fail or fragment their budget), and
+ * loops that cannot afford the device-wide synchronisation that cudaMalloc
+ * and cudaFree may imply.  The fix-up pass of the apply needs scratch for the
+ * partial sums on tile faces; here that scratch is a fixed 32 MiB array
+ * (4 Mi doubles) compiled into libfemgpu.so, which every GPU that loads the
+ * library keeps until the process exits.  Operators whose face scratch
+ * (about 0.22 * n_dofs doubles for Q2) exceeds it are rejected with
+ * FG_INVALID_ARGUMENT.  The call allocates and frees nothing.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls whose GPU work overlaps in time (other streams, other handles,
+ * other threads) race on it and give wrong results; calls on one stream are
+ * ordered and safe.  Nothing needs clearing between calls: every slot read is
+ * written earlier in the same call.  Same vectors and semantics as
+ * fg_op_apply_native. */
+FG_API int fg_op_apply_native_noalloc(fg_op *op, const double *x, double *y, int accumulate,
+                                      int constrained);
+
 /* Diagonal of the (constrained) operator, 1 on essential DOFs (the Jacobi
  * diagonal CsrMatrix::diagonal gives after apply_dirichlet). */
 FG_API int fg_op_diagonal(fg_op *op, double *d, int constrained, int mem);
