@@ -268,7 +268,7 @@ def main():
     bytes_canon, bytes_nomap = canonical_bytes(n, p)
     peak, peak_kind = measured_peak()
     achieved = bytes_canon / per_apply_s / 1e9
-    tr = profile_traffic(f"pa_apply_fp64_q{p}_{n}.txt")
+    tr = profile_traffic("pa_apply_fp64_q2_64.txt") if (n, p) == (128, 2) else None
     launches_per_apply = 2 if (op.nx > 32 or op.ny > 4 or op.nz > 1) else 1
 
     # e2e through the public C ABI with pinned host buffers
@@ -304,13 +304,44 @@ def main():
         bb = b.reshape(op.NK, op.NJ, op.NI)
         bb[0], bb[-1], bb[:, 0], bb[:, -1], bb[:, :, 0], bb[:, :, -1] = 0, 0, 0, 0, 0, 0
         mass.close()
-        for name, pc in (("plain_fp64_chebyshev4", femgpu.PC_CHEBYSHEV), ("plain_fp64_jacobi", femgpu.PC_JACOBI)):
+        runs = (("plain_fp64_chebyshev4", femgpu.PC_CHEBYSHEV, femgpu.FP64),
+                ("plain_fp64_jacobi", femgpu.PC_JACOBI, femgpu.FP64),
+                ("fp32_ir_chebyshev4", femgpu.PC_CHEBYSHEV, femgpu.FP32_IR),
+                ("fp32_ir_jacobi", femgpu.PC_JACOBI, femgpu.FP32_IR))
+        x_plain = None
+        for name, pc, prec in runs:
             xs = np.zeros(N)
-            cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4)
+            cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec)
             r = op.pcg(b, xs, cfg, pc)
-            solve[name] = {"iterations": r.iterations, "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual,
+            if x_plain is None:
+                x_plain = xs.copy()
+            solve[name] = {"iterations": r.iterations, "outer_iterations": r.outer_iterations,
+                           "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual,
                            "converged": r.converged, "applies": r.applies,
-                           "lmax": r.lmax if pc == femgpu.PC_CHEBYSHEV else None}
+                           "lmax": r.lmax if pc == femgpu.PC_CHEBYSHEV else None,
+                           "rel_diff_vs_plain_fp64_chebyshev": float(np.linalg.norm(xs - x_plain) / np.linalg.norm(x_plain))}
+        best_plain = min(solve["plain_fp64_chebyshev4"]["solve_s"], solve["plain_fp64_jacobi"]["solve_s"])
+        best_chosen = min(solve["fp32_ir_chebyshev4"]["solve_s"], solve["fp32_ir_jacobi"]["solve_s"])
+        solve["speedup_best_chosen_vs_best_plain"] = best_plain / best_chosen
+
+    # FP32 apply throughput (chosen precision form), same workload
+    x32 = x.float()
+    y32 = torch.zeros_like(x32)
+    for _ in range(3):
+        op.apply_native_f32(x32.data_ptr(), y32.data_ptr())
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(args.steps):
+        op.apply_native_f32(x32.data_ptr(), y32.data_ptr())
+    g1.record(stream)
+    torch.cuda.synchronize()
+    t32 = g0.elapsed_time(g1) / args.steps
+    E = n ** 3
+    bytes32 = 6 * (p + 1) ** 3 * E * 4 + 2 * N * 4
+    fp32_apply = {"ms": t32, "gdof_s": N / (t32 / 1e3) / 1e9, "bytes_per_apply": bytes32,
+                  "achieved_gbs": bytes32 / (t32 / 1e3) / 1e9,
+                  "frac": bytes32 / (t32 / 1e3) / 1e9 / peak}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -342,6 +373,7 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "solve": solve,
+            "fp32_apply": fp32_apply,
         }
         print(json.dumps(out), flush=True)
     op.close()

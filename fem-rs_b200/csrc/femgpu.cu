@@ -163,6 +163,13 @@ struct fg_op {
     double *cres = nullptr, *cd = nullptr, *ct = nullptr;
     double *partials = nullptr;
     SolverState *st = nullptr;
+    // FP32 operator data and inner-solve work vectors (iterative refinement)
+    float *qd32 = nullptr, *face32 = nullptr, *dinv32 = nullptr;
+    float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *ap32 = nullptr, *e32 = nullptr,
+          *b32 = nullptr, *cres32 = nullptr, *cd32 = nullptr, *ct32 = nullptr, *xs32 = nullptr,
+          *ys32 = nullptr;
+    int64_t qsize = 0;
+    SolverState *st32 = nullptr;
     int *d_err = nullptr;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -177,6 +184,11 @@ static void free_op(fg_op *op) {
                       op->xw, op->bw, op->cres, op->cd, op->ct, op->partials};
     for (double *b : bufs)
         if (b) cudaFree(b);
+    float *fb[] = {op->qd32, op->face32, op->dinv32, op->r32, op->z32, op->p32, op->ap32, op->e32,
+                   op->b32, op->cres32, op->cd32, op->ct32, op->xs32, op->ys32};
+    for (float *b : fb)
+        if (b) cudaFree(b);
+    if (op->st32) cudaFree(op->st32);
     if (op->st) cudaFree(op->st);
     if (op->d_err) cudaFree(op->d_err);
     if (op->ev0) cudaEventDestroy(op->ev0);
@@ -185,76 +197,98 @@ static void free_op(fg_op *op) {
     delete op;
 }
 
-static int alloc_vec(double **p, int64_t n) {
-    CK(cudaMalloc(p, sizeof(double) * std::max<int64_t>(n, 1)));
-    CK(cudaMemset(*p, 0, sizeof(double) * std::max<int64_t>(n, 1)));
+template <typename T> static int alloc_vec(T **p, int64_t n) {
+    CK(cudaMalloc(p, sizeof(T) * std::max<int64_t>(n, 1)));
+    CK(cudaMemset(*p, 0, sizeof(T) * std::max<int64_t>(n, 1)));
     return FG_OK;
 }
 
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <int P, int OPK>
-static int launch_apply_t(fg_op *op, const Grid &g, const double *x, double *y, int accumulate,
-                          const int *skip) {
-    using C = KCfg<P>;
-    using SM = ApplySmem<P, double, C::WY, C::S, NComp<OPK>::v>;
+template <int P> struct KCfg32;  // FP32 apply: same tile (WY) as FP64, deeper rings
+template <> struct KCfg32<1> { static constexpr int WY = 4, S = 6, MINB = 4; };
+template <> struct KCfg32<2> { static constexpr int WY = 4, S = 4, MINB = 3; };
+template <> struct KCfg32<3> { static constexpr int WY = 2, S = 3, MINB = 2; };
+template <int P, typename T> struct KC;
+template <int P> struct KC<P, double> : KCfg<P> {};
+template <int P> struct KC<P, float> : KCfg32<P> {};
+
+template <typename T> struct TmapType;
+template <> struct TmapType<double> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT64; };
+template <> struct TmapType<float> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; };
+
+template <int P, int OPK, typename T>
+static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const T *x, T *y,
+                          int accumulate, const int *skip) {
+    using C = KC<P, T>;
+    static_assert(C::WY == KCfg<P>::WY, "FP32 and FP64 share the item tiling");
+    using SM = ApplySmem<P, T, C::WY, C::S, NComp<OPK>::v>;
     static bool attr_set[64] = {};
-    auto kern = pa_apply_kernel<P, OPK, double, C::WY, C::S, C::MINB>;
+    auto kern = pa_apply_kernel<P, OPK, T, C::WY, C::S, C::MINB>;
     if (!attr_set[op->device]) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
         attr_set[op->device] = true;
     }
     CUtensorMap tmap;
     cuuint64_t gdim[3] = {(cuuint64_t)g.NI, (cuuint64_t)g.NJ, (cuuint64_t)g.NK};
-    cuuint64_t gstr[2] = {(cuuint64_t)g.NIp * sizeof(double),
-                          (cuuint64_t)g.NIp * g.NJ * sizeof(double)};
+    cuuint64_t gstr[2] = {(cuuint64_t)g.NIp * sizeof(T), (cuuint64_t)g.NIp * g.NJ * sizeof(T)};
     cuuint32_t box[3] = {(cuuint32_t)SM::XW, (cuuint32_t)SM::RY, (cuuint32_t)(P + 1)};
     cuuint32_t estr[3] = {1, 1, 1};
-    CUresult cr = g_encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(x), gdim,
-                           gstr, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult cr = g_encode(&tmap, TmapType<T>::v, 3, const_cast<T *>(x), gdim, gstr, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
-    ApplyArgs<double> A{g, op->qd, y, op->face, accumulate, op->d_err, skip};
+    ApplyArgs<T> A{g, qd, y, face, accumulate, op->d_err, skip};
     kern<<<g.n_items(), C::WY * 32, SM::bytes, op->stream>>>(tmap, A);
     CK(cudaGetLastError());
     return FG_OK;
 }
 
-template <int P>
-static int launch_apply_p(fg_op *op, const Grid &g, const double *x, double *y, int accumulate,
-                          const int *skip) {
+template <int P, typename T>
+static int launch_apply_p(fg_op *op, const Grid &g, const T *qd, T *face, const T *x, T *y,
+                          int accumulate, const int *skip) {
     switch (op->kind) {
-    case FG_MASS: return launch_apply_t<P, 1>(op, g, x, y, accumulate, skip);
-    case FG_DIFF: return launch_apply_t<P, 2>(op, g, x, y, accumulate, skip);
-    default: return launch_apply_t<P, 3>(op, g, x, y, accumulate, skip);
+    case FG_MASS: return launch_apply_t<P, 1, T>(op, g, qd, face, x, y, accumulate, skip);
+    case FG_DIFF: return launch_apply_t<P, 2, T>(op, g, qd, face, x, y, accumulate, skip);
+    default: return launch_apply_t<P, 3, T>(op, g, qd, face, x, y, accumulate, skip);
     }
 }
 
-static int launch_fixup(fg_op *op, const Grid &g, double *y, const int *skip) {
-    const int64_t total = (int64_t)(g.ntx - 1) * g.NJ * g.NK + (int64_t)(g.nty - 1) * g.NI * g.NK +
-                          (int64_t)(g.ntz - 1) * g.NI * g.NJ;
-    if (total <= 0) return FG_OK;
-    const int threads = 256;
-    const int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 16);
-    fixup_kernel<double><<<blocks, threads, 0, op->stream>>>(g, y, op->face, skip);
+static dim3 fixup_grid(const Grid &g) {
+    const int planes = (g.ntx - 1) + (g.nty - 1) + (g.ntz - 1);
+    const int w = std::max(g.NI, g.NJ), h = std::max(g.NJ, g.NK);
+    return dim3((w + 127) / 128, h, planes);
+}
+
+template <typename T>
+static int launch_fixup(fg_op *op, const Grid &g, T *y, const T *face, const int *skip) {
+    const dim3 grid = fixup_grid(g);
+    if (grid.z == 0) return FG_OK;
+    fixup_kernel<T><<<grid, 128, 0, op->stream>>>(g, y, face, skip);
     CK(cudaGetLastError());
     return FG_OK;
 }
 
-static int apply_native(fg_op *op, const double *x, double *y, int accumulate, int constrained,
-                        const int *skip) {
+// y (+)= A x on native vectors with the given precision's quadrature data.
+template <typename T>
+static int apply_native_t(fg_op *op, const T *qd, T *face, const T *x, T *y, int accumulate,
+                          int constrained, const int *skip) {
     Grid g = op->g;
     g.ess = constrained ? op->ess_tags : 0;
     int rc;
     switch (op->p) {
-    case 1: rc = launch_apply_p<1>(op, g, x, y, accumulate, skip); break;
-    case 2: rc = launch_apply_p<2>(op, g, x, y, accumulate, skip); break;
-    default: rc = launch_apply_p<3>(op, g, x, y, accumulate, skip); break;
+    case 1: rc = launch_apply_p<1, T>(op, g, qd, face, x, y, accumulate, skip); break;
+    case 2: rc = launch_apply_p<2, T>(op, g, qd, face, x, y, accumulate, skip); break;
+    default: rc = launch_apply_p<3, T>(op, g, qd, face, x, y, accumulate, skip); break;
     }
     if (rc) return rc;
-    return launch_fixup(op, g, y, skip);
+    return launch_fixup<T>(op, g, y, face, skip);
+}
+
+static int apply_native(fg_op *op, const double *x, double *y, int accumulate, int constrained,
+                        const int *skip) {
+    return apply_native_t<double>(op, op->qd, op->face, x, y, accumulate, constrained, skip);
 }
 
 template <int P, int OPK> static int launch_diag_t(fg_op *op, const Grid &g, double *y) {
@@ -281,15 +315,15 @@ static int diag_native(fg_op *op, double *y, int constrained) {
     default: rc = launch_diag_p<3>(op, g, y); break;
     }
     if (rc) return rc;
-    return launch_fixup(op, g, y, nullptr);
+    return launch_fixup<double>(op, g, y, op->face, nullptr);
 }
 
-template <int P, int OPK>
-static int launch_setup_t(fg_op *op, SetupArgs &S) {
+template <int P, int OPK, typename T = double>
+static int launch_setup_t(fg_op *op, SetupArgs &S, T *qd = nullptr) {
     const int64_t total = (int64_t)op->g.nx * op->g.ny * op->g.nz * (P + 1) * (P + 1) * (P + 1);
     const int threads = 256;
     const int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 32);
-    qdata_setup_kernel<P, OPK, double><<<blocks, threads, 0, op->stream>>>(S, op->qd);
+    qdata_setup_kernel<P, OPK, T><<<blocks, threads, 0, op->stream>>>(S, qd ? qd : (T *)op->qd);
     CK(cudaGetLastError());
     return FG_OK;
 }
@@ -330,7 +364,7 @@ FG_API void fg_cfg_default(fg_cfg *c) {
     c->lmax = 0.0;
     c->lmin_ratio = 30.0;
     c->lmax_safety = 1.1;
-    c->inner_rtol = 1e-4;
+    c->inner_rtol = 0.1;
     c->check_interval = 10;
 }
 
@@ -451,6 +485,7 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
         default: rc = launch_setup_p<3>(op, S, &qsize); break;
         }
     }
+    op->qsize = qsize;
     if (!rc && cudaStreamSynchronize(op->stream) != cudaSuccess)
         rc = fail(FG_CUDA_ERROR, "qdata setup failed: %s", cudaGetErrorString(cudaGetLastError()));
     cleanup_in();
@@ -554,19 +589,16 @@ FG_API int fg_op_diagonal(fg_op *op, double *d, int constrained, int mem) {
     return check_device_error(op);
 }
 
+}  // extern "C"
+
 // ---------------------------------------------------------------------------
 // PCG
 // ---------------------------------------------------------------------------
-static int ensure_solver_buffers(fg_op *op, bool cheb) {
+static int ensure_solver_buffers(fg_op *op) {
     int rc;
-    double **v[] = {&op->r, &op->z, &op->pv, &op->ap, &op->xw, &op->bw};
+    double **v[] = {&op->r, &op->z, &op->pv, &op->ap, &op->xw, &op->bw, &op->cres, &op->cd, &op->ct};
     for (double **b : v)
         if (!*b && (rc = alloc_vec(b, op->Nn))) return rc;
-    if (cheb) {
-        double **c[] = {&op->cres, &op->cd, &op->ct};
-        for (double **b : c)
-            if (!*b && (rc = alloc_vec(b, op->Nn))) return rc;
-    }
     return FG_OK;
 }
 
@@ -575,19 +607,50 @@ static int ensure_dinv(fg_op *op) {
     int rc;
     if (!op->dinv && (rc = alloc_vec(&op->dinv, op->Nn))) return rc;
     if ((rc = diag_native(op, op->ys, 1))) return rc;
-    k_invert_diag<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->g, op->ys, op->dinv);
+    k_invert_diag<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->g, op->ys, op->dinv);
     CK(cudaGetLastError());
     op->have_dinv = true;
     return FG_OK;
 }
 
-static int read_state(fg_op *op, SolverState *h) {
-    CK(cudaMemcpyAsync(h, op->st, sizeof(SolverState), cudaMemcpyDeviceToHost, op->stream));
+// FP32 copy of the quadrature data (same layout) and the FP32 work vectors.
+static int ensure_fp32(fg_op *op) {
+    int rc;
+    if (!op->qd32) {
+        if ((rc = alloc_vec(&op->qd32, op->qsize))) return rc;
+        k_to_f32<<<VEC_GRID * 4, VEC_THREADS, 0, op->stream>>>(op->qsize, op->qd, op->qd32);
+        CK(cudaGetLastError());
+    }
+    if (!op->face32 && (rc = alloc_vec(&op->face32, (int64_t)op->g.n_items() * op->g.face_stride())))
+        return rc;
+    float **v[] = {&op->r32, &op->z32, &op->p32, &op->ap32, &op->e32, &op->b32, &op->cres32,
+                   &op->cd32, &op->ct32, &op->xs32, &op->ys32};
+    for (float **b : v)
+        if (!*b && (rc = alloc_vec(b, op->Nn))) return rc;
+    if (!op->st32) {
+        CK(cudaMalloc(&op->st32, sizeof(SolverState)));
+        CK(cudaMemset(op->st32, 0, sizeof(SolverState)));
+    }
+    return FG_OK;
+}
+
+static int ensure_dinv32(fg_op *op) {
+    int rc;
+    if (op->dinv32) return FG_OK;
+    if ((rc = ensure_dinv(op))) return rc;
+    if ((rc = alloc_vec(&op->dinv32, op->Nn))) return rc;
+    k_to_f32<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->Nn, op->dinv, op->dinv32);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+static int read_state(fg_op *op, SolverState *h, const SolverState *dev = nullptr) {
+    CK(cudaMemcpyAsync(h, dev ? dev : op->st, sizeof(SolverState), cudaMemcpyDeviceToHost, op->stream));
     CK(cudaStreamSynchronize(op->stream));
     return FG_OK;
 }
 
-// lambda_max(D^-1 A) by power iteration from the hashed start vector
+// lambda_max(D^-1 A) by power iteration from the hashed start vector (FP64)
 static int estimate_lmax(fg_op *op, int iters, double *out) {
     int rc;
     const int64_t n = op->Nn;
@@ -607,7 +670,7 @@ static int estimate_lmax(fg_op *op, int iters, double *out) {
 }
 
 struct ChebCoef {
-    double inv_theta;
+    double inv_theta = 0.0;
     std::vector<double> c1, c2;
 };
 static ChebCoef cheb_coefs(double lmin, double lmax, int k) {
@@ -625,23 +688,142 @@ static ChebCoef cheb_coefs(double lmin, double lmax, int k) {
     return c;
 }
 
+// Buffers of one PCG run in storage precision T.
+template <typename T> struct PcgBufs {
+    const T *qd;
+    T *face;
+    const T *dinv;
+    T *x, *b, *r, *z, *p, *ap, *cres, *cd, *ct;
+    SolverState *st;
+};
+
 // z = Chebyshev(D^-1 A) r (Saad Alg. 12.1, zero start, k sweeps)
-static int cheb_apply(fg_op *op, const ChebCoef &cc, const double *r, double *z, const int *skip,
-                      int64_t *applies) {
+template <typename T>
+static int cheb_apply(fg_op *op, const PcgBufs<T> &B, const ChebCoef &cc, const T *r, T *z,
+                      const int *skip) {
     const int64_t n = op->Nn;
-    const SolverState *sst = skip ? op->st : nullptr;
-    k_cheb_first<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, r, op->dinv, op->cres, op->cd, z,
-                                                           cc.inv_theta, sst);
+    const SolverState *sst = skip ? B.st : nullptr;
+    k_cheb_first<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, r, B.dinv, B.cres, B.cd, z,
+                                                              cc.inv_theta, sst);
     CK(cudaGetLastError());
     for (size_t s = 0; s < cc.c1.size(); ++s) {
-        int rc = apply_native(op, op->cd, op->ct, 0, 1, skip);
+        int rc = apply_native_t<T>(op, B.qd, B.face, B.cd, B.ct, 0, 1, skip);
         if (rc) return rc;
-        ++*applies;
-        k_cheb_step<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->ct, op->dinv, op->cres, op->cd,
-                                                              z, cc.c1[s], cc.c2[s], sst);
+        k_cheb_step<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.ct, B.dinv, B.cres, B.cd, z,
+                                                                 cc.c1[s], cc.c2[s], sst);
         CK(cudaGetLastError());
     }
     return FG_OK;
+}
+
+// PCG on the constrained operator in storage precision T (reductions in FP64),
+// par_solver.rs:262-342 semantics.  The state (rtol, atol, max_iter) must be
+// loaded into B.st before the call.  x_zero: the initial guess is zero (the
+// first residual needs no apply).  Returns the final host copy of the state.
+template <typename T>
+static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebCoef *cc,
+                   int max_iter, int check_interval, bool x_zero, SolverState *h,
+                   int64_t *applies) {
+    int rc;
+    const int64_t n = op->Nn;
+    const int *skip = &B.st->done;
+    const bool cheb = cc != nullptr;
+    if (x_zero) {
+        CK(cudaMemsetAsync(B.ap, 0, sizeof(T) * n, op->stream));
+    } else {
+        if ((rc = apply_native_t<T>(op, B.qd, B.face, B.x, B.ap, 0, 1, nullptr))) return rc;
+        ++*applies;
+    }
+    k_pcg_init<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.b, B.ap, B.dinv, B.r, B.z, B.p,
+                                                            jacobi_like ? 1 : 0, op->partials, B.st);
+    CK(cudaGetLastError());
+    if (cheb) {
+        if ((rc = cheb_apply<T>(op, B, *cc, B.r, B.z, skip))) return rc;
+        k_pcg_rz<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.r, B.z, op->partials, B.st, 1);
+        k_pcg_pupdate<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.p, B.st, 1);
+        CK(cudaGetLastError());
+    }
+    int launched = 0;
+    while (launched < max_iter) {
+        const int chunk = std::min(check_interval, max_iter - launched);
+        for (int k = 0; k < chunk; ++k) {
+            if ((rc = apply_native_t<T>(op, B.qd, B.face, B.p, B.ap, 0, 1, skip))) return rc;
+            k_pcg_pap<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.ap, op->partials, B.st);
+            k_pcg_update<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(
+                n, B.x, B.r, B.p, B.ap, B.dinv, B.z, cheb ? 0 : 1, op->partials, B.st);
+            if (cheb) {
+                if ((rc = cheb_apply<T>(op, B, *cc, B.r, B.z, skip))) return rc;
+                k_pcg_rz<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.r, B.z, op->partials, B.st, 0);
+            }
+            k_pcg_pupdate<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.p, B.st, 0);
+            CK(cudaGetLastError());
+        }
+        launched += chunk;
+        if ((rc = read_state(op, h, B.st))) return rc;
+        if (h->done) break;
+    }
+    if ((rc = read_state(op, h, B.st))) return rc;
+    // applies actually executed: one per iteration started, the smoother after the
+    // initial residual and after every update that left the solve running
+    const int km1 = cheb ? (int)cc->c1.size() : 0;
+    const bool stopped_by_update = h->converged || (!h->breakdown && h->iter >= max_iter);
+    if (!(h->iter == 0 && h->done && !h->breakdown)) *applies += km1;
+    *applies += h->iter + (h->breakdown ? 1 : 0);
+    *applies += (int64_t)km1 * (h->iter - (stopped_by_update ? 1 : 0));
+    return FG_OK;
+}
+
+static void set_state(fg_op *op, SolverState *dst, double rtol, double atol, int max_iter) {
+    SolverState h{};
+    h.rtol = rtol;
+    h.atol = atol;
+    h.max_iter = max_iter;
+    cudaMemcpyAsync(dst, &h, sizeof h, cudaMemcpyHostToDevice, op->stream);
+}
+
+extern "C" {
+
+static int to_native32(fg_op *op, float *dst, const float *src, int mem) {
+    const Grid &g = op->g;
+    CK(cudaMemcpy2DAsync(dst, sizeof(float) * g.NIp, src, sizeof(float) * g.NI, sizeof(float) * g.NI,
+                         (size_t)g.NJ * g.NK,
+                         mem == FG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, op->stream));
+    return FG_OK;
+}
+static int from_native32(fg_op *op, float *dst, const float *src, int mem) {
+    const Grid &g = op->g;
+    CK(cudaMemcpy2DAsync(dst, sizeof(float) * g.NI, src, sizeof(float) * g.NIp, sizeof(float) * g.NI,
+                         (size_t)g.NJ * g.NK,
+                         mem == FG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, op->stream));
+    return FG_OK;
+}
+
+FG_API int fg_op_apply_f32(fg_op *op, const float *x, float *y, int accumulate, int constrained,
+                           int mem) {
+    if (!op || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    int rc;
+    if ((rc = ensure_fp32(op))) return rc;
+    if ((rc = to_native32(op, op->xs32, x, mem))) return rc;
+    if (accumulate && (rc = to_native32(op, op->ys32, y, mem))) return rc;
+    if ((rc = apply_native_t<float>(op, op->qd32, op->face32, op->xs32, op->ys32, accumulate,
+                                    constrained, nullptr)))
+        return rc;
+    if ((rc = from_native32(op, y, op->ys32, mem))) return rc;
+    return check_device_error(op);
+}
+
+FG_API int fg_op_apply_native_f32(fg_op *op, const float *x, float *y, int accumulate,
+                                  int constrained) {
+    if (!op || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (x == y) return fail(FG_INVALID_ARGUMENT, "x and y must not alias");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    int rc;
+    if ((rc = ensure_fp32(op))) return rc;
+    return apply_native_t<float>(op, op->qd32, op->face32, x, y, accumulate, constrained, nullptr);
 }
 
 FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, fg_result *res,
@@ -650,7 +832,8 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
     fg_cfg cfg;
     if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
     if (cfg.max_iter < 0) return fail(FG_INVALID_ARGUMENT, "max_iter < 0");
-    if (cfg.precision != FG_FP64) return fail(FG_UNSUPPORTED, "precision %d not available", cfg.precision);
+    if (cfg.precision != FG_FP64 && cfg.precision != FG_FP32_IR)
+        return fail(FG_UNSUPPORTED, "precision %d not available", cfg.precision);
     if (cfg.precond < 0 || cfg.precond > 2) return fail(FG_INVALID_ARGUMENT, "bad precond");
     if (cfg.precond == FG_PC_CHEBYSHEV && cfg.cheb_degree < 1)
         return fail(FG_INVALID_ARGUMENT, "cheb_degree must be >= 1");
@@ -658,14 +841,15 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
     std::lock_guard<std::mutex> lk(op->mu);
     CK(cudaSetDevice(op->device));
     const bool cheb = cfg.precond == FG_PC_CHEBYSHEV;
+    const bool ir = cfg.precision == FG_FP32_IR;
     int rc;
-    if ((rc = ensure_solver_buffers(op, true))) return rc;
-    double *dinv_use = op->dinv;
+    if ((rc = ensure_solver_buffers(op))) return rc;
+    const double *dinv_use = op->dinv;
     if (cfg.precond == FG_PC_NONE) {
         // operator CG: z = r, i.e. Jacobi with an identity diagonal (pads zero)
         if (!op->ones) {
             if ((rc = alloc_vec(&op->ones, op->Nn))) return rc;
-            k_invert_diag<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->g, op->ones, op->ones);
+            k_invert_diag<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->g, op->ones, op->ones);
             CK(cudaGetLastError());
         }
         dinv_use = op->ones;
@@ -675,7 +859,6 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
         dinv_use = op->dinv;
     }
     double lmax = 0.0, lmin = 0.0;
-    int64_t applies = 0;
     if (cheb) {
         if (cfg.lmax > 0) {
             lmax = cfg.lmax;
@@ -691,56 +874,94 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
     }
     const ChebCoef cc = cheb ? cheb_coefs(lmin, lmax, cfg.cheb_degree) : ChebCoef{};
     if ((rc = to_native(op, op->bw, b, mem)) || (rc = to_native(op, op->xw, x, mem))) return rc;
-    SolverState h{};
-    h.rtol = cfg.rtol;
-    h.atol = cfg.atol;
-    h.max_iter = cfg.max_iter;
-    CK(cudaMemcpyAsync(op->st, &h, sizeof h, cudaMemcpyHostToDevice, op->stream));
-    CK(cudaEventRecord(op->ev0, op->stream));
     const int64_t n = op->Nn;
-    const int *skip = &op->st->done;
-    // r0 = b - A x0
-    if ((rc = apply_native(op, op->xw, op->ap, 0, 1, nullptr))) return rc;
-    ++applies;
-    k_pcg_init<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, dinv_use, op->r, op->z,
-                                                         op->pv, cheb ? 0 : 1, op->partials, op->st);
-    CK(cudaGetLastError());
-    if (cheb) {
-        if ((rc = cheb_apply(op, cc, op->r, op->z, skip, &applies))) return rc;
-        k_pcg_rz<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r, op->z, op->partials, op->st, 1);
-        k_pcg_pupdate<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z, op->pv, op->st, 1);
-        CK(cudaGetLastError());
-    }
-    int iters_launched = 0;
-    while (iters_launched < cfg.max_iter) {
-        const int chunk = std::min(cfg.check_interval, cfg.max_iter - iters_launched);
-        for (int k = 0; k < chunk; ++k) {
-            if ((rc = apply_native(op, op->pv, op->ap, 0, 1, skip))) return rc;
-            k_pcg_pap<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->pv, op->ap, op->partials, op->st);
-            k_pcg_update<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->xw, op->r, op->pv, op->ap,
-                                                                   dinv_use, op->z, cheb ? 0 : 1,
-                                                                   op->partials, op->st);
-            if (cheb) {
-                if ((rc = cheb_apply(op, cc, op->r, op->z, skip, &applies))) return rc;
-                k_pcg_rz<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r, op->z, op->partials, op->st, 0);
-            }
-            k_pcg_pupdate<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z, op->pv, op->st, 0);
-            CK(cudaGetLastError());
+    int64_t applies = 0;
+    SolverState h{};
+    int outer = 1, inner_total = 0, status = FG_OK;
+    CK(cudaEventRecord(op->ev0, op->stream));
+    if (!ir) {
+        PcgBufs<double> B{op->qd, op->face, dinv_use, op->xw, op->bw, op->r, op->z, op->pv,
+                          op->ap, op->cres, op->cd, op->ct, op->st};
+        set_state(op, op->st, cfg.rtol, cfg.atol, cfg.max_iter);
+        if ((rc = pcg_run<double>(op, B, !cheb, cheb ? &cc : nullptr, cfg.max_iter,
+                                  cfg.check_interval, false, &h, &applies)))
+            return rc;
+        inner_total = h.iter;
+        status = h.converged ? FG_OK : (h.breakdown ? FG_BREAKDOWN : FG_CONVERGENCE_FAILED);
+    } else {
+        // Mixed-precision PCG with reliable updates: FP32 applies, smoother and
+        // iterates; FP64 solution, true residual and dot products.
+        if ((rc = ensure_fp32(op))) return rc;
+        const float *dinv32 = nullptr;
+        if (cfg.precond == FG_PC_NONE) {
+            if (!op->dinv32 && (rc = alloc_vec(&op->dinv32, op->Nn))) return rc;
+            k_to_f32<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->ones, op->dinv32);
+            dinv32 = op->dinv32;
+        } else {
+            if ((rc = ensure_dinv32(op))) return rc;
+            dinv32 = op->dinv32;
         }
-        iters_launched += chunk;
+        PcgBufs<float> B{op->qd32, op->face32, dinv32, op->e32, nullptr, op->r32, op->z32, op->p32,
+                         op->ap32, op->cres32, op->cd32, op->ct32, op->st};
+        SolverState h0{};
+        h0.rtol = cfg.rtol;
+        h0.atol = cfg.atol;
+        h0.max_iter = cfg.max_iter;
+        h0.delta = (cfg.inner_rtol > 0 && cfg.inner_rtol < 1) ? cfg.inner_rtol : 0.1;
+        CK(cudaMemcpyAsync(op->st, &h0, sizeof h0, cudaMemcpyHostToDevice, op->stream));
+        CK(cudaMemsetAsync(op->e32, 0, sizeof(float) * n, op->stream));
+        const int *done = &op->st->done;
+        const int *skip_rel = &op->st->skip_rel;
+        // r = b - A x (FP64), r_lo = r
+        if ((rc = apply_native(op, op->xw, op->ap, 0, 1, nullptr))) return rc;
+        ++applies;
+        k_rel_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->r32,
+                                                                 op->partials, op->st, 1);
+        // z = M r_lo ; p = z ; rz
+        auto precond = [&](int init) -> int {
+            if (cheb) {
+                int rc2 = cheb_apply<float>(op, B, cc, op->r32, op->z32, done);
+                if (rc2) return rc2;
+                k_pcg_rz<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r32, op->z32,
+                                                                          op->partials, op->st, init);
+            } else {
+                k_jacobi_rz<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r32, dinv32, op->z32,
+                                                                             op->partials, op->st, init);
+            }
+            k_pcg_pupdate<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z32, op->p32, op->st, init);
+            CK(cudaGetLastError());
+            return FG_OK;
+        };
+        if ((rc = precond(1))) return rc;
+        int launched = 0;
+        while (launched < cfg.max_iter) {
+            const int chunk = std::min(cfg.check_interval, cfg.max_iter - launched);
+            for (int k = 0; k < chunk; ++k) {
+                if ((rc = apply_native_t<float>(op, op->qd32, op->face32, op->p32, op->ap32, 0, 1, done)))
+                    return rc;
+                k_pcg_pap<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->p32, op->ap32,
+                                                                           op->partials, op->st);
+                k_rel_step<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->e32, op->r32, op->p32,
+                                                                     op->ap32, op->partials, op->st);
+                // reliable update (kernels return at once unless triggered)
+                k_rel_xupdate<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->xw, op->e32, op->st);
+                if ((rc = apply_native(op, op->xw, op->ap, 0, 1, skip_rel))) return rc;
+                k_rel_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->r32,
+                                                                         op->partials, op->st, 0);
+                if ((rc = precond(0))) return rc;
+            }
+            launched += chunk;
+            if ((rc = read_state(op, &h))) return rc;
+            if (h.done) break;
+        }
         if ((rc = read_state(op, &h))) return rc;
-        if (h.done) break;
+        inner_total = h.iter;
+        outer = (int)h.tmp[1];  // reliable (FP64 residual-replacing) updates
+        status = h.converged ? FG_OK : (h.breakdown ? FG_BREAKDOWN : FG_CONVERGENCE_FAILED);
+        const int km1 = cheb ? (int)cc.c1.size() : 0;
+        applies += (int64_t)h.iter * (1 + km1) + km1;
     }
     CK(cudaEventRecord(op->ev1, op->stream));
-    if ((rc = read_state(op, &h))) return rc;
-    // applies actually executed: initial residual (+ initial smoother), one per
-    // iteration started, and the smoother after every update that left the solve running
-    const int km1 = cheb ? cfg.cheb_degree - 1 : 0;
-    const bool stopped_by_update = h.converged || (!h.breakdown && h.iter >= cfg.max_iter);
-    int64_t done_applies = 1;
-    if (!(h.iter == 0 && h.done && !h.breakdown)) done_applies += km1;
-    done_applies += h.iter + (h.breakdown ? 1 : 0);
-    done_applies += (int64_t)km1 * (h.iter - (stopped_by_update ? 1 : 0));
     // true residual in FP64
     if ((rc = apply_native(op, op->xw, op->ap, 0, 1, nullptr))) return rc;
     k_true_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->partials, op->st);
@@ -751,21 +972,21 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
     float ms = 0.f;
     cudaEventElapsedTime(&ms, op->ev0, op->ev1);
     if ((rc = check_device_error(op))) return rc;
-    int status = h.converged ? FG_OK : (h.breakdown ? FG_BREAKDOWN : FG_CONVERGENCE_FAILED);
+    const bool conv = status == FG_OK;
     if (res) {
-        res->converged = h.converged;
-        res->iterations = h.converged ? h.iter : (h.breakdown ? h.iter : cfg.max_iter);
-        res->final_residual = h.res;
+        res->converged = conv;
+        res->iterations = conv ? inner_total : (status == FG_BREAKDOWN ? inner_total : cfg.max_iter);
+        res->final_residual = ir ? h.res : h.res;
         res->true_residual = h2.tmp[0];
         res->status = status;
-        res->outer_iterations = 1;
-        res->applies = done_applies;
+        res->outer_iterations = outer;
+        res->applies = applies;
         res->lmax = lmax;
         res->solve_ms = ms;
     }
     if (cfg.print_level >= 1)
-        fprintf(stderr, "fg_pcg: %s after %d iterations, residual %.3e (true %.3e)\n",
-                h.converged ? "converged" : "not converged", h.iter, h.res, h2.tmp[0]);
+        fprintf(stderr, "fg_pcg: %s after %d iterations (%d outer), residual %.3e (true %.3e)\n",
+                conv ? "converged" : "not converged", inner_total, outer, h.res, h2.tmp[0]);
     if (status == FG_OK) t_last_status = FG_OK;
     else if (status == FG_BREAKDOWN) fail(status, "CG breakdown: p^T A p is near zero");
     else fail(status, "solver did not converge in %d iterations (residual = %.3e)", cfg.max_iter, h.res);
@@ -865,12 +1086,9 @@ extern "C" FG_API int fg_op_apply_native_noalloc(fg_op *op, const double *x, dou
     default: rc = noalloc_launch_apply_p<3>(op, g, x, y, accumulate, face); break;
     }
     if (rc) return rc;
-    const int64_t total = (int64_t)(g.ntx - 1) * g.NJ * g.NK + (int64_t)(g.nty - 1) * g.NI * g.NK +
-                          (int64_t)(g.ntz - 1) * g.NI * g.NJ;
-    if (total > 0) {
-        const int threads = 256;
-        const int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 16);
-        fixup_kernel<double><<<blocks, threads, 0, op->stream>>>(g, y, face, nullptr);
+    const dim3 grid = fixup_grid(g);
+    if (grid.z > 0) {
+        fixup_kernel<double><<<grid, 128, 0, op->stream>>>(g, y, face, nullptr);
         CK(cudaGetLastError());
     }
     return FG_OK;

@@ -488,74 +488,66 @@ __global__ void __launch_bounds__(WY * 32) pa_diag_kernel(const ApplyArgs<T> A) 
 // ---------------------------------------------------------------------------
 // Fix-up: for every DOF on an item's lower face that a neighbour item also
 // touches, add the neighbours' face-slot partials to the owner's value, in a
-// fixed (dz, dy, dx) order.  One thread per candidate DOF; the three plane
-// families are enumerated once each (x-planes own their DOFs, y-planes skip
-// DOFs on x-planes, z-planes skip DOFs on x- or y-planes).
+// fixed (dz, dy, dx) order.  Grid: x = position along a DOF row, y = the row
+// (K for x/y planes, J for z planes), z = plane (x planes first, then y, then
+// z).  x planes own all their DOFs, y planes skip DOFs on x planes, z planes
+// skip DOFs on x or y planes.  32-bit index arithmetic throughout.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void fixup_kernel(const Grid g, T *__restrict__ y, const T *__restrict__ face,
-                             const int *skip) {
+__device__ __forceinline__ T fixup_sum(const Grid &g, int I, int J, int K, T own,
+                                       const T *__restrict__ face) {
+    const int P = g.p;
+    const int SXe = 32 * P, SYe = g.WY * P, SZe = g.TZ * P;
+    const int sx = (I > 0 && I < g.NI - 1 && I % SXe == 0);
+    const int sy = (J > 0 && J < g.NJ - 1 && J % SYe == 0);
+    const int sz = (K > 0 && K < g.NK - 1 && K % SZe == 0);
+    const int tx = min(I / SXe, g.ntx - 1), ty = min(J / SYe, g.nty - 1), tz = min(K / SZe, g.ntz - 1);
+    const int fs = g.face_stride(), fxs = g.fx(), fys = g.fy();
+    T sum = own;
+    for (int dz = 0; dz <= sz; ++dz)
+        for (int dy = 0; dy <= sy; ++dy)
+            for (int dx = 0; dx <= sx; ++dx) {
+                if (!(dx | dy | dz)) continue;
+                const int nx_ = tx - dx, ny_ = ty - dy, nz_ = tz - dz;
+                const int nb = (nz_ * g.nty + ny_) * g.ntx + nx_;
+                const int I0 = nx_ * SXe, J0 = ny_ * SYe, K0 = nz_ * SZe;
+                const T *fb = face + (int64_t)nb * fs;
+                if (dx)
+                    sum += fb[(K - K0) * (SYe + 1) + (J - J0)];
+                else if (dy)
+                    sum += fb[fxs + (K - K0) * (SXe + 1) + (I - I0)];
+                else
+                    sum += fb[fxs + fys + (J - J0) * (SXe + 1) + (I - I0)];
+            }
+    return sum;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) fixup_kernel(const Grid g, T *__restrict__ y,
+                                                    const T *__restrict__ face, const int *skip) {
     if (skip && *skip) return;
     const int P = g.p;
     const int SXe = 32 * P, SYe = g.WY * P, SZe = g.TZ * P;
-    const int64_t nX = (int64_t)(g.ntx - 1) * g.NJ * g.NK;
-    const int64_t nY = (int64_t)(g.nty - 1) * g.NI * g.NK;
-    const int64_t nZ = (int64_t)(g.ntz - 1) * g.NI * g.NJ;
-    const int64_t total = nX + nY + nZ;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        int I, J, K;
-        if (t < nX) {
-            const int64_t per = (int64_t)g.NJ * g.NK;
-            const int k = (int)(t / per) + 1;
-            const int64_t r = t % per;
-            J = (int)(r % g.NJ);
-            K = (int)(r / g.NJ);
-            I = k * SXe;
-        } else if (t < nX + nY) {
-            const int64_t u = t - nX, per = (int64_t)g.NI * g.NK;
-            const int k = (int)(u / per) + 1;
-            const int64_t r = u % per;
-            I = (int)(r % g.NI);
-            K = (int)(r / g.NI);
-            J = k * SYe;
-            if (I > 0 && I % SXe == 0 && I < g.NI - 1) continue;
-        } else {
-            const int64_t u = t - nX - nY, per = (int64_t)g.NI * g.NJ;
-            const int k = (int)(u / per) + 1;
-            const int64_t r = u % per;
-            I = (int)(r % g.NI);
-            J = (int)(r / g.NI);
-            K = k * SZe;
-            if (I > 0 && I % SXe == 0 && I < g.NI - 1) continue;
-            if (J > 0 && J % SYe == 0 && J < g.NJ - 1) continue;
-        }
-        if (g.is_ess(I, J, K)) continue;  // final value written by the owner item
-        const int sx = (I > 0 && I % SXe == 0 && I < g.NI - 1);
-        const int sy = (J > 0 && J % SYe == 0 && J < g.NJ - 1);
-        const int sz = (K > 0 && K % SZe == 0 && K < g.NK - 1);
-        const int tx = min(I / SXe, g.ntx - 1), ty = min(J / SYe, g.nty - 1),
-                  tz = min(K / SZe, g.ntz - 1);
-        const int64_t d = g.dof(I, J, K);
-        T sum = y[d];
-        const int fs = g.face_stride(), fxs = g.fx(), fys = g.fy();
-        for (int dz = 0; dz <= sz; ++dz)
-            for (int dy = 0; dy <= sy; ++dy)
-                for (int dx = 0; dx <= sx; ++dx) {
-                    if (!(dx | dy | dz)) continue;
-                    const int nx_ = tx - dx, ny_ = ty - dy, nz_ = tz - dz;
-                    const int nb = (nz_ * g.nty + ny_) * g.ntx + nx_;
-                    const int I0 = nx_ * SXe, J0 = ny_ * SYe, K0 = nz_ * SZe;
-                    const T *fb = face + (int64_t)nb * fs;
-                    if (dx)
-                        sum += fb[(K - K0) * (SYe + 1) + (J - J0)];
-                    else if (dy)
-                        sum += fb[fxs + (K - K0) * (SXe + 1) + (I - I0)];
-                    else
-                        sum += fb[fxs + fys + (J - J0) * (SXe + 1) + (I - I0)];
-                }
-        y[d] = sum;
+    const int pl = blockIdx.z;
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = blockIdx.y;
+    int I, J, K;
+    if (pl < g.ntx - 1) {            // x plane I = (pl+1) SXe: u -> J, row -> K
+        if (u >= g.NJ || row >= g.NK) return;
+        I = (pl + 1) * SXe; J = u; K = row;
+    } else if (pl < g.ntx - 1 + g.nty - 1) {  // y plane: u -> I, row -> K
+        if (u >= g.NI || row >= g.NK) return;
+        I = u; J = (pl - (g.ntx - 1) + 1) * SYe; K = row;
+        if (I > 0 && I < g.NI - 1 && I % SXe == 0) return;
+    } else {                          // z plane: u -> I, row -> J
+        if (u >= g.NI || row >= g.NJ) return;
+        I = u; J = row; K = (pl - (g.ntx - 1) - (g.nty - 1) + 1) * SZe;
+        if (I > 0 && I < g.NI - 1 && I % SXe == 0) return;
+        if (J > 0 && J < g.NJ - 1 && J % SYe == 0) return;
     }
+    if (g.is_ess(I, J, K)) return;  // final value written by the owner item
+    const int64_t d = g.dof(I, J, K);
+    y[d] = fixup_sum<T>(g, I, J, K, y[d], face);
 }
 
 // ---------------------------------------------------------------------------

@@ -21,7 +21,9 @@ struct SolverState {
     double rtol, atol;
     double rho;                // power iteration: ||w||
     double tmp[4];
+    double maxr, delta;        // reliable updates: residual norm at the last update, trigger ratio
     int iter, done, converged, breakdown, max_iter;
+    int trigger, skip_rel;     // reliable update pending / its kernels skip
     unsigned int ticket;
 };
 
@@ -87,22 +89,23 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double *partials, Solv
     for (int64_t i = (int64_t)blockIdx.x * VEC_THREADS + threadIdx.x; i < (n); i += (int64_t)gridDim.x * VEC_THREADS)
 
 // r = b - ap; z = dinv r (jacobi) ; p = z ; rz = r.z ; bb = b.b
-__global__ void __launch_bounds__(VEC_THREADS) k_pcg_init(int64_t n, const double *__restrict__ b,
-                                                          const double *__restrict__ ap,
-                                                          const double *__restrict__ dinv,
-                                                          double *__restrict__ r, double *__restrict__ z,
-                                                          double *__restrict__ p, int jacobi,
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_pcg_init(int64_t n, const T *__restrict__ b,
+                                                          const T *__restrict__ ap,
+                                                          const T *__restrict__ dinv,
+                                                          T *__restrict__ r, T *__restrict__ z,
+                                                          T *__restrict__ p, int jacobi,
                                                           double *partials, SolverState *st) {
     double v[2] = {0.0, 0.0};
     FG_VEC_LOOP(i, n) {
-        const double ri = b[i] - ap[i];
+        const T ri = b[i] - ap[i];
         r[i] = ri;
-        v[1] += b[i] * b[i];
+        v[1] += (double)b[i] * (double)b[i];
         if (jacobi) {
-            const double zi = dinv[i] * ri;
+            const T zi = dinv[i] * ri;
             z[i] = zi;
             p[i] = zi;
-            v[0] += ri * zi;
+            v[0] += (double)ri * (double)zi;
         }
     }
     double tot[2];
@@ -123,12 +126,13 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_init(int64_t n, const doubl
 }
 
 // pap = p.ap ; alpha = rz / pap  (breakdown if |pap| < 1e-30)
-__global__ void __launch_bounds__(VEC_THREADS) k_pcg_pap(int64_t n, const double *__restrict__ p,
-                                                         const double *__restrict__ ap,
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_pcg_pap(int64_t n, const T *__restrict__ p,
+                                                         const T *__restrict__ ap,
                                                          double *partials, SolverState *st) {
     if (st->done) return;
     double v[1] = {0.0};
-    FG_VEC_LOOP(i, n) v[0] += p[i] * ap[i];
+    FG_VEC_LOOP(i, n) v[0] += (double)p[i] * (double)ap[i];
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {
         st->pap = tot[0];
@@ -142,25 +146,26 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_pap(int64_t n, const double
 }
 
 // x += alpha p ; r -= alpha ap ; [jacobi: z = dinv r, rz_new] ; rr ; convergence
-__global__ void __launch_bounds__(VEC_THREADS) k_pcg_update(int64_t n, double *__restrict__ x,
-                                                            double *__restrict__ r,
-                                                            const double *__restrict__ p,
-                                                            const double *__restrict__ ap,
-                                                            const double *__restrict__ dinv,
-                                                            double *__restrict__ z, int jacobi,
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_pcg_update(int64_t n, T *__restrict__ x,
+                                                            T *__restrict__ r,
+                                                            const T *__restrict__ p,
+                                                            const T *__restrict__ ap,
+                                                            const T *__restrict__ dinv,
+                                                            T *__restrict__ z, int jacobi,
                                                             double *partials, SolverState *st) {
     if (st->done) return;
-    const double alpha = st->alpha;
+    const T alpha = (T)st->alpha;
     double v[2] = {0.0, 0.0};
     FG_VEC_LOOP(i, n) {
         x[i] += alpha * p[i];
-        const double ri = r[i] - alpha * ap[i];
+        const T ri = r[i] - alpha * ap[i];
         r[i] = ri;
-        v[0] += ri * ri;
+        v[0] += (double)ri * (double)ri;
         if (jacobi) {
-            const double zi = dinv[i] * ri;
+            const T zi = dinv[i] * ri;
             z[i] = zi;
-            v[1] += ri * zi;
+            v[1] += (double)ri * (double)zi;
         }
     }
     double tot[2];
@@ -182,12 +187,13 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_update(int64_t n, double *_
 }
 
 // rz_new = r.z ; beta = rz_new / rz ; rz = rz_new   (non-Jacobi preconditioners)
-__global__ void __launch_bounds__(VEC_THREADS) k_pcg_rz(int64_t n, const double *__restrict__ r,
-                                                        const double *__restrict__ z,
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_pcg_rz(int64_t n, const T *__restrict__ r,
+                                                        const T *__restrict__ z,
                                                         double *partials, SolverState *st, int init) {
     if (st->done) return;
     double v[1] = {0.0};
-    FG_VEC_LOOP(i, n) v[0] += r[i] * z[i];
+    FG_VEC_LOOP(i, n) v[0] += (double)r[i] * (double)z[i];
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {
         if (!init) st->beta = tot[0] / st->rz;
@@ -196,43 +202,46 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_rz(int64_t n, const double 
 }
 
 // p = z + beta p   (init: p = z)
-__global__ void __launch_bounds__(VEC_THREADS) k_pcg_pupdate(int64_t n, const double *__restrict__ z,
-                                                             double *__restrict__ p,
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_pcg_pupdate(int64_t n, const T *__restrict__ z,
+                                                             T *__restrict__ p,
                                                              const SolverState *st, int init) {
     if (st->done) return;
-    const double beta = init ? 0.0 : st->beta;
+    const T beta = init ? T(0) : (T)st->beta;
     FG_VEC_LOOP(i, n) p[i] = z[i] + beta * p[i];
 }
 
 // Chebyshev sweep 1 from zero: res = dinv r ; d = res / theta ; z = d
-__global__ void __launch_bounds__(VEC_THREADS) k_cheb_first(int64_t n, const double *__restrict__ r,
-                                                            const double *__restrict__ dinv,
-                                                            double *__restrict__ res,
-                                                            double *__restrict__ d,
-                                                            double *__restrict__ z, double inv_theta,
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_cheb_first(int64_t n, const T *__restrict__ r,
+                                                            const T *__restrict__ dinv,
+                                                            T *__restrict__ res,
+                                                            T *__restrict__ d,
+                                                            T *__restrict__ z, double inv_theta,
                                                             const SolverState *st) {
     if (st && st->done) return;
     FG_VEC_LOOP(i, n) {
-        const double s = dinv[i] * r[i];
+        const T s = dinv[i] * r[i];
         res[i] = s;
-        const double di = s * inv_theta;
+        const T di = s * (T)inv_theta;
         d[i] = di;
         z[i] = di;
     }
 }
 
 // Chebyshev sweep: res -= dinv t ; d = c1 d + c2 res ; z += d
-__global__ void __launch_bounds__(VEC_THREADS) k_cheb_step(int64_t n, const double *__restrict__ t,
-                                                           const double *__restrict__ dinv,
-                                                           double *__restrict__ res,
-                                                           double *__restrict__ d,
-                                                           double *__restrict__ z, double c1,
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_cheb_step(int64_t n, const T *__restrict__ t,
+                                                           const T *__restrict__ dinv,
+                                                           T *__restrict__ res,
+                                                           T *__restrict__ d,
+                                                           T *__restrict__ z, double c1,
                                                            double c2, const SolverState *st) {
     if (st && st->done) return;
     FG_VEC_LOOP(i, n) {
-        const double s = res[i] - dinv[i] * t[i];
+        const T s = res[i] - dinv[i] * t[i];
         res[i] = s;
-        const double di = c1 * d[i] + c2 * s;
+        const T di = (T)c1 * d[i] + (T)c2 * s;
         d[i] = di;
         z[i] += di;
     }
@@ -303,13 +312,179 @@ __global__ void __launch_bounds__(VEC_THREADS) k_dinv_norm(int64_t n, double *__
 }
 
 // dinv = 1/d if |d| > 1e-30 else 1 on real DOFs (par_solver.rs:271-274); pads 0
+template <typename T>
 __global__ void __launch_bounds__(VEC_THREADS) k_invert_diag(const Grid g, const double *__restrict__ d,
-                                                             double *__restrict__ dinv) {
+                                                             T *__restrict__ dinv) {
     const int64_t n = (int64_t)g.NIp * g.NJ * g.NK;
     FG_VEC_LOOP(i, n) {
         const int I = (int)(i % g.NIp);
         const double di = d[i];
-        dinv[i] = (I < g.NI) ? (fabs(di) > 1e-30 ? 1.0 / di : 1.0) : 0.0;
+        dinv[i] = (T)((I < g.NI) ? (fabs(di) > 1e-30 ? 1.0 / di : 1.0) : 0.0);
+    }
+}
+
+// ---- FP64 iterative refinement around an FP32 inner solve ----------------
+
+// r = b - ap (FP64); st->rr = ||r||^2, st->res = ||r|| / bnorm; on the first
+// call (init) also st->bnorm = ||b||.  Sets done/converged against rtol/atol.
+__global__ void __launch_bounds__(VEC_THREADS) k_ir_residual(int64_t n, const double *__restrict__ b,
+                                                             const double *__restrict__ ap,
+                                                             double *__restrict__ r, double *partials,
+                                                             SolverState *st, int init) {
+    double v[2] = {0.0, 0.0};
+    FG_VEC_LOOP(i, n) {
+        const double ri = b[i] - ap[i];
+        r[i] = ri;
+        v[0] += ri * ri;
+        if (init) v[1] += b[i] * b[i];
+    }
+    double tot[2];
+    if (grid_sum<2>(v, partials, st, tot) && threadIdx.x == 0) {
+        if (init) {
+            st->bb = tot[1];
+            st->bnorm = sqrt(tot[1]);
+            st->iter = 0;
+            st->converged = 0;
+            st->breakdown = 0;
+            st->done = 0;
+        }
+        st->rr = tot[0];
+        const double rn = sqrt(tot[0]);
+        st->res = st->bnorm > 0.0 ? rn / st->bnorm : 0.0;
+        if (st->bnorm < 1e-30 || st->res < st->rtol || rn < st->atol) {
+            st->converged = 1;
+            st->done = 1;
+        }
+    }
+}
+
+// r32 = r / ||r|| (the inner solve sees a unit right-hand side)
+__global__ void __launch_bounds__(VEC_THREADS) k_ir_to_f32(int64_t n, const double *__restrict__ r,
+                                                           float *__restrict__ r32,
+                                                           const SolverState *st) {
+    const double s = st->rr > 0.0 ? 1.0 / sqrt(st->rr) : 0.0;
+    FG_VEC_LOOP(i, n) r32[i] = (float)(r[i] * s);
+}
+
+// x += ||r|| * e   (FP64 solution update)
+__global__ void __launch_bounds__(VEC_THREADS) k_ir_update(int64_t n, double *__restrict__ x,
+                                                           const float *__restrict__ e,
+                                                           const SolverState *st) {
+    const double s = sqrt(st->rr);
+    FG_VEC_LOOP(i, n) x[i] += s * (double)e[i];
+}
+
+// FP32 copy of an FP64 vector
+__global__ void __launch_bounds__(VEC_THREADS) k_to_f32(int64_t n, const double *__restrict__ a,
+                                                        float *__restrict__ b) {
+    FG_VEC_LOOP(i, n) b[i] = (float)a[i];
+}
+
+// ---- mixed-precision PCG with reliable updates -----------------------------
+// FP32 iterates (x_lo: correction since the last update, r_lo, p, z), FP64
+// solution x and FP64 dot products.  When ||r_lo|| has dropped by `delta`
+// since the last update (or meets rtol, or max_iter is reached) the update is
+// "reliable": x += x_lo, x_lo = 0, r_lo = b - A x recomputed in FP64.  The
+// search direction p is kept, so the Krylov space is not thrown away.
+
+// x_lo += alpha p ; r_lo -= alpha ap ; rr ; sets trigger
+__global__ void __launch_bounds__(VEC_THREADS) k_rel_step(int64_t n, float *__restrict__ xlo,
+                                                          float *__restrict__ r,
+                                                          const float *__restrict__ p,
+                                                          const float *__restrict__ ap,
+                                                          double *partials, SolverState *st) {
+    if (st->done) return;
+    const float alpha = (float)st->alpha;
+    double v[1] = {0.0};
+    FG_VEC_LOOP(i, n) {
+        xlo[i] += alpha * p[i];
+        const float ri = r[i] - alpha * ap[i];
+        r[i] = ri;
+        v[0] += (double)ri * (double)ri;
+    }
+    double tot[1];
+    if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {
+        st->iter += 1;
+        st->rr = tot[0];
+        const double rn = sqrt(tot[0]);
+        const int trig = (rn < st->delta * st->maxr) || (rn / st->bnorm < st->rtol) ||
+                         (rn < st->atol) || (st->iter >= st->max_iter);
+        st->trigger = trig;
+        st->skip_rel = !trig;
+    }
+}
+
+// reliable update, part 1: x += x_lo ; x_lo = 0
+__global__ void __launch_bounds__(VEC_THREADS) k_rel_xupdate(int64_t n, double *__restrict__ x,
+                                                             float *__restrict__ xlo,
+                                                             const SolverState *st) {
+    if (!st->trigger) return;
+    FG_VEC_LOOP(i, n) {
+        x[i] += (double)xlo[i];
+        xlo[i] = 0.0f;
+    }
+}
+
+// reliable update, part 2 (after ap = A x in FP64): r_lo = b - ap ; true residual
+// check; on init also bnorm.  init also runs when trigger is clear.
+__global__ void __launch_bounds__(VEC_THREADS) k_rel_residual(int64_t n, const double *__restrict__ b,
+                                                              const double *__restrict__ ap,
+                                                              float *__restrict__ r,
+                                                              double *partials, SolverState *st,
+                                                              int init) {
+    if (!init && !st->trigger) return;
+    double v[2] = {0.0, 0.0};
+    FG_VEC_LOOP(i, n) {
+        const double ri = b[i] - ap[i];
+        r[i] = (float)ri;
+        v[0] += ri * ri;
+        if (init) v[1] += b[i] * b[i];
+    }
+    double tot[2];
+    if (grid_sum<2>(v, partials, st, tot) && threadIdx.x == 0) {
+        if (init) {
+            st->bb = tot[1];
+            st->bnorm = sqrt(tot[1]);
+            st->iter = 0;
+            st->converged = 0;
+            st->breakdown = 0;
+            st->done = 0;
+            st->tmp[1] = 0.0;
+        } else {
+            st->tmp[1] += 1.0;  // reliable updates done
+        }
+        const double rn = sqrt(tot[0]);
+        st->rr = tot[0];
+        st->maxr = rn;
+        st->res = st->bnorm > 0.0 ? rn / st->bnorm : 0.0;
+        st->trigger = 0;
+        st->skip_rel = 1;
+        if (st->bnorm < 1e-30 || st->res < st->rtol || rn < st->atol) {
+            st->converged = 1;
+            st->done = 1;
+        } else if (st->iter >= st->max_iter) {
+            st->done = 1;
+        }
+    }
+}
+
+// z = dinv r ; rz_new = r.z ; beta (init: rz only)
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_jacobi_rz(int64_t n, const T *__restrict__ r,
+                                                           const T *__restrict__ dinv,
+                                                           T *__restrict__ z, double *partials,
+                                                           SolverState *st, int init) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    FG_VEC_LOOP(i, n) {
+        const T zi = dinv[i] * r[i];
+        z[i] = zi;
+        v[0] += (double)r[i] * (double)zi;
+    }
+    double tot[1];
+    if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {
+        if (!init) st->beta = tot[0] / st->rz;
+        st->rz = tot[0];
     }
 }
 

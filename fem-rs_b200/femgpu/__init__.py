@@ -37,7 +37,7 @@ TAG_ALL = 63
 EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "fg_op_ndofs",
            "fg_op_layout", "fg_op_native_len", "fg_op_set_stream", "fg_op_apply",
            "fg_op_apply_native", "fg_op_diagonal", "fg_pcg", "fg_op_check",
-           "fg_op_apply_native_noalloc")
+           "fg_op_apply_native_noalloc", "fg_op_apply_f32", "fg_op_apply_native_f32")
 
 
 class FgMesh(C.Structure):
@@ -85,6 +85,8 @@ def lib():
         L.fg_op_diagonal.argtypes = [vp, vp, i, i]
         L.fg_pcg.argtypes = [vp, vp, vp, vp, vp, i]
         L.fg_op_check.argtypes = [vp]
+        L.fg_op_apply_f32.argtypes = [vp, vp, vp, i, i, i]
+        L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
 
@@ -145,7 +147,7 @@ class SolverConfig:
     lmin_ratio: float = 30.0
     lmax_safety: float = 1.1
     precision: int = FP64
-    inner_rtol: float = 1e-4
+    inner_rtol: float = 0.1
     check_interval: int = 10
 
     def to_c(self, precond):
@@ -275,6 +277,10 @@ class PAOperator:
     def apply_native(self, x_ptr, y_ptr, accumulate=False, constrained=True):
         """Device pointers in the native (padded) layout; asynchronous."""
         _check(lib().fg_op_apply_native(self._h, x_ptr, y_ptr, int(accumulate), int(constrained)))
+
+    def apply_native_f32(self, x_ptr, y_ptr, accumulate=False, constrained=True):
+        """FP32 apply on float32 device vectors in the native layout; asynchronous."""
+        _check(lib().fg_op_apply_native_f32(self._h, x_ptr, y_ptr, int(accumulate), int(constrained)))
 
     def diagonal(self, constrained=True):
         d = np.zeros(self.n_dofs())

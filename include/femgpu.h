@@ -97,18 +97,19 @@ typedef struct {
     double lmax;           /* <= 0: estimate; lambda_max = lmax_safety * estimate */
     double lmin_ratio;     /* lambda_min = lambda_max / lmin_ratio (default 30) */
     double lmax_safety;    /* default 1.1 */
-    double inner_rtol;     /* FP32_IR: inner relative tolerance (default 1e-4) */
+    double inner_rtol;     /* FP32_IR: FP32 residual reduction between FP64 reliable
+                              updates (default 0.1) */
     int32_t check_interval;/* iterations between host polls of the device flag */
     int32_t reserved;
 } fg_cfg;
 
 typedef struct {
     int32_t converged;
-    int32_t iterations;      /* PCG iterations (inner iterations summed for FP32_IR) */
+    int32_t iterations;      /* PCG iterations */
     double final_residual;   /* ||r||/||b|| of the recurrence residual */
     double true_residual;    /* ||b - A x||/||b|| recomputed in FP64 at exit */
     int32_t status;          /* fg_status */
-    int32_t outer_iterations;/* FP32_IR refinement steps */
+    int32_t outer_iterations;/* FP32_IR: FP64 reliable updates of x and the residual */
     int64_t applies;         /* operator applications */
     double lmax;             /* Chebyshev upper bound used */
     double solve_ms;         /* device time of the solve */
@@ -153,6 +154,15 @@ FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, in
  * on the handle's stream, no host synchronisation. */
 FG_API int fg_op_apply_native(fg_op *op, const double *x, double *y, int accumulate,
                               int constrained);
+
+/* FP32 form of the apply (the chosen precision form of the iterative
+ * refinement): quadrature data rounded to FP32 once, FP32 vectors, FP32
+ * arithmetic.  Same layouts and semantics as fg_op_apply / fg_op_apply_native
+ * (MatFreeOperator::apply / apply_zero, crates/assembly/src/partial.rs:45-57). */
+FG_API int fg_op_apply_f32(fg_op *op, const float *x, float *y, int accumulate, int constrained,
+                           int mem);
+FG_API int fg_op_apply_native_f32(fg_op *op, const float *x, float *y, int accumulate,
+                                  int constrained);
 
 /* fg_op_apply_native_noalloc: fg_op_apply_native without any device memory
  * management.  This entry point has no counterpart in the reference (fem-rs
