@@ -309,39 +309,66 @@ def main():
                 ("fp32_ir_chebyshev4", femgpu.PC_CHEBYSHEV, femgpu.FP32_IR),
                 ("fp32_ir_jacobi", femgpu.PC_JACOBI, femgpu.FP32_IR))
         x_plain = None
-        for name, pc, prec in runs:
-            xs = np.zeros(N)
-            cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec)
-            r = op.pcg(b, xs, cfg, pc)
-            if x_plain is None:
-                x_plain = xs.copy()
-            solve[name] = {"iterations": r.iterations, "outer_iterations": r.outer_iterations,
-                           "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual,
-                           "converged": r.converged, "applies": r.applies,
-                           "lmax": r.lmax if pc == femgpu.PC_CHEBYSHEV else None,
-                           "rel_diff_vs_plain_fp64_chebyshev": float(np.linalg.norm(xs - x_plain) / np.linalg.norm(x_plain))}
-        best_plain = min(solve["plain_fp64_chebyshev4"]["solve_s"], solve["plain_fp64_jacobi"]["solve_s"])
-        best_chosen = min(solve["fp32_ir_chebyshev4"]["solve_s"], solve["fp32_ir_jacobi"]["solve_s"])
-        solve["speedup_best_chosen_vs_best_plain"] = best_plain / best_chosen
+        for fmt, suffix in ((femgpu.QDATA_FULL, ""), (femgpu.QDATA_AFFINE, "_affine")):
+            op.set_qdata_format(fmt)
+            for name, pc, prec in runs:
+                xs = np.zeros(N)
+                cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec)
+                r = op.pcg(b, xs, cfg, pc)
+                if x_plain is None:
+                    x_plain = xs.copy()
+                solve[name + suffix] = {
+                    "iterations": r.iterations, "reliable_updates": r.outer_iterations if prec else 0,
+                    "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual, "converged": r.converged,
+                    "applies": r.applies, "lmax": r.lmax if pc == femgpu.PC_CHEBYSHEV else None,
+                    "rel_err_vs_plain_fp64_chebyshev": float(np.linalg.norm(xs - x_plain) / np.linalg.norm(x_plain))}
+        op.set_qdata_format(femgpu.QDATA_FULL)
 
-    # FP32 apply throughput (chosen precision form), same workload
+        def best(keys):
+            return min(solve[k]["solve_s"] for k in keys)
+        plain = best(["plain_fp64_chebyshev4", "plain_fp64_jacobi"])
+        solve["speedup"] = {
+            "fp32_vs_plain_same_full_qdata": plain / best(["fp32_ir_chebyshev4", "fp32_ir_jacobi"]),
+            "fp32_affine_vs_plain_full_qdata": plain / best(["fp32_ir_chebyshev4_affine", "fp32_ir_jacobi_affine"]),
+            "fp32_affine_vs_plain_affine": best(["plain_fp64_chebyshev4_affine", "plain_fp64_jacobi_affine"])
+            / best(["fp32_ir_chebyshev4_affine", "fp32_ir_jacobi_affine"]),
+            "note": "plain = drop-in FP64 PCG with the full (general-geometry) quadrature data; "
+                    "_affine = compressed qdata valid for constant-J elements, reported as such"}
+
+    # FP32 apply throughput (chosen precision form) and the affine-compressed
+    # format, same workload
     x32 = x.float()
     y32 = torch.zeros_like(x32)
-    for _ in range(3):
-        op.apply_native_f32(x32.data_ptr(), y32.data_ptr())
-    torch.cuda.synchronize()
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    for _ in range(args.steps):
-        op.apply_native_f32(x32.data_ptr(), y32.data_ptr())
-    g1.record(stream)
-    torch.cuda.synchronize()
-    t32 = g0.elapsed_time(g1) / args.steps
+
+    def time_apply(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        return g0.elapsed_time(g1) / args.steps
+
     E = n ** 3
-    bytes32 = 6 * (p + 1) ** 3 * E * 4 + 2 * N * 4
-    fp32_apply = {"ms": t32, "gdof_s": N / (t32 / 1e3) / 1e9, "bytes_per_apply": bytes32,
-                  "achieved_gbs": bytes32 / (t32 / 1e3) / 1e9,
-                  "frac": bytes32 / (t32 / 1e3) / 1e9 / peak}
+    q3 = (p + 1) ** 3
+    variants = {}
+    for fmt, tag in ((femgpu.QDATA_FULL, "full"), (femgpu.QDATA_AFFINE, "affine")):
+        op.set_qdata_format(fmt)
+        for prec, es in (("fp64", 8), ("fp32", 4)):
+            if prec == "fp64":
+                t = time_apply(lambda: op.apply_native(x.data_ptr(), y.data_ptr()))
+            else:
+                t = time_apply(lambda: op.apply_native_f32(x32.data_ptr(), y32.data_ptr()))
+            qbytes = (6 * q3 * E if tag == "full" else (6 + q3) * E) * es
+            nbytes = qbytes + 2 * N * es
+            variants[f"{prec}_{tag}"] = {"ms": t, "gdof_s": N / (t / 1e3) / 1e9, "bytes_per_apply": nbytes,
+                                         "achieved_gbs": nbytes / (t / 1e3) / 1e9,
+                                         "frac": nbytes / (t / 1e3) / 1e9 / peak}
+    op.set_qdata_format(femgpu.QDATA_FULL)
+    fp32_apply = variants
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -373,7 +400,7 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "solve": solve,
-            "fp32_apply": fp32_apply,
+            "apply_variants": fp32_apply,
         }
         print(json.dumps(out), flush=True)
     op.close()

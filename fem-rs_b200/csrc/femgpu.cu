@@ -170,6 +170,10 @@ struct fg_op {
           *ys32 = nullptr;
     int64_t qsize = 0;
     SolverState *st32 = nullptr;
+    // affine-compressed quadrature data (fg_op_set_qdata_format), FP64 and FP32
+    int fmt = 0;
+    double *qa64 = nullptr;
+    float *qa32 = nullptr;
     int *d_err = nullptr;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -189,6 +193,8 @@ static void free_op(fg_op *op) {
     for (float *b : fb)
         if (b) cudaFree(b);
     if (op->st32) cudaFree(op->st32);
+    if (op->qa64) cudaFree(op->qa64);
+    if (op->qa32) cudaFree(op->qa32);
     if (op->st) cudaFree(op->st);
     if (op->d_err) cudaFree(op->d_err);
     if (op->ev0) cudaEventDestroy(op->ev0);
@@ -218,14 +224,15 @@ template <typename T> struct TmapType;
 template <> struct TmapType<double> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT64; };
 template <> struct TmapType<float> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; };
 
-template <int P, int OPK, typename T>
+template <int P, int OPK, typename T, int FMT>
 static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const T *x, T *y,
                           int accumulate, const int *skip) {
     using C = KC<P, T>;
     static_assert(C::WY == KCfg<P>::WY, "FP32 and FP64 share the item tiling");
-    using SM = ApplySmem<P, T, C::WY, C::S, NComp<OPK>::v>;
+    constexpr int S = FMT == 0 ? C::S : 2;  // affine format: one element layer per stage
+    using SM = ApplySmem<P, T, C::WY, S, stage_elems<P, OPK, FMT>() / 32>;
     static bool attr_set[64] = {};
-    auto kern = pa_apply_kernel<P, OPK, T, C::WY, C::S, C::MINB>;
+    auto kern = pa_apply_kernel<P, OPK, T, C::WY, S, C::MINB, FMT>;
     if (!attr_set[op->device]) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
         attr_set[op->device] = true;
@@ -245,13 +252,26 @@ static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const 
     return FG_OK;
 }
 
+template <typename T> static const T *qdata_of(fg_op *op);
+template <> const double *qdata_of<double>(fg_op *op) { return op->fmt ? op->qa64 : op->qd; }
+template <> const float *qdata_of<float>(fg_op *op) { return op->fmt ? op->qa32 : op->qd32; }
+
 template <int P, typename T>
-static int launch_apply_p(fg_op *op, const Grid &g, const T *qd, T *face, const T *x, T *y,
+static int launch_apply_p(fg_op *op, const Grid &g, const T *, T *face, const T *x, T *y,
                           int accumulate, const int *skip) {
+    const T *qd = qdata_of<T>(op);
+    if (!qd) return fail(FG_INVALID_ARGUMENT, "quadrature data for this precision/format not built");
+    if (op->fmt == 0) {
+        switch (op->kind) {
+        case FG_MASS: return launch_apply_t<P, 1, T, 0>(op, g, qd, face, x, y, accumulate, skip);
+        case FG_DIFF: return launch_apply_t<P, 2, T, 0>(op, g, qd, face, x, y, accumulate, skip);
+        default: return launch_apply_t<P, 3, T, 0>(op, g, qd, face, x, y, accumulate, skip);
+        }
+    }
     switch (op->kind) {
-    case FG_MASS: return launch_apply_t<P, 1, T>(op, g, qd, face, x, y, accumulate, skip);
-    case FG_DIFF: return launch_apply_t<P, 2, T>(op, g, qd, face, x, y, accumulate, skip);
-    default: return launch_apply_t<P, 3, T>(op, g, qd, face, x, y, accumulate, skip);
+    case FG_MASS: return launch_apply_t<P, 1, T, 1>(op, g, qd, face, x, y, accumulate, skip);
+    case FG_DIFF: return launch_apply_t<P, 2, T, 1>(op, g, qd, face, x, y, accumulate, skip);
+    default: return launch_apply_t<P, 3, T, 1>(op, g, qd, face, x, y, accumulate, skip);
     }
 }
 
@@ -594,6 +614,59 @@ FG_API int fg_op_diagonal(fg_op *op, double *d, int constrained, int mem) {
 // ---------------------------------------------------------------------------
 // PCG
 // ---------------------------------------------------------------------------
+template <int P, int OPK, typename T> static void launch_compress(fg_op *op, T *dst) {
+    const int64_t total = (int64_t)op->g.nx * op->g.ny * op->g.nz * (P + 1) * (P + 1) * (P + 1);
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+    qdata_compress_kernel<P, OPK, T><<<blocks, 256, 0, op->stream>>>(op->g, op->qd, dst, op->d_err);
+}
+template <int P, typename T> static void launch_compress_p(fg_op *op, T *dst) {
+    switch (op->kind) {
+    case FG_MASS: launch_compress<P, 1, T>(op, dst); break;
+    case FG_DIFF: launch_compress<P, 2, T>(op, dst); break;
+    default: launch_compress<P, 3, T>(op, dst); break;
+    }
+}
+template <typename T> static int64_t affine_size(fg_op *op) {
+    auto sz = [&](auto pk, auto ok) -> int64_t {
+        constexpr int P = decltype(pk)::value, OPK = decltype(ok)::value;
+        return qd_size_fmt<P, OPK, 1>(op->g);
+    };
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    using I3 = std::integral_constant<int, 3>;
+    const int k = op->kind;
+    switch (op->p) {
+    case 1: return k == 1 ? sz(I1{}, I1{}) : k == 2 ? sz(I1{}, I2{}) : sz(I1{}, I3{});
+    case 2: return k == 1 ? sz(I2{}, I1{}) : k == 2 ? sz(I2{}, I2{}) : sz(I2{}, I3{});
+    default: return k == 1 ? sz(I3{}, I1{}) : k == 2 ? sz(I3{}, I2{}) : sz(I3{}, I3{});
+    }
+}
+// Affine-compressed quadrature data in precision T, derived from the full FP64
+// data; refused (FG_UNSUPPORTED) when an element's J is not constant.
+template <typename T> static int build_affine(fg_op *op, T **out) {
+    int rc;
+    T *dst = nullptr;
+    if ((rc = alloc_vec(&dst, affine_size<T>(op)))) return rc;
+    CK(cudaMemsetAsync(op->d_err, 0, sizeof(int), op->stream));
+    switch (op->p) {
+    case 1: launch_compress_p<1, T>(op, dst); break;
+    case 2: launch_compress_p<2, T>(op, dst); break;
+    default: launch_compress_p<3, T>(op, dst); break;
+    }
+    CK(cudaGetLastError());
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, op->d_err, sizeof(int), cudaMemcpyDeviceToHost, op->stream));
+    CK(cudaStreamSynchronize(op->stream));
+    if (herr) {
+        cudaFree(dst);
+        cudaMemsetAsync(op->d_err, 0, sizeof(int), op->stream);
+        return fail(FG_UNSUPPORTED, "affine quadrature-data format refused: the mesh has elements "
+                                    "whose Jacobian is not constant");
+    }
+    *out = dst;
+    return FG_OK;
+}
+
 static int ensure_solver_buffers(fg_op *op) {
     int rc;
     double **v[] = {&op->r, &op->z, &op->pv, &op->ap, &op->xw, &op->bw, &op->cres, &op->cd, &op->ct};
@@ -623,6 +696,7 @@ static int ensure_fp32(fg_op *op) {
     }
     if (!op->face32 && (rc = alloc_vec(&op->face32, (int64_t)op->g.n_items() * op->g.face_stride())))
         return rc;
+    if (op->fmt == 1 && !op->qa32 && (rc = build_affine<float>(op, &op->qa32))) return rc;
     float **v[] = {&op->r32, &op->z32, &op->p32, &op->ap32, &op->e32, &op->b32, &op->cres32,
                    &op->cd32, &op->ct32, &op->xs32, &op->ys32};
     for (float **b : v)
@@ -795,6 +869,21 @@ static int from_native32(fg_op *op, float *dst, const float *src, int mem) {
     CK(cudaMemcpy2DAsync(dst, sizeof(float) * g.NI, src, sizeof(float) * g.NIp, sizeof(float) * g.NI,
                          (size_t)g.NJ * g.NK,
                          mem == FG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, op->stream));
+    return FG_OK;
+}
+
+FG_API int fg_op_set_qdata_format(fg_op *op, int format) {
+    if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
+    if (format != FG_QDATA_FULL && format != FG_QDATA_AFFINE)
+        return fail(FG_INVALID_ARGUMENT, "bad quadrature-data format %d", format);
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    if (format == FG_QDATA_AFFINE) {
+        int rc;
+        if (!op->qa64 && (rc = build_affine<double>(op, &op->qa64))) return rc;
+        if (op->qd32 && !op->qa32 && (rc = build_affine<float>(op, &op->qa32))) return rc;
+    }
+    op->fmt = format;
     return FG_OK;
 }
 
@@ -1031,7 +1120,7 @@ template <int P, int OPK>
 static int noalloc_launch_apply_t(fg_op *op, const Grid &g, const double *x, double *y,
                                   int accumulate, double *face) {
     using C = KCfg<P>;
-    using SM = ApplySmem<P, double, C::WY, C::S, NComp<OPK>::v>;
+    using SM = ApplySmem<P, double, C::WY, C::S, stage_elems<P, OPK, 0>() / 32>;
     auto kern = pa_apply_kernel<P, OPK, double, C::WY, C::S, C::MINB>;
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
     CUtensorMap tmap;

@@ -61,14 +61,39 @@ template <typename T> struct ApplyArgs {
     const int *skip;  // if non-null and *skip != 0 the kernel returns at once
 };
 
-// Shared-memory plan of the apply kernel (bytes).
+// Quadrature-data formats.
+//  FMT 0 (full): NC components per quadrature point (6 symmetric w|detJ| kappa
+//    J^-1 J^-T, and/or w|detJ| rho); streamed one quadrature column per stage.
+//  FMT 1 (affine-compressed, valid when J is constant over each element): per
+//    element the 6 components of |detJ| J^-1 J^-T (diffusion), per quadrature
+//    point the scalars w kappa c_k (diffusion) and/or w |detJ| rho c_m (mass);
+//    streamed one element layer per stage.
+//    layout [item][warp][layer][NCE + Q^3 NCQ][lane], NCE = 6 (diffusion) or 0,
+//    quadrature point (col = qy*Q+qx, qz) at NCE + (col*Q + qz)*NCQ.
+template <int OPK> struct AffineComp {
+    static constexpr int NCE = (OPK & 2) ? 6 : 0;
+    static constexpr int NCQ = ((OPK & 2) ? 1 : 0) + ((OPK & 1) ? 1 : 0);
+};
+template <int P, int OPK, int FMT> constexpr int stage_elems() {
+    return FMT == 0 ? (P + 1) * NComp<OPK>::v * 32
+                    : (AffineComp<OPK>::NCE + (P + 1) * (P + 1) * (P + 1) * AffineComp<OPK>::NCQ) * 32;
+}
+template <int P, int OPK, int FMT>
+__host__ __device__ inline int64_t qd_size_fmt(const Grid &g) {
+    // stages per layer: Q^2 columns (FMT 0) or 1 (FMT 1)
+    constexpr int U = FMT == 0 ? (P + 1) * (P + 1) : 1;
+    return (int64_t)g.n_items() * g.WY * g.TZ * U * stage_elems<P, OPK, FMT>();
+}
+
+// Shared-memory plan of the apply kernel (bytes).  NC here is the stage size
+// in units of 32-lane vectors.
 template <int P, typename T, int WY, int S, int NC> struct ApplySmem {
     static constexpr int D = P + 1, Q = P + 1;
     static constexpr int XW = round_up(32 * P + 1, 16 / (int)sizeof(T));
     static constexpr int RY = WY * P + 1;
     static constexpr int XTILE = (P + 1) * RY * XW;               // elements
     static constexpr int XB = round_up(XTILE * (int)sizeof(T), 128);
-    static constexpr int STAGE = Q * NC * 32;                     // elements
+    static constexpr int STAGE = NC * 32;                         // elements
     static constexpr int QB = STAGE * (int)sizeof(T);
     static constexpr int off_q = 2 * XB;
     static constexpr int off_y = off_q + WY * S * QB;
@@ -175,13 +200,15 @@ __device__ __forceinline__ void merge_and_store(T (&out)[P + 1][P + 1][P + 1], c
 // ---------------------------------------------------------------------------
 // The apply kernel.
 // ---------------------------------------------------------------------------
-template <int P, int OPK, typename T, int WY, int S, int MINB>
+template <int P, int OPK, typename T, int WY, int S, int MINB, int FMT = 0>
 __global__ void __launch_bounds__(WY * 32, MINB)
     pa_apply_kernel(const __grid_constant__ CUtensorMap xmap, const ApplyArgs<T> A) {
     constexpr int D = P + 1, Q = P + 1, NC = NComp<OPK>::v;
     constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
     constexpr int COLS = Q * Q;
-    using SM = ApplySmem<P, T, WY, S, NC>;
+    constexpr int UPL = FMT == 0 ? COLS : 1;  // stream units per layer
+    constexpr int NCE = AffineComp<OPK>::NCE, NCQ = AffineComp<OPK>::NCQ;
+    using SM = ApplySmem<P, T, WY, S, stage_elems<P, OPK, FMT>() / 32>;
     constexpr int STAGE = SM::STAGE, XW = SM::XW, RY = SM::RY;
     using TB = Tab<T>;
 
@@ -204,8 +231,8 @@ __global__ void __launch_bounds__(WY * 32, MINB)
     const int lane_last = min(31, g.nx - 1 - tx * 32);
     const int w_last = min(WY - 1, g.ny - 1 - ty * WY);
     const int I0 = tx * 32 * P, J0 = ty * WY * P, K0 = tz * g.TZ * P;
-    const int total_cols = nl * COLS;
-    const T *qdw = A.qd + (int64_t)(item * WY + warp) * g.TZ * COLS * STAGE;
+    const int total_cols = nl * UPL;
+    const T *qdw = A.qd + (int64_t)(item * WY + warp) * g.TZ * UPL * STAGE;
     T *qsw = qs + warp * S * STAGE;
     uint64_t *qbw = qbar + warp * S;
     constexpr uint32_t XBYTES = (uint32_t)(SM::XTILE * sizeof(T));
@@ -305,6 +332,17 @@ __global__ void __launch_bounds__(WY * 32, MINB)
                 }
         }
         // ---- per quadrature column: B in z, D, B^T in z (in place) --------
+        T Ge[6] = {0, 0, 0, 0, 0, 0};
+        const T *ql = nullptr;  // layer stage (FMT 1)
+        if (FMT == 1) {
+            const int j = lz;
+            const int s = j % S;
+            if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+            q_waited = j + 1;
+            ql = qsw + s * STAGE;
+#pragma unroll
+            for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
+        }
 #pragma unroll
         for (int qy = 0; qy < Q; ++qy)
 #pragma unroll
@@ -312,9 +350,11 @@ __global__ void __launch_bounds__(WY * 32, MINB)
                 const int col = qy * Q + qx;
                 const int j = lz * COLS + col;
                 const int s = j % S;
-                if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-                q_waited = j + 1;
-                const T *qc = qsw + s * STAGE;
+                if (FMT == 0) {
+                    if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+                    q_waited = j + 1;
+                }
+                const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
                 T vx[Q], vy[Q], vz[Q], vu[Q];
 #pragma unroll
                 for (int qz = 0; qz < Q; ++qz) {
@@ -328,15 +368,27 @@ __global__ void __launch_bounds__(WY * 32, MINB)
                         }
                         if (HM) ui += TB::B(P, qz, c) * C0[c][qy][qx];
                     }
-                    const T *qq = qc + qz * (NC * 32) + lane;
-                    if (HK) {
-                        const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128],
-                                d5 = qq[160];
-                        vx[qz] = d0 * gx + d1 * gy + d2 * gz;
-                        vy[qz] = d1 * gx + d3 * gy + d4 * gz;
-                        vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                    if (FMT == 0) {
+                        const T *qq = qc + qz * (NC * 32) + lane;
+                        if (HK) {
+                            const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128],
+                                    d5 = qq[160];
+                            vx[qz] = d0 * gx + d1 * gy + d2 * gz;
+                            vy[qz] = d1 * gx + d3 * gy + d4 * gz;
+                            vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                        }
+                        if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
+                    } else {
+                        const T *qq = qc + (NCE + (col * Q + qz) * NCQ) * 32 + lane;
+                        if (HK) {
+                            const T sk = qq[0];
+                            const T hx = sk * gx, hy = sk * gy, hz = sk * gz;
+                            vx[qz] = Ge[0] * hx + Ge[1] * hy + Ge[2] * hz;
+                            vy[qz] = Ge[1] * hx + Ge[3] * hy + Ge[4] * hz;
+                            vz[qz] = Ge[2] * hx + Ge[4] * hy + Ge[5] * hz;
+                        }
+                        if (HM) vu[qz] = qq[(HK ? 1 : 0) * 32] * ui;
                     }
-                    if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
                 }
 #pragma unroll
                 for (int c = 0; c < D; ++c) {
@@ -354,14 +406,26 @@ __global__ void __launch_bounds__(WY * 32, MINB)
                     C1[c][qy][qx] = e1;
                     C2[c][qy][qx] = e2;
                 }
-                __syncwarp();
-                if (lane == 0 && ok && j + S < total_cols) {
-                    fence_proxy_async();
-                    mbar_arrive_expect_tx(&qbw[s], QBYTES);
-                    bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
-                    q_issued = j + S + 1;
+                if (FMT == 0) {
+                    __syncwarp();
+                    if (lane == 0 && ok && j + S < total_cols) {
+                        fence_proxy_async();
+                        mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                        bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                        q_issued = j + S + 1;
+                    }
                 }
             }
+        if (FMT == 1) {
+            const int j = lz, s = j % S;
+            __syncwarp();
+            if (lane == 0 && ok && j + S < total_cols) {
+                fence_proxy_async();
+                mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                q_issued = j + S + 1;
+            }
+        }
         // ---- B^T: contractions in y then x --------------------------------
         T out[D][D][D];
 #pragma unroll
@@ -565,6 +629,54 @@ struct SetupArgs {
     double gx[4], gw[4];    // Gauss rule for Q = p+1 points
     int *err;
 };
+
+// Affine-compressed quadrature data (FMT 1) derived from the full FP64 data:
+// on an element with constant J every D_q is w_q kappa_q times the same
+// symmetric matrix |detJ| J^-1 J^-T, so G_e = D_{q0} and s_q = tr(D_q)/tr(D_{q0})
+// reproduce D_q = s_q G_e.  Each thread (element, quadrature point) checks
+// that identity to 1e-10 relative and raises FG_DERR_BOUNDS otherwise (the
+// mesh is not affine: the format is refused).  The mass scalar is copied.
+template <int P, int OPK, typename T>
+__global__ void qdata_compress_kernel(const Grid g, const double *__restrict__ qfull,
+                                      T *__restrict__ qaff, int *err) {
+    constexpr int Q = P + 1, NC = NComp<OPK>::v;
+    constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
+    constexpr int NCE = AffineComp<OPK>::NCE, NCQ = AffineComp<OPK>::NCQ;
+    constexpr int STG = stage_elems<P, OPK, 1>();
+    const int64_t E = (int64_t)g.nx * g.ny * g.nz;
+    const int64_t total = E * Q * Q * Q;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int q = (int)(t % (Q * Q * Q));
+        const int64_t e = t / (Q * Q * Q);
+        const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
+        const int ex = (int)(e % g.nx), ey = (int)((e / g.nx) % g.ny), ez = (int)(e / ((int64_t)g.nx * g.ny));
+        const int tx = ex / 32, lane = ex % 32, ty = ey / g.WY, wy = ey % g.WY, tz = ez / g.TZ,
+                  lz = ez % g.TZ;
+        const int item = (tz * g.nty + ty) * g.ntx + tx;
+        const int col = qy * Q + qx;
+        const double *src = qfull + qd_index<P, OPK>(g, item, wy, lz, col, qz, 0, lane);
+        const double *src0 = qfull + qd_index<P, OPK>(g, item, wy, lz, 0, 0, 0, lane);
+        T *base = qaff + ((((int64_t)item * g.WY + wy) * g.TZ + lz) * STG) + lane;
+        T *qq = base + (NCE + (col * Q + qz) * NCQ) * 32;
+        if (HK) {
+            const double tr = src[0] + src[96] + src[160];
+            const double tr0 = src0[0] + src0[96] + src0[160];
+            const double sq = tr0 != 0.0 ? tr / tr0 : 0.0;
+            double nrm = 0.0, dif = 0.0;
+            for (int k = 0; k < 6; ++k) {
+                nrm = fmax(nrm, fabs(src[k * 32]));
+                dif = fmax(dif, fabs(src[k * 32] - sq * src0[k * 32]));
+            }
+            if (dif > 1e-10 * nrm && err) atomicOr(err, FG_DERR_BOUNDS);
+            qq[0] = (T)sq;
+            if (q == 0)
+                for (int k = 0; k < 6; ++k) base[k * 32] = (T)src0[k * 32];
+        }
+        if (HM) qq[(HK ? 1 : 0) * 32] = (T)src[(HK ? 6 : 0) * 32];
+        (void)NC;
+    }
+}
 
 template <int P, int OPK, typename T>
 __global__ void qdata_setup_kernel(const SetupArgs S, T *__restrict__ qd) {

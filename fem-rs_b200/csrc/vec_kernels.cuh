@@ -88,6 +88,20 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double *partials, Solv
 #define FG_VEC_LOOP(i, n) \
     for (int64_t i = (int64_t)blockIdx.x * VEC_THREADS + threadIdx.x; i < (n); i += (int64_t)gridDim.x * VEC_THREADS)
 
+// 4-wide groups: native vectors have a length that is a multiple of 4 (the row
+// pitch is), and cudaMalloc alignment makes every group 16/32-byte aligned.
+template <typename T> struct alignas(4 * sizeof(T)) V4 { T a[4]; };
+template <typename T> __device__ __forceinline__ V4<T> ld4(const T *p, int64_t q) {
+    return reinterpret_cast<const V4<T> *>(p)[q];
+}
+template <typename T> __device__ __forceinline__ void st4(T *p, int64_t q, const V4<T> &v) {
+    reinterpret_cast<V4<T> *>(p)[q] = v;
+}
+#define FG_VEC4_LOOP(q, n)                                                                  \
+    for (int64_t q = (int64_t)blockIdx.x * VEC_THREADS + threadIdx.x; q < ((n) >> 2);       \
+         q += (int64_t)gridDim.x * VEC_THREADS)
+#define FG_K4 _Pragma("unroll") for (int k = 0; k < 4; ++k)
+
 // r = b - ap; z = dinv r (jacobi) ; p = z ; rz = r.z ; bb = b.b
 template <typename T>
 __global__ void __launch_bounds__(VEC_THREADS) k_pcg_init(int64_t n, const T *__restrict__ b,
@@ -97,15 +111,22 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_init(int64_t n, const T *__
                                                           T *__restrict__ p, int jacobi,
                                                           double *partials, SolverState *st) {
     double v[2] = {0.0, 0.0};
-    FG_VEC_LOOP(i, n) {
-        const T ri = b[i] - ap[i];
-        r[i] = ri;
-        v[1] += (double)b[i] * (double)b[i];
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> bv = ld4(b, q), av = ld4(ap, q);
+        V4<T> rv, zv, dv;
+        if (jacobi) dv = ld4(dinv, q);
+        FG_K4 {
+            rv.a[k] = bv.a[k] - av.a[k];
+            v[1] += (double)bv.a[k] * (double)bv.a[k];
+            if (jacobi) {
+                zv.a[k] = dv.a[k] * rv.a[k];
+                v[0] += (double)rv.a[k] * (double)zv.a[k];
+            }
+        }
+        st4(r, q, rv);
         if (jacobi) {
-            const T zi = dinv[i] * ri;
-            z[i] = zi;
-            p[i] = zi;
-            v[0] += (double)ri * (double)zi;
+            st4(z, q, zv);
+            st4(p, q, zv);
         }
     }
     double tot[2];
@@ -132,7 +153,10 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_pap(int64_t n, const T *__r
                                                          double *partials, SolverState *st) {
     if (st->done) return;
     double v[1] = {0.0};
-    FG_VEC_LOOP(i, n) v[0] += (double)p[i] * (double)ap[i];
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> pv = ld4(p, q), av = ld4(ap, q);
+        FG_K4 v[0] += (double)pv.a[k] * (double)av.a[k];
+    }
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {
         st->pap = tot[0];
@@ -157,16 +181,23 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_update(int64_t n, T *__rest
     if (st->done) return;
     const T alpha = (T)st->alpha;
     double v[2] = {0.0, 0.0};
-    FG_VEC_LOOP(i, n) {
-        x[i] += alpha * p[i];
-        const T ri = r[i] - alpha * ap[i];
-        r[i] = ri;
-        v[0] += (double)ri * (double)ri;
-        if (jacobi) {
-            const T zi = dinv[i] * ri;
-            z[i] = zi;
-            v[1] += (double)ri * (double)zi;
+    FG_VEC4_LOOP(q, n) {
+        V4<T> xv = ld4(x, q), rv = ld4(r, q);
+        const V4<T> pv = ld4(p, q), av = ld4(ap, q);
+        V4<T> dv, zv;
+        if (jacobi) dv = ld4(dinv, q);
+        FG_K4 {
+            xv.a[k] += alpha * pv.a[k];
+            rv.a[k] = rv.a[k] - alpha * av.a[k];
+            v[0] += (double)rv.a[k] * (double)rv.a[k];
+            if (jacobi) {
+                zv.a[k] = dv.a[k] * rv.a[k];
+                v[1] += (double)rv.a[k] * (double)zv.a[k];
+            }
         }
+        st4(x, q, xv);
+        st4(r, q, rv);
+        if (jacobi) st4(z, q, zv);
     }
     double tot[2];
     if (grid_sum<2>(v, partials, st, tot) && threadIdx.x == 0) {
@@ -193,7 +224,10 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_rz(int64_t n, const T *__re
                                                         double *partials, SolverState *st, int init) {
     if (st->done) return;
     double v[1] = {0.0};
-    FG_VEC_LOOP(i, n) v[0] += (double)r[i] * (double)z[i];
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> rv = ld4(r, q), zv = ld4(z, q);
+        FG_K4 v[0] += (double)rv.a[k] * (double)zv.a[k];
+    }
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {
         if (!init) st->beta = tot[0] / st->rz;
@@ -208,7 +242,12 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_pupdate(int64_t n, const T 
                                                              const SolverState *st, int init) {
     if (st->done) return;
     const T beta = init ? T(0) : (T)st->beta;
-    FG_VEC_LOOP(i, n) p[i] = z[i] + beta * p[i];
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> zv = ld4(z, q);
+        V4<T> pv = ld4(p, q);
+        FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        st4(p, q, pv);
+    }
 }
 
 // Chebyshev sweep 1 from zero: res = dinv r ; d = res / theta ; z = d
@@ -220,12 +259,17 @@ __global__ void __launch_bounds__(VEC_THREADS) k_cheb_first(int64_t n, const T *
                                                             T *__restrict__ z, double inv_theta,
                                                             const SolverState *st) {
     if (st && st->done) return;
-    FG_VEC_LOOP(i, n) {
-        const T s = dinv[i] * r[i];
-        res[i] = s;
-        const T di = s * (T)inv_theta;
-        d[i] = di;
-        z[i] = di;
+    const T it = (T)inv_theta;
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> rv = ld4(r, q), dv = ld4(dinv, q);
+        V4<T> sv, dd;
+        FG_K4 {
+            sv.a[k] = dv.a[k] * rv.a[k];
+            dd.a[k] = sv.a[k] * it;
+        }
+        st4(res, q, sv);
+        st4(d, q, dd);
+        st4(z, q, dd);
     }
 }
 
@@ -238,12 +282,18 @@ __global__ void __launch_bounds__(VEC_THREADS) k_cheb_step(int64_t n, const T *_
                                                            T *__restrict__ z, double c1,
                                                            double c2, const SolverState *st) {
     if (st && st->done) return;
-    FG_VEC_LOOP(i, n) {
-        const T s = res[i] - dinv[i] * t[i];
-        res[i] = s;
-        const T di = (T)c1 * d[i] + (T)c2 * s;
-        d[i] = di;
-        z[i] += di;
+    const T a1 = (T)c1, a2 = (T)c2;
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> tv = ld4(t, q), dv = ld4(dinv, q);
+        V4<T> sv = ld4(res, q), dd = ld4(d, q), zv = ld4(z, q);
+        FG_K4 {
+            sv.a[k] = sv.a[k] - dv.a[k] * tv.a[k];
+            dd.a[k] = a1 * dd.a[k] + a2 * sv.a[k];
+            zv.a[k] += dd.a[k];
+        }
+        st4(res, q, sv);
+        st4(d, q, dd);
+        st4(z, q, zv);
     }
 }
 
@@ -252,9 +302,12 @@ __global__ void __launch_bounds__(VEC_THREADS) k_true_residual(int64_t n, const 
                                                                const double *__restrict__ ap,
                                                                double *partials, SolverState *st) {
     double v[1] = {0.0};
-    FG_VEC_LOOP(i, n) {
-        const double s = b[i] - ap[i];
-        v[0] += s * s;
+    FG_VEC4_LOOP(q, n) {
+        const V4<double> bv = ld4(b, q), av = ld4(ap, q);
+        FG_K4 {
+            const double s = bv.a[k] - av.a[k];
+            v[0] += s * s;
+        }
     }
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0)
@@ -294,7 +347,11 @@ __global__ void __launch_bounds__(VEC_THREADS) k_scale_by_rho(int64_t n, const d
     const double rho = st->rho;
     if (!(rho > 1e-14)) return;
     const double inv = 1.0 / rho;
-    FG_VEC_LOOP(i, n) v[i] = w[i] * inv;
+    FG_VEC4_LOOP(q, n) {
+        V4<double> wv = ld4(w, q);
+        FG_K4 wv.a[k] *= inv;
+        st4(v, q, wv);
+    }
 }
 
 // w = dinv * w ; rho = ||w||
@@ -302,10 +359,14 @@ __global__ void __launch_bounds__(VEC_THREADS) k_dinv_norm(int64_t n, double *__
                                                            const double *__restrict__ dinv,
                                                            double *partials, SolverState *st) {
     double acc[1] = {0.0};
-    FG_VEC_LOOP(i, n) {
-        const double s = dinv[i] * w[i];
-        w[i] = s;
-        acc[0] += s * s;
+    FG_VEC4_LOOP(q, n) {
+        V4<double> wv = ld4(w, q);
+        const V4<double> dv = ld4(dinv, q);
+        FG_K4 {
+            wv.a[k] *= dv.a[k];
+            acc[0] += wv.a[k] * wv.a[k];
+        }
+        st4(w, q, wv);
     }
     double tot[1];
     if (grid_sum<1>(acc, partials, st, tot) && threadIdx.x == 0) st->rho = sqrt(tot[0]);
@@ -332,11 +393,15 @@ __global__ void __launch_bounds__(VEC_THREADS) k_ir_residual(int64_t n, const do
                                                              double *__restrict__ r, double *partials,
                                                              SolverState *st, int init) {
     double v[2] = {0.0, 0.0};
-    FG_VEC_LOOP(i, n) {
-        const double ri = b[i] - ap[i];
-        r[i] = ri;
-        v[0] += ri * ri;
-        if (init) v[1] += b[i] * b[i];
+    FG_VEC4_LOOP(q, n) {
+        const V4<double> bv = ld4(b, q), av = ld4(ap, q);
+        V4<double> rv;
+        FG_K4 {
+            rv.a[k] = bv.a[k] - av.a[k];
+            v[0] += rv.a[k] * rv.a[k];
+            if (init) v[1] += bv.a[k] * bv.a[k];
+        }
+        st4(r, q, rv);
     }
     double tot[2];
     if (grid_sum<2>(v, partials, st, tot) && threadIdx.x == 0) {
@@ -363,7 +428,12 @@ __global__ void __launch_bounds__(VEC_THREADS) k_ir_to_f32(int64_t n, const doub
                                                            float *__restrict__ r32,
                                                            const SolverState *st) {
     const double s = st->rr > 0.0 ? 1.0 / sqrt(st->rr) : 0.0;
-    FG_VEC_LOOP(i, n) r32[i] = (float)(r[i] * s);
+    FG_VEC4_LOOP(q, n) {
+        const V4<double> rv = ld4(r, q);
+        V4<float> o;
+        FG_K4 o.a[k] = (float)(rv.a[k] * s);
+        st4(r32, q, o);
+    }
 }
 
 // x += ||r|| * e   (FP64 solution update)
@@ -371,7 +441,12 @@ __global__ void __launch_bounds__(VEC_THREADS) k_ir_update(int64_t n, double *__
                                                            const float *__restrict__ e,
                                                            const SolverState *st) {
     const double s = sqrt(st->rr);
-    FG_VEC_LOOP(i, n) x[i] += s * (double)e[i];
+    FG_VEC4_LOOP(q, n) {
+        V4<double> xv = ld4(x, q);
+        const V4<float> ev = ld4(e, q);
+        FG_K4 xv.a[k] += s * (double)ev.a[k];
+        st4(x, q, xv);
+    }
 }
 
 // FP32 copy of an FP64 vector
@@ -396,11 +471,16 @@ __global__ void __launch_bounds__(VEC_THREADS) k_rel_step(int64_t n, float *__re
     if (st->done) return;
     const float alpha = (float)st->alpha;
     double v[1] = {0.0};
-    FG_VEC_LOOP(i, n) {
-        xlo[i] += alpha * p[i];
-        const float ri = r[i] - alpha * ap[i];
-        r[i] = ri;
-        v[0] += (double)ri * (double)ri;
+    FG_VEC4_LOOP(q, n) {
+        V4<float> xv = ld4(xlo, q), rv = ld4(r, q);
+        const V4<float> pv = ld4(p, q), av = ld4(ap, q);
+        FG_K4 {
+            xv.a[k] += alpha * pv.a[k];
+            rv.a[k] = rv.a[k] - alpha * av.a[k];
+            v[0] += (double)rv.a[k] * (double)rv.a[k];
+        }
+        st4(xlo, q, xv);
+        st4(r, q, rv);
     }
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {
@@ -419,9 +499,12 @@ __global__ void __launch_bounds__(VEC_THREADS) k_rel_xupdate(int64_t n, double *
                                                              float *__restrict__ xlo,
                                                              const SolverState *st) {
     if (!st->trigger) return;
-    FG_VEC_LOOP(i, n) {
-        x[i] += (double)xlo[i];
-        xlo[i] = 0.0f;
+    FG_VEC4_LOOP(q, n) {
+        V4<double> xv = ld4(x, q);
+        const V4<float> lv = ld4(xlo, q);
+        FG_K4 xv.a[k] += (double)lv.a[k];
+        st4(x, q, xv);
+        st4(xlo, q, V4<float>{{0.0f, 0.0f, 0.0f, 0.0f}});
     }
 }
 
@@ -434,11 +517,16 @@ __global__ void __launch_bounds__(VEC_THREADS) k_rel_residual(int64_t n, const d
                                                               int init) {
     if (!init && !st->trigger) return;
     double v[2] = {0.0, 0.0};
-    FG_VEC_LOOP(i, n) {
-        const double ri = b[i] - ap[i];
-        r[i] = (float)ri;
-        v[0] += ri * ri;
-        if (init) v[1] += b[i] * b[i];
+    FG_VEC4_LOOP(q, n) {
+        const V4<double> bv = ld4(b, q), av = ld4(ap, q);
+        V4<float> rv;
+        FG_K4 {
+            const double ri = bv.a[k] - av.a[k];
+            rv.a[k] = (float)ri;
+            v[0] += ri * ri;
+            if (init) v[1] += bv.a[k] * bv.a[k];
+        }
+        st4(r, q, rv);
     }
     double tot[2];
     if (grid_sum<2>(v, partials, st, tot) && threadIdx.x == 0) {
@@ -476,10 +564,14 @@ __global__ void __launch_bounds__(VEC_THREADS) k_jacobi_rz(int64_t n, const T *_
                                                            SolverState *st, int init) {
     if (st->done) return;
     double v[1] = {0.0};
-    FG_VEC_LOOP(i, n) {
-        const T zi = dinv[i] * r[i];
-        z[i] = zi;
-        v[0] += (double)r[i] * (double)zi;
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> rv = ld4(r, q), dv = ld4(dinv, q);
+        V4<T> zv;
+        FG_K4 {
+            zv.a[k] = dv.a[k] * rv.a[k];
+            v[0] += (double)rv.a[k] * (double)zv.a[k];
+        }
+        st4(z, q, zv);
     }
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {

@@ -31,13 +31,15 @@ MASS, DIFF, MASS_DIFF = 1, 2, 3
 HOST, DEVICE = 0, 1
 PC_NONE, PC_JACOBI, PC_CHEBYSHEV = 0, 1, 2
 FP64, FP32_IR = 0, 1
+QDATA_FULL, QDATA_AFFINE = 0, 1
 TAG_ALL = 63
 
 # every symbol include/femgpu.h declares
 EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "fg_op_ndofs",
            "fg_op_layout", "fg_op_native_len", "fg_op_set_stream", "fg_op_apply",
            "fg_op_apply_native", "fg_op_diagonal", "fg_pcg", "fg_op_check",
-           "fg_op_apply_native_noalloc", "fg_op_apply_f32", "fg_op_apply_native_f32")
+           "fg_op_apply_native_noalloc", "fg_op_apply_f32", "fg_op_apply_native_f32",
+           "fg_op_set_qdata_format")
 
 
 class FgMesh(C.Structure):
@@ -86,6 +88,7 @@ def lib():
         L.fg_pcg.argtypes = [vp, vp, vp, vp, vp, i]
         L.fg_op_check.argtypes = [vp]
         L.fg_op_apply_f32.argtypes = [vp, vp, vp, i, i, i]
+        L.fg_op_set_qdata_format.argtypes = [vp, i]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
@@ -281,6 +284,10 @@ class PAOperator:
     def apply_native_f32(self, x_ptr, y_ptr, accumulate=False, constrained=True):
         """FP32 apply on float32 device vectors in the native layout; asynchronous."""
         _check(lib().fg_op_apply_native_f32(self._h, x_ptr, y_ptr, int(accumulate), int(constrained)))
+
+    def set_qdata_format(self, fmt):
+        """QDATA_FULL (general geometry) or QDATA_AFFINE (constant-J elements only)."""
+        _check(lib().fg_op_set_qdata_format(self._h, int(fmt)))
 
     def diagonal(self, constrained=True):
         d = np.zeros(self.n_dofs())

@@ -71,6 +71,9 @@ enum fg_mem { FG_HOST = 0, FG_DEVICE = 1 };
 enum fg_precond { FG_PC_NONE = 0, FG_PC_JACOBI = 1, FG_PC_CHEBYSHEV = 2 };
 enum fg_precision { FG_FP64 = 0, FG_FP32_IR = 1 };
 
+/* Quadrature-data formats (fg_op_set_qdata_format). */
+enum fg_qdata_format { FG_QDATA_FULL = 0, FG_QDATA_AFFINE = 1 };
+
 /* Boundary tags (simplex.rs:650-679 order): bit t-1 selects tag t. */
 enum fg_tag {
     FG_TAG_Z0 = 1, FG_TAG_Z1 = 2, FG_TAG_Y0 = 4, FG_TAG_Y1 = 8, FG_TAG_X0 = 16, FG_TAG_X1 = 32,
@@ -154,6 +157,18 @@ FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, in
  * on the handle's stream, no host synchronisation. */
 FG_API int fg_op_apply_native(fg_op *op, const double *x, double *y, int accumulate,
                               int constrained);
+
+/* Choose the quadrature-data format of the handle's applies and solves.
+ * FG_QDATA_FULL (default): 6 symmetric components w|detJ| kappa J^-1 J^-T per
+ * quadrature point (the general form of the reference's qdata,
+ * crates/assembly/src/reed/qfunction.rs:155-192, in 3-D).  FG_QDATA_AFFINE:
+ * valid only when J is constant over every element (parallelepipeds, e.g.
+ * uniform boxes): 6 components of |detJ| J^-1 J^-T per element and one scalar
+ * w kappa per quadrature point (plus w|detJ| rho for mass), about 5x fewer
+ * bytes per apply.  Built from the full data on first use; returns
+ * FG_UNSUPPORTED (format unchanged) when the mesh is not affine.  The Jacobi
+ * diagonal and fg_op_apply_native_noalloc always use the full data. */
+FG_API int fg_op_set_qdata_format(fg_op *op, int format);
 
 /* FP32 form of the apply (the chosen precision form of the iterative
  * refinement): quadrature data rounded to FP32 once, FP32 vectors, FP32
