@@ -171,6 +171,7 @@ struct fg_op {
     int64_t qsize = 0;
     SolverState *st32 = nullptr;
     // affine-compressed quadrature data (fg_op_set_qdata_format), FP64 and FP32
+    double *sd_u = nullptr, *sd_k1 = nullptr, *sd_w = nullptr;  // SDIRK-2 stepping
     int fmt = 0;
     double *qa64 = nullptr;
     float *qa32 = nullptr;
@@ -194,6 +195,9 @@ static void free_op(fg_op *op) {
         if (b) cudaFree(b);
     if (op->st32) cudaFree(op->st32);
     if (op->qa64) cudaFree(op->qa64);
+    if (op->sd_u) cudaFree(op->sd_u);
+    if (op->sd_k1) cudaFree(op->sd_k1);
+    if (op->sd_w) cudaFree(op->sd_w);
     if (op->qa32) cudaFree(op->qa32);
     if (op->st) cudaFree(op->st);
     if (op->d_err) cudaFree(op->d_err);
@@ -915,11 +919,7 @@ FG_API int fg_op_apply_native_f32(fg_op *op, const float *x, float *y, int accum
     return apply_native_t<float>(op, op->qd32, op->face32, x, y, accumulate, constrained, nullptr);
 }
 
-FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, fg_result *res,
-                  int mem) {
-    if (!op || !b || !x) return fail(FG_INVALID_ARGUMENT, "NULL argument");
-    fg_cfg cfg;
-    if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
+static int validate_cfg(fg_cfg &cfg) {
     if (cfg.max_iter < 0) return fail(FG_INVALID_ARGUMENT, "max_iter < 0");
     if (cfg.precision != FG_FP64 && cfg.precision != FG_FP32_IR)
         return fail(FG_UNSUPPORTED, "precision %d not available", cfg.precision);
@@ -927,8 +927,12 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
     if (cfg.precond == FG_PC_CHEBYSHEV && cfg.cheb_degree < 1)
         return fail(FG_INVALID_ARGUMENT, "cheb_degree must be >= 1");
     if (cfg.check_interval < 1) cfg.check_interval = 10;
-    std::lock_guard<std::mutex> lk(op->mu);
-    CK(cudaSetDevice(op->device));
+    return FG_OK;
+}
+
+// PCG on op->bw (right-hand side) from op->xw (initial guess), both native and
+// resident; the solution is left in op->xw.  The caller holds op->mu.
+static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
     const bool cheb = cfg.precond == FG_PC_CHEBYSHEV;
     const bool ir = cfg.precision == FG_FP32_IR;
     int rc;
@@ -962,7 +966,6 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
         lmin = lmax / (cfg.lmin_ratio > 0 ? cfg.lmin_ratio : 30.0);
     }
     const ChebCoef cc = cheb ? cheb_coefs(lmin, lmax, cfg.cheb_degree) : ChebCoef{};
-    if ((rc = to_native(op, op->bw, b, mem)) || (rc = to_native(op, op->xw, x, mem))) return rc;
     const int64_t n = op->Nn;
     int64_t applies = 0;
     SolverState h{};
@@ -1055,7 +1058,6 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
     if ((rc = apply_native(op, op->xw, op->ap, 0, 1, nullptr))) return rc;
     k_true_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->partials, op->st);
     CK(cudaGetLastError());
-    if ((rc = from_native(op, x, op->xw, mem))) return rc;
     SolverState h2;
     if ((rc = read_state(op, &h2))) return rc;
     float ms = 0.f;
@@ -1080,6 +1082,130 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
     else if (status == FG_BREAKDOWN) fail(status, "CG breakdown: p^T A p is near zero");
     else fail(status, "solver did not converge in %d iterations (residual = %.3e)", cfg.max_iter, h.res);
     return status;
+}
+
+FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, fg_result *res,
+                  int mem) {
+    if (!op || !b || !x) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    fg_cfg cfg;
+    if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
+    int rc;
+    if ((rc = validate_cfg(cfg))) return rc;
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    if ((rc = ensure_solver_buffers(op))) return rc;
+    if ((rc = to_native(op, op->bw, b, mem)) || (rc = to_native(op, op->xw, x, mem))) return rc;
+    const int status = pcg_core(op, cfg, res);
+    if (status != FG_OK && status != FG_CONVERGENCE_FAILED && status != FG_BREAKDOWN) return status;
+    if ((rc = from_native(op, x, op->xw, mem))) return rc;
+    CK(cudaStreamSynchronize(op->stream));
+    if (status != FG_OK) {  // restore the solver's message
+        if (status == FG_BREAKDOWN) fail(status, "CG breakdown: p^T A p is near zero");
+        else fail(status, "solver did not converge in %d iterations", cfg.max_iter);
+    }
+    return status;
+}
+
+// SDIRK-2 heat stepping (examples/mfem_ex10_heat_equation.rs:201-250,
+// gamma = 1 - 1/sqrt(2) as crates/solver/src/ode.rs:441): M u_t + K u = 0,
+// homogeneous Dirichlet.  Per step:
+//   (M + g dt K) k1 = -K u,          u2 = u + dt (1-g) k1,
+//   (M + g dt K) k2 = -K u2,         u += dt ((1-g) k1 + g k2).
+// Stage solves run on the device with the PCG core, warm-started from the
+// previous stage's k (the reference starts every solve from zero).
+FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_steps,
+                     const fg_cfg *cfg_in, fg_sdirk_result *out, int mem) {
+    if (!stiff || !stage || !u) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (stiff == stage) return fail(FG_INVALID_ARGUMENT, "stiff and stage must be distinct handles");
+    if (n_steps < 0 || !(dt > 0)) return fail(FG_INVALID_ARGUMENT, "bad dt or n_steps");
+    if (stiff->device != stage->device || stiff->N != stage->N || stiff->g.NI != stage->g.NI ||
+        stiff->g.NJ != stage->g.NJ || stiff->g.NK != stage->g.NK || stiff->p != stage->p)
+        return fail(FG_DIMENSION_MISMATCH, "stiff and stage operators live on different meshes");
+    fg_cfg cfg;
+    if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
+    int rc;
+    if ((rc = validate_cfg(cfg))) return rc;
+    std::scoped_lock lk(stiff->mu, stage->mu);
+    CK(cudaSetDevice(stage->device));
+    cudaStream_t saved = stiff->stream;
+    stiff->stream = stage->stream;  // one stream orders both operators' work
+    struct Restore { fg_op *o; cudaStream_t s; ~Restore() { o->stream = s; } } restore{stiff, saved};
+    CK(cudaStreamSynchronize(saved));
+    if ((rc = ensure_solver_buffers(stage))) return rc;
+    for (double **b : {&stage->sd_u, &stage->sd_k1, &stage->sd_w})
+        if (!*b && (rc = alloc_vec(b, stage->Nn))) return rc;
+    const int64_t n = stage->Nn;
+    const double g = 1.0 - std::sqrt(0.5);
+    if ((rc = to_native(stage, stage->sd_u, u, mem))) return rc;
+    CK(cudaMemsetAsync(stage->xw, 0, sizeof(double) * n, stage->stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    CK(cudaEventRecord(e0, stage->stream));
+    int64_t total_it = 0, applies = 0;
+    int max_it = 0, failed = 0;
+    auto stage_solve = [&](const double *ucur) -> int {
+        int r2 = apply_native(stiff, ucur, stage->sd_w, 0, 1, nullptr);
+        if (r2) return r2;
+        ++applies;
+        k_lincomb2<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->bw, -1.0, stage->sd_w, 0.0,
+                                                                 stage->sd_w);
+        CK(cudaGetLastError());
+        fg_result r{};
+        const int st = pcg_core(stage, cfg, &r);
+        if (st != FG_OK && st != FG_CONVERGENCE_FAILED && st != FG_BREAKDOWN) return st;
+        if (st != FG_OK) ++failed;
+        total_it += r.iterations;
+        applies += r.applies;
+        max_it = std::max(max_it, (int)r.iterations);
+        return FG_OK;
+    };
+    for (int step = 0; step < n_steps; ++step) {
+        if ((rc = stage_solve(stage->sd_u))) return rc;                 // k1 in xw
+        CK(cudaMemcpyAsync(stage->sd_k1, stage->xw, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                           stage->stream));
+        // u2 = u + dt (1-g) k1 (held in the solver's r buffer until the stiff apply reads it)
+        k_lincomb2<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->r, 1.0, stage->sd_u,
+                                                                 dt * (1.0 - g), stage->sd_k1);
+        if ((rc = apply_native(stiff, stage->r, stage->sd_w, 0, 1, nullptr))) return rc;
+        ++applies;
+        k_lincomb2<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->bw, -1.0, stage->sd_w, 0.0,
+                                                                 stage->sd_w);
+        {
+            fg_result r{};
+            const int st = pcg_core(stage, cfg, &r);                     // k2 in xw (warm: k1)
+            if (st != FG_OK && st != FG_CONVERGENCE_FAILED && st != FG_BREAKDOWN) return st;
+            if (st != FG_OK) ++failed;
+            total_it += r.iterations;
+            applies += r.applies;
+            max_it = std::max(max_it, (int)r.iterations);
+        }
+        // u += dt (1-g) k1 + dt g k2
+        k_lincomb2<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->sd_w, dt * (1.0 - g),
+                                                                 stage->sd_k1, dt * g, stage->xw);
+        k_lincomb2<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->sd_u, 1.0, stage->sd_u, 1.0,
+                                                                 stage->sd_w);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(e1, stage->stream));
+    if ((rc = from_native(stage, u, stage->sd_u, mem))) return rc;
+    CK(cudaStreamSynchronize(stage->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (out) {
+        out->steps = n_steps;
+        out->total_iterations = total_it;
+        out->max_stage_iterations = max_it;
+        out->failed_solves = failed;
+        out->applies = applies;
+        out->time_ms = ms;
+    }
+    if ((rc = check_device_error(stage))) return rc;
+    if (failed) return fail(FG_CONVERGENCE_FAILED, "%d stage solves did not converge", failed);
+    t_last_status = FG_OK;
+    return FG_OK;
 }
 
 }  // extern "C"

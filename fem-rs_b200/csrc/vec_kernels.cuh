@@ -580,4 +580,16 @@ __global__ void __launch_bounds__(VEC_THREADS) k_jacobi_rz(int64_t n, const T *_
     }
 }
 
+// out = a x + b y   (FP64; SDIRK stage combinations)
+__global__ void __launch_bounds__(VEC_THREADS) k_lincomb2(int64_t n, double *__restrict__ out, double a,
+                                                          const double *__restrict__ x, double b,
+                                                          const double *__restrict__ y) {
+    FG_VEC4_LOOP(q, n) {
+        const V4<double> xv = ld4(x, q), yv = ld4(y, q);
+        V4<double> o;
+        FG_K4 o.a[k] = a * xv.a[k] + b * yv.a[k];
+        st4(out, q, o);
+    }
+}
+
 }  // namespace fg

@@ -39,7 +39,7 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_op_layout", "fg_op_native_len", "fg_op_set_stream", "fg_op_apply",
            "fg_op_apply_native", "fg_op_diagonal", "fg_pcg", "fg_op_check",
            "fg_op_apply_native_noalloc", "fg_op_apply_f32", "fg_op_apply_native_f32",
-           "fg_op_set_qdata_format")
+           "fg_op_set_qdata_format", "fg_sdirk2")
 
 
 class FgMesh(C.Structure):
@@ -52,6 +52,12 @@ class FgCfg(C.Structure):
                 ("precision", C.c_int32), ("power_iters", C.c_int32), ("lmax", C.c_double),
                 ("lmin_ratio", C.c_double), ("lmax_safety", C.c_double), ("inner_rtol", C.c_double),
                 ("check_interval", C.c_int32), ("reserved", C.c_int32)]
+
+
+class FgSdirkResult(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("max_stage_iterations", C.c_int32), ("total_iterations", C.c_int64),
+                ("failed_solves", C.c_int32), ("reserved", C.c_int32), ("applies", C.c_int64),
+                ("time_ms", C.c_double)]
 
 
 class FgResult(C.Structure):
@@ -89,6 +95,7 @@ def lib():
         L.fg_op_check.argtypes = [vp]
         L.fg_op_apply_f32.argtypes = [vp, vp, vp, i, i, i]
         L.fg_op_set_qdata_format.argtypes = [vp, i]
+        L.fg_sdirk2.argtypes = [vp, vp, vp, d, i, vp, vp, i]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
@@ -386,6 +393,23 @@ def solve_pcg_chebyshev(op: PAOperator, b, x, cfg=None):
     """PCG with a Chebyshev(D^-1 A) preconditioner of cfg.cheb_degree sweeps."""
     cfg = cfg or SolverConfig()
     return op.pcg(b, x, cfg, PC_CHEBYSHEV)
+
+
+SDIRK2_GAMMA = 1.0 - 2.0 ** -0.5  # crates/solver/src/ode.rs:441
+
+
+def sdirk2(stiff: PAOperator, stage: PAOperator, u, dt, n_steps, cfg=None, precond=PC_JACOBI):
+    """SDIRK-2 heat stepping (examples/mfem_ex10_heat_equation.rs:201-250) on the
+    device; ``stage`` must be M + gamma*dt*K.  ``u`` is updated in place.
+    Returns a dict with iteration counts and the device time."""
+    cfg = cfg or SolverConfig(rtol=1e-10)
+    pu, mu = _as_f64(u)
+    r = FgSdirkResult()
+    rc = lib().fg_sdirk2(stiff.handle, stage.handle, pu, float(dt), int(n_steps),
+                         C.byref(cfg.to_c(precond)), C.byref(r), mu)
+    _check(rc)
+    return dict(steps=r.steps, total_iterations=int(r.total_iterations),
+                max_stage_iterations=r.max_stage_iterations, applies=int(r.applies), time_ms=r.time_ms)
 
 
 def unit_cube_vertices(nx, ny, nz):

@@ -213,6 +213,26 @@ FG_API int fg_op_diagonal(fg_op *op, double *d, int constrained, int mem);
 FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg, fg_result *res,
                   int mem);
 
+typedef struct {
+    int32_t steps;
+    int32_t max_stage_iterations;
+    int64_t total_iterations;  /* PCG iterations over all stage solves */
+    int32_t failed_solves;
+    int32_t reserved;
+    int64_t applies;
+    double time_ms;            /* device time of the stepping loop */
+} fg_sdirk_result;
+
+/* SDIRK-2 heat stepping M u_t + K u = 0 with the constrained operators
+ * (examples/mfem_ex10_heat_equation.rs:201-250; gamma = 1 - 1/sqrt(2),
+ * crates/solver/src/ode.rs:441).  `stiff` is K (FG_DIFF); `stage` is
+ * M + gamma*dt*K (FG_MASS_DIFF with c_mass = 1, c_diff = gamma*dt) on the same
+ * mesh.  Each stage solves (M + gamma dt K) k = -K u_stage with fg_pcg's
+ * solver and cfg, warm-started from the previous stage's k.  u: initial
+ * condition in (zero on the Dirichlet DOFs), u(n_steps*dt) out. */
+FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_steps,
+                     const fg_cfg *cfg, fg_sdirk_result *res, int mem);
+
 /* Synchronise the handle's stream and report device-side errors
  * (FG_DEVICE_TIMEOUT, FG_BOUNDS). */
 FG_API int fg_op_check(fg_op *op);
