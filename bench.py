@@ -206,6 +206,10 @@ def main():
     ap.add_argument("--workload", default="c1a", choices=sorted(WORKLOADS))
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-heat", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-n", type=int, default=256)
+    ap.add_argument("--heat-steps", type=int, default=500)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -370,6 +374,86 @@ def main():
     op.set_qdata_format(femgpu.QDATA_FULL)
     fp32_apply = variants
 
+    # SDIRK-2 heat stepping, 64^3 Q2, lognormal kappa, dt = 1e-3,
+    # u0 = sin sin sin; FP64 stage solves vs FP32 (reliable-update) stage solves
+    heat = None
+    if not args.no_heat:
+        hn, hp, dt = 64, 2, 1e-3
+        hk = lognormal_kappa_q(hn, hn, hn, hp, sigma2=1.0, ell=0.1, seed=rank)
+        K = femgpu.PADiffusionOperator((hn, hn, hn), hp, kappa=hk)
+        S = femgpu.PAMassDiffusionOperator((hn, hn, hn), hp, 1.0, femgpu.SDIRK2_GAMMA * dt, kappa=hk)
+        K.set_stream(stream.cuda_stream)
+        S.set_stream(stream.cuda_stream)
+        xs1 = np.linspace(0, 1, hn * hp + 1)
+        u0 = (np.sin(np.pi * xs1)[:, None, None] * np.sin(np.pi * xs1)[None, :, None]
+              * np.sin(np.pi * xs1)[None, None, :]).ravel()
+        u0.reshape(hn * hp + 1, hn * hp + 1, hn * hp + 1)[[0, -1], :, :] = 0.0
+        u0.reshape(hn * hp + 1, hn * hp + 1, hn * hp + 1)[:, [0, -1], :] = 0.0
+        u0.reshape(hn * hp + 1, hn * hp + 1, hn * hp + 1)[:, :, [0, -1]] = 0.0
+        heat = {"workload": f"{hn}^3 Q2 SDIRK-2, dt={dt}, {args.heat_steps} steps, stage rtol 1e-10, warm start"}
+        finals = {}
+        for name, prec, pc in (("fp64_chebyshev4", femgpu.FP64, femgpu.PC_CHEBYSHEV),
+                               ("fp32_chebyshev4", femgpu.FP32_IR, femgpu.PC_CHEBYSHEV)):
+            u = u0.copy()
+            info = femgpu.sdirk2(K, S, u, dt, args.heat_steps,
+                                 femgpu.SolverConfig(rtol=1e-10, max_iter=5000, precision=prec), pc)
+            finals[name] = u
+            heat[name] = {"time_s": info["time_ms"] / 1e3, "stage_iterations": info["total_iterations"],
+                          "max_stage_iterations": info["max_stage_iterations"], "applies": info["applies"]}
+        ref = finals["fp64_chebyshev4"]
+        for name in finals:
+            heat[name]["rel_l2_diff_vs_fp64_chebyshev"] = float(np.linalg.norm(finals[name] - ref) / np.linalg.norm(ref))
+        K.close()
+        S.close()
+
+    # batched uneven solves, n ~ U{8..48}, p ~ U{1,2,3}, own lognormal
+    # kappa (sigma2 ~ U[0.25,2], ell ~ U[0.05,0.3]) and RHS M xi, FP32 mixed precision
+    batch = None
+    if not args.no_batch:
+        brng = np.random.default_rng(7000 + rank)
+        bops, bbs = [], []
+        total = 0
+        t_setup = time.perf_counter()
+        for i in range(args.batch_n):
+            bn, bp = int(brng.integers(8, 49)), int(brng.integers(1, 4))
+            kq = lognormal_kappa_q(bn, bn, bn, bp, sigma2=float(brng.uniform(0.25, 2.0)),
+                                   ell=float(brng.uniform(0.05, 0.3)), seed=100000 * rank + i, device=dev)
+            o = femgpu.PADiffusionOperator((bn, bn, bn), bp, kappa=kq)
+            m = femgpu.PAMassOperator((bn, bn, bn), bp)
+            xi = brng.standard_normal(o.n_dofs())
+            bb = m.matvec(xi)
+            m.close()
+            bb3 = bb.reshape(o.NK, o.NJ, o.NI)
+            bb3[[0, -1]] = 0.0
+            bb3[:, [0, -1]] = 0.0
+            bb3[:, :, [0, -1]] = 0.0
+            bops.append(o)
+            bbs.append(bb)
+            total += o.n_dofs()
+        t_setup = time.perf_counter() - t_setup
+        cfgb = femgpu.SolverConfig(rtol=1e-8, max_iter=5000, precision=femgpu.FP32_IR, check_interval=10)
+        bxs = [np.zeros_like(v) for v in bbs]
+        ok, bres = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
+        t_batch = bres[0].solve_ms / 1e3
+        # the same solves one after another (single-instance launches)
+        t_seq = 0.0
+        seq_iters = []
+        for o, v in zip(bops, bbs):
+            xs1 = np.zeros_like(v)
+            r1 = o.pcg(v, xs1, cfgb, femgpu.PC_CHEBYSHEV)
+            t_seq += r1.solve_ms / 1e3
+            seq_iters.append(r1.iterations)
+        batch = {"instances": len(bops), "total_dofs": total, "all_converged": bool(ok),
+                 "max_true_residual": max(r.true_residual for r in bres),
+                 "iterations_min_max": [min(r.iterations for r in bres), max(r.iterations for r in bres)],
+                 "max_iteration_diff_vs_single": int(max(abs(a.iterations - b) for a, b in zip(bres, seq_iters))),
+                 "batched_solve_s": t_batch, "sequential_single_solves_s": t_seq,
+                 "speedup_batched_vs_sequential": t_seq / t_batch,
+                 "dof_iterations_per_s": sum(o.n_dofs() * r.iterations for o, r in zip(bops, bres)) / t_batch,
+                 "setup_s": t_setup}
+        for o in bops:
+            o.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -401,6 +485,8 @@ def main():
             "cpu_baseline": cpu,
             "solve": solve,
             "apply_variants": fp32_apply,
+            "heat": heat,
+            "batch": batch,
         }
         print(json.dumps(out), flush=True)
     op.close()

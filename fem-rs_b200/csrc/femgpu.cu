@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -1084,6 +1085,83 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
     return status;
 }
 
+// ---------------------------------------------------------------------------
+// Batched mixed-precision PCG (many independent operators in one launch per
+// phase).  Helpers live outside extern "C" (templates).
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+template <int P, typename T, int FMT>
+static int encode_xmap_t(const Grid &g, const T *x, CUtensorMap *tmap) {
+    using C = KC<P, T>;
+    constexpr int S = FMT == 0 ? C::S : 2;
+    using SM = ApplySmem<P, T, C::WY, S, 1>;
+    cuuint64_t gdim[3] = {(cuuint64_t)g.NI, (cuuint64_t)g.NJ, (cuuint64_t)g.NK};
+    cuuint64_t gstr[2] = {(cuuint64_t)g.NIp * sizeof(T), (cuuint64_t)g.NIp * g.NJ * sizeof(T)};
+    cuuint32_t box[3] = {(cuuint32_t)SM::XW, (cuuint32_t)SM::RY, (cuuint32_t)(P + 1)};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult cr = g_encode(tmap, TmapType<T>::v, 3, const_cast<T *>(x), gdim, gstr, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
+    return FG_OK;
+}
+template <typename T> static int encode_xmap(fg_op *op, const T *x, CUtensorMap *tmap) {
+    switch (op->p) {
+    case 1: return encode_xmap_t<1, T, 0>(op->g, x, tmap);
+    case 2: return encode_xmap_t<2, T, 0>(op->g, x, tmap);
+    default: return encode_xmap_t<3, T, 0>(op->g, x, tmap);
+    }
+}
+
+struct BatchGroup {
+    int p, kind, fmt;
+    std::vector<int> inst;
+    int2 *bmap = nullptr;
+    int nblocks = 0;
+};
+
+template <int P, int OPK, typename T, int FMT>
+static int launch_batched_t(cudaStream_t st, const BatchGroup &G, const ApplyArgs<T> *args,
+                            const CUtensorMap *tm, int nslots, int slot) {
+    using C = KC<P, T>;
+    constexpr int S = FMT == 0 ? C::S : 2;
+    using SM = ApplySmem<P, T, C::WY, S, stage_elems<P, OPK, FMT>() / 32>;
+    auto kern = pa_apply_batched_kernel<P, OPK, T, C::WY, S, C::MINB, FMT>;
+    static bool attr_set[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (!attr_set[dev]) {  // set once, before any capture (see fg_batch_pcg)
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
+        attr_set[dev] = true;
+    }
+    if (!args) return FG_OK;  // attribute preparation only
+    BatchApply<T> B{args, tm, G.bmap, nslots, slot};
+    kern<<<G.nblocks, C::WY * 32, SM::bytes, st>>>(B);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+template <typename T>
+static int launch_batched(cudaStream_t st, const BatchGroup &G, const ApplyArgs<T> *args,
+                          const CUtensorMap *tm, int nslots, int slot) {
+#define FG_BL(P_, K_, F_) \
+    if (G.p == P_ && G.kind == K_ && G.fmt == F_) return launch_batched_t<P_, K_, T, F_>(st, G, args, tm, nslots, slot);
+    FG_BL(1, 1, 0) FG_BL(1, 2, 0) FG_BL(1, 3, 0) FG_BL(2, 1, 0) FG_BL(2, 2, 0) FG_BL(2, 3, 0)
+    FG_BL(3, 1, 0) FG_BL(3, 2, 0) FG_BL(3, 3, 0)
+    FG_BL(1, 1, 1) FG_BL(1, 2, 1) FG_BL(1, 3, 1) FG_BL(2, 1, 1) FG_BL(2, 2, 1) FG_BL(2, 3, 1)
+    FG_BL(3, 1, 1) FG_BL(3, 2, 1) FG_BL(3, 3, 1)
+#undef FG_BL
+    return fail(FG_UNSUPPORTED, "no batched kernel for this order/kind/format");
+}
+
+template <typename T> static int dev_upload(T **dst, const std::vector<T> &v) {
+    CK(cudaMalloc(dst, sizeof(T) * std::max<size_t>(v.size(), 1)));
+    CK(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return FG_OK;
+}
+
+extern "C" {
+
 FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, fg_result *res,
                   int mem) {
     if (!op || !b || !x) return fail(FG_INVALID_ARGUMENT, "NULL argument");
@@ -1104,6 +1182,258 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
         else fail(status, "solver did not converge in %d iterations", cfg.max_iter);
     }
     return status;
+}
+
+// Batched solves (configs[2] form): every operator is solved by the
+// mixed-precision PCG (FP32 applies and smoother, FP64 reliable updates and
+// dot products) of fg_pcg, but each phase of an iteration is one launch over
+// all instances (per order/kind/format group for the applies), converged
+// instances are masked per instance on the device, and chunks of
+// check_interval iterations are captured once in a CUDA graph and replayed.
+FG_API int fg_batch_pcg(fg_op *const *ops, int n, const double *const *b, double *const *x,
+                        const fg_cfg *cfg_in, fg_result *results, int mem) {
+    if (!ops || n <= 0 || !b || !x) return fail(FG_INVALID_ARGUMENT, "bad batch arguments");
+    fg_cfg cfg;
+    if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
+    int rc;
+    if ((rc = validate_cfg(cfg))) return rc;
+    if (cfg.precision != FG_FP32_IR)
+        return fail(FG_UNSUPPORTED, "batched solves run the FP32 mixed-precision form only");
+    if (cfg.precond != FG_PC_JACOBI && cfg.precond != FG_PC_CHEBYSHEV)
+        return fail(FG_UNSUPPORTED, "batched solves need the Jacobi or Chebyshev preconditioner");
+    const bool cheb = cfg.precond == FG_PC_CHEBYSHEV;
+    if (cheb && cfg.cheb_degree > BATCH_MAXK) return fail(FG_INVALID_ARGUMENT, "cheb_degree too large");
+    std::vector<fg_op *> sorted(ops, ops + n);
+    for (int i = 0; i < n; ++i)
+        if (!ops[i] || !b[i] || !x[i]) return fail(FG_INVALID_ARGUMENT, "NULL instance %d", i);
+    std::sort(sorted.begin(), sorted.end());
+    if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+        return fail(FG_INVALID_ARGUMENT, "an operator appears twice in the batch");
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (fg_op *o : sorted) locks.emplace_back(o->mu);
+    const int dev = ops[0]->device;
+    for (int i = 0; i < n; ++i)
+        if (ops[i]->device != dev) return fail(FG_INVALID_ARGUMENT, "batch spans devices");
+    CK(cudaSetDevice(dev));
+    // per-instance preparation on each operator's own stream
+    std::vector<double> lmax(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        fg_op *o = ops[i];
+        if ((rc = ensure_solver_buffers(o)) || (rc = ensure_fp32(o)) || (rc = ensure_dinv32(o))) return rc;
+        if (cheb) {
+            if (cfg.lmax > 0) lmax[i] = cfg.lmax;
+            else {
+                if (!o->have_lmax) {
+                    if ((rc = estimate_lmax(o, cfg.power_iters > 0 ? cfg.power_iters : 20, &o->lmax_est)))
+                        return rc;
+                    o->have_lmax = true;
+                }
+                lmax[i] = (cfg.lmax_safety > 0 ? cfg.lmax_safety : 1.1) * o->lmax_est;
+            }
+        }
+        if ((rc = to_native(o, o->bw, b[i], mem)) || (rc = to_native(o, o->xw, x[i], mem))) return rc;
+        CK(cudaStreamSynchronize(o->stream));
+    }
+    cudaStream_t bs;
+    CK(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+    // device tables
+    constexpr int VBX = 64;
+    std::vector<ApplyArgs<float>> a32(2 * n);
+    std::vector<ApplyArgs<double>> a64(n);
+    std::vector<CUtensorMap> t32(2 * n), t64(n);
+    std::vector<FixArgs<float>> f32(2 * n);
+    std::vector<FixArgs<double>> f64(n);
+    std::vector<BatchVec> bv(n);
+    SolverState *d_st = nullptr;
+    double *d_part = nullptr;
+    CK(cudaMalloc(&d_st, sizeof(SolverState) * n));
+    CK(cudaMalloc(&d_part, sizeof(double) * 2 * VBX * n));
+    std::vector<SolverState> hst(n);
+    for (int i = 0; i < n; ++i) {
+        fg_op *o = ops[i];
+        Grid g = o->g;
+        g.ess = o->ess_tags;
+        const float *q32 = qdata_of<float>(o);
+        const double *q64 = qdata_of<double>(o);
+        a32[2 * i] = ApplyArgs<float>{g, q32, o->ap32, o->face32, 0, o->d_err, &d_st[i].done};
+        a32[2 * i + 1] = ApplyArgs<float>{g, q32, o->ct32, o->face32, 0, o->d_err, &d_st[i].done};
+        a64[i] = ApplyArgs<double>{g, q64, o->ap, o->face, 0, o->d_err, &d_st[i].skip_rel};
+        if ((rc = encode_xmap<float>(o, o->p32, &t32[2 * i])) ||
+            (rc = encode_xmap<float>(o, o->cd32, &t32[2 * i + 1])) ||
+            (rc = encode_xmap<double>(o, o->xw, &t64[i])))
+            return rc;
+        f32[2 * i] = FixArgs<float>{g, o->ap32, o->face32, &d_st[i].done};
+        f32[2 * i + 1] = FixArgs<float>{g, o->ct32, o->face32, &d_st[i].done};
+        f64[i] = FixArgs<double>{g, o->ap, o->face, &d_st[i].skip_rel};
+        BatchVec &B = bv[i];
+        B.n = o->Nn;
+        B.x64 = o->xw; B.b64 = o->bw; B.ap64 = o->ap;
+        B.r = o->r32; B.z = o->z32; B.p = o->p32; B.ap = o->ap32; B.e = o->e32;
+        B.cres = o->cres32; B.cd = o->cd32; B.ct = o->ct32; B.dinv = o->dinv32;
+        B.partials = d_part + (size_t)2 * VBX * i;
+        B.st = &d_st[i];
+        if (cheb) {
+            const ChebCoef cc = cheb_coefs(lmax[i] / (cfg.lmin_ratio > 0 ? cfg.lmin_ratio : 30.0), lmax[i],
+                                           cfg.cheb_degree);
+            B.inv_theta = cc.inv_theta;
+            for (size_t k = 0; k < cc.c1.size(); ++k) { B.c1[k] = cc.c1[k]; B.c2[k] = cc.c2[k]; }
+        }
+        SolverState &h = hst[i];
+        h = SolverState{};
+        h.rtol = cfg.rtol; h.atol = cfg.atol; h.max_iter = cfg.max_iter;
+        h.delta = (cfg.inner_rtol > 0 && cfg.inner_rtol < 1) ? cfg.inner_rtol : 0.1;
+        h.skip_rel = 0;  // the initial FP64 residual always runs
+    }
+    // groups of equal (order, kind, format); block maps
+    std::vector<BatchGroup> groups;
+    for (int i = 0; i < n; ++i) {
+        fg_op *o = ops[i];
+        auto it = std::find_if(groups.begin(), groups.end(), [&](const BatchGroup &G) {
+            return G.p == o->p && G.kind == o->kind && G.fmt == o->fmt;
+        });
+        if (it == groups.end()) { groups.push_back(BatchGroup{o->p, o->kind, o->fmt, {}}); it = groups.end() - 1; }
+        it->inst.push_back(i);
+    }
+    ApplyArgs<float> *d_a32 = nullptr;
+    ApplyArgs<double> *d_a64 = nullptr;
+    CUtensorMap *d_t32 = nullptr, *d_t64 = nullptr;
+    FixArgs<float> *d_f32 = nullptr;
+    FixArgs<double> *d_f64 = nullptr;
+    BatchVec *d_bv = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    auto cleanup = [&]() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto &G : groups) if (G.bmap) cudaFree(G.bmap);
+        void *ptrs[] = {d_a32, d_a64, d_t32, d_t64, d_f32, d_f64, d_bv, d_st, d_part};
+        for (void *p : ptrs) if (p) cudaFree(p);
+        cudaStreamDestroy(bs);
+    };
+    struct Guard { std::function<void()> f; ~Guard() { f(); } } guard{cleanup};
+    for (auto &G : groups) {
+        std::vector<int2> m;
+        for (int i : G.inst)
+            for (int it = 0; it < ops[i]->g.n_items(); ++it) m.push_back(make_int2(i, it));
+        G.nblocks = (int)m.size();
+        if ((rc = dev_upload(&G.bmap, m))) return rc;
+    }
+    if ((rc = dev_upload(&d_a32, a32)) || (rc = dev_upload(&d_a64, a64)) || (rc = dev_upload(&d_t32, t32)) ||
+        (rc = dev_upload(&d_t64, t64)) || (rc = dev_upload(&d_f32, f32)) || (rc = dev_upload(&d_f64, f64)) ||
+        (rc = dev_upload(&d_bv, bv)))
+        return rc;
+    CK(cudaMemcpy(d_st, hst.data(), sizeof(SolverState) * n, cudaMemcpyHostToDevice));
+    const dim3 vgrid(VBX, n), fgrid(64, n);
+    auto apply32 = [&](int slot) -> int {
+        for (auto &G : groups) {
+            int r2 = launch_batched<float>(bs, G, d_a32, d_t32, 2, slot);
+            if (r2) return r2;
+        }
+        fixup_batched_kernel<float><<<fgrid, 128, 0, bs>>>(d_f32, 2, slot);
+        CK(cudaGetLastError());
+        return FG_OK;
+    };
+    auto apply64 = [&]() -> int {
+        for (auto &G : groups) {
+            int r2 = launch_batched<double>(bs, G, d_a64, d_t64, 1, 0);
+            if (r2) return r2;
+        }
+        fixup_batched_kernel<double><<<fgrid, 128, 0, bs>>>(d_f64, 1, 0);
+        CK(cudaGetLastError());
+        return FG_OK;
+    };
+    auto precond = [&](int init) -> int {
+        if (cheb) {
+            kb_cheb_first<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv);
+            for (int sidx = 0; sidx + 1 < cfg.cheb_degree; ++sidx) {
+                int r2 = apply32(1);
+                if (r2) return r2;
+                kb_cheb_step<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, sidx);
+            }
+            kb_rz<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, init, 0);
+        } else {
+            kb_rz<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, init, 1);
+        }
+        kb_pupdate<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, init);
+        CK(cudaGetLastError());
+        return FG_OK;
+    };
+    for (auto &G : groups)  // kernel attributes are set outside the graph capture
+        if ((rc = launch_batched<float>(bs, G, nullptr, nullptr, 2, 0)) ||
+            (rc = launch_batched<double>(bs, G, nullptr, nullptr, 1, 0)))
+            return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    CK(cudaEventRecord(e0, bs));
+    kb_zero_e<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv);
+    if ((rc = apply64())) return rc;
+    kb_rel_residual<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, 1);
+    if ((rc = precond(1))) return rc;
+    // one chunk of iterations, captured once and replayed
+    const int chunk = std::max(1, cfg.check_interval);
+    CK(cudaStreamBeginCapture(bs, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < chunk; ++k) {
+        if ((rc = apply32(0))) { cudaStreamEndCapture(bs, &graph); return rc; }
+        kb_pap<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv);
+        kb_rel_step<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv);
+        kb_rel_xupdate<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv);
+        if ((rc = apply64())) { cudaStreamEndCapture(bs, &graph); return rc; }
+        kb_rel_residual<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, 0);
+        if ((rc = precond(0))) { cudaStreamEndCapture(bs, &graph); return rc; }
+    }
+    CK(cudaStreamEndCapture(bs, &graph));
+    CK(cudaGraphInstantiate(&gexec, graph, 0));
+    int launched = 0;
+    while (launched < cfg.max_iter) {
+        CK(cudaGraphLaunch(gexec, bs));
+        launched += chunk;
+        CK(cudaMemcpyAsync(hst.data(), d_st, sizeof(SolverState) * n, cudaMemcpyDeviceToHost, bs));
+        CK(cudaStreamSynchronize(bs));
+        bool all = true;
+        for (int i = 0; i < n && all; ++i) all = hst[i].done != 0;
+        if (all) break;
+    }
+    CK(cudaEventRecord(e1, bs));
+    // true residuals in FP64 (every instance)
+    for (int i = 0; i < n; ++i) hst[i].skip_rel = 0;
+    for (int i = 0; i < n; ++i)
+        CK(cudaMemcpyAsync(&d_st[i].skip_rel, &hst[i].skip_rel, sizeof(int), cudaMemcpyHostToDevice, bs));
+    if ((rc = apply64())) return rc;
+    kb_true_residual<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(hst.data(), d_st, sizeof(SolverState) * n, cudaMemcpyDeviceToHost, bs));
+    CK(cudaStreamSynchronize(bs));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int nfail = 0;
+    for (int i = 0; i < n; ++i) {
+        fg_op *o = ops[i];
+        if ((rc = from_native(o, x[i], o->xw, mem))) return rc;
+        const SolverState &h = hst[i];
+        const int status = h.converged ? FG_OK : (h.breakdown ? FG_BREAKDOWN : FG_CONVERGENCE_FAILED);
+        if (status != FG_OK) ++nfail;
+        if (results) {
+            fg_result &r = results[i];
+            r.converged = h.converged;
+            r.iterations = h.converged ? h.iter : (h.breakdown ? h.iter : cfg.max_iter);
+            r.final_residual = h.res;
+            r.true_residual = h.tmp[0];
+            r.status = status;
+            r.outer_iterations = (int)h.tmp[1];
+            r.applies = (int64_t)h.iter * (1 + (cheb ? cfg.cheb_degree - 1 : 0));
+            r.lmax = lmax[i];
+            r.solve_ms = ms;
+        }
+    }
+    for (int i = 0; i < n; ++i) CK(cudaStreamSynchronize(ops[i]->stream));
+    for (int i = 0; i < n; ++i)
+        if ((rc = check_device_error(ops[i]))) return rc;
+    if (nfail) return fail(FG_CONVERGENCE_FAILED, "%d of %d batched solves did not converge", nfail, n);
+    t_last_status = FG_OK;
+    return FG_OK;
 }
 
 // SDIRK-2 heat stepping (examples/mfem_ex10_heat_equation.rs:201-250,
@@ -1144,6 +1474,28 @@ FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_ste
     CK(cudaEventRecord(e0, stage->stream));
     int64_t total_it = 0, applies = 0;
     int max_it = 0, failed = 0;
+    // Each stage is solved for b/||b|| (and the warm start scaled alike), then
+    // scaled back: CG is scale-invariant, but the reference's absolute
+    // breakdown test |p^T A p| < 1e-30 (par_solver.rs:294) would otherwise trip
+    // once the decaying solution makes the stage right-hand sides tiny.
+    double *scal = nullptr;  // ||b|| kept in a device scalar between the two calls
+    auto normalise = [&](bool before) -> int {
+        if (before) {
+            k_norm_tmp<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->bw, stage->partials, stage->st);
+            k_scale_tmp<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->bw, stage->st, 1);
+            k_scale_tmp<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->xw, stage->st, 1);
+            CK(cudaMemcpyAsync(scal, &stage->st->tmp[2], sizeof(double), cudaMemcpyDeviceToDevice,
+                               stage->stream));
+        } else {
+            CK(cudaMemcpyAsync(&stage->st->tmp[2], scal, sizeof(double), cudaMemcpyDeviceToDevice,
+                               stage->stream));
+            k_scale_tmp<<<VEC_GRID, VEC_THREADS, 0, stage->stream>>>(n, stage->xw, stage->st, 0);
+        }
+        CK(cudaGetLastError());
+        return FG_OK;
+    };
+    CK(cudaMalloc(&scal, sizeof(double)));
+    struct FreeScal { double *p; ~FreeScal() { cudaFree(p); } } free_scal{scal};
     auto stage_solve = [&](const double *ucur) -> int {
         int r2 = apply_native(stiff, ucur, stage->sd_w, 0, 1, nullptr);
         if (r2) return r2;
@@ -1152,8 +1504,11 @@ FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_ste
                                                                  stage->sd_w);
         CK(cudaGetLastError());
         fg_result r{};
-        const int st = pcg_core(stage, cfg, &r);
+        int st = normalise(true);
+        if (st) return st;
+        st = pcg_core(stage, cfg, &r);
         if (st != FG_OK && st != FG_CONVERGENCE_FAILED && st != FG_BREAKDOWN) return st;
+        if (int s2 = normalise(false)) return s2;
         if (st != FG_OK) ++failed;
         total_it += r.iterations;
         applies += r.applies;
@@ -1173,8 +1528,11 @@ FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_ste
                                                                  stage->sd_w);
         {
             fg_result r{};
-            const int st = pcg_core(stage, cfg, &r);                     // k2 in xw (warm: k1)
+            int st = normalise(true);
+            if (st) return st;
+            st = pcg_core(stage, cfg, &r);                               // k2 in xw (warm: k1)
             if (st != FG_OK && st != FG_CONVERGENCE_FAILED && st != FG_BREAKDOWN) return st;
+            if (int s2 = normalise(false)) return s2;
             if (st != FG_OK) ++failed;
             total_it += r.iterations;
             applies += r.applies;

@@ -200,9 +200,9 @@ __device__ __forceinline__ void merge_and_store(T (&out)[P + 1][P + 1][P + 1], c
 // ---------------------------------------------------------------------------
 // The apply kernel.
 // ---------------------------------------------------------------------------
-template <int P, int OPK, typename T, int WY, int S, int MINB, int FMT = 0>
-__global__ void __launch_bounds__(WY * 32, MINB)
-    pa_apply_kernel(const __grid_constant__ CUtensorMap xmap, const ApplyArgs<T> A) {
+template <int P, int OPK, typename T, int WY, int S, int FMT>
+__device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const ApplyArgs<T> &A,
+                                              const int item) {
     constexpr int D = P + 1, Q = P + 1, NC = NComp<OPK>::v;
     constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
     constexpr int COLS = Q * Q;
@@ -214,6 +214,7 @@ __global__ void __launch_bounds__(WY * 32, MINB)
 
     if (A.skip && *A.skip) return;
     const Grid g = A.g;
+    const CUtensorMap &xmap = *xmap_ptr;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T *xs = reinterpret_cast<T *>(smem_raw);
     T *qs = reinterpret_cast<T *>(smem_raw + SM::off_q);
@@ -223,7 +224,6 @@ __global__ void __launch_bounds__(WY * 32, MINB)
     uint64_t *qbar = xbar + 2;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int item = blockIdx.x;
     const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty, tz = item / (g.ntx * g.nty);
     const int nl = min(g.TZ, g.nz - tz * g.TZ);
     const int ex = tx * 32 + lane, ey = ty * WY + warp;
@@ -478,6 +478,30 @@ __global__ void __launch_bounds__(WY * 32, MINB)
     }
 }
 
+// Single operator: one CTA per item; the x tile map is a kernel parameter.
+template <int P, int OPK, typename T, int WY, int S, int MINB, int FMT = 0>
+__global__ void __launch_bounds__(WY * 32, MINB)
+    pa_apply_kernel(const __grid_constant__ CUtensorMap xmap, const ApplyArgs<T> A) {
+    pa_apply_body<P, OPK, T, WY, S, FMT>(&xmap, A, blockIdx.x);
+}
+
+// Batched operators (many independent instances of the same order, kind and
+// format in one launch): block b works on item bmap[b].y of instance
+// bmap[b].x; each instance's arguments and x tile maps (one per input slot,
+// encoded once per batch, 64-byte aligned in global memory) come from tables.
+template <typename T> struct BatchApply {
+    const ApplyArgs<T> *args;    // [instance][slot]
+    const CUtensorMap *tmaps;    // [instance][slot]
+    const int2 *bmap;            // [block] -> (instance, item)
+    int nslots, slot;
+};
+template <int P, int OPK, typename T, int WY, int S, int MINB, int FMT = 0>
+__global__ void __launch_bounds__(WY * 32, MINB) pa_apply_batched_kernel(const BatchApply<T> B) {
+    const int2 m = B.bmap[blockIdx.x];
+    const int k = m.x * B.nslots + B.slot;
+    pa_apply_body<P, OPK, T, WY, S, FMT>(&B.tmaps[k], B.args[k], m.y);
+}
+
 // ---------------------------------------------------------------------------
 // Diagonal of the operator (Jacobi).  Same item decomposition and scatter; the
 // element diagonal sum_q g_i^T D_q g_i (+ m_q phi_i^2) is formed directly from
@@ -612,6 +636,46 @@ __global__ void __launch_bounds__(128) fixup_kernel(const Grid g, T *__restrict_
     if (g.is_ess(I, J, K)) return;  // final value written by the owner item
     const int64_t d = g.dof(I, J, K);
     y[d] = fixup_sum<T>(g, I, J, K, y[d], face);
+}
+
+// Batched fix-up: blockIdx.y = instance; blocks stride over the instance's
+// rows of shared-face DOFs (x planes: rows K of J, y planes: rows K of I,
+// z planes: rows J of I), threads over the row.
+template <typename T> struct FixArgs {
+    Grid g;
+    T *y;
+    const T *face;
+    const int *skip;
+};
+template <typename T>
+__global__ void __launch_bounds__(128) fixup_batched_kernel(const FixArgs<T> *args, int nslots,
+                                                            int slot) {
+    const FixArgs<T> &A = args[blockIdx.y * nslots + slot];
+    if (A.skip && *A.skip) return;
+    const Grid &g = A.g;
+    const int SXe = 32 * g.p, SYe = g.WY * g.p, SZe = g.TZ * g.p;
+    const int rx = (g.ntx - 1) * g.NK, ry = (g.nty - 1) * g.NK, rz = (g.ntz - 1) * g.NJ;
+    for (int r = blockIdx.x; r < rx + ry + rz; r += gridDim.x) {
+        int fam, pl, row, len;
+        if (r < rx) { fam = 0; pl = r / g.NK; row = r % g.NK; len = g.NJ; }
+        else if (r < rx + ry) { fam = 1; pl = (r - rx) / g.NK; row = (r - rx) % g.NK; len = g.NI; }
+        else { fam = 2; pl = (r - rx - ry) / g.NJ; row = (r - rx - ry) % g.NJ; len = g.NI; }
+        for (int u = threadIdx.x; u < len; u += blockDim.x) {
+            int I, J, K;
+            if (fam == 0) { I = (pl + 1) * SXe; J = u; K = row; }
+            else if (fam == 1) {
+                I = u; J = (pl + 1) * SYe; K = row;
+                if (I > 0 && I < g.NI - 1 && I % SXe == 0) continue;
+            } else {
+                I = u; J = row; K = (pl + 1) * SZe;
+                if (I > 0 && I < g.NI - 1 && I % SXe == 0) continue;
+                if (J > 0 && J < g.NJ - 1 && J % SYe == 0) continue;
+            }
+            if (g.is_ess(I, J, K)) continue;
+            const int64_t d = g.dof(I, J, K);
+            A.y[d] = fixup_sum<T>(g, I, J, K, A.y[d], A.face);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -592,4 +592,244 @@ __global__ void __launch_bounds__(VEC_THREADS) k_lincomb2(int64_t n, double *__r
     }
 }
 
+// ---- batched solves: blockIdx.y = instance ---------------------------------
+// Per-instance pointers, state and Chebyshev coefficients; reductions use the
+// instance's own partials and ticket (grid_sum over gridDim.x blocks).
+constexpr int BATCH_MAXK = 16;
+struct BatchVec {
+    int64_t n;
+    double *x64, *b64, *ap64;
+    float *r, *z, *p, *ap, *e, *cres, *cd, *ct;
+    const float *dinv;
+    double *partials;
+    SolverState *st;
+    double inv_theta;
+    double c1[BATCH_MAXK], c2[BATCH_MAXK];
+};
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_pap(const BatchVec *bv) {
+    const BatchVec &B = bv[blockIdx.y];
+    SolverState *st = B.st;
+    if (st->done) return;
+    double v[1] = {0.0};
+    FG_VEC4_LOOP(q, B.n) {
+        const V4<float> pv = ld4(B.p, q), av = ld4(B.ap, q);
+        FG_K4 v[0] += (double)pv.a[k] * (double)av.a[k];
+    }
+    double tot[1];
+    if (grid_sum<1>(v, B.partials, st, tot) && threadIdx.x == 0) {
+        st->pap = tot[0];
+        if (fabs(tot[0]) < 1e-30) {
+            st->breakdown = 1;
+            st->done = 1;
+            st->skip_rel = 1;
+        } else {
+            st->alpha = st->rz / tot[0];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_rel_step(const BatchVec *bv) {
+    const BatchVec &B = bv[blockIdx.y];
+    SolverState *st = B.st;
+    if (st->done) return;
+    const float alpha = (float)st->alpha;
+    double v[1] = {0.0};
+    FG_VEC4_LOOP(q, B.n) {
+        V4<float> xv = ld4(B.e, q), rv = ld4(B.r, q);
+        const V4<float> pv = ld4(B.p, q), av = ld4(B.ap, q);
+        FG_K4 {
+            xv.a[k] += alpha * pv.a[k];
+            rv.a[k] = rv.a[k] - alpha * av.a[k];
+            v[0] += (double)rv.a[k] * (double)rv.a[k];
+        }
+        st4(B.e, q, xv);
+        st4(B.r, q, rv);
+    }
+    double tot[1];
+    if (grid_sum<1>(v, B.partials, st, tot) && threadIdx.x == 0) {
+        st->iter += 1;
+        st->rr = tot[0];
+        const double rn = sqrt(tot[0]);
+        const int trig = (rn < st->delta * st->maxr) || (rn / st->bnorm < st->rtol) ||
+                         (rn < st->atol) || (st->iter >= st->max_iter);
+        st->trigger = trig;
+        st->skip_rel = !trig;
+    }
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_rel_xupdate(const BatchVec *bv) {
+    const BatchVec &B = bv[blockIdx.y];
+    if (!B.st->trigger) return;
+    FG_VEC4_LOOP(q, B.n) {
+        V4<double> xv = ld4(B.x64, q);
+        const V4<float> lv = ld4(B.e, q);
+        FG_K4 xv.a[k] += (double)lv.a[k];
+        st4(B.x64, q, xv);
+        st4(B.e, q, V4<float>{{0.0f, 0.0f, 0.0f, 0.0f}});
+    }
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_rel_residual(const BatchVec *bv, int init) {
+    const BatchVec &B = bv[blockIdx.y];
+    SolverState *st = B.st;
+    if (!init && !st->trigger) return;
+    double v[2] = {0.0, 0.0};
+    FG_VEC4_LOOP(q, B.n) {
+        const V4<double> bb = ld4(B.b64, q), av = ld4(B.ap64, q);
+        V4<float> rv;
+        FG_K4 {
+            const double ri = bb.a[k] - av.a[k];
+            rv.a[k] = (float)ri;
+            v[0] += ri * ri;
+            if (init) v[1] += bb.a[k] * bb.a[k];
+        }
+        st4(B.r, q, rv);
+    }
+    double tot[2];
+    if (grid_sum<2>(v, B.partials, st, tot) && threadIdx.x == 0) {
+        if (init) {
+            st->bb = tot[1];
+            st->bnorm = sqrt(tot[1]);
+            st->iter = 0;
+            st->converged = 0;
+            st->breakdown = 0;
+            st->done = 0;
+            st->tmp[1] = 0.0;
+        } else {
+            st->tmp[1] += 1.0;
+        }
+        const double rn = sqrt(tot[0]);
+        st->rr = tot[0];
+        st->maxr = rn;
+        st->res = st->bnorm > 0.0 ? rn / st->bnorm : 0.0;
+        st->trigger = 0;
+        st->skip_rel = 1;
+        if (st->bnorm < 1e-30 || st->res < st->rtol || rn < st->atol) {
+            st->converged = 1;
+            st->done = 1;
+        } else if (st->iter >= st->max_iter) {
+            st->done = 1;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_cheb_first(const BatchVec *bv) {
+    const BatchVec &B = bv[blockIdx.y];
+    if (B.st->done) return;
+    const float it = (float)B.inv_theta;
+    FG_VEC4_LOOP(q, B.n) {
+        const V4<float> rv = ld4(B.r, q), dv = ld4(B.dinv, q);
+        V4<float> sv, dd;
+        FG_K4 {
+            sv.a[k] = dv.a[k] * rv.a[k];
+            dd.a[k] = sv.a[k] * it;
+        }
+        st4(B.cres, q, sv);
+        st4(B.cd, q, dd);
+        st4(B.z, q, dd);
+    }
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_cheb_step(const BatchVec *bv, int s) {
+    const BatchVec &B = bv[blockIdx.y];
+    if (B.st->done) return;
+    const float a1 = (float)B.c1[s], a2 = (float)B.c2[s];
+    FG_VEC4_LOOP(q, B.n) {
+        const V4<float> tv = ld4(B.ct, q), dv = ld4(B.dinv, q);
+        V4<float> sv = ld4(B.cres, q), dd = ld4(B.cd, q), zv = ld4(B.z, q);
+        FG_K4 {
+            sv.a[k] = sv.a[k] - dv.a[k] * tv.a[k];
+            dd.a[k] = a1 * dd.a[k] + a2 * sv.a[k];
+            zv.a[k] += dd.a[k];
+        }
+        st4(B.cres, q, sv);
+        st4(B.cd, q, dd);
+        st4(B.z, q, zv);
+    }
+}
+
+// jacobi: z = dinv r first; then rz_new = r.z, beta (init: rz only)
+__global__ void __launch_bounds__(VEC_THREADS) kb_rz(const BatchVec *bv, int init, int jacobi) {
+    const BatchVec &B = bv[blockIdx.y];
+    SolverState *st = B.st;
+    if (st->done) return;
+    double v[1] = {0.0};
+    FG_VEC4_LOOP(q, B.n) {
+        const V4<float> rv = ld4(B.r, q);
+        V4<float> zv;
+        if (jacobi) {
+            const V4<float> dv = ld4(B.dinv, q);
+            FG_K4 zv.a[k] = dv.a[k] * rv.a[k];
+            st4(B.z, q, zv);
+        } else {
+            zv = ld4(B.z, q);
+        }
+        FG_K4 v[0] += (double)rv.a[k] * (double)zv.a[k];
+    }
+    double tot[1];
+    if (grid_sum<1>(v, B.partials, st, tot) && threadIdx.x == 0) {
+        if (!init) st->beta = tot[0] / st->rz;
+        st->rz = tot[0];
+    }
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_pupdate(const BatchVec *bv, int init) {
+    const BatchVec &B = bv[blockIdx.y];
+    if (B.st->done) return;
+    const float beta = init ? 0.0f : (float)B.st->beta;
+    FG_VEC4_LOOP(q, B.n) {
+        const V4<float> zv = ld4(B.z, q);
+        V4<float> pv = ld4(B.p, q);
+        FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        st4(B.p, q, pv);
+    }
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_zero_e(const BatchVec *bv) {
+    const BatchVec &B = bv[blockIdx.y];
+    FG_VEC4_LOOP(q, B.n) st4(B.e, q, V4<float>{{0.0f, 0.0f, 0.0f, 0.0f}});
+}
+
+__global__ void __launch_bounds__(VEC_THREADS) kb_true_residual(const BatchVec *bv) {
+    const BatchVec &B = bv[blockIdx.y];
+    SolverState *st = B.st;
+    double v[1] = {0.0};
+    FG_VEC4_LOOP(q, B.n) {
+        const V4<double> bb = ld4(B.b64, q), av = ld4(B.ap64, q);
+        FG_K4 {
+            const double s = bb.a[k] - av.a[k];
+            v[0] += s * s;
+        }
+    }
+    double tot[1];
+    if (grid_sum<1>(v, B.partials, st, tot) && threadIdx.x == 0)
+        st->tmp[0] = st->bnorm > 0.0 ? sqrt(tot[0]) / st->bnorm : 0.0;
+}
+
+// st->tmp[2] = ||v|| (FP64)
+__global__ void __launch_bounds__(VEC_THREADS) k_norm_tmp(int64_t n, const double *__restrict__ v,
+                                                          double *partials, SolverState *st) {
+    double a[1] = {0.0};
+    FG_VEC4_LOOP(q, n) {
+        const V4<double> x = ld4(v, q);
+        FG_K4 a[0] += x.a[k] * x.a[k];
+    }
+    double tot[1];
+    if (grid_sum<1>(a, partials, st, tot) && threadIdx.x == 0) st->tmp[2] = sqrt(tot[0]);
+}
+
+// v *= 1/tmp[2] (inverse = 1) or v *= tmp[2]; no-op when tmp[2] == 0
+__global__ void __launch_bounds__(VEC_THREADS) k_scale_tmp(int64_t n, double *__restrict__ v,
+                                                           const SolverState *st, int inverse) {
+    const double s = st->tmp[2];
+    if (!(s > 0.0)) return;
+    const double f = inverse ? 1.0 / s : s;
+    FG_VEC4_LOOP(q, n) {
+        V4<double> x = ld4(v, q);
+        FG_K4 x.a[k] *= f;
+        st4(v, q, x);
+    }
+}
+
 }  // namespace fg

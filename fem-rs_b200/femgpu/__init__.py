@@ -39,7 +39,7 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_op_layout", "fg_op_native_len", "fg_op_set_stream", "fg_op_apply",
            "fg_op_apply_native", "fg_op_diagonal", "fg_pcg", "fg_op_check",
            "fg_op_apply_native_noalloc", "fg_op_apply_f32", "fg_op_apply_native_f32",
-           "fg_op_set_qdata_format", "fg_sdirk2")
+           "fg_op_set_qdata_format", "fg_sdirk2", "fg_batch_pcg")
 
 
 class FgMesh(C.Structure):
@@ -96,6 +96,7 @@ def lib():
         L.fg_op_apply_f32.argtypes = [vp, vp, vp, i, i, i]
         L.fg_op_set_qdata_format.argtypes = [vp, i]
         L.fg_sdirk2.argtypes = [vp, vp, vp, d, i, vp, vp, i]
+        L.fg_batch_pcg.argtypes = [vp, i, vp, vp, vp, vp, i]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
@@ -393,6 +394,33 @@ def solve_pcg_chebyshev(op: PAOperator, b, x, cfg=None):
     """PCG with a Chebyshev(D^-1 A) preconditioner of cfg.cheb_degree sweeps."""
     cfg = cfg or SolverConfig()
     return op.pcg(b, x, cfg, PC_CHEBYSHEV)
+
+
+def batch_pcg(ops, bs, xs, cfg=None, precond=PC_CHEBYSHEV):
+    """Solve n independent systems together (fg_batch_pcg): FP32 mixed-precision
+    PCG, one launch per phase over all instances, CUDA-graph replayed.  Returns
+    (all_converged, [SolveResult])."""
+    cfg = cfg or SolverConfig(rtol=1e-8, precision=FP32_IR)
+    n = len(ops)
+    hs = (C.c_void_p * n)(*[o.handle for o in ops])
+    pb = (C.c_void_p * n)()
+    px = (C.c_void_p * n)()
+    mem = None
+    for i in range(n):
+        pb[i], m1 = _as_f64(bs[i])
+        px[i], m2 = _as_f64(xs[i])
+        mem = m1 if mem is None else mem
+        if m1 != mem or m2 != mem:
+            raise TypeError("all vectors must live in one memory space")
+    res = (FgResult * n)()
+    c = cfg.to_c(precond)
+    rc = lib().fg_batch_pcg(hs, n, pb, px, C.byref(c), res, mem)
+    if rc not in (FG_OK, FG_CONVERGENCE_FAILED):
+        _check(rc)
+    out = [SolveResult(bool(r.converged), int(r.iterations), float(r.final_residual), float(r.true_residual),
+                       int(r.applies), float(r.lmax), float(r.solve_ms), int(r.outer_iterations), int(r.status))
+           for r in res]
+    return rc == FG_OK, out
 
 
 SDIRK2_GAMMA = 1.0 - 2.0 ** -0.5  # crates/solver/src/ode.rs:441

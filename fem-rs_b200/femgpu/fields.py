@@ -59,8 +59,34 @@ def gaussian_field_q(nx, ny, nz, nq, sigma2=1.0, ell=0.1, seed=0):
     return np.ascontiguousarray(g).reshape(-1)
 
 
-def lognormal_kappa_q(nx, ny, nz, p, sigma2=1.0, ell=0.1, seed=0):
-    g = gaussian_field_q(nx, ny, nz, p + 1, sigma2, ell, seed)
+def gaussian_field_q_torch(nx, ny, nz, nq, sigma2=1.0, ell=0.1, seed=0, device="cuda"):
+    """Same construction as gaussian_field_q with the three contractions and
+    the normal draws on a torch device (seeded torch generator), returned as a
+    host float64 array in the [E][qz][qy][qx] layout."""
+    import torch
+
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed))
+    X, Y, Z = nx * nq, ny * nq, nz * nq
+    Lx = torch.from_numpy(_factor_1d(qp_coords_1d(nx, nq), ell)).to(device)
+    Ly = torch.from_numpy(_factor_1d(qp_coords_1d(ny, nq), ell)).to(device)
+    Lz = torch.from_numpy(_factor_1d(qp_coords_1d(nz, nq), ell)).to(device)
+    g = torch.randn((Z, Y, X), generator=gen, dtype=torch.float64, device=device)
+    g = g @ Lx.T
+    g = torch.matmul(Ly, g)
+    g = (Lz @ g.reshape(Z, Y * X)).reshape(Z, Y, X)
+    g *= float(np.sqrt(sigma2))
+    g = g.reshape(nz, nq, ny, nq, nx, nq).permute(0, 2, 4, 1, 3, 5).contiguous()
+    return g.reshape(-1).cpu().numpy()
+
+
+def lognormal_kappa_q(nx, ny, nz, p, sigma2=1.0, ell=0.1, seed=0, device=None):
+    """kappa = exp(g) at the quadrature points; device="cuda" draws on the GPU
+    (a different, equally seeded stream of normals than the numpy path)."""
+    if device is not None:
+        g = gaussian_field_q_torch(nx, ny, nz, p + 1, sigma2, ell, seed, device)
+    else:
+        g = gaussian_field_q(nx, ny, nz, p + 1, sigma2, ell, seed)
     np.exp(g, out=g)
     return g
 

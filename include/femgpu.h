@@ -213,6 +213,19 @@ FG_API int fg_op_diagonal(fg_op *op, double *d, int constrained, int mem);
 FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg, fg_result *res,
                   int mem);
 
+/* Batched solves: n independent operators (any mix of orders and sizes)
+ * solved together by the FP32 mixed-precision PCG of fg_pcg (cfg->precision
+ * must be FG_FP32_IR; Jacobi or Chebyshev preconditioner).  Each phase of an
+ * iteration is one launch over all instances (one per order/kind/format group
+ * for the applies), converged instances are masked on the device, and chunks
+ * of cfg->check_interval iterations are captured once in a CUDA graph and
+ * replayed.  b[i], x[i]: plain vectors of operator i (x: guess in, solution
+ * out); results[i] per instance.  Returns FG_CONVERGENCE_FAILED if any
+ * instance did not converge.  No reference counterpart: fem-rs solves one
+ * system per call (crates/solver/src/lib.rs:281-297). */
+FG_API int fg_batch_pcg(fg_op *const *ops, int n, const double *const *b, double *const *x,
+                        const fg_cfg *cfg, fg_result *results, int mem);
+
 typedef struct {
     int32_t steps;
     int32_t max_stage_iterations;

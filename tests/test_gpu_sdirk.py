@@ -104,3 +104,18 @@ def test_sdirk_fp32_stages_match_fp64(precond):
     femgpu.sdirk2(K, S, u64, dt, steps, femgpu.SolverConfig(rtol=1e-10), precond)
     femgpu.sdirk2(K, S, u32, dt, steps, femgpu.SolverConfig(rtol=1e-10, precision=femgpu.FP32_IR), precond)
     assert np.linalg.norm(u32 - u64) <= 1e-7 * np.linalg.norm(u64)
+
+
+@pytest.mark.parametrize("prec", [femgpu.FP64, femgpu.FP32_IR])
+def test_sdirk_survives_strong_decay(prec):
+    """The stage right-hand sides shrink with the solution (here by ~1e-120);
+    stage solves on normalised right-hand sides must still all converge."""
+    need_gpu()
+    n, p, dt, steps = 5, 2, 1e-3, 200
+    K, S = make_ops(n, p, 50.0, dt)
+    mesh = O.Mesh(n, n, n, p)
+    u = initial(n, p)
+    u[O.ess_mask(mesh) == 1] = 0.0
+    info = femgpu.sdirk2(K, S, u, dt, steps, femgpu.SolverConfig(rtol=1e-10, precision=prec), femgpu.PC_CHEBYSHEV)
+    assert info["steps"] == steps
+    assert np.all(np.isfinite(u)) and np.abs(u).max() < 1e-100
