@@ -47,6 +47,8 @@ static int fail(int status, const char *fmt, ...) {
                         __FILE__, __LINE__);                                               \
     } while (0)
 
+#include "unet_host.cuh"
+
 // ---------------------------------------------------------------------------
 // 1-D tables: Gauss-Legendre (crates/element/src/quadrature.rs:12-32) and
 // equispaced Lagrange polynomials (quad.rs:92-105, seg.rs:119-121 conventions).
@@ -173,6 +175,10 @@ struct fg_op {
     SolverState *st32 = nullptr;
     // affine-compressed quadrature data (fg_op_set_qdata_format), FP64 and FP32
     double *sd_u = nullptr, *sd_k1 = nullptr, *sd_w = nullptr;  // SDIRK-2 stepping
+    // learned coarse correction (Q1 operators): coarse log kappa, network, scratch
+    float *nn_lk = nullptr, *nn_rc = nullptr;
+    double *nn_scale = nullptr;
+    fg_unet *nn = nullptr;
     int fmt = 0;
     double *qa64 = nullptr;
     float *qa32 = nullptr;
@@ -197,6 +203,9 @@ static void free_op(fg_op *op) {
     if (op->st32) cudaFree(op->st32);
     if (op->qa64) cudaFree(op->qa64);
     if (op->sd_u) cudaFree(op->sd_u);
+    if (op->nn_lk) cudaFree(op->nn_lk);
+    if (op->nn_rc) cudaFree(op->nn_rc);
+    if (op->nn_scale) cudaFree(op->nn_scale);
     if (op->sd_k1) cudaFree(op->sd_k1);
     if (op->sd_w) cudaFree(op->sd_w);
     if (op->qa32) cudaFree(op->qa32);
@@ -802,7 +811,7 @@ static int cheb_apply(fg_op *op, const PcgBufs<T> &B, const ChebCoef &cc, const 
 template <typename T>
 static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebCoef *cc,
                    int max_iter, int check_interval, bool x_zero, SolverState *h,
-                   int64_t *applies) {
+                   int64_t *applies, const std::function<int(int)> &on_chunk = nullptr) {
     int rc;
     const int64_t n = op->Nn;
     const int *skip = &B.st->done;
@@ -839,6 +848,7 @@ static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebC
         }
         launched += chunk;
         if ((rc = read_state(op, h, B.st))) return rc;
+        if (on_chunk && !h->done && (rc = on_chunk(h->iter))) return rc;
         if (h->done) break;
     }
     if ((rc = read_state(op, h, B.st))) return rc;
@@ -849,6 +859,86 @@ static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebC
     if (!(h->iter == 0 && h->done && !h->breakdown)) *applies += km1;
     *applies += h->iter + (h->breakdown ? 1 : 0);
     *applies += (int64_t)km1 * (h->iter - (stopped_by_update ? 1 : 0));
+    return FG_OK;
+}
+
+// ---- learned coarse correction inside the preconditioner -------------------
+static Vol nn_coarse_vol(const fg_op *op) {
+    return Vol{1, (op->g.NK + 1) / 2, (op->g.NJ + 1) / 2, (op->g.NI + 1) / 2};
+}
+
+// z += s P(UNet(R r / s, R log kappa)),  s = rms(R r)
+template <typename T> static int nn_precond_add(fg_op *op, const T *r, T *z) {
+    fg_unet *u = op->nn;
+    u->stream = op->stream;
+    const Vol Vc = nn_coarse_vol(op);
+    int rc;
+    if ((rc = unet_ensure_bufs(u, 1, Vc.Z, Vc.Y, Vc.X))) return rc;
+    Grid g = op->g;
+    g.ess = op->ess_tags;
+    const int64_t nv = Vc.nvox();
+    int blocks;
+    grid_launch(nv, blocks);
+    fe_restrict_kernel<T><<<blocks, 256, 0, op->stream>>>(g, r, op->nn_rc, Vc);
+    rms_kernel<<<1, 256, 0, op->stream>>>(op->nn_rc, nv, op->nn_scale);
+    pack_input_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, op->nn_lk, nv, op->nn_scale,
+                                                      TView{u->buf.x0, 2, 0});
+    CK(cudaGetLastError());
+    if ((rc = unet_forward(u))) return rc;
+    fe_prolong_kernel<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(g, TView{u->buf.out, 8, 0}, Vc, z,
+                                                                   op->nn_scale, 1);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+// Flexible CG (FCG(1), Notay) with z = Chebyshev(r) [+ learned correction];
+// once `budget` iterations pass without convergence the learned term is
+// dropped and the solve continues as plain Chebyshev-preconditioned CG from
+// the current iterate (the fallback).  FP64 storage.
+static int fcg_nn_run(fg_op *op, const PcgBufs<double> &B, const ChebCoef &cc, int max_iter,
+                      int check_interval, int budget, SolverState *h, int64_t *applies,
+                      int *fell_back) {
+    int rc;
+    const int64_t n = op->Nn;
+    const int *skip = &B.st->done;
+    bool nn_on = op->nn != nullptr;
+    *fell_back = 0;
+    if ((rc = apply_native_t<double>(op, B.qd, B.face, B.x, B.ap, 0, 1, nullptr))) return rc;
+    ++*applies;
+    k_pcg_init<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.b, B.ap, B.dinv, B.r, B.z, B.p,
+                                                                 0, op->partials, B.st);
+    auto direction = [&](int init) -> int {
+        int r2 = cheb_apply<double>(op, B, cc, B.r, B.z, skip);
+        if (r2) return r2;
+        if (nn_on && (r2 = nn_precond_add<double>(op, B.r, B.z))) return r2;
+        k_fcg_zap<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.ap, op->partials, B.st, init);
+        k_pcg_pupdate<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.p, B.st, init);
+        k_fcg_pr<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.r, op->partials, B.st);
+        CK(cudaGetLastError());
+        return FG_OK;
+    };
+    if ((rc = direction(1))) return rc;
+    int launched = 0;
+    while (launched < max_iter) {
+        const int chunk = std::min(check_interval, max_iter - launched);
+        for (int k = 0; k < chunk; ++k) {
+            if ((rc = apply_native_t<double>(op, B.qd, B.face, B.p, B.ap, 0, 1, skip))) return rc;
+            k_pcg_pap<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.ap, op->partials, B.st);
+            k_pcg_update<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.x, B.r, B.p, B.ap, B.dinv,
+                                                                           B.z, 0, op->partials, B.st);
+            if ((rc = direction(0))) return rc;
+        }
+        launched += chunk;
+        if ((rc = read_state(op, h, B.st))) return rc;
+        if (h->done) break;
+        if (nn_on && budget > 0 && h->iter >= budget) {
+            nn_on = false;
+            *fell_back = 1;
+        }
+    }
+    if ((rc = read_state(op, h, B.st))) return rc;
+    const int km1 = (int)cc.c1.size();
+    *applies += (int64_t)(h->iter + 1) * (1 + km1);
     return FG_OK;
 }
 
@@ -924,8 +1014,8 @@ static int validate_cfg(fg_cfg &cfg) {
     if (cfg.max_iter < 0) return fail(FG_INVALID_ARGUMENT, "max_iter < 0");
     if (cfg.precision != FG_FP64 && cfg.precision != FG_FP32_IR)
         return fail(FG_UNSUPPORTED, "precision %d not available", cfg.precision);
-    if (cfg.precond < 0 || cfg.precond > 2) return fail(FG_INVALID_ARGUMENT, "bad precond");
-    if (cfg.precond == FG_PC_CHEBYSHEV && cfg.cheb_degree < 1)
+    if (cfg.precond < 0 || cfg.precond > 3) return fail(FG_INVALID_ARGUMENT, "bad precond");
+    if ((cfg.precond == FG_PC_CHEBYSHEV || cfg.precond == FG_PC_CHEB_NN) && cfg.cheb_degree < 1)
         return fail(FG_INVALID_ARGUMENT, "cheb_degree must be >= 1");
     if (cfg.check_interval < 1) cfg.check_interval = 10;
     return FG_OK;
@@ -934,7 +1024,11 @@ static int validate_cfg(fg_cfg &cfg) {
 // PCG on op->bw (right-hand side) from op->xw (initial guess), both native and
 // resident; the solution is left in op->xw.  The caller holds op->mu.
 static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
-    const bool cheb = cfg.precond == FG_PC_CHEBYSHEV;
+    const bool learned = cfg.precond == FG_PC_CHEB_NN;
+    if (learned && (!op->nn || !op->nn_lk))
+        return fail(FG_INVALID_ARGUMENT, "FG_PC_CHEB_NN needs fg_op_set_nodal_kappa and fg_op_attach_unet");
+    const bool cheb = cfg.precond == FG_PC_CHEBYSHEV || learned;
+    int fell_back = 0;
     const bool ir = cfg.precision == FG_FP32_IR;
     int rc;
     if ((rc = ensure_solver_buffers(op))) return rc;
@@ -976,8 +1070,12 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
         PcgBufs<double> B{op->qd, op->face, dinv_use, op->xw, op->bw, op->r, op->z, op->pv,
                           op->ap, op->cres, op->cd, op->ct, op->st};
         set_state(op, op->st, cfg.rtol, cfg.atol, cfg.max_iter);
-        if ((rc = pcg_run<double>(op, B, !cheb, cheb ? &cc : nullptr, cfg.max_iter,
-                                  cfg.check_interval, false, &h, &applies)))
+        if (learned) {
+            if ((rc = fcg_nn_run(op, B, cc, cfg.max_iter, cfg.check_interval, cfg.nn_budget, &h, &applies,
+                                 &fell_back)))
+                return rc;
+        } else if ((rc = pcg_run<double>(op, B, !cheb, cheb ? &cc : nullptr, cfg.max_iter,
+                                         cfg.check_interval, false, &h, &applies)))
             return rc;
         inner_total = h.iter;
         status = h.converged ? FG_OK : (h.breakdown ? FG_BREAKDOWN : FG_CONVERGENCE_FAILED);
@@ -1011,7 +1109,19 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
         k_rel_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->r32,
                                                                  op->partials, op->st, 1);
         // z = M r_lo ; p = z ; rz
+        bool nn_on = learned;
         auto precond = [&](int init) -> int {
+            if (learned) {  // flexible directions: z = Chebyshev(r) [+ learned correction]
+                int rc2 = cheb_apply<float>(op, B, cc, op->r32, op->z32, done);
+                if (rc2) return rc2;
+                if (nn_on && (rc2 = nn_precond_add<float>(op, op->r32, op->z32))) return rc2;
+                k_fcg_zap<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z32, op->ap32, op->partials,
+                                                                           op->st, init);
+                k_pcg_pupdate<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z32, op->p32, op->st, init);
+                k_fcg_pr<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->p32, op->r32, op->partials, op->st);
+                CK(cudaGetLastError());
+                return FG_OK;
+            }
             if (cheb) {
                 int rc2 = cheb_apply<float>(op, B, cc, op->r32, op->z32, done);
                 if (rc2) return rc2;
@@ -1046,6 +1156,10 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
             launched += chunk;
             if ((rc = read_state(op, &h))) return rc;
             if (h.done) break;
+            if (nn_on && cfg.nn_budget > 0 && h.iter >= cfg.nn_budget) {
+                nn_on = false;
+                fell_back = 1;
+            }
         }
         if ((rc = read_state(op, &h))) return rc;
         inner_total = h.iter;
@@ -1075,6 +1189,7 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
         res->applies = applies;
         res->lmax = lmax;
         res->solve_ms = ms;
+        res->nn_fallback = fell_back;
     }
     if (cfg.print_level >= 1)
         fprintf(stderr, "fg_pcg: %s after %d iterations (%d outer), residual %.3e (true %.3e)\n",
@@ -1666,3 +1781,319 @@ extern "C" FG_API int fg_op_apply_native_noalloc(fg_op *op, const double *x, dou
     }
     return FG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Learned coarse correction: network handle, training, attachment.
+// ---------------------------------------------------------------------------
+static int unet_params_layout(const fg_unet *u, std::vector<int64_t> *offs) {
+    int64_t o = 0;
+    for (int l = 0; l < NLAYERS; ++l) {
+        offs->push_back(o);
+        o += (int64_t)u->L[l].cout * 27 * u->L[l].cin + u->L[l].cout;
+    }
+    offs->push_back(o);
+    return FG_OK;
+}
+
+static int unet_copy_params(fg_unet *u, float *host, bool to_host, bool grads) {
+    for (int l = 0; l < NLAYERS; ++l) {
+        ConvLayer &L = u->L[l];
+        const int K = 27 * L.cin;
+        float *w = grads ? L.gw : L.w, *b = grads ? L.gb : L.b;
+        if (to_host) {
+            CK(cudaMemcpy2D(host, K * sizeof(float), w, L.kp * sizeof(float), K * sizeof(float), L.cout,
+                            cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(host + (int64_t)L.cout * K, b, L.cout * sizeof(float), cudaMemcpyDeviceToHost));
+        } else {
+            CK(cudaMemcpy2D(w, L.kp * sizeof(float), host, K * sizeof(float), K * sizeof(float), L.cout,
+                            cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(b, host + (int64_t)L.cout * K, L.cout * sizeof(float), cudaMemcpyHostToDevice));
+            f32_to_bf16_kernel<<<64, 256>>>(L.w, L.wb, (int64_t)L.cout * L.kp);
+            CK(cudaGetLastError());
+        }
+        host += (int64_t)L.cout * K + L.cout;
+    }
+    CK(cudaDeviceSynchronize());
+    return FG_OK;
+}
+
+// input [B][Z][Y][X][2] FP32 (device or host) -> network input buffer
+static int unet_load_input(fg_unet *u, const float *in, int mem) {
+    UnetBufs &b = u->buf;
+    const int64_t nv = b.v0.nvox();
+    const float *src = in;
+    float *tmp = nullptr;
+    if (mem == FG_HOST) {
+        CK(cudaMalloc(&tmp, nv * 2 * sizeof(float)));
+        CK(cudaMemcpyAsync(tmp, in, nv * 2 * sizeof(float), cudaMemcpyHostToDevice, u->stream));
+        src = tmp;
+    }
+    int blocks;
+    grid_launch(nv, blocks);
+    f32x2_to_x0_kernel<<<blocks, 256, 0, u->stream>>>(src, nv, TView{b.x0, 2, 0});
+    CK(cudaGetLastError());
+    if (tmp) {
+        CK(cudaStreamSynchronize(u->stream));
+        cudaFree(tmp);
+    }
+    return FG_OK;
+}
+
+static int unet_load_target(fg_unet *u, const float *t, int mem) {
+    const int64_t nv = u->buf.v0.nvox();
+    CK(cudaMemcpyAsync(u->buf.target, t, nv * sizeof(float),
+                       mem == FG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, u->stream));
+    return FG_OK;
+}
+
+// forward + loss + backward; loss on the host (block partials summed in order)
+static int unet_loss_grad(fg_unet *u, float *loss) {
+    UnetBufs &b = u->buf;
+    int rc;
+    if ((rc = unet_forward(u))) return rc;
+    const int64_t nv = b.v0.nvox();
+    const int blocks = (int)std::min<int64_t>((nv + 255) / 256, 1024);
+    mse_kernel<<<blocks, 256, 0, u->stream>>>(TView{b.out, 8, 0}, b.target, nv, 8, TView{b.dout, 8, 0}, b.msep);
+    CK(cudaGetLastError());
+    if ((rc = unet_backward(u))) return rc;
+    std::vector<float> part(blocks);
+    CK(cudaMemcpyAsync(part.data(), b.msep, blocks * sizeof(float), cudaMemcpyDeviceToHost, u->stream));
+    CK(cudaStreamSynchronize(u->stream));
+    double s = 0.0;
+    for (float v : part) s += v;
+    if (loss) *loss = (float)(s / (double)nv);
+    return FG_OK;
+}
+
+extern "C" {
+
+FG_API int fg_unet_create(const int channels[3], uint64_t seed, fg_unet **out) {
+    if (!out) return fail(FG_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int c[3] = {16, 32, 48};
+    if (channels)
+        for (int i = 0; i < 3; ++i) c[i] = channels[i];
+    const int allowed[] = {8, 16, 32, 48, 64};
+    for (int i = 0; i < 3; ++i)
+        if (std::find(std::begin(allowed), std::end(allowed), c[i]) == std::end(allowed))
+            return fail(FG_UNSUPPORTED, "channel count %d not supported (8, 16, 32, 48, 64)", c[i]);
+    if (c[1] + c[0] > 80 || c[2] + c[1] > 80 + 32)
+        return fail(FG_UNSUPPORTED, "channel counts too large");
+    fg_unet *u = new fg_unet();
+    CK(cudaGetDevice(&u->device));
+    u->C0 = c[0]; u->C1 = c[1]; u->C2 = c[2];
+    const int cin[NLAYERS] = {2, c[0], c[0], c[1], c[1], c[2], c[2] + c[1], c[1] + c[0], c[0]};
+    const int cout[NLAYERS] = {c[0], c[0], c[1], c[1], c[2], c[2], c[1], c[0], 8};
+    for (int l = 0; l < NLAYERS; ++l) {
+        int rc = unet_layer_alloc(u->L[l], cin[l], cout[l], seed * 16 + l);
+        if (rc) { fg_unet_destroy(u); return rc; }
+    }
+    CK(cudaDeviceSynchronize());
+    *out = u;
+    return FG_OK;
+}
+
+FG_API void fg_unet_destroy(fg_unet *u) {
+    if (!u) return;
+    cudaSetDevice(u->device);
+    cudaDeviceSynchronize();
+    for (auto &L : u->L) {
+        void *p[] = {L.w, L.b, L.wb, L.gw, L.gb, L.mw, L.vw, L.mb, L.vb};
+        for (void *q : p) if (q) cudaFree(q);
+    }
+    unet_free_bufs(u->buf);
+    if (u->wflip) cudaFree(u->wflip);
+    delete u;
+}
+
+FG_API int64_t fg_unet_num_params(const fg_unet *u) {
+    if (!u) return -1;
+    std::vector<int64_t> o;
+    unet_params_layout(u, &o);
+    return o.back();
+}
+
+FG_API int fg_unet_get_params(fg_unet *u, float *host) {
+    if (!u || !host) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    CK(cudaSetDevice(u->device));
+    return unet_copy_params(u, host, true, false);
+}
+
+FG_API int fg_unet_set_params(fg_unet *u, const float *host) {
+    if (!u || !host) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    CK(cudaSetDevice(u->device));
+    return unet_copy_params(u, const_cast<float *>(host), false, false);
+}
+
+FG_API int fg_unet_get_grads(fg_unet *u, float *host) {
+    if (!u || !host) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    CK(cudaSetDevice(u->device));
+    return unet_copy_params(u, host, true, true);
+}
+
+FG_API int fg_unet_forward(fg_unet *u, const float *in, int B, int Z, int Y, int X, float *out, int mem) {
+    if (!u || !in || !out || B < 1) return fail(FG_INVALID_ARGUMENT, "bad arguments");
+    CK(cudaSetDevice(u->device));
+    u->stream = nullptr;
+    int rc;
+    if ((rc = unet_ensure_bufs(u, B, Z, Y, X)) || (rc = unet_load_input(u, in, mem)) || (rc = unet_forward(u)))
+        return rc;
+    const int64_t nv = u->buf.v0.nvox();
+    float *dst = out, *tmp = nullptr;
+    if (mem == FG_HOST) { CK(cudaMalloc(&tmp, nv * sizeof(float))); dst = tmp; }
+    int blocks;
+    grid_launch(nv, blocks);
+    out0_to_f32_kernel<<<blocks, 256, 0, u->stream>>>(TView{u->buf.out, 8, 0}, nv, dst);
+    CK(cudaGetLastError());
+    if (tmp) {
+        CK(cudaMemcpy(out, tmp, nv * sizeof(float), cudaMemcpyDeviceToHost));
+        cudaFree(tmp);
+    }
+    CK(cudaDeviceSynchronize());
+    return FG_OK;
+}
+
+// Loss and gradients of the mean squared error between output channel 0 and
+// target (no parameter update); fg_unet_get_grads reads them.
+FG_API int fg_unet_loss_grad(fg_unet *u, const float *in, const float *target, int B, int Z, int Y, int X,
+                             float *loss, int mem) {
+    if (!u || !in || !target || B < 1) return fail(FG_INVALID_ARGUMENT, "bad arguments");
+    CK(cudaSetDevice(u->device));
+    u->stream = nullptr;
+    int rc;
+    if ((rc = unet_ensure_bufs(u, B, Z, Y, X)) || (rc = unet_load_input(u, in, mem)) ||
+        (rc = unet_load_target(u, target, mem)) || (rc = unet_loss_grad(u, loss)))
+        return rc;
+    CK(cudaDeviceSynchronize());
+    return FG_OK;
+}
+
+// One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss of the batch.
+FG_API int fg_unet_train_step(fg_unet *u, const float *in, const float *target, int B, int Z, int Y, int X,
+                              float lr, float *loss, int mem) {
+    int rc;
+    if ((rc = fg_unet_loss_grad(u, in, target, B, Z, Y, X, loss, mem))) return rc;
+    u->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.f - std::pow(b1, (float)u->step), bc2 = 1.f - std::pow(b2, (float)u->step);
+    for (auto &L : u->L) {
+        const int nw = L.cout * L.kp;
+        adam_kernel<<<64, 256, 0, u->stream>>>(L.w, L.gw, L.mw, L.vw, nw, lr, b1, b2, 1e-8f, bc1, bc2, L.wb);
+        adam_kernel<<<1, 64, 0, u->stream>>>(L.b, L.gb, L.mb, L.vb, L.cout, lr, b1, b2, 1e-8f, bc1, bc2, nullptr);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(u->stream));
+    return FG_OK;
+}
+
+// Coarse log-kappa channel of the learned correction: kappa at the DOFs
+// (plain layout, host), restricted to the coarse vertex grid.
+FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal) {
+    if (!op || !kappa_nodal) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (op->p != 1 || op->g.nx % 8 || op->g.ny % 8 || op->g.nz % 8)
+        return fail(FG_UNSUPPORTED, "the learned correction needs a Q1 operator with element counts "
+                                    "that are multiples of 8");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    int rc;
+    if ((rc = ensure_solver_buffers(op))) return rc;
+    const Vol Vc = nn_coarse_vol(op);
+    const int64_t nv = Vc.nvox();
+    if (!op->nn_lk) {
+        CK(cudaMalloc(&op->nn_lk, nv * sizeof(float)));
+        CK(cudaMalloc(&op->nn_rc, nv * sizeof(float)));
+        CK(cudaMalloc(&op->nn_scale, 4 * sizeof(double)));
+    }
+    std::vector<double> lg(op->N);
+    for (int64_t i = 0; i < op->N; ++i) lg[i] = std::log(std::max(kappa_nodal[i], 1e-300));
+    if ((rc = to_native(op, op->cd, lg.data(), FG_HOST))) return rc;
+    Grid g = op->g;
+    int blocks;
+    grid_launch(nv, blocks);
+    fe_restrict_kernel<double><<<blocks, 256, 0, op->stream>>>(g, op->cd, op->nn_lk, Vc);
+    CK(cudaGetLastError());
+    // full weighting averages (its weights sum to 1 away from the boundary)
+    CK(cudaStreamSynchronize(op->stream));
+    return FG_OK;
+}
+
+FG_API int fg_op_attach_unet(fg_op *op, fg_unet *net) {
+    if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
+    std::lock_guard<std::mutex> lk(op->mu);
+    if (net && net->device != op->device) return fail(FG_INVALID_ARGUMENT, "network on another device");
+    op->nn = net;
+    return FG_OK;
+}
+
+// Training pairs from a plain Chebyshev-PCG solve of A x = b (x0 = 0): at
+// iterations 0, every, 2*every, ... the iterate x_k gives
+//   input  [Zc][Yc][Xc][2] = (R (b - A x_k) / s_k, R log kappa),
+//   target [Zc][Yc][Xc]    = (x* - x_k) at the coarse vertices / s_k,
+// s_k = rms(R (b - A x_k)); device FP32 outputs, up to max_pairs.
+FG_API int fg_op_collect_pairs(fg_op *op, const double *b, const fg_cfg *cfg_in, int every, int max_pairs,
+                               float *d_in, float *d_target, int *n_pairs) {
+    if (!op || !b || !d_in || !d_target || !n_pairs || every < 1 || max_pairs < 1)
+        return fail(FG_INVALID_ARGUMENT, "bad arguments");
+    if (!op->nn_lk) return fail(FG_INVALID_ARGUMENT, "call fg_op_set_nodal_kappa first");
+    fg_cfg cfg;
+    if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
+    cfg.precision = FG_FP64;
+    cfg.precond = FG_PC_CHEBYSHEV;
+    cfg.check_interval = every;
+    int rc;
+    if ((rc = validate_cfg(cfg))) return rc;
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    if ((rc = ensure_solver_buffers(op)) || (rc = ensure_dinv(op))) return rc;
+    if (!op->have_lmax) {
+        if ((rc = estimate_lmax(op, cfg.power_iters > 0 ? cfg.power_iters : 20, &op->lmax_est))) return rc;
+        op->have_lmax = true;
+    }
+    const double lmax = (cfg.lmax_safety > 0 ? cfg.lmax_safety : 1.1) * op->lmax_est;
+    const ChebCoef cc = cheb_coefs(lmax / (cfg.lmin_ratio > 0 ? cfg.lmin_ratio : 30.0), lmax, cfg.cheb_degree);
+    const int64_t n = op->Nn;
+    std::vector<double *> stash;
+    auto cleanup = [&]() { for (double *p : stash) cudaFree(p); };
+    struct G { std::function<void()> f; ~G() { f(); } } guard{cleanup};
+    auto push = [&]() -> int {
+        if ((int)stash.size() >= max_pairs) return FG_OK;
+        double *p = nullptr;
+        CK(cudaMalloc(&p, n * sizeof(double)));
+        CK(cudaMemcpyAsync(p, op->xw, n * sizeof(double), cudaMemcpyDeviceToDevice, op->stream));
+        stash.push_back(p);
+        return FG_OK;
+    };
+    if ((rc = to_native(op, op->bw, b, FG_HOST))) return rc;
+    CK(cudaMemsetAsync(op->xw, 0, n * sizeof(double), op->stream));
+    if ((rc = push())) return rc;
+    PcgBufs<double> B{op->qd, op->face, op->dinv, op->xw, op->bw, op->r, op->z, op->pv, op->ap,
+                      op->cres, op->cd, op->ct, op->st};
+    set_state(op, op->st, cfg.rtol, cfg.atol, cfg.max_iter);
+    SolverState h{};
+    int64_t applies = 0;
+    if ((rc = pcg_run<double>(op, B, false, &cc, cfg.max_iter, every, false, &h, &applies,
+                              [&](int) { return push(); })))
+        return rc;
+    Grid g = op->g;
+    g.ess = op->ess_tags;
+    const Vol Vc = nn_coarse_vol(op);
+    const int64_t nv = Vc.nvox();
+    int blocks;
+    grid_launch(nv, blocks);
+    for (size_t j = 0; j < stash.size(); ++j) {
+        if ((rc = apply_native(op, stash[j], op->ap, 0, 1, nullptr))) return rc;
+        k_lincomb2<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r, 1.0, op->bw, -1.0, op->ap);
+        fe_restrict_kernel<double><<<blocks, 256, 0, op->stream>>>(g, op->r, op->nn_rc, Vc);
+        rms_kernel<<<1, 256, 0, op->stream>>>(op->nn_rc, nv, op->nn_scale);
+        pack_input_f32_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, op->nn_lk, nv, op->nn_scale,
+                                                              d_in + (int64_t)j * nv * 2);
+        pair_target_kernel<<<blocks, 256, 0, op->stream>>>(g, op->xw, stash[j], Vc, op->nn_scale,
+                                                           d_target + (int64_t)j * nv);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(op->stream));
+    *n_pairs = (int)stash.size();
+    return check_device_error(op);
+}
+
+}  // extern "C"

@@ -832,4 +832,38 @@ __global__ void __launch_bounds__(VEC_THREADS) k_scale_tmp(int64_t n, double *__
     }
 }
 
+// ---- flexible CG (Notay's FCG with one stored direction) -------------------
+// beta = -(z . A p_old) / (p_old . A p_old)  (0 on init);  then p = z + beta p
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_fcg_zap(int64_t n, const T *__restrict__ z,
+                                                         const T *__restrict__ ap, double *partials,
+                                                         SolverState *st, int init) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    if (!init) {
+        FG_VEC4_LOOP(q, n) {
+            const V4<T> zv = ld4(z, q), av = ld4(ap, q);
+            FG_K4 v[0] += (double)zv.a[k] * (double)av.a[k];
+        }
+    }
+    double tot[1];
+    if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0)
+        st->beta = init ? 0.0 : -tot[0] / st->pap;
+}
+
+// rz = p . r (the FCG step numerator; alpha = rz / pap in k_pcg_pap)
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_fcg_pr(int64_t n, const T *__restrict__ p,
+                                                        const T *__restrict__ r, double *partials,
+                                                        SolverState *st) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> pv = ld4(p, q), rv = ld4(r, q);
+        FG_K4 v[0] += (double)pv.a[k] * (double)rv.a[k];
+    }
+    double tot[1];
+    if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) st->rz = tot[0];
+}
+
 }  // namespace fg

@@ -29,7 +29,7 @@ FG_OK, FG_CONVERGENCE_FAILED, FG_DIMENSION_MISMATCH, FG_BREAKDOWN = 0, 1, 2, 3
 FG_UNSUPPORTED, FG_DEVICE_TIMEOUT, FG_BOUNDS, FG_CUDA_ERROR, FG_INVALID_ARGUMENT = 4, 5, 6, 7, 8
 MASS, DIFF, MASS_DIFF = 1, 2, 3
 HOST, DEVICE = 0, 1
-PC_NONE, PC_JACOBI, PC_CHEBYSHEV = 0, 1, 2
+PC_NONE, PC_JACOBI, PC_CHEBYSHEV, PC_CHEB_NN = 0, 1, 2, 3
 FP64, FP32_IR = 0, 1
 QDATA_FULL, QDATA_AFFINE = 0, 1
 TAG_ALL = 63
@@ -39,7 +39,10 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_op_layout", "fg_op_native_len", "fg_op_set_stream", "fg_op_apply",
            "fg_op_apply_native", "fg_op_diagonal", "fg_pcg", "fg_op_check",
            "fg_op_apply_native_noalloc", "fg_op_apply_f32", "fg_op_apply_native_f32",
-           "fg_op_set_qdata_format", "fg_sdirk2", "fg_batch_pcg")
+           "fg_op_set_qdata_format", "fg_sdirk2", "fg_batch_pcg",
+           "fg_unet_create", "fg_unet_destroy", "fg_unet_num_params", "fg_unet_get_params",
+           "fg_unet_set_params", "fg_unet_get_grads", "fg_unet_forward", "fg_unet_loss_grad",
+           "fg_unet_train_step", "fg_op_set_nodal_kappa", "fg_op_attach_unet", "fg_op_collect_pairs")
 
 
 class FgMesh(C.Structure):
@@ -51,7 +54,7 @@ class FgCfg(C.Structure):
                 ("print_level", C.c_int32), ("precond", C.c_int32), ("cheb_degree", C.c_int32),
                 ("precision", C.c_int32), ("power_iters", C.c_int32), ("lmax", C.c_double),
                 ("lmin_ratio", C.c_double), ("lmax_safety", C.c_double), ("inner_rtol", C.c_double),
-                ("check_interval", C.c_int32), ("reserved", C.c_int32)]
+                ("check_interval", C.c_int32), ("nn_budget", C.c_int32)]
 
 
 class FgSdirkResult(C.Structure):
@@ -63,7 +66,8 @@ class FgSdirkResult(C.Structure):
 class FgResult(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("final_residual", C.c_double),
                 ("true_residual", C.c_double), ("status", C.c_int32), ("outer_iterations", C.c_int32),
-                ("applies", C.c_int64), ("lmax", C.c_double), ("solve_ms", C.c_double)]
+                ("applies", C.c_int64), ("lmax", C.c_double), ("solve_ms", C.c_double),
+                ("nn_fallback", C.c_int32), ("reserved", C.c_int32)]
 
 
 _lib = None
@@ -97,6 +101,19 @@ def lib():
         L.fg_op_set_qdata_format.argtypes = [vp, i]
         L.fg_sdirk2.argtypes = [vp, vp, vp, d, i, vp, vp, i]
         L.fg_batch_pcg.argtypes = [vp, i, vp, vp, vp, vp, i]
+        L.fg_unet_create.argtypes = [vp, C.c_uint64, C.POINTER(vp)]
+        L.fg_unet_destroy.argtypes = [vp]
+        L.fg_unet_destroy.restype = None
+        L.fg_unet_num_params.argtypes = [vp]
+        L.fg_unet_num_params.restype = i64
+        for nm in ("fg_unet_get_params", "fg_unet_set_params", "fg_unet_get_grads"):
+            getattr(L, nm).argtypes = [vp, vp]
+        L.fg_unet_forward.argtypes = [vp, vp, i, i, i, i, vp, i]
+        L.fg_unet_loss_grad.argtypes = [vp, vp, vp, i, i, i, i, vp, i]
+        L.fg_unet_train_step.argtypes = [vp, vp, vp, i, i, i, i, C.c_float, vp, i]
+        L.fg_op_set_nodal_kappa.argtypes = [vp, vp]
+        L.fg_op_attach_unet.argtypes = [vp, vp]
+        L.fg_op_collect_pairs.argtypes = [vp, vp, vp, i, i, vp, vp, vp]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
@@ -160,6 +177,7 @@ class SolverConfig:
     precision: int = FP64
     inner_rtol: float = 0.1
     check_interval: int = 10
+    nn_budget: int = 0
 
     def to_c(self, precond):
         c = FgCfg()
@@ -169,6 +187,7 @@ class SolverConfig:
         c.precond, c.cheb_degree, c.precision = precond, self.cheb_degree, self.precision
         c.power_iters, c.lmax, c.lmin_ratio = self.power_iters, self.lmax, self.lmin_ratio
         c.lmax_safety, c.inner_rtol, c.check_interval = self.lmax_safety, self.inner_rtol, self.check_interval
+        c.nn_budget = self.nn_budget
         return c
 
 
@@ -331,7 +350,7 @@ class PAOperator:
         rc = lib().fg_pcg(self._h, pb, px, C.byref(c), C.byref(r), mb)
         res = SolveResult(bool(r.converged), int(r.iterations), float(r.final_residual),
                           float(r.true_residual), int(r.applies), float(r.lmax), float(r.solve_ms),
-                          int(r.outer_iterations), int(r.status))
+                          int(r.outer_iterations), int(r.status), extra={"nn_fallback": int(r.nn_fallback)})
         if rc not in (FG_OK, FG_CONVERGENCE_FAILED):
             _check(rc)
         return res
@@ -438,6 +457,118 @@ def sdirk2(stiff: PAOperator, stage: PAOperator, u, dt, n_steps, cfg=None, preco
     _check(rc)
     return dict(steps=r.steps, total_iterations=int(r.total_iterations),
                 max_stage_iterations=r.max_stage_iterations, applies=int(r.applies), time_ms=r.time_ms)
+
+
+class UNet:
+    """Learned coarse correction network (fg_unet): BF16 3-D U-net, FP32
+    accumulation, trained by the library's own forward/backward kernels."""
+
+    def __init__(self, channels=(16, 32, 48), seed=0):
+        self.channels = tuple(int(c) for c in channels)
+        h = C.c_void_p()
+        ch = (C.c_int * 3)(*self.channels)
+        _check(lib().fg_unet_create(ch, int(seed), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fg_unet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def num_params(self):
+        return int(lib().fg_unet_num_params(self._h))
+
+    def get_params(self):
+        a = np.zeros(self.num_params, dtype=np.float32)
+        _check(lib().fg_unet_get_params(self._h, a.ctypes.data))
+        return a
+
+    def set_params(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        assert a.size == self.num_params
+        _check(lib().fg_unet_set_params(self._h, a.ctypes.data))
+
+    def get_grads(self):
+        a = np.zeros(self.num_params, dtype=np.float32)
+        _check(lib().fg_unet_get_grads(self._h, a.ctypes.data))
+        return a
+
+    def forward(self, inp):
+        """inp: float32 [B,Z,Y,X,2] (numpy) -> [B,Z,Y,X]"""
+        inp = np.ascontiguousarray(inp, dtype=np.float32)
+        B, Z, Y, X, _ = inp.shape
+        out = np.zeros((B, Z, Y, X), dtype=np.float32)
+        _check(lib().fg_unet_forward(self._h, inp.ctypes.data, B, Z, Y, X, out.ctypes.data, HOST))
+        return out
+
+    def _step(self, fn, inp, target, *extra):
+        loss = C.c_float()
+        if isinstance(inp, np.ndarray):
+            inp = np.ascontiguousarray(inp, dtype=np.float32)
+            target = np.ascontiguousarray(target, dtype=np.float32)
+            B, Z, Y, X, _ = inp.shape
+            _check(fn(self._h, inp.ctypes.data, target.ctypes.data, B, Z, Y, X, *extra, C.byref(loss), HOST))
+        else:  # torch CUDA tensors
+            B, Z, Y, X, _ = inp.shape
+            _check(fn(self._h, inp.data_ptr(), target.data_ptr(), B, Z, Y, X, *extra, C.byref(loss), DEVICE))
+        return float(loss.value)
+
+    def loss_grad(self, inp, target):
+        return self._step(lib().fg_unet_loss_grad, inp, target)
+
+    def train_step(self, inp, target, lr):
+        return self._step(lib().fg_unet_train_step, inp, target, C.c_float(lr))
+
+
+def set_nodal_kappa(op, kappa_nodal):
+    k = np.ascontiguousarray(kappa_nodal, dtype=np.float64)
+    _check(lib().fg_op_set_nodal_kappa(op.handle, k.ctypes.data))
+
+
+def attach_unet(op, net):
+    _check(lib().fg_op_attach_unet(op.handle, None if net is None else net.handle))
+
+
+def collect_pairs(op, b, every, max_pairs, cfg=None):
+    """Training pairs (torch CUDA float32 tensors in [n,Zc,Yc,Xc,2], target [n,Zc,Yc,Xc])."""
+    import torch
+    cfg = cfg or SolverConfig(rtol=1e-10, max_iter=20000)
+    Zc, Yc, Xc = (op.NK + 1) // 2, (op.NJ + 1) // 2, (op.NI + 1) // 2
+    din = torch.zeros((max_pairs, Zc, Yc, Xc, 2), dtype=torch.float32, device="cuda")
+    dt = torch.zeros((max_pairs, Zc, Yc, Xc), dtype=torch.float32, device="cuda")
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    npairs = C.c_int()
+    c = cfg.to_c(PC_CHEBYSHEV)
+    _check(lib().fg_op_collect_pairs(op.handle, b.ctypes.data, C.byref(c), int(every), int(max_pairs),
+                                     din.data_ptr(), dt.data_ptr(), C.byref(npairs)))
+    n = npairs.value
+    return din[:n], dt[:n]
+
+
+def nodal_kappa_from_q(kq, nx, ny, nz, p=1):
+    """kappa at the DOFs of a Q1 grid: average of the kappa values of the
+    quadrature points of the (up to 8) elements around each vertex."""
+    nq = p + 1
+    k = np.asarray(kq).reshape(nz, ny, nx, nq ** 3).mean(axis=-1)
+    acc = np.zeros((nz + 1, ny + 1, nx + 1))
+    cnt = np.zeros_like(acc)
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                acc[dz:dz + nz, dy:dy + ny, dx:dx + nx] += k
+                cnt[dz:dz + nz, dy:dy + ny, dx:dx + nx] += 1
+    return (acc / cnt).ravel()
 
 
 def unit_cube_vertices(nx, ny, nz):

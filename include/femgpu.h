@@ -68,7 +68,7 @@ enum fg_kind { FG_MASS = 1, FG_DIFF = 2, FG_MASS_DIFF = 3 };
 enum fg_mem { FG_HOST = 0, FG_DEVICE = 1 };
 
 /* Preconditioners and precisions of fg_pcg. */
-enum fg_precond { FG_PC_NONE = 0, FG_PC_JACOBI = 1, FG_PC_CHEBYSHEV = 2 };
+enum fg_precond { FG_PC_NONE = 0, FG_PC_JACOBI = 1, FG_PC_CHEBYSHEV = 2, FG_PC_CHEB_NN = 3 };
 enum fg_precision { FG_FP64 = 0, FG_FP32_IR = 1 };
 
 /* Quadrature-data formats (fg_op_set_qdata_format). */
@@ -103,7 +103,9 @@ typedef struct {
     double inner_rtol;     /* FP32_IR: FP32 residual reduction between FP64 reliable
                               updates (default 0.1) */
     int32_t check_interval;/* iterations between host polls of the device flag */
-    int32_t reserved;
+    int32_t nn_budget;     /* FG_PC_CHEB_NN: iterations after which an unconverged solve
+                              drops the learned term and continues as plain Chebyshev-
+                              preconditioned CG (0 = never) */
 } fg_cfg;
 
 typedef struct {
@@ -116,6 +118,8 @@ typedef struct {
     int64_t applies;         /* operator applications */
     double lmax;             /* Chebyshev upper bound used */
     double solve_ms;         /* device time of the solve */
+    int32_t nn_fallback;     /* FG_PC_CHEB_NN: 1 if the solve fell back to plain Chebyshev */
+    int32_t reserved;
 } fg_result;
 
 /* Defaults of SolverConfig::default() (crates/solver/src/lib.rs:116-120). */
@@ -245,6 +249,43 @@ typedef struct {
  * condition in (zero on the Dirichlet DOFs), u(n_steps*dt) out. */
 FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_steps,
                      const fg_cfg *cfg, fg_sdirk_result *res, int mem);
+
+/* ---- learned coarse correction ------------------------------------------
+ * No reference counterpart (fem-rs has no learned components).  A small 3-D
+ * U-net (3 levels, channels c0/c1/c2, default 16/32/48, ~250k parameters,
+ * BF16 tensors with FP32 accumulation) maps a restricted residual and the
+ * restricted log-coefficient to an error correction on the vertex grid
+ * coarsened once from a Q1 operator's DOF grid; with FG_PC_CHEB_NN, fg_pcg
+ * runs flexible CG with z = Chebyshev(r) + s P(UNet(R r / s, R log kappa)). */
+typedef struct fg_unet fg_unet;
+FG_API int fg_unet_create(const int channels[3], uint64_t seed, fg_unet **out);
+FG_API void fg_unet_destroy(fg_unet *net);
+FG_API int64_t fg_unet_num_params(const fg_unet *net);
+/* Parameters / gradients as one FP32 array: per layer W[cout][27][cin] (tap =
+ * (dz+1)*9 + (dy+1)*3 + (dx+1)), then b[cout]; layers in the order
+ * l0a, l0b, l1a, l1b, l2a, l2b, l1c, l0c, out. */
+FG_API int fg_unet_get_params(fg_unet *net, float *params);
+FG_API int fg_unet_set_params(fg_unet *net, const float *params);
+FG_API int fg_unet_get_grads(fg_unet *net, float *grads);
+/* in: [B][Z][Y][X][2] FP32, out: [B][Z][Y][X] FP32 (channel 0); Z, Y, X = 1 mod 4, >= 5. */
+FG_API int fg_unet_forward(fg_unet *net, const float *in, int B, int Z, int Y, int X, float *out, int mem);
+/* mean squared error of output channel 0 against target [B][Z][Y][X] and its
+ * gradients (no update) / one Adam step with learning rate lr. */
+FG_API int fg_unet_loss_grad(fg_unet *net, const float *in, const float *target, int B, int Z, int Y,
+                             int X, float *loss, int mem);
+FG_API int fg_unet_train_step(fg_unet *net, const float *in, const float *target, int B, int Z, int Y,
+                              int X, float lr, float *loss, int mem);
+/* kappa at the DOFs (plain layout, host) for the log-coefficient channel;
+ * Q1 operators whose element counts are multiples of 8 only. */
+FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal);
+/* Attach (or with NULL detach) a network used by FG_PC_CHEB_NN. */
+FG_API int fg_op_attach_unet(fg_op *op, fg_unet *net);
+/* Training pairs from a plain Chebyshev-PCG solve (x0 = 0): at iterations
+ * 0, every, 2*every, ... input [Zc][Yc][Xc][2] = (R r_k / s_k, R log kappa),
+ * target [Zc][Yc][Xc] = (x* - x_k) at the coarse vertices / s_k, with
+ * s_k = rms(R r_k); device FP32 buffers for max_pairs pairs. */
+FG_API int fg_op_collect_pairs(fg_op *op, const double *b, const fg_cfg *cfg, int every, int max_pairs,
+                               float *in, float *target, int *n_pairs);
 
 /* Synchronise the handle's stream and report device-side errors
  * (FG_DEVICE_TIMEOUT, FG_BOUNDS). */
