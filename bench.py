@@ -37,10 +37,10 @@ sys.path.insert(0, os.path.join(ROOT, "fem-rs_b200"))
 METRIC = "time to 1e-8 FP64 residual & PA GDOF/s on 1 B200: chosen vs plain FP64 PCG"
 WORKLOADS = {
     # name: (n elements per direction, order)
-    "c1a": (128, 2),   # 128^3 Q2, 17.0M DOFs (headline)
-    "c1b": (64, 3),    # 64^3 Q3, 7.2M DOFs
-    "c4": (128, 1),    # 128^3 Q1, 2.15M DOFs
-    "small": (64, 2),  # 64^3 Q2, 2.15M DOFs (profiling case, qdata 340 MB > L2)
+    "q2_128": (128, 2),  # 128^3 Q2, 17.0M DOFs (headline)
+    "q3_64": (64, 3),    # 64^3 Q3, 7.2M DOFs
+    "q1_128": (128, 1),  # 128^3 Q1, 2.15M DOFs
+    "q2_64": (64, 2),    # 64^3 Q2, 2.15M DOFs (profiling case, qdata 340 MB > L2)
 }
 
 
@@ -203,7 +203,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c1a", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="q2_128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-heat", action="store_true")
@@ -374,7 +374,7 @@ def main():
     op.set_qdata_format(femgpu.QDATA_FULL)
     fp32_apply = variants
 
-    # configs[3]: SDIRK-2 heat stepping, 64^3 Q2, lognormal kappa, dt = 1e-3,
+    # SDIRK-2 heat stepping, 64^3 Q2, lognormal kappa, dt = 1e-3,
     # u0 = sin sin sin; FP64 stage solves vs FP32 (reliable-update) stage solves
     heat = None
     if not args.no_heat:
@@ -406,7 +406,7 @@ def main():
         K.close()
         S.close()
 
-    # configs[2]: batched uneven solves, n ~ U{8..48}, p ~ U{1,2,3}, own lognormal
+    # batched uneven solves, n ~ U{8..48}, p ~ U{1,2,3}, own lognormal
     # kappa (sigma2 ~ U[0.25,2], ell ~ U[0.05,0.3]) and RHS M xi, FP32 mixed precision
     batch = None
     if not args.no_batch:

@@ -176,8 +176,10 @@ struct fg_op {
     // affine-compressed quadrature data (fg_op_set_qdata_format), FP64 and FP32
     double *sd_u = nullptr, *sd_k1 = nullptr, *sd_w = nullptr;  // SDIRK-2 stepping
     // learned coarse correction (Q1 operators): coarse log kappa, network, scratch
-    float *nn_lk = nullptr, *nn_rc = nullptr;
+    float *nn_lk = nullptr, *nn_rc = nullptr, *nn_oc = nullptr;
+    std::vector<float *> nn_tmp;  // intermediate levels 1 .. nn_levels-1
     double *nn_scale = nullptr;
+    int nn_levels = 1;  // coarsenings between the DOF lattice and the network volume
     fg_unet *nn = nullptr;
     int fmt = 0;
     double *qa64 = nullptr;
@@ -205,6 +207,8 @@ static void free_op(fg_op *op) {
     if (op->sd_u) cudaFree(op->sd_u);
     if (op->nn_lk) cudaFree(op->nn_lk);
     if (op->nn_rc) cudaFree(op->nn_rc);
+    if (op->nn_oc) cudaFree(op->nn_oc);
+    for (float *t : op->nn_tmp) cudaFree(t);
     if (op->nn_scale) cudaFree(op->nn_scale);
     if (op->sd_k1) cudaFree(op->sd_k1);
     if (op->sd_w) cudaFree(op->sd_w);
@@ -863,32 +867,76 @@ static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebC
 }
 
 // ---- learned coarse correction inside the preconditioner -------------------
-static Vol nn_coarse_vol(const fg_op *op) {
-    return Vol{1, (op->g.NK + 1) / 2, (op->g.NJ + 1) / 2, (op->g.NI + 1) / 2};
+// The DOF lattice (NI, NJ, NK) -- uniform for equispaced nodes of any order --
+// is coarsened nn_levels = L times (vertex-centred) to the network volume.
+// rcoarse = R^L r, s = rms(rcoarse), network input (rcoarse / s, R^L log kappa),
+// correction c = s 8^L P^L n (zero on essential DOFs).  With P^T = 8 R per
+// level the Galerkin optimum is n = (P^T A P)^{-1} (R^L r / s), whose scale
+// does not depend on the fine resolution.
+static Vol nn_vol(const fg_op *op, int level) {
+    Vol v{1, op->g.NK, op->g.NJ, op->g.NI};
+    for (int l = 0; l < level; ++l) v = Vol{1, (v.Z + 1) / 2, (v.Y + 1) / 2, (v.X + 1) / 2};
+    return v;
+}
+static Vol nn_coarse_vol(const fg_op *op) { return nn_vol(op, op->nn_levels); }
+static double nn_mult(const fg_op *op) { return std::ldexp(1.0, 3 * op->nn_levels); }
+
+// network-level coarse field of a fine native vector r (FP32, into dst)
+template <typename T> static int nn_restrict(fg_op *op, const T *r, float *dst) {
+    Grid g = op->g;
+    const int L = op->nn_levels;
+    int blocks;
+    Vol v1 = nn_vol(op, 1);
+    grid_launch(v1.nvox(), blocks);
+    fe_restrict_kernel<T><<<blocks, 256, 0, op->stream>>>(g, r, L == 1 ? dst : op->nn_tmp[0], v1);
+    for (int l = 2; l <= L; ++l) {
+        const Vol vf = nn_vol(op, l - 1), vc = nn_vol(op, l);
+        grid_launch(vc.nvox(), blocks);
+        restrict_f32_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_tmp[l - 2], vf, l == L ? dst : op->nn_tmp[l - 1],
+                                                            vc, 1.f);
+    }
+    CK(cudaGetLastError());
+    return FG_OK;
 }
 
-// z += s P(UNet(R r / s, R log kappa)),  s = rms(R r)
+// fine native z (+)= scale[0] * mult * P^L (network-level FP32 field oc)
+template <typename T>
+static int nn_prolong(fg_op *op, const float *oc, T *z, const double *scale, double mult, int accumulate) {
+    Grid g = op->g;
+    g.ess = op->ess_tags;
+    const float *f = oc;
+    for (int l = op->nn_levels - 1; l >= 1; --l) {
+        const Vol vc = nn_vol(op, l + 1), vf = nn_vol(op, l);
+        int blocks;
+        grid_launch(vf.nvox(), blocks);
+        prolong_f32_kernel<<<blocks, 256, 0, op->stream>>>(f, vc, op->nn_tmp[l - 1], vf);
+        f = op->nn_tmp[l - 1];
+    }
+    fe_prolong_f32_kernel<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(g, f, nn_vol(op, 1), z, scale, mult,
+                                                                        accumulate);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+// z += s 8^L P^L(UNet(R^L r / s, R^L log kappa)),  s = rms(R^L r)
 template <typename T> static int nn_precond_add(fg_op *op, const T *r, T *z) {
     fg_unet *u = op->nn;
     u->stream = op->stream;
     const Vol Vc = nn_coarse_vol(op);
     int rc;
     if ((rc = unet_ensure_bufs(u, 1, Vc.Z, Vc.Y, Vc.X))) return rc;
-    Grid g = op->g;
-    g.ess = op->ess_tags;
     const int64_t nv = Vc.nvox();
     int blocks;
     grid_launch(nv, blocks);
-    fe_restrict_kernel<T><<<blocks, 256, 0, op->stream>>>(g, r, op->nn_rc, Vc);
+    if ((rc = nn_restrict<T>(op, r, op->nn_rc))) return rc;
     rms_kernel<<<1, 256, 0, op->stream>>>(op->nn_rc, nv, op->nn_scale);
     pack_input_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, op->nn_lk, nv, op->nn_scale,
                                                       TView{u->buf.x0, 2, 0});
     CK(cudaGetLastError());
     if ((rc = unet_forward(u))) return rc;
-    fe_prolong_kernel<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(g, TView{u->buf.out, 8, 0}, Vc, z,
-                                                                   op->nn_scale, 1);
+    out0_to_f32_kernel<<<blocks, 256, 0, op->stream>>>(TView{u->buf.out, 8, 0}, nv, op->nn_oc);
     CK(cudaGetLastError());
-    return FG_OK;
+    return nn_prolong<T>(op, op->nn_oc, z, op->nn_scale, nn_mult(op), 1);
 }
 
 // Flexible CG (FCG(1), Notay) with z = Chebyshev(r) [+ learned correction];
@@ -1299,7 +1347,7 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
     return status;
 }
 
-// Batched solves (configs[2] form): every operator is solved by the
+// Batched solves (hundreds of uneven instances): every operator is solved by the
 // mixed-precision PCG (FP32 applies and smoother, FP64 reliable updates and
 // dot products) of fg_pcg, but each phase of an iteration is one launch over
 // all instances (per order/kind/format group for the applies), converged
@@ -1865,6 +1913,21 @@ static int unet_loss_grad(fg_unet *u, float *loss) {
     return FG_OK;
 }
 
+// Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the gradients in gw/gb
+static int unet_adam(fg_unet *u, float lr) {
+    u->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.f - std::pow(b1, (float)u->step), bc2 = 1.f - std::pow(b2, (float)u->step);
+    for (auto &L : u->L) {
+        const int nw = L.cout * L.kp;
+        adam_kernel<<<64, 256, 0, u->stream>>>(L.w, L.gw, L.mw, L.vw, nw, lr, b1, b2, 1e-8f, bc1, bc2, L.wb);
+        adam_kernel<<<1, 64, 0, u->stream>>>(L.b, L.gb, L.mb, L.vb, L.cout, lr, b1, b2, 1e-8f, bc1, bc2, nullptr);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(u->stream));
+    return FG_OK;
+}
+
 extern "C" {
 
 FG_API int fg_unet_create(const int channels[3], uint64_t seed, fg_unet **out) {
@@ -1973,46 +2036,52 @@ FG_API int fg_unet_train_step(fg_unet *u, const float *in, const float *target, 
                               float lr, float *loss, int mem) {
     int rc;
     if ((rc = fg_unet_loss_grad(u, in, target, B, Z, Y, X, loss, mem))) return rc;
-    u->step += 1;
-    const float b1 = 0.9f, b2 = 0.999f;
-    const float bc1 = 1.f - std::pow(b1, (float)u->step), bc2 = 1.f - std::pow(b2, (float)u->step);
-    for (auto &L : u->L) {
-        const int nw = L.cout * L.kp;
-        adam_kernel<<<64, 256, 0, u->stream>>>(L.w, L.gw, L.mw, L.vw, nw, lr, b1, b2, 1e-8f, bc1, bc2, L.wb);
-        adam_kernel<<<1, 64, 0, u->stream>>>(L.b, L.gb, L.mb, L.vb, L.cout, lr, b1, b2, 1e-8f, bc1, bc2, nullptr);
-    }
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(u->stream));
-    return FG_OK;
+    return unet_adam(u, lr);
 }
 
 // Coarse log-kappa channel of the learned correction: kappa at the DOFs
-// (plain layout, host), restricted to the coarse vertex grid.
-FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal) {
+// (plain layout, host), restricted `levels` times (1 to 4) to the network
+// volume.  Every level's extents must be odd and the network volume's 1 mod 4
+// and >= 5, so the DOF lattice's cell counts (p times the element counts) must
+// be multiples of 4 * 2^levels.
+FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal, int levels) {
     if (!op || !kappa_nodal) return fail(FG_INVALID_ARGUMENT, "NULL argument");
-    if (op->p != 1 || op->g.nx % 8 || op->g.ny % 8 || op->g.nz % 8)
-        return fail(FG_UNSUPPORTED, "the learned correction needs a Q1 operator with element counts "
-                                    "that are multiples of 8");
+    if (levels < 1 || levels > 4) return fail(FG_INVALID_ARGUMENT, "levels must be 1 to 4");
+    const int m = 4 << levels;
+    const int cx = op->g.NI - 1, cy = op->g.NJ - 1, cz = op->g.NK - 1;
+    if (cx % m || cy % m || cz % m || cx / m < 1 || cy / m < 1 || cz / m < 1)
+        return fail(FG_UNSUPPORTED, "the learned correction needs DOF-lattice cell counts (p * elements) "
+                                    "that are multiples of %d", m);
     std::lock_guard<std::mutex> lk(op->mu);
     CK(cudaSetDevice(op->device));
     int rc;
     if ((rc = ensure_solver_buffers(op))) return rc;
+    if (op->nn_lk && op->nn_levels != levels) {
+        float *bufs[] = {op->nn_lk, op->nn_rc, op->nn_oc};
+        for (float *b : bufs) cudaFree(b);
+        for (float *t : op->nn_tmp) cudaFree(t);
+        op->nn_tmp.clear();
+        op->nn_lk = op->nn_rc = op->nn_oc = nullptr;
+    }
+    op->nn_levels = levels;
     const Vol Vc = nn_coarse_vol(op);
     const int64_t nv = Vc.nvox();
     if (!op->nn_lk) {
         CK(cudaMalloc(&op->nn_lk, nv * sizeof(float)));
         CK(cudaMalloc(&op->nn_rc, nv * sizeof(float)));
-        CK(cudaMalloc(&op->nn_scale, 4 * sizeof(double)));
+        CK(cudaMalloc(&op->nn_oc, nv * sizeof(float)));
+        for (int l = 1; l < levels; ++l) {
+            float *t = nullptr;
+            CK(cudaMalloc(&t, nn_vol(op, l).nvox() * sizeof(float)));
+            op->nn_tmp.push_back(t);
+        }
+        if (!op->nn_scale) CK(cudaMalloc(&op->nn_scale, 4 * sizeof(double)));
     }
     std::vector<double> lg(op->N);
     for (int64_t i = 0; i < op->N; ++i) lg[i] = std::log(std::max(kappa_nodal[i], 1e-300));
     if ((rc = to_native(op, op->cd, lg.data(), FG_HOST))) return rc;
-    Grid g = op->g;
-    int blocks;
-    grid_launch(nv, blocks);
-    fe_restrict_kernel<double><<<blocks, 256, 0, op->stream>>>(g, op->cd, op->nn_lk, Vc);
-    CK(cudaGetLastError());
     // full weighting averages (its weights sum to 1 away from the boundary)
+    if ((rc = nn_restrict<double>(op, op->cd, op->nn_lk))) return rc;
     CK(cudaStreamSynchronize(op->stream));
     return FG_OK;
 }
@@ -2083,16 +2152,128 @@ FG_API int fg_op_collect_pairs(fg_op *op, const double *b, const fg_cfg *cfg_in,
     for (size_t j = 0; j < stash.size(); ++j) {
         if ((rc = apply_native(op, stash[j], op->ap, 0, 1, nullptr))) return rc;
         k_lincomb2<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r, 1.0, op->bw, -1.0, op->ap);
-        fe_restrict_kernel<double><<<blocks, 256, 0, op->stream>>>(g, op->r, op->nn_rc, Vc);
+        if ((rc = nn_restrict<double>(op, op->r, op->nn_rc))) return rc;
         rms_kernel<<<1, 256, 0, op->stream>>>(op->nn_rc, nv, op->nn_scale);
         pack_input_f32_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, op->nn_lk, nv, op->nn_scale,
                                                               d_in + (int64_t)j * nv * 2);
-        pair_target_kernel<<<blocks, 256, 0, op->stream>>>(g, op->xw, stash[j], Vc, op->nn_scale,
+        pair_target_kernel<<<blocks, 256, 0, op->stream>>>(g, op->xw, stash[j], Vc, 1 << op->nn_levels, op->nn_scale,
                                                            d_target + (int64_t)j * nv);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(op->stream));
     *n_pairs = (int)stash.size();
+    return check_device_error(op);
+}
+
+// Residuals of a plain Chebyshev-PCG solve of A x = b (x0 = 0) at iterations
+// 0, every, 2*every, ...: up to max_res native-layout FP64 vectors written to
+// d_out ([max_res][fg_op_native_len], device); the count in *n_res.
+FG_API int fg_op_collect_residuals(fg_op *op, const double *b, const fg_cfg *cfg_in, int every, int max_res,
+                                   double *d_out, int *n_res) {
+    if (!op || !b || !d_out || !n_res || every < 1 || max_res < 1)
+        return fail(FG_INVALID_ARGUMENT, "bad arguments");
+    fg_cfg cfg;
+    if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
+    cfg.precision = FG_FP64;
+    cfg.precond = FG_PC_CHEBYSHEV;
+    cfg.check_interval = every;
+    int rc;
+    if ((rc = validate_cfg(cfg))) return rc;
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    if ((rc = ensure_solver_buffers(op)) || (rc = ensure_dinv(op))) return rc;
+    if (!op->have_lmax) {
+        if ((rc = estimate_lmax(op, cfg.power_iters > 0 ? cfg.power_iters : 20, &op->lmax_est))) return rc;
+        op->have_lmax = true;
+    }
+    const double lmax = (cfg.lmax_safety > 0 ? cfg.lmax_safety : 1.1) * op->lmax_est;
+    const ChebCoef cc = cheb_coefs(lmax / (cfg.lmin_ratio > 0 ? cfg.lmin_ratio : 30.0), lmax, cfg.cheb_degree);
+    const int64_t n = op->Nn;
+    int count = 0;
+    auto push = [&]() -> int {
+        if (count >= max_res) return FG_OK;
+        CK(cudaMemcpyAsync(d_out + (int64_t)count * n, op->r, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                           op->stream));
+        ++count;
+        return FG_OK;
+    };
+    if ((rc = to_native(op, op->bw, b, FG_HOST))) return rc;
+    CK(cudaMemsetAsync(op->xw, 0, n * sizeof(double), op->stream));
+    CK(cudaMemcpyAsync(op->r, op->bw, n * sizeof(double), cudaMemcpyDeviceToDevice, op->stream));
+    if ((rc = push())) return rc;
+    PcgBufs<double> B{op->qd, op->face, op->dinv, op->xw, op->bw, op->r, op->z, op->pv, op->ap,
+                      op->cres, op->cd, op->ct, op->st};
+    set_state(op, op->st, cfg.rtol, cfg.atol, cfg.max_iter);
+    SolverState h{};
+    int64_t applies = 0;
+    if ((rc = pcg_run<double>(op, B, false, &cc, cfg.max_iter, every, false, &h, &applies,
+                              [&](int) { return push(); })))
+        return rc;
+    CK(cudaStreamSynchronize(op->stream));
+    *n_res = count;
+    return check_device_error(op);
+}
+
+// One Adam step of the learned coarse correction on the energy loss of B
+// residuals r_b (device, native layout, [B][fg_op_native_len] FP64, zero on
+// essential DOFs).  Per sample, with s = rms(R^L r) and network output n,
+//   c = s 8^L P^L n  (zero on essential DOFs),
+//   loss_b = (1/2 c.Ac - c.r) / (s^2 64^L Nc),   Nc = network voxels,
+// whose minimiser over c in range(P^L) is the Galerkin coarse correction;
+// d loss_b / d n = R^L (A c - r) / (s Nc)  (P^T = 8 R per level).  The
+// reported loss is the batch mean.
+FG_API int fg_unet_train_energy(fg_unet *u, fg_op *op, const double *d_res, int B, float lr, float *loss) {
+    if (!u || !op || !d_res || B < 1) return fail(FG_INVALID_ARGUMENT, "bad arguments");
+    if (!op->nn_lk) return fail(FG_INVALID_ARGUMENT, "call fg_op_set_nodal_kappa first");
+    if (u->device != op->device) return fail(FG_INVALID_ARGUMENT, "network on another device");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    int rc;
+    if ((rc = ensure_solver_buffers(op))) return rc;
+    u->stream = op->stream;
+    const Vol Vc = nn_coarse_vol(op);
+    if ((rc = unet_ensure_bufs(u, B, Vc.Z, Vc.Y, Vc.X))) return rc;
+    const int64_t nv = Vc.nvox(), n = op->Nn;
+    double *tb = nullptr;  // per sample: s, c.Ac, c.r
+    CK(cudaMalloc(&tb, (size_t)B * 4 * sizeof(double)));
+    struct Free { double *p; ~Free() { cudaFree(p); } } fr{tb};
+    int blocks;
+    grid_launch(nv, blocks);
+    UnetBufs &ub = u->buf;
+    for (int b = 0; b < B; ++b) {
+        if ((rc = nn_restrict<double>(op, d_res + (int64_t)b * n, op->nn_rc))) return rc;
+        rms_kernel<<<1, 256, 0, op->stream>>>(op->nn_rc, nv, tb + 4 * b);
+        pack_input_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, op->nn_lk, nv, tb + 4 * b,
+                                                          TView{ub.x0 + (int64_t)b * nv * 2, 2, 0});
+    }
+    CK(cudaGetLastError());
+    if ((rc = unet_forward(u))) return rc;
+    const float coef = (float)(1.0 / ((double)nv * B));
+    const double mult = nn_mult(op);
+    for (int b = 0; b < B; ++b) {
+        const double *r = d_res + (int64_t)b * n;
+        out0_to_f32_kernel<<<blocks, 256, 0, op->stream>>>(TView{ub.out + (int64_t)b * nv * 8, 8, 0}, nv,
+                                                           op->nn_oc);
+        if ((rc = nn_prolong<double>(op, op->nn_oc, op->pv, tb + 4 * b, mult, 0))) return rc;
+        if ((rc = apply_native(op, op->pv, op->ap, 0, 1, nullptr))) return rc;
+        k_energy_terms<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->pv, op->ap, r, op->partials, op->st);
+        CK(cudaMemcpyAsync(tb + 4 * b + 1, &op->st->tmp[0], 2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                           op->stream));
+        if ((rc = nn_restrict<double>(op, op->ap, op->nn_rc))) return rc;
+        energy_grad_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, nv, coef, tb + 4 * b,
+                                                           TView{ub.dout + (int64_t)b * nv * 8, 8, 0});
+        CK(cudaGetLastError());
+    }
+    if ((rc = unet_backward(u))) return rc;
+    if ((rc = unet_adam(u, lr))) return rc;
+    std::vector<double> h((size_t)B * 4);
+    CK(cudaMemcpy(h.data(), tb, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    double L = 0.0;
+    for (int b = 0; b < B; ++b) {
+        const double sc = h[4 * b] > 0.0 ? h[4 * b] : 1.0;
+        L += (0.5 * h[4 * b + 1] - h[4 * b + 2]) / (sc * sc * mult * mult * (double)nv);
+    }
+    if (loss) *loss = (float)(L / B);
     return check_device_error(op);
 }
 

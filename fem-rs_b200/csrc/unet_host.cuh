@@ -140,22 +140,32 @@ static int unet_ensure_bufs(fg_unet *u, int B, int Z, int Y, int X) {
     return FG_OK;
 }
 
-static int conv_fwd(fg_unet *u, const ConvLayer &l, const TView &in, const Vol &V, const __nv_bfloat16 *w,
-                    int cin, int cout, int kp, const float *bias, TView out, int relu) {
-    const int64_t nv = V.nvox();
-    const int blocks = (int)((nv + 63) / 64);
+template <int KS>
+static int conv_fwd_ks(fg_unet *u, const TView &in, const Vol &V, const __nv_bfloat16 *w, int cin, int cout,
+                       int kp, const float *bias, TView out, int relu) {
+    const int64_t tiles = (V.nvox() + 15) / 16;
+    const int blocks = (int)((tiles + (4 / KS) - 1) / (4 / KS));
     switch (cout / 8) {
-    case 1: conv3_fwd_kernel<1><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 2: conv3_fwd_kernel<2><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 4: conv3_fwd_kernel<4><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 6: conv3_fwd_kernel<6><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 8: conv3_fwd_kernel<8><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 10: conv3_fwd_kernel<10><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
+    case 1: conv3_fwd_kernel<1, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
+    case 2: conv3_fwd_kernel<2, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
+    case 4: conv3_fwd_kernel<4, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
+    case 6: conv3_fwd_kernel<6, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
+    case 8: conv3_fwd_kernel<8, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
+    case 10: conv3_fwd_kernel<10, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
     default: return fail(FG_UNSUPPORTED, "conv output channels %d not supported", cout);
     }
-    (void)l;
     CK(cudaGetLastError());
     return FG_OK;
+}
+
+// K split chosen so that about 148 x 32 warps are in flight
+static int conv_fwd(fg_unet *u, const ConvLayer &l, const TView &in, const Vol &V, const __nv_bfloat16 *w,
+                    int cin, int cout, int kp, const float *bias, TView out, int relu) {
+    (void)l;
+    const int64_t tiles = (V.nvox() + 15) / 16;
+    if (tiles >= 148 * 32) return conv_fwd_ks<1>(u, in, V, w, cin, cout, kp, bias, out, relu);
+    if (tiles >= 148 * 16) return conv_fwd_ks<2>(u, in, V, w, cin, cout, kp, bias, out, relu);
+    return conv_fwd_ks<4>(u, in, V, w, cin, cout, kp, bias, out, relu);
 }
 
 static int layer_fwd(fg_unet *u, int li, const TView &in, const Vol &V, TView out, int relu) {

@@ -85,17 +85,23 @@ __device__ __forceinline__ uint32_t gather_pair(const TView &in, const Vol &V, c
     return ld_bf16x2(in.p + vv * in.cs + in.co + c.ci);
 }
 
-// One warp: 16 voxels x NT*8 output channels.  Cin even, Cout = NT*8 <= 64.
-template <int NT>
+// One tile: 16 voxels x NT*8 output channels, computed by KS warps that split
+// the K loop (KS in {1, 2, 4}; a block of 4 warps holds 4/KS tiles) and sum
+// their accumulators in shared memory in warp order.  Small volumes use KS = 4
+// so that the serial chain of gathers per warp is short.  Cin even,
+// Cout = NT*8 <= 80.
+template <int NT, int KS>
 __global__ void __launch_bounds__(128) conv3_fwd_kernel(const TView in, const Vol V, int Cin,
                                                         const __nv_bfloat16 *__restrict__ W, int Kp,
                                                         const float *__restrict__ bias, TView out,
                                                         int relu) {
+    constexpr int TPB = 4 / KS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = warp / KS, part = warp % KS;
     const int gid = lane >> 2, t4 = lane & 3;
     const int64_t nv = V.nvox();
-    const int64_t m0 = ((int64_t)blockIdx.x * 4 + warp) * 16;
-    if (m0 >= nv) return;
+    const int64_t m0 = ((int64_t)blockIdx.x * TPB + tile) * 16;
+    const bool active = m0 < nv;
     const int K = 27 * Cin;
     const int64_t v0 = m0 + gid, v1 = m0 + gid + 8;
     int b0, z0, y0, x0, b1, z1, y1, x1;
@@ -105,20 +111,42 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(const TView in, const Vo
     float acc[NT][4];
 #pragma unroll
     for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
-    for (int k0 = 0; k0 < Kp; k0 += 16) {
-        const int ka = k0 + t4 * 2, kb = ka + 8;
-        const KCol ca = kcol(ka, Cin, K), cb = kcol(kb, Cin, K);
-        uint32_t a[4];
-        a[0] = gather_pair(in, V, ca, ok0, b0, z0, y0, x0);
-        a[1] = gather_pair(in, V, ca, ok1, b1, z1, y1, x1);
-        a[2] = gather_pair(in, V, cb, ok0, b0, z0, y0, x0);
-        a[3] = gather_pair(in, V, cb, ok1, b1, z1, y1, x1);
+    if (active) {
+#pragma unroll 4
+        for (int k0 = part * 16; k0 < Kp; k0 += 16 * KS) {
+            const int ka = k0 + t4 * 2, kb = ka + 8;
+            const KCol ca = kcol(ka, Cin, K), cb = kcol(kb, Cin, K);
+            uint32_t a[4];
+            a[0] = gather_pair(in, V, ca, ok0, b0, z0, y0, x0);
+            a[1] = gather_pair(in, V, ca, ok1, b1, z1, y1, x1);
+            a[2] = gather_pair(in, V, cb, ok0, b0, z0, y0, x0);
+            a[3] = gather_pair(in, V, cb, ok1, b1, z1, y1, x1);
 #pragma unroll
-        for (int j = 0; j < NT; ++j) {
-            const __nv_bfloat16 *wr = W + (int64_t)(j * 8 + gid) * Kp;
-            mma_bf16_16816(acc[j], a, ld_bf16x2(wr + ka), ld_bf16x2(wr + kb));
+            for (int j = 0; j < NT; ++j) {
+                const __nv_bfloat16 *wr = W + (int64_t)(j * 8 + gid) * Kp;
+                mma_bf16_16816(acc[j], a, ld_bf16x2(wr + ka), ld_bf16x2(wr + kb));
+            }
         }
     }
+    if constexpr (KS > 1) {
+        __shared__ float red[TPB * (KS - 1)][NT * 4][32];
+        if (part > 0) {
+            const int slot = tile * (KS - 1) + part - 1;
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) red[slot][j * 4 + e][lane] = acc[j][e];
+        }
+        __syncthreads();
+        if (part > 0) return;
+#pragma unroll
+        for (int q = 0; q < KS - 1; ++q)
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[j][e] += red[tile * (KS - 1) + q][j * 4 + e][lane];
+    }
+    if (!active) return;
 #pragma unroll
     for (int j = 0; j < NT; ++j) {
         const int n = j * 8 + t4 * 2;
@@ -436,15 +464,86 @@ __global__ void fe_prolong_kernel(const Grid g, const TView in, const Vol Vc, T 
     }
 }
 
-// training pair from a PCG iterate: target = (x* - x_k) injected at coarse
-// vertices, / scale
+// single-channel FP32 vertex-centred transfers between coarse levels
+__global__ void restrict_f32_kernel(const float *__restrict__ f, const Vol Vf, float *__restrict__ c,
+                                    const Vol Vc, float scale) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < Vc.nvox(); i += (int64_t)gridDim.x * blockDim.x) {
+        int b, z, y, x;
+        vox_coords(Vc, i, b, z, y, x);
+        float s = 0.f;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int fz = 2 * z + dz, fy = 2 * y + dy, fx = 2 * x + dx;
+                    if (fz < 0 || fz >= Vf.Z || fy < 0 || fy >= Vf.Y || fx < 0 || fx >= Vf.X) continue;
+                    const float w = (dz ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dx ? 0.5f : 1.f) * 0.125f;
+                    s += w * f[(((int64_t)b * Vf.Z + fz) * Vf.Y + fy) * Vf.X + fx];
+                }
+        c[i] = scale * s;
+    }
+}
+__global__ void prolong_f32_kernel(const float *__restrict__ c, const Vol Vc, float *__restrict__ f,
+                                   const Vol Vf) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < Vf.nvox(); i += (int64_t)gridDim.x * blockDim.x) {
+        int b, z, y, x;
+        vox_coords(Vf, i, b, z, y, x);
+        float s = 0.f;
+        for (int a = 0; a <= (z & 1); ++a)
+            for (int bb = 0; bb <= (y & 1); ++bb)
+                for (int d = 0; d <= (x & 1); ++d) {
+                    const float w = ((z & 1) ? 0.5f : 1.f) * ((y & 1) ? 0.5f : 1.f) * ((x & 1) ? 0.5f : 1.f);
+                    s += w * c[(((int64_t)b * Vc.Z + (z >> 1) + a) * Vc.Y + (y >> 1) + bb) * Vc.X + (x >> 1) + d];
+                }
+        f[i] = s;
+    }
+}
+
+// z (native, T) (+)= scale[0] * mult * P(cf) for an FP32 field cf on the
+// first coarse level; zero on essential DOFs and pads
+template <typename T>
+__global__ void fe_prolong_f32_kernel(const Grid g, const float *__restrict__ cf, const Vol Vc, T *__restrict__ z,
+                                      const double *__restrict__ scale, double mult, int accumulate) {
+    const double sc = (scale ? scale[0] : 1.0) * mult;
+    const int64_t n = (int64_t)g.NIp * g.NJ * g.NK;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int I = (int)(i % g.NIp);
+        const int64_t row = i / g.NIp;
+        const int J = (int)(row % g.NJ), K = (int)(row / g.NJ);
+        double s = 0.0;
+        if (I < g.NI && !g.is_ess(I, J, K)) {
+            for (int a = 0; a <= (K & 1); ++a)
+                for (int bb = 0; bb <= (J & 1); ++bb)
+                    for (int d = 0; d <= (I & 1); ++d) {
+                        const double w = ((K & 1) ? 0.5 : 1.0) * ((J & 1) ? 0.5 : 1.0) * ((I & 1) ? 0.5 : 1.0);
+                        s += w * (double)cf[((int64_t)((K >> 1) + a) * Vc.Y + (J >> 1) + bb) * Vc.X + (I >> 1) + d];
+                    }
+            s *= sc;
+        }
+        z[i] = accumulate ? (T)((double)z[i] + s) : (T)s;
+    }
+}
+
+// energy-loss gradient into the output-gradient buffer:
+// dout[v][0] = coef / scale[0] * g[v], other channels 0
+__global__ void energy_grad_kernel(const float *__restrict__ gc, int64_t nv, float coef,
+                                   const double *__restrict__ scale, TView dout) {
+    const float f = (float)(coef / (scale[0] > 0.0 ? scale[0] : 1.0));
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
+        __nv_bfloat16 *o = dout.p + i * dout.cs + dout.co;
+        o[0] = __float2bfloat16(f * gc[i]);
+        for (int c = 1; c < dout.cs; ++c) o[c] = __float2bfloat16(0.f);
+    }
+}
+
+// training pair from a PCG iterate: target = (x* - x_k) injected at the
+// network vertices (every stride-th DOF), / scale
 __global__ void pair_target_kernel(const Grid g, const double *__restrict__ xs, const double *__restrict__ xk,
-                                   const Vol Vc, const double *__restrict__ scale, float *__restrict__ t) {
+                                   const Vol Vc, int stride, const double *__restrict__ scale, float *__restrict__ t) {
     const double s = scale[0] > 0.0 ? scale[0] : 1.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < Vc.nvox(); i += (int64_t)gridDim.x * blockDim.x) {
         int b, z, y, x;
         vox_coords(Vc, i, b, z, y, x);
-        const int64_t d = g.dof(2 * x, 2 * y, 2 * z);
+        const int64_t d = g.dof(stride * x, stride * y, stride * z);
         t[i] = (float)((xs[d] - xk[d]) / s);
     }
 }

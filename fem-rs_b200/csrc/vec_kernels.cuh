@@ -832,6 +832,29 @@ __global__ void __launch_bounds__(VEC_THREADS) k_scale_tmp(int64_t n, double *__
     }
 }
 
+// energy terms of a coarse correction c:  st->tmp[0] = c . (A c),
+// st->tmp[1] = c . r;  ac <- A c - r
+__global__ void __launch_bounds__(VEC_THREADS) k_energy_terms(int64_t n, const double *__restrict__ c,
+                                                              double *__restrict__ ac, const double *__restrict__ r,
+                                                              double *partials, SolverState *st) {
+    double a[2] = {0.0, 0.0};
+    FG_VEC4_LOOP(q, n) {
+        const V4<double> cv = ld4(c, q), rv = ld4(r, q);
+        V4<double> av = ld4(ac, q);
+        FG_K4 {
+            a[0] += cv.a[k] * av.a[k];
+            a[1] += cv.a[k] * rv.a[k];
+            av.a[k] -= rv.a[k];
+        }
+        st4(ac, q, av);
+    }
+    double tot[2];
+    if (grid_sum<2>(a, partials, st, tot) && threadIdx.x == 0) {
+        st->tmp[0] = tot[0];
+        st->tmp[1] = tot[1];
+    }
+}
+
 // ---- flexible CG (Notay's FCG with one stored direction) -------------------
 // beta = -(z . A p_old) / (p_old . A p_old)  (0 on init);  then p = z + beta p
 template <typename T>

@@ -42,7 +42,8 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_op_set_qdata_format", "fg_sdirk2", "fg_batch_pcg",
            "fg_unet_create", "fg_unet_destroy", "fg_unet_num_params", "fg_unet_get_params",
            "fg_unet_set_params", "fg_unet_get_grads", "fg_unet_forward", "fg_unet_loss_grad",
-           "fg_unet_train_step", "fg_op_set_nodal_kappa", "fg_op_attach_unet", "fg_op_collect_pairs")
+           "fg_unet_train_step", "fg_op_set_nodal_kappa", "fg_op_attach_unet", "fg_op_collect_pairs",
+           "fg_op_collect_residuals", "fg_unet_train_energy")
 
 
 class FgMesh(C.Structure):
@@ -111,9 +112,11 @@ def lib():
         L.fg_unet_forward.argtypes = [vp, vp, i, i, i, i, vp, i]
         L.fg_unet_loss_grad.argtypes = [vp, vp, vp, i, i, i, i, vp, i]
         L.fg_unet_train_step.argtypes = [vp, vp, vp, i, i, i, i, C.c_float, vp, i]
-        L.fg_op_set_nodal_kappa.argtypes = [vp, vp]
+        L.fg_op_set_nodal_kappa.argtypes = [vp, vp, i]
         L.fg_op_attach_unet.argtypes = [vp, vp]
         L.fg_op_collect_pairs.argtypes = [vp, vp, vp, i, i, vp, vp, vp]
+        L.fg_op_collect_residuals.argtypes = [vp, vp, vp, i, i, vp, vp]
+        L.fg_unet_train_energy.argtypes = [vp, vp, vp, i, C.c_float, vp]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
@@ -530,10 +533,33 @@ class UNet:
     def train_step(self, inp, target, lr):
         return self._step(lib().fg_unet_train_step, inp, target, C.c_float(lr))
 
+    def train_energy(self, op, res, lr):
+        """One Adam step on the energy loss of the residuals ``res`` (torch CUDA
+        float64 tensor [B, native_len]) for the operator ``op``; returns the
+        batch-mean loss (c.Ac/2 - c.r) / (s^2 Nc)."""
+        assert res.dtype.is_floating_point and res.element_size() == 8 and res.is_contiguous()
+        assert res.shape[-1] == op.native_len
+        loss = C.c_float()
+        _check(lib().fg_unet_train_energy(self._h, op.handle, res.data_ptr(), int(res.shape[0]),
+                                          C.c_float(lr), C.byref(loss)))
+        return float(loss.value)
 
-def set_nodal_kappa(op, kappa_nodal):
+
+def set_nodal_kappa(op, kappa_nodal, levels=1):
+    """kappa at the DOFs for the log-coefficient channel; ``levels`` (1 to 4)
+    coarsenings between the DOF lattice and the network volume."""
     k = np.ascontiguousarray(kappa_nodal, dtype=np.float64)
-    _check(lib().fg_op_set_nodal_kappa(op.handle, k.ctypes.data))
+    _check(lib().fg_op_set_nodal_kappa(op.handle, k.ctypes.data, int(levels)))
+    op._nn_levels = int(levels)
+
+
+def nn_volume(op):
+    """(Z, Y, X) of the network volume of an operator after set_nodal_kappa."""
+    L = getattr(op, "_nn_levels", 1)
+    z, y, x = op.NK, op.NJ, op.NI
+    for _ in range(L):
+        z, y, x = (z + 1) // 2, (y + 1) // 2, (x + 1) // 2
+    return z, y, x
 
 
 def attach_unet(op, net):
@@ -544,7 +570,7 @@ def collect_pairs(op, b, every, max_pairs, cfg=None):
     """Training pairs (torch CUDA float32 tensors in [n,Zc,Yc,Xc,2], target [n,Zc,Yc,Xc])."""
     import torch
     cfg = cfg or SolverConfig(rtol=1e-10, max_iter=20000)
-    Zc, Yc, Xc = (op.NK + 1) // 2, (op.NJ + 1) // 2, (op.NI + 1) // 2
+    Zc, Yc, Xc = nn_volume(op)
     din = torch.zeros((max_pairs, Zc, Yc, Xc, 2), dtype=torch.float32, device="cuda")
     dt = torch.zeros((max_pairs, Zc, Yc, Xc), dtype=torch.float32, device="cuda")
     b = np.ascontiguousarray(b, dtype=np.float64)
@@ -556,18 +582,40 @@ def collect_pairs(op, b, every, max_pairs, cfg=None):
     return din[:n], dt[:n]
 
 
+def collect_residuals(op, b, every, max_res, cfg=None):
+    """Recurrence residuals of a plain Chebyshev-PCG solve from x0 = 0 at
+    iterations 0, every, 2*every, ... (torch CUDA float64 [n, native_len])."""
+    import torch
+    cfg = cfg or SolverConfig(rtol=1e-10, max_iter=20000)
+    out = torch.zeros((max_res, op.native_len), dtype=torch.float64, device="cuda")
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n = C.c_int()
+    c = cfg.to_c(PC_CHEBYSHEV)
+    _check(lib().fg_op_collect_residuals(op.handle, b.ctypes.data, C.byref(c), int(every), int(max_res),
+                                         out.data_ptr(), C.byref(n)))
+    return out[:n.value]
+
+
 def nodal_kappa_from_q(kq, nx, ny, nz, p=1):
-    """kappa at the DOFs of a Q1 grid: average of the kappa values of the
-    quadrature points of the (up to 8) elements around each vertex."""
+    """kappa on the DOF lattice ((p*nz+1, p*ny+1, p*nx+1), plain layout): at each
+    lattice node the mean over the elements whose closed box holds it of the
+    element's mean quadrature-point kappa."""
     nq = p + 1
-    k = np.asarray(kq).reshape(nz, ny, nx, nq ** 3).mean(axis=-1)
-    acc = np.zeros((nz + 1, ny + 1, nx + 1))
+    try:
+        import torch
+        if isinstance(kq, torch.Tensor):
+            kq = kq.detach().double().cpu().numpy()
+    except ImportError:
+        pass
+    k = np.asarray(kq, dtype=np.float64).reshape(nz, ny, nx, nq ** 3).mean(axis=-1)
+    acc = np.zeros((p * nz + 1, p * ny + 1, p * nx + 1))
     cnt = np.zeros_like(acc)
-    for dz in (0, 1):
-        for dy in (0, 1):
-            for dx in (0, 1):
-                acc[dz:dz + nz, dy:dy + ny, dx:dx + nx] += k
-                cnt[dz:dz + nz, dy:dy + ny, dx:dx + nx] += 1
+    for dz in range(p + 1):
+        for dy in range(p + 1):
+            for dx in range(p + 1):
+                sl = (slice(dz, dz + p * nz, p), slice(dy, dy + p * ny, p), slice(dx, dx + p * nx, p))
+                acc[sl] += k
+                cnt[sl] += 1
     return (acc / cnt).ravel()
 
 

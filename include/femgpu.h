@@ -255,8 +255,10 @@ FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_ste
  * U-net (3 levels, channels c0/c1/c2, default 16/32/48, ~250k parameters,
  * BF16 tensors with FP32 accumulation) maps a restricted residual and the
  * restricted log-coefficient to an error correction on the vertex grid
- * coarsened once from a Q1 operator's DOF grid; with FG_PC_CHEB_NN, fg_pcg
- * runs flexible CG with z = Chebyshev(r) + s P(UNet(R r / s, R log kappa)). */
+ * coarsened L = 1..4 times from an operator's DOF lattice (equispaced nodes
+ * of any order form a uniform lattice; full-weighting R, trilinear P); with
+ * FG_PC_CHEB_NN, fg_pcg runs flexible CG with
+ * z = Chebyshev(r) + s 8^L P^L(UNet(R^L r / s, R^L log kappa)), s = rms(R^L r). */
 typedef struct fg_unet fg_unet;
 FG_API int fg_unet_create(const int channels[3], uint64_t seed, fg_unet **out);
 FG_API void fg_unet_destroy(fg_unet *net);
@@ -275,9 +277,10 @@ FG_API int fg_unet_loss_grad(fg_unet *net, const float *in, const float *target,
                              int X, float *loss, int mem);
 FG_API int fg_unet_train_step(fg_unet *net, const float *in, const float *target, int B, int Z, int Y,
                               int X, float lr, float *loss, int mem);
-/* kappa at the DOFs (plain layout, host) for the log-coefficient channel;
- * Q1 operators whose element counts are multiples of 8 only. */
-FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal);
+/* kappa at the DOFs (plain layout, host) for the log-coefficient channel and
+ * the coarsening depth levels (1 to 4); the DOF lattice's cell counts
+ * (p * elements per direction) must be multiples of 4 * 2^levels. */
+FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal, int levels);
 /* Attach (or with NULL detach) a network used by FG_PC_CHEB_NN. */
 FG_API int fg_op_attach_unet(fg_op *op, fg_unet *net);
 /* Training pairs from a plain Chebyshev-PCG solve (x0 = 0): at iterations
@@ -286,6 +289,15 @@ FG_API int fg_op_attach_unet(fg_op *op, fg_unet *net);
  * s_k = rms(R r_k); device FP32 buffers for max_pairs pairs. */
 FG_API int fg_op_collect_pairs(fg_op *op, const double *b, const fg_cfg *cfg, int every, int max_pairs,
                                float *in, float *target, int *n_pairs);
+/* Recurrence residuals of a plain Chebyshev-PCG solve (x0 = 0) at iterations
+ * 0, every, 2*every, ...: device FP64, native layout, [max_res][native_len]. */
+FG_API int fg_op_collect_residuals(fg_op *op, const double *b, const fg_cfg *cfg, int every, int max_res,
+                                   double *res, int *n_res);
+/* One Adam step on the energy loss of B residuals res (device, native layout,
+ * [B][native_len], zero on essential DOFs): per sample c = s 8^L P^L UNet(...),
+ * loss = (c.Ac/2 - c.r) / (s^2 64^L Nc), Nc = network voxels; its minimiser
+ * over range(P^L) is the Galerkin coarse correction.  *loss = batch mean. */
+FG_API int fg_unet_train_energy(fg_unet *net, fg_op *op, const double *res, int B, float lr, float *loss);
 
 /* Synchronise the handle's stream and report device-side errors
  * (FG_DEVICE_TIMEOUT, FG_BOUNDS). */

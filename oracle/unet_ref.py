@@ -151,13 +151,19 @@ def forward(params, inp, c=(16, 32, 48)):
 def loss_grad(params, inp, target, c=(16, 32, 48)):
     """(loss, flat gradient) of mean((out[...,0] - target)^2)."""
     A = forward(params, inp, c)
-    W = A["W"]
     nv = target.size
     d = A["out"][..., 0] - target
     loss = float((d * d).sum() / nv)
-    g = {}
     dout = np.zeros_like(A["out"])
     dout[..., 0] = bf16(2.0 * d / nv)
+    return loss, backward(A, dout, c)
+
+
+def backward(A, dout, c=(16, 32, 48)):
+    """Flat parameter gradient from the activations A of forward() and the
+    (BF16-rounded) output gradient dout [B,Z,Y,X,8]."""
+    W = A["W"]
+    g = {}
     c0, c1, c2 = c
     mask = lambda a: (a > 0).astype(np.float64)
     g["out"] = conv_bwd(A["g0"], W["out"][0], dout)[:2]
@@ -189,4 +195,4 @@ def loss_grad(params, inp, target, c=(16, 32, 48)):
     da0 = bf16(da0) * mask(A["a0"])
     dW, db, _ = conv_bwd(A["x0"], W["l0a"][0], da0)
     g["l0a"] = (dW, db)
-    return loss, pack(g, c)
+    return pack(g, c)

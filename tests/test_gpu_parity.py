@@ -132,7 +132,7 @@ def test_reference_known_answers_on_gpu():
 
 
 def test_pcg_jacobi_matches_oracle_iterations_c0():
-    """24^3 Q1, kappa = 1, PCG-Jacobi, rtol 1e-10 (mfem_ex1 template)."""
+    """Poisson on 24^3 Q1, kappa = 1, PCG-Jacobi, rtol 1e-10 (mfem_ex1 template)."""
     need_gpu()
     n = 24
     mesh = O.Mesh(n, n, n, 1)

@@ -74,15 +74,15 @@ def test_training_reduces_loss():
     assert last < 0.5 * l0, (l0, last)
 
 
-def _q1_problem(n, seed):
-    kq = lognormal_kappa_q(n, n, n, 1, seed=seed)
-    mesh = O.Mesh(n, n, n, 1)
+def _q1_problem(n, seed, p=1):
+    kq = lognormal_kappa_q(n, n, n, p, seed=seed)
+    mesh = O.Mesh(n, n, n, p)
     mask = O.ess_mask(mesh)
     rng = np.random.default_rng(seed)
     b = O.pa_apply(mesh, O.Coef(O.MASS), rng.standard_normal(mesh.ndofs))
     b[mask == 1] = 0.0
-    op = femgpu.PADiffusionOperator((n, n, n), 1, kappa=kq)
-    femgpu.set_nodal_kappa(op, femgpu.nodal_kappa_from_q(kq, n, n, n))
+    op = femgpu.PADiffusionOperator((n, n, n), p, kappa=kq)
+    femgpu.set_nodal_kappa(op, femgpu.nodal_kappa_from_q(kq, n, n, n, p))
     return mesh, mask, kq, b, op
 
 
@@ -120,6 +120,102 @@ def test_learned_fcg_trains_solves_and_falls_back():
     assert r.converged and r.extra["nn_fallback"] == 1 and r.true_residual <= 1e-8
 
 
+def _restrict_levels(v, shape, levels):
+    """R^L of a plain-layout vertex field, rounded to FP32 after each level."""
+    a = np.asarray(v, dtype=np.float64).reshape((1,) + shape + (1,))
+    for _ in range(levels):
+        a = R.restrict(a).astype(np.float32).astype(np.float64)
+    return a[0, ..., 0]
+
+
+@pytest.mark.parametrize("p,levels", [(1, 1), (1, 2), (2, 2)])
+def test_energy_loss_gradients_match_reference(p, levels):
+    """fg_unet_train_energy: loss (c.Ac/2 - c.r)/(s^2 64^L Nc), c = s 8^L P^L n,
+    and every parameter gradient against the NumPy network with the oracle's
+    constrained apply."""
+    need_gpu()
+    n, B = 16 // p, 2
+    mesh, mask, kq, _, op = _q1_problem(n, 31, p)
+    kn = femgpu.nodal_kappa_from_q(kq, n, n, n, p)
+    femgpu.set_nodal_kappa(op, kn, levels)
+    shape = (p * n + 1,) * 3
+    Vc = femgpu.nn_volume(op)
+    assert Vc == ((p * n >> levels) + 1,) * 3
+    rng = np.random.default_rng(32)
+    res = rng.standard_normal((B, mesh.ndofs))
+    res[:, mask == 1] = 0.0
+    dres = torch.tensor(np.stack([op.to_native(r) for r in res]), device="cuda")
+    net = femgpu.UNet(seed=13)
+    params = net.get_params()
+    loss = net.train_energy(op, dres, 0.0)
+    g = net.get_grads()
+    # reference
+    lk = _restrict_levels(np.log(kn), shape, levels).astype(np.float32)
+    nv = int(np.prod(Vc))
+    inp = np.zeros((B,) + Vc + (2,), dtype=np.float32)
+    scales = []
+    for b in range(B):
+        rc = _restrict_levels(res[b], shape, levels).astype(np.float32)
+        s = float(np.sqrt(np.mean(rc.astype(np.float64) ** 2)))
+        scales.append(s)
+        inp[b, ..., 0] = (rc / s).astype(np.float32)
+        inp[b, ..., 1] = lk
+    A = R.forward(params, inp)
+    coef = 1.0 / (nv * B)
+    mult = 8.0 ** levels
+    dout = np.zeros_like(A["out"])
+    loss_ref = 0.0
+    coefq = O.Coef(O.DIFF, kappa_q=kq)
+    for b in range(B):
+        c = A["out"][b:b + 1, ..., :1]
+        for _ in range(levels):
+            c = R.prolong(c, (1,) + tuple(2 * d - 1 for d in c.shape[1:4]))
+        c = scales[b] * mult * c[0, ..., 0].ravel()
+        c[mask == 1] = 0.0
+        ac = O.apply_constrained(mesh, coefq, mask, c)
+        loss_ref += (0.5 * c @ ac - c @ res[b]) / (scales[b] ** 2 * mult ** 2 * nv) / B
+        gc = _restrict_levels(ac - res[b], shape, levels)
+        dout[b, ..., 0] = R.bf16(coef / scales[b] * gc)
+    g_ref = R.backward(A, dout)
+    assert abs(loss - loss_ref) <= 1e-2 * abs(loss_ref) + 1e-6, (loss, loss_ref)
+    o = 0
+    for name, (ci, co) in zip(R.LAYERS, R.layer_shapes()):
+        nw = co * 27 * ci
+        for part, sl in (("W", slice(o, o + nw)), ("b", slice(o + nw, o + nw + co))):
+            e = rel(g[sl], g_ref[sl])
+            assert e <= 5e-2, (name, part, e)
+        o += nw + co
+
+
+def test_energy_training_reduces_loss_and_helps_fcg():
+    """Energy-loss training on residuals of plain Chebyshev-PCG: the loss
+    falls, and flexible CG with the trained two-level correction converges to
+    the FP64 target on a held-out coefficient field."""
+    need_gpu()
+    n = 32
+    net = femgpu.UNet(seed=17)
+    fields = []
+    for seed in (41, 42):
+        mesh, mask, kq, b, op = _q1_problem(n, seed)
+        femgpu.set_nodal_kappa(op, femgpu.nodal_kappa_from_q(kq, n, n, n), 2)
+        fields.append((op, femgpu.collect_residuals(op, b, every=2, max_res=24)))
+    assert all(r.shape[0] >= 8 for _, r in fields)
+    first = [net.train_energy(op, r[:8].contiguous(), 0.0) for op, r in fields]
+    for it in range(60):
+        op, r = fields[it % 2]
+        k = (it * 4) % (r.shape[0] - 4)
+        net.train_energy(op, r[k:k + 4].contiguous(), 2e-3)
+    last = [net.train_energy(op, r[:8].contiguous(), 0.0) for op, r in fields]
+    # the loss is negative at a useful correction (energy decrease)
+    assert sum(last) < sum(first) and sum(last) < 0.0, (first, last)
+    mesh, mask, kq, b, op = _q1_problem(n, 98)
+    femgpu.set_nodal_kappa(op, femgpu.nodal_kappa_from_q(kq, n, n, n), 2)
+    femgpu.attach_unet(op, net)
+    x = np.zeros(mesh.ndofs)
+    r = op.pcg(b, x, femgpu.SolverConfig(rtol=1e-8, max_iter=2000), femgpu.PC_CHEB_NN)
+    assert r.converged and r.true_residual <= 1e-8
+
+
 def test_learned_precond_requires_network():
     need_gpu()
     op = femgpu.PADiffusionOperator((8, 8, 8), 1)
@@ -128,3 +224,7 @@ def test_learned_precond_requires_network():
         op.pcg(b, np.zeros_like(b), femgpu.SolverConfig(), femgpu.PC_CHEB_NN)
     with pytest.raises(femgpu.SolverError):
         femgpu.set_nodal_kappa(femgpu.PADiffusionOperator((6, 8, 8), 1), np.ones(7 * 9 * 9))
+    with pytest.raises(femgpu.SolverError):
+        femgpu.set_nodal_kappa(femgpu.PADiffusionOperator((8, 8, 8), 1), np.ones(9 * 9 * 9), 2)
+    with pytest.raises(femgpu.SolverError):
+        femgpu.set_nodal_kappa(femgpu.PADiffusionOperator((16, 16, 16), 1), np.ones(17 ** 3), 5)
