@@ -339,6 +339,46 @@ def main():
             "note": "plain = drop-in FP64 PCG with the full (general-geometry) quadrature data; "
                     "_affine = compressed qdata valid for constant-J elements, reported as such"}
 
+        # learned coarse correction (flexible CG, z = Chebyshev(r) + network
+        # correction) with the committed weights trained for this mesh and order
+        # on other kappa seeds; budget = the plain iteration count of the same
+        # form, beyond which the solve falls back to plain Chebyshev-PCG
+        wpath = os.path.join(ROOT, "fem-rs_b200", "femgpu", "weights", f"unet_q{p}_{n}.npz")
+        meta = None
+        if os.path.exists(wpath):
+            from femgpu import learned as learned_mod
+            net, meta = learned_mod.load(wpath)
+            if meta["first_seed"] <= rank < meta["first_seed"] + meta["train_fields"]:
+                # this rank's kappa seed was a training field: no held-out number
+                solve["learned_skipped"] = f"kappa seed {rank} is among the training seeds of {os.path.basename(wpath)}"
+                meta = None
+        if meta is not None:
+            femgpu.set_nodal_kappa(op, femgpu.nodal_kappa_from_q(kq, n, n, n, p), int(meta["levels"]))
+            femgpu.attach_unet(op, net)
+            for name, prec, fmt, plain_key in (
+                    ("learned_fp64_chebyshev4", femgpu.FP64, femgpu.QDATA_FULL, "plain_fp64_chebyshev4"),
+                    ("learned_fp32_ir_chebyshev4_affine", femgpu.FP32_IR, femgpu.QDATA_AFFINE,
+                     "fp32_ir_chebyshev4_affine")):
+                op.set_qdata_format(fmt)
+                xs = np.zeros(N)
+                cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec,
+                                          nn_budget=solve[plain_key]["iterations"])
+                r = op.pcg(b, xs, cfg, femgpu.PC_CHEB_NN)
+                solve[name] = {
+                    "iterations": r.iterations, "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual,
+                    "converged": r.converged, "nn_fallback": r.extra["nn_fallback"],
+                    "iterations_of_plain_same_form": solve[plain_key]["iterations"],
+                    "rel_err_vs_plain_fp64_chebyshev": float(np.linalg.norm(xs - x_plain) / np.linalg.norm(x_plain))}
+            femgpu.attach_unet(op, None)
+            op.set_qdata_format(femgpu.QDATA_FULL)
+            solve["learned_weights"] = {"file": os.path.relpath(wpath, ROOT), "levels": meta["levels"],
+                                        "train_fields": meta["train_fields"], "first_seed": meta["first_seed"],
+                                        "params": meta["params"]}
+            solve["speedup"]["learned_fp64_vs_plain_fp64"] = plain / solve["learned_fp64_chebyshev4"]["solve_s"]
+            solve["speedup"]["learned_fp32_affine_vs_plain_fp64"] = (
+                plain / solve["learned_fp32_ir_chebyshev4_affine"]["solve_s"])
+            del net
+
     # FP32 apply throughput (chosen precision form) and the affine-compressed
     # format, same workload
     x32 = x.float()

@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <functional>
 #include <cmath>
 #include <cstdarg>
@@ -187,6 +188,8 @@ struct fg_op {
     int *d_err = nullptr;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t cap_stream = nullptr;  // private stream for CUDA-graph capture
+    bool graphs = true;                 // replay solver chunks as CUDA graphs
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -218,6 +221,7 @@ static void free_op(fg_op *op) {
     if (op->ev0) cudaEventDestroy(op->ev0);
     if (op->ev1) cudaEventDestroy(op->ev1);
     if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
+    if (op->cap_stream) cudaStreamDestroy(op->cap_stream);
     delete op;
 }
 
@@ -463,6 +467,10 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
     if (cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(FG_CUDA_ERROR, "cudaStreamCreate failed"));
     op->own_stream = true;
+    {
+        const char *e = std::getenv("FG_SOLVER_GRAPHS");
+        op->graphs = !(e && e[0] == '0');
+    }
     if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)))
         return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
     if (cudaMalloc(&op->st, sizeof(SolverState)) != cudaSuccess ||
@@ -812,6 +820,69 @@ static int cheb_apply(fg_op *op, const PcgBufs<T> &B, const ChebCoef &cc, const 
 // par_solver.rs:262-342 semantics.  The state (rtol, atol, max_iter) must be
 // loaded into B.st before the call.  x_zero: the initial guess is zero (the
 // first residual needs no apply).  Returns the final host copy of the state.
+// A chunk of solver iterations (the launches between two host reads of the
+// solver state).  The first chunk with a given key is launched directly, which
+// also performs every one-time step of the launchers (kernel attributes,
+// lazily sized buffers); the second is captured on a private stream into a
+// CUDA graph; later ones replay that graph on the handle's stream.  Kernel
+// arguments, buffers and the order of launches are the same in every chunk
+// of a solve, and all per-iteration state lives in device memory, so a replay
+// performs exactly the launches of a direct chunk.
+struct ChunkGraph {
+    cudaGraphExec_t exec = nullptr;
+    int key = -1, iters = 0, seen = 0;
+    ChunkGraph() = default;
+    ChunkGraph(const ChunkGraph &) = delete;
+    ChunkGraph &operator=(const ChunkGraph &) = delete;
+    ~ChunkGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
+static int run_chunk(fg_op *op, ChunkGraph &cg, int key, int iters, const std::function<int()> &iteration) {
+    auto direct = [&]() -> int {
+        for (int k = 0; k < iters; ++k) {
+            const int rc = iteration();
+            if (rc) return rc;
+        }
+        return FG_OK;
+    };
+    if (!op->graphs) return direct();
+    if (cg.exec && cg.key == key && cg.iters == iters) {
+        CK(cudaGraphLaunch(cg.exec, op->stream));
+        return FG_OK;
+    }
+    if (cg.key != key || cg.iters != iters) {
+        if (cg.exec) cudaGraphExecDestroy(cg.exec);
+        cg.exec = nullptr;
+        cg.key = key;
+        cg.iters = iters;
+        cg.seen = 0;
+    }
+    if (cg.seen++ == 0) return direct();
+    if (!op->cap_stream) CK(cudaStreamCreateWithFlags(&op->cap_stream, cudaStreamNonBlocking));
+    const cudaStream_t saved = op->stream;
+    CK(cudaStreamBeginCapture(op->cap_stream, cudaStreamCaptureModeThreadLocal));
+    op->stream = op->cap_stream;
+    const int rc = direct();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(op->cap_stream, &graph);
+    op->stream = saved;
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ce != cudaSuccess) return fail(FG_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(&cg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        cg.exec = nullptr;
+        return fail(FG_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(ie));
+    }
+    CK(cudaGraphLaunch(cg.exec, op->stream));
+    return FG_OK;
+}
+
 template <typename T>
 static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebCoef *cc,
                    int max_iter, int check_interval, bool x_zero, SolverState *h,
@@ -836,20 +907,24 @@ static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebC
         CK(cudaGetLastError());
     }
     int launched = 0;
+    ChunkGraph cg;
+    auto iteration = [&]() -> int {
+        int r2;
+        if ((r2 = apply_native_t<T>(op, B.qd, B.face, B.p, B.ap, 0, 1, skip))) return r2;
+        k_pcg_pap<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.ap, op->partials, B.st);
+        k_pcg_update<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(
+            n, B.x, B.r, B.p, B.ap, B.dinv, B.z, cheb ? 0 : 1, op->partials, B.st);
+        if (cheb) {
+            if ((r2 = cheb_apply<T>(op, B, *cc, B.r, B.z, skip))) return r2;
+            k_pcg_rz<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.r, B.z, op->partials, B.st, 0);
+        }
+        k_pcg_pupdate<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.p, B.st, 0);
+        CK(cudaGetLastError());
+        return FG_OK;
+    };
     while (launched < max_iter) {
         const int chunk = std::min(check_interval, max_iter - launched);
-        for (int k = 0; k < chunk; ++k) {
-            if ((rc = apply_native_t<T>(op, B.qd, B.face, B.p, B.ap, 0, 1, skip))) return rc;
-            k_pcg_pap<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.ap, op->partials, B.st);
-            k_pcg_update<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(
-                n, B.x, B.r, B.p, B.ap, B.dinv, B.z, cheb ? 0 : 1, op->partials, B.st);
-            if (cheb) {
-                if ((rc = cheb_apply<T>(op, B, *cc, B.r, B.z, skip))) return rc;
-                k_pcg_rz<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.r, B.z, op->partials, B.st, 0);
-            }
-            k_pcg_pupdate<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.p, B.st, 0);
-            CK(cudaGetLastError());
-        }
+        if ((rc = run_chunk(op, cg, 0, chunk, iteration))) return rc;
         launched += chunk;
         if ((rc = read_state(op, h, B.st))) return rc;
         if (on_chunk && !h->done && (rc = on_chunk(h->iter))) return rc;
@@ -912,8 +987,7 @@ static int nn_prolong(fg_op *op, const float *oc, T *z, const double *scale, dou
         prolong_f32_kernel<<<blocks, 256, 0, op->stream>>>(f, vc, op->nn_tmp[l - 1], vf);
         f = op->nn_tmp[l - 1];
     }
-    fe_prolong_f32_kernel<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(g, f, nn_vol(op, 1), z, scale, mult,
-                                                                        accumulate);
+    fe_prolong_f32_kernel<T><<<VEC_GRID, 256, 0, op->stream>>>(g, f, nn_vol(op, 1), z, scale, mult, accumulate);
     CK(cudaGetLastError());
     return FG_OK;
 }
@@ -929,7 +1003,7 @@ template <typename T> static int nn_precond_add(fg_op *op, const T *r, T *z) {
     int blocks;
     grid_launch(nv, blocks);
     if ((rc = nn_restrict<T>(op, r, op->nn_rc))) return rc;
-    rms_kernel<<<1, 256, 0, op->stream>>>(op->nn_rc, nv, op->nn_scale);
+    rms_kernel<<<1, 1024, 0, op->stream>>>(op->nn_rc, nv, op->nn_scale);
     pack_input_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, op->nn_lk, nv, op->nn_scale,
                                                       TView{u->buf.x0, 2, 0});
     CK(cudaGetLastError());
@@ -967,15 +1041,18 @@ static int fcg_nn_run(fg_op *op, const PcgBufs<double> &B, const ChebCoef &cc, i
     };
     if ((rc = direction(1))) return rc;
     int launched = 0;
+    ChunkGraph cg;
+    auto iteration = [&]() -> int {
+        int r2;
+        if ((r2 = apply_native_t<double>(op, B.qd, B.face, B.p, B.ap, 0, 1, skip))) return r2;
+        k_pcg_pap<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.ap, op->partials, B.st);
+        k_pcg_update<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.x, B.r, B.p, B.ap, B.dinv,
+                                                                       B.z, 0, op->partials, B.st);
+        return direction(0);
+    };
     while (launched < max_iter) {
         const int chunk = std::min(check_interval, max_iter - launched);
-        for (int k = 0; k < chunk; ++k) {
-            if ((rc = apply_native_t<double>(op, B.qd, B.face, B.p, B.ap, 0, 1, skip))) return rc;
-            k_pcg_pap<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.ap, op->partials, B.st);
-            k_pcg_update<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.x, B.r, B.p, B.ap, B.dinv,
-                                                                           B.z, 0, op->partials, B.st);
-            if ((rc = direction(0))) return rc;
-        }
+        if ((rc = run_chunk(op, cg, nn_on ? 1 : 0, chunk, iteration))) return rc;
         launched += chunk;
         if ((rc = read_state(op, h, B.st))) return rc;
         if (h->done) break;
@@ -1185,22 +1262,23 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
         };
         if ((rc = precond(1))) return rc;
         int launched = 0;
+        ChunkGraph cg;
+        auto iteration = [&]() -> int {
+            int r2;
+            if ((r2 = apply_native_t<float>(op, op->qd32, op->face32, op->p32, op->ap32, 0, 1, done))) return r2;
+            k_pcg_pap<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->p32, op->ap32, op->partials, op->st);
+            k_rel_step<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->e32, op->r32, op->p32, op->ap32,
+                                                                 op->partials, op->st);
+            // reliable update (kernels return at once unless triggered)
+            k_rel_xupdate<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->xw, op->e32, op->st);
+            if ((r2 = apply_native(op, op->xw, op->ap, 0, 1, skip_rel))) return r2;
+            k_rel_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->r32, op->partials,
+                                                                     op->st, 0);
+            return precond(0);
+        };
         while (launched < cfg.max_iter) {
             const int chunk = std::min(cfg.check_interval, cfg.max_iter - launched);
-            for (int k = 0; k < chunk; ++k) {
-                if ((rc = apply_native_t<float>(op, op->qd32, op->face32, op->p32, op->ap32, 0, 1, done)))
-                    return rc;
-                k_pcg_pap<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->p32, op->ap32,
-                                                                           op->partials, op->st);
-                k_rel_step<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->e32, op->r32, op->p32,
-                                                                     op->ap32, op->partials, op->st);
-                // reliable update (kernels return at once unless triggered)
-                k_rel_xupdate<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->xw, op->e32, op->st);
-                if ((rc = apply_native(op, op->xw, op->ap, 0, 1, skip_rel))) return rc;
-                k_rel_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->r32,
-                                                                         op->partials, op->st, 0);
-                if ((rc = precond(0))) return rc;
-            }
+            if ((rc = run_chunk(op, cg, nn_on ? 1 : 0, chunk, iteration))) return rc;
             launched += chunk;
             if ((rc = read_state(op, &h))) return rc;
             if (h.done) break;
@@ -2052,6 +2130,7 @@ FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal, int level
     if (cx % m || cy % m || cz % m || cx / m < 1 || cy / m < 1 || cz / m < 1)
         return fail(FG_UNSUPPORTED, "the learned correction needs DOF-lattice cell counts (p * elements) "
                                     "that are multiples of %d", m);
+    if (op->Nn >= (int64_t)1 << 31) return fail(FG_UNSUPPORTED, "the learned correction needs < 2^31 DOFs");
     std::lock_guard<std::mutex> lk(op->mu);
     CK(cudaSetDevice(op->device));
     int rc;
@@ -2153,7 +2232,7 @@ FG_API int fg_op_collect_pairs(fg_op *op, const double *b, const fg_cfg *cfg_in,
         if ((rc = apply_native(op, stash[j], op->ap, 0, 1, nullptr))) return rc;
         k_lincomb2<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->r, 1.0, op->bw, -1.0, op->ap);
         if ((rc = nn_restrict<double>(op, op->r, op->nn_rc))) return rc;
-        rms_kernel<<<1, 256, 0, op->stream>>>(op->nn_rc, nv, op->nn_scale);
+        rms_kernel<<<1, 1024, 0, op->stream>>>(op->nn_rc, nv, op->nn_scale);
         pack_input_f32_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, op->nn_lk, nv, op->nn_scale,
                                                               d_in + (int64_t)j * nv * 2);
         pair_target_kernel<<<blocks, 256, 0, op->stream>>>(g, op->xw, stash[j], Vc, 1 << op->nn_levels, op->nn_scale,
@@ -2242,7 +2321,7 @@ FG_API int fg_unet_train_energy(fg_unet *u, fg_op *op, const double *d_res, int 
     UnetBufs &ub = u->buf;
     for (int b = 0; b < B; ++b) {
         if ((rc = nn_restrict<double>(op, d_res + (int64_t)b * n, op->nn_rc))) return rc;
-        rms_kernel<<<1, 256, 0, op->stream>>>(op->nn_rc, nv, tb + 4 * b);
+        rms_kernel<<<1, 1024, 0, op->stream>>>(op->nn_rc, nv, tb + 4 * b);
         pack_input_kernel<<<blocks, 256, 0, op->stream>>>(op->nn_rc, op->nn_lk, nv, tb + 4 * b,
                                                           TView{ub.x0 + (int64_t)b * nv * 2, 2, 0});
     }

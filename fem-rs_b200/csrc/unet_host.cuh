@@ -140,18 +140,28 @@ static int unet_ensure_bufs(fg_unet *u, int B, int Z, int Y, int X) {
     return FG_OK;
 }
 
+template <int NT, int KS>
+static void conv_launch(fg_unet *u, bool tapmajor, int blocks, const TView &in, const Vol &V,
+                        const __nv_bfloat16 *w, int cin, int kp, const float *bias, TView out, int relu) {
+    if (tapmajor)
+        conv3_fwd16_kernel<NT, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu);
+    else
+        conv3_fwd_kernel<NT, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu);
+}
+
 template <int KS>
 static int conv_fwd_ks(fg_unet *u, const TView &in, const Vol &V, const __nv_bfloat16 *w, int cin, int cout,
                        int kp, const float *bias, TView out, int relu) {
     const int64_t tiles = (V.nvox() + 15) / 16;
     const int blocks = (int)((tiles + (4 / KS) - 1) / (4 / KS));
+    const bool tm = cin % 16 == 0 && in.cs % 4 == 0 && in.co % 4 == 0;
     switch (cout / 8) {
-    case 1: conv3_fwd_kernel<1, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 2: conv3_fwd_kernel<2, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 4: conv3_fwd_kernel<4, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 6: conv3_fwd_kernel<6, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 8: conv3_fwd_kernel<8, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
-    case 10: conv3_fwd_kernel<10, KS><<<blocks, 128, 0, u->stream>>>(in, V, cin, w, kp, bias, out, relu); break;
+    case 1: conv_launch<1, KS>(u, tm, blocks, in, V, w, cin, kp, bias, out, relu); break;
+    case 2: conv_launch<2, KS>(u, tm, blocks, in, V, w, cin, kp, bias, out, relu); break;
+    case 4: conv_launch<4, KS>(u, tm, blocks, in, V, w, cin, kp, bias, out, relu); break;
+    case 6: conv_launch<6, KS>(u, tm, blocks, in, V, w, cin, kp, bias, out, relu); break;
+    case 8: conv_launch<8, KS>(u, tm, blocks, in, V, w, cin, kp, bias, out, relu); break;
+    case 10: conv_launch<10, KS>(u, tm, blocks, in, V, w, cin, kp, bias, out, relu); break;
     default: return fail(FG_UNSUPPORTED, "conv output channels %d not supported", cout);
     }
     CK(cudaGetLastError());
@@ -175,6 +185,37 @@ static int layer_fwd(fg_unet *u, int li, const TView &in, const Vol &V, TView ou
 
 static void grid_launch(int64_t n, int &blocks) { blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16); }
 
+static bool vec8(const TView &a, const TView &b, int C) {
+    return C % 8 == 0 && a.cs % 8 == 0 && a.co % 8 == 0 && b.cs % 8 == 0 && b.co % 8 == 0;
+}
+
+// channel-wise trilinear prolongation Vc -> Vf (out = scale P in (+ out))
+static void launch_prolong(fg_unet *u, const TView &in, const Vol &Vc, TView out, const Vol &Vf, int C,
+                           float scale, int accumulate) {
+    int blocks;
+    if (vec8(in, out, C)) {
+        grid_launch(Vf.nvox() * (C / 8), blocks);
+        prolong_kernel<8><<<blocks, 256, 0, u->stream>>>(in, Vc, out, Vf, C, scale, accumulate);
+    } else {
+        grid_launch(Vf.nvox() * (C / 2), blocks);
+        prolong_kernel<2><<<blocks, 256, 0, u->stream>>>(in, Vc, out, Vf, C, scale, accumulate);
+    }
+}
+
+// channel-wise full-weighting restriction Vf -> Vc (out = scale R in)
+static void launch_restrict(fg_unet *u, const TView &in, const Vol &Vf, TView out, const Vol &Vc, int C,
+                            float scale) {
+    int blocks;
+    // 8 channels per thread only when that still gives a few threads per SM lane
+    if (vec8(in, out, C) && Vc.nvox() * (C / 8) >= 148 * 512) {
+        grid_launch(Vc.nvox() * (C / 8), blocks);
+        restrict_kernel<8><<<blocks, 256, 0, u->stream>>>(in, Vf, out, Vc, C, scale);
+    } else {
+        grid_launch(Vc.nvox() * (C / 2), blocks);
+        restrict_kernel<2><<<blocks, 256, 0, u->stream>>>(in, Vf, out, Vc, C, scale);
+    }
+}
+
 static int unet_forward(fg_unet *u) {
     UnetBufs &b = u->buf;
     const int C0 = u->C0, C1 = u->C1, C2 = u->C2;
@@ -184,17 +225,13 @@ static int unet_forward(fg_unet *u) {
         up1{b.cat1, C2 + C1, 0}, cat1{b.cat1, C2 + C1, 0}, g1{b.g1, C1, 0}, up0{b.cat0, C1 + C0, 0},
         cat0{b.cat0, C1 + C0, 0}, g0{b.g0, C0, 0}, out{b.out, 8, 0};
     if ((rc = layer_fwd(u, L0A, x0, b.v0, a0, 1)) || (rc = layer_fwd(u, L0B, a0, b.v0, h0, 1))) return rc;
-    grid_launch(b.v1.nvox() * C0, blocks);
-    restrict_kernel<<<blocks, 256, 0, u->stream>>>(h0, b.v0, x1, b.v1, C0, 1.f);
+    launch_restrict(u, h0, b.v0, x1, b.v1, C0, 1.f);
     if ((rc = layer_fwd(u, L1A, x1, b.v1, a1, 1)) || (rc = layer_fwd(u, L1B, a1, b.v1, h1, 1))) return rc;
-    grid_launch(b.v2.nvox() * C1, blocks);
-    restrict_kernel<<<blocks, 256, 0, u->stream>>>(h1, b.v1, x2, b.v2, C1, 1.f);
+    launch_restrict(u, h1, b.v1, x2, b.v2, C1, 1.f);
     if ((rc = layer_fwd(u, L2A, x2, b.v2, a2, 1)) || (rc = layer_fwd(u, L2B, a2, b.v2, h2, 1))) return rc;
-    grid_launch(b.v1.nvox() * C2, blocks);
-    prolong_kernel<<<blocks, 256, 0, u->stream>>>(h2, b.v2, up1, b.v1, C2, 1.f, 0);
+    launch_prolong(u, h2, b.v2, up1, b.v1, C2, 1.f, 0);
     if ((rc = layer_fwd(u, L1C, cat1, b.v1, g1, 1))) return rc;
-    grid_launch(b.v0.nvox() * C1, blocks);
-    prolong_kernel<<<blocks, 256, 0, u->stream>>>(g1, b.v1, up0, b.v0, C1, 1.f, 0);
+    launch_prolong(u, g1, b.v1, up0, b.v0, C1, 1.f, 0);
     if ((rc = layer_fwd(u, L0C, cat0, b.v0, g0, 1)) || (rc = layer_fwd(u, LOUT, g0, b.v0, out, 0))) return rc;
     CK(cudaGetLastError());
     return FG_OK;
@@ -256,25 +293,21 @@ static int unet_backward(fg_unet *u) {
     if ((rc = relu_bwd(u, dg0, g0, b.v0, C0))) return rc;
     if ((rc = layer_bwd(u, L0C, cat0, b.v0, dg0, &dcat0))) return rc;
     // P^T = 8 R : gradient of the level-1 output g1 from the prolongated channels
-    grid_launch(b.v1.nvox() * C1, blocks);
-    restrict_kernel<<<blocks, 256, 0, u->stream>>>(dup0, b.v0, dg1, b.v1, C1, 8.f);
+    launch_restrict(u, dup0, b.v0, dg1, b.v1, C1, 8.f);
     if ((rc = relu_bwd(u, dg1, g1, b.v1, C1))) return rc;
     if ((rc = layer_bwd(u, L1C, cat1, b.v1, dg1, &dcat1))) return rc;
-    grid_launch(b.v2.nvox() * C2, blocks);
-    restrict_kernel<<<blocks, 256, 0, u->stream>>>(dup1, b.v1, dh2, b.v2, C2, 8.f);
+    launch_restrict(u, dup1, b.v1, dh2, b.v2, C2, 8.f);
     if ((rc = relu_bwd(u, dh2, h2, b.v2, C2))) return rc;
     if ((rc = layer_bwd(u, L2B, a2, b.v2, dh2, &da2))) return rc;
     if ((rc = relu_bwd(u, da2, a2, b.v2, C2))) return rc;
     if ((rc = layer_bwd(u, L2A, x2, b.v2, da2, &dx2))) return rc;
     // R^T = P / 8 : add the down-path gradient to the skip gradient of h1
-    grid_launch(b.v1.nvox() * C1, blocks);
-    prolong_kernel<<<blocks, 256, 0, u->stream>>>(dx2, b.v2, dh1, b.v1, C1, 0.125f, 1);
+    launch_prolong(u, dx2, b.v2, dh1, b.v1, C1, 0.125f, 1);
     if ((rc = relu_bwd(u, dh1, h1, b.v1, C1))) return rc;
     if ((rc = layer_bwd(u, L1B, a1, b.v1, dh1, &da1))) return rc;
     if ((rc = relu_bwd(u, da1, a1, b.v1, C1))) return rc;
     if ((rc = layer_bwd(u, L1A, x1, b.v1, da1, &dx1))) return rc;
-    grid_launch(b.v0.nvox() * C0, blocks);
-    prolong_kernel<<<blocks, 256, 0, u->stream>>>(dx1, b.v1, dh0, b.v0, C0, 0.125f, 1);
+    launch_prolong(u, dx1, b.v1, dh0, b.v0, C0, 0.125f, 1);
     if ((rc = relu_bwd(u, dh0, h0, b.v0, C0))) return rc;
     if ((rc = layer_bwd(u, L0B, a0, b.v0, dh0, &da0))) return rc;
     if ((rc = relu_bwd(u, da0, a0, b.v0, C0))) return rc;

@@ -162,6 +162,100 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(const TView in, const Vo
     }
 }
 
+// Tap-major variant for Cin a multiple of 16 (channel views 4-aligned): the
+// neighbour offset and bounds test are computed once per tap and voxel, and
+// each 16-channel block is one 8-byte load per voxel and per weight row.  The
+// 16 GEMM columns of a block are permuted so that lane t4 holds channels
+// 4*t4 .. 4*t4+3 in both operands: fragment columns (2*t4, 2*t4+1) are
+// channels 4*t4 + (0, 1) and columns (2*t4+8, 2*t4+9) are 4*t4 + (2, 3).
+// The permutation is the same for A and B, so the product is unchanged.
+__device__ __forceinline__ uint2 ld_bf16x4(const __nv_bfloat16 *p) {
+    return *reinterpret_cast<const uint2 *>(p);
+}
+
+template <int NT, int KS>
+__global__ void __launch_bounds__(128) conv3_fwd16_kernel(const TView in, const Vol V, int Cin,
+                                                          const __nv_bfloat16 *__restrict__ W, int Kp,
+                                                          const float *__restrict__ bias, TView out,
+                                                          int relu) {
+    constexpr int TPB = 4 / KS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = warp / KS, part = warp % KS;
+    const int gid = lane >> 2, t4 = lane & 3;
+    const int64_t nv = V.nvox();
+    const int64_t m0 = ((int64_t)blockIdx.x * TPB + tile) * 16;
+    const bool active = m0 < nv;
+    const int64_t v0 = m0 + gid, v1 = m0 + gid + 8;
+    int b0, z0, y0, x0, b1, z1, y1, x1;
+    vox_coords(V, v0 < nv ? v0 : 0, b0, z0, y0, x0);
+    vox_coords(V, v1 < nv ? v1 : 0, b1, z1, y1, x1);
+    const bool ok0 = v0 < nv, ok1 = v1 < nv;
+    float acc[NT][4];
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    if (active) {
+        const __nv_bfloat16 *wl = W + (int64_t)gid * Kp + 4 * t4;
+        for (int tap = part; tap < 27; tap += KS) {
+            const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+            const __nv_bfloat16 *p0 = nullptr, *p1 = nullptr;
+            {
+                const int zz = z0 + dz, yy = y0 + dy, xx = x0 + dx;
+                if (ok0 && zz >= 0 && zz < V.Z && yy >= 0 && yy < V.Y && xx >= 0 && xx < V.X)
+                    p0 = in.p + ((((int64_t)b0 * V.Z + zz) * V.Y + yy) * V.X + xx) * in.cs + in.co + 4 * t4;
+            }
+            {
+                const int zz = z1 + dz, yy = y1 + dy, xx = x1 + dx;
+                if (ok1 && zz >= 0 && zz < V.Z && yy >= 0 && yy < V.Y && xx >= 0 && xx < V.X)
+                    p1 = in.p + ((((int64_t)b1 * V.Z + zz) * V.Y + yy) * V.X + xx) * in.cs + in.co + 4 * t4;
+            }
+            const __nv_bfloat16 *wt = wl + tap * Cin;
+#pragma unroll 2
+            for (int c0 = 0; c0 < Cin; c0 += 16) {
+                const uint2 a0 = p0 ? ld_bf16x4(p0 + c0) : make_uint2(0u, 0u);
+                const uint2 a1 = p1 ? ld_bf16x4(p1 + c0) : make_uint2(0u, 0u);
+                const uint32_t a[4] = {a0.x, a1.x, a0.y, a1.y};
+#pragma unroll
+                for (int j = 0; j < NT; ++j) {
+                    const uint2 bw = ld_bf16x4(wt + (int64_t)j * 8 * Kp + c0);
+                    mma_bf16_16816(acc[j], a, bw.x, bw.y);
+                }
+            }
+        }
+    }
+    if constexpr (KS > 1) {
+        __shared__ float red[TPB * (KS - 1)][NT * 4][32];
+        if (part > 0) {
+            const int slot = tile * (KS - 1) + part - 1;
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) red[slot][j * 4 + e][lane] = acc[j][e];
+        }
+        __syncthreads();
+        if (part > 0) return;
+#pragma unroll
+        for (int q = 0; q < KS - 1; ++q)
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[j][e] += red[tile * (KS - 1) + q][j * 4 + e][lane];
+    }
+    if (!active) return;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+        const int n = j * 8 + t4 * 2;
+        const float bb0 = bias ? bias[n] : 0.f, bb1 = bias ? bias[n + 1] : 0.f;
+        float r0 = acc[j][0] + bb0, r1 = acc[j][1] + bb1, r2 = acc[j][2] + bb0, r3 = acc[j][3] + bb1;
+        if (relu) {
+            r0 = fmaxf(r0, 0.f); r1 = fmaxf(r1, 0.f); r2 = fmaxf(r2, 0.f); r3 = fmaxf(r3, 0.f);
+        }
+        if (ok0)
+            *reinterpret_cast<__nv_bfloat162 *>(out.p + v0 * out.cs + out.co + n) = __floats2bfloat162_rn(r0, r1);
+        if (ok1)
+            *reinterpret_cast<__nv_bfloat162 *>(out.p + v1 * out.cs + out.co + n) = __floats2bfloat162_rn(r2, r3);
+    }
+}
+
 // Weight gradient partials: block (n-block of 32 columns, voxel chunk), warp =
 // m-tile of 16 output channels.  part[chunk][co][Kp] (FP32).
 __global__ void __launch_bounds__(128) conv3_wgrad_kernel(const TView in, const Vol V, int Cin,
@@ -295,54 +389,108 @@ __global__ void relu_bwd_kernel(TView dy, const TView y, int64_t nv, int C) {
     }
 }
 
-// Vertex-centred transfer between a fine volume (Zf,Yf,Xf odd) and its coarse
-// volume ((Zf+1)/2, ...): prolongation P (trilinear hat weights 1, 1/2) and
-// restriction R = P^T / 8 (full weighting 1/4, 1/2, 1/4 per direction).
-// out = scale * (P in) or scale * (R in), over C channels.
+template <int VW> struct BVec;
+template <> struct BVec<2> {
+    static __device__ __forceinline__ void ld(const __nv_bfloat16 *p, float (&f)[2]) {
+        const float2 t = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p));
+        f[0] = t.x; f[1] = t.y;
+    }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, const float (&f)[2]) {
+        *reinterpret_cast<__nv_bfloat162 *>(p) = __floats2bfloat162_rn(f[0], f[1]);
+    }
+};
+template <> struct BVec<8> {
+    static __device__ __forceinline__ void ld(const __nv_bfloat16 *p, float (&f)[8]) {
+        const uint4 u = *reinterpret_cast<const uint4 *>(p);
+        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            __nv_bfloat162 h;
+            memcpy(&h, &w[k], 4);
+            const float2 t = __bfloat1622float2(h);
+            f[2 * k] = t.x; f[2 * k + 1] = t.y;
+        }
+    }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, const float (&f)[8]) {
+        uint32_t w[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
+            memcpy(&w[k], &h, 4);
+        }
+        *reinterpret_cast<uint4 *>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+};
+
+// trilinear prolongation of C channels, VW channels per thread (C, channel
+// stride and offset multiples of VW)
+template <int VW>
 __global__ void prolong_kernel(const TView in, const Vol Vc, TView out, const Vol Vf, int C, float scale,
                                int accumulate) {
-    const int64_t total = Vf.nvox() * C;
+    const int G = C / VW;
+    const int64_t total = Vf.nvox() * G;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
+        const int c = (int)(i % G) * VW;
+        const int64_t v = i / G;
         int b, z, y, x;
-        vox_coords(Vf, i / C, b, z, y, x);
-        float s = 0.f;
+        vox_coords(Vf, v, b, z, y, x);
+        float s[VW];
+#pragma unroll
+        for (int k = 0; k < VW; ++k) s[k] = 0.f;
         const int cz0 = z >> 1, cy0 = y >> 1, cx0 = x >> 1;
         for (int a = 0; a <= (z & 1); ++a)
             for (int bb = 0; bb <= (y & 1); ++bb)
                 for (int d = 0; d <= (x & 1); ++d) {
                     const float w = ((z & 1) ? 0.5f : 1.f) * ((y & 1) ? 0.5f : 1.f) * ((x & 1) ? 0.5f : 1.f);
                     const int64_t vc = (((int64_t)b * Vc.Z + cz0 + a) * Vc.Y + cy0 + bb) * Vc.X + cx0 + d;
-                    s += w * __bfloat162float(in.p[vc * in.cs + in.co + c]);
+                    float f[VW];
+                    BVec<VW>::ld(in.p + vc * in.cs + in.co + c, f);
+#pragma unroll
+                    for (int k = 0; k < VW; ++k) s[k] += w * f[k];
                 }
-        __nv_bfloat16 *o = out.p + (i / C) * out.cs + out.co + c;
-        *o = __float2bfloat16(scale * s + (accumulate ? __bfloat162float(*o) : 0.f));
+        __nv_bfloat16 *o = out.p + v * out.cs + out.co + c;
+        float prev[VW];
+        if (accumulate) BVec<VW>::ld(o, prev);
+#pragma unroll
+        for (int k = 0; k < VW; ++k) s[k] = scale * s[k] + (accumulate ? prev[k] : 0.f);
+        BVec<VW>::st(o, s);
     }
 }
 
+// full-weighting restriction of C channels, VW channels per thread
+template <int VW>
 __global__ void restrict_kernel(const TView in, const Vol Vf, TView out, const Vol Vc, int C, float scale) {
-    const int64_t total = Vc.nvox() * C;
+    const int G = C / VW;
+    const int64_t total = Vc.nvox() * G;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
+        const int c = (int)(i % G) * VW;
+        const int64_t v = i / G;
         int b, z, y, x;
-        vox_coords(Vc, i / C, b, z, y, x);
-        float s = 0.f;
+        vox_coords(Vc, v, b, z, y, x);
+        float s[VW];
+#pragma unroll
+        for (int k = 0; k < VW; ++k) s[k] = 0.f;
+#pragma unroll
         for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
             for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int fz = 2 * z + dz, fy = 2 * y + dy, fx = 2 * x + dx;
                     if (fz < 0 || fz >= Vf.Z || fy < 0 || fy >= Vf.Y || fx < 0 || fx >= Vf.X) continue;
                     const float w = (dz ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dx ? 0.5f : 1.f) * 0.125f;
                     const int64_t vf = (((int64_t)b * Vf.Z + fz) * Vf.Y + fy) * Vf.X + fx;
-                    s += w * __bfloat162float(in.p[vf * in.cs + in.co + c]);
+                    float f[VW];
+                    BVec<VW>::ld(in.p + vf * in.cs + in.co + c, f);
+#pragma unroll
+                    for (int k = 0; k < VW; ++k) s[k] += w * f[k];
                 }
-        out.p[(i / C) * out.cs + out.co + c] = __float2bfloat16(scale * s);
+#pragma unroll
+        for (int k = 0; k < VW; ++k) s[k] *= scale;
+        BVec<VW>::st(out.p + v * out.cs + out.co + c, s);
     }
 }
 
-// loss = mean over voxels of (out[.][0] - t)^2 ; grad = 2 (out - t) / nv into channel 0
-// (other output channels get zero gradient).  Partial sums per block, summed in
-// block order by the host.
 __global__ void __launch_bounds__(256) mse_kernel(const TView out, const float *__restrict__ target,
                                                   int64_t nv, int Cout, TView grad, float *__restrict__ partial) {
     __shared__ float sm[256];
@@ -406,14 +554,14 @@ __global__ void fe_restrict_kernel(const Grid g, const T *__restrict__ r, float 
     }
 }
 
-// out[0] = sqrt(mean(v^2)) over n values (single block, fixed order)
-__global__ void __launch_bounds__(256) rms_kernel(const float *__restrict__ v, int64_t n, double *__restrict__ out) {
-    __shared__ double sm[256];
+// out[0] = sqrt(mean(v^2)) over n values (single block of 1024, fixed order)
+__global__ void __launch_bounds__(1024) rms_kernel(const float *__restrict__ v, int64_t n, double *__restrict__ out) {
+    __shared__ double sm[1024];
     double s = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += 256) s += (double)v[i] * (double)v[i];
+    for (int64_t i = threadIdx.x; i < n; i += 1024) s += (double)v[i] * (double)v[i];
     sm[threadIdx.x] = s;
     __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
+    for (int w = 512; w > 0; w >>= 1) {
         if (threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
         __syncthreads();
     }
@@ -501,23 +649,31 @@ __global__ void prolong_f32_kernel(const float *__restrict__ c, const Vol Vc, fl
 // z (native, T) (+)= scale[0] * mult * P(cf) for an FP32 field cf on the
 // first coarse level; zero on essential DOFs and pads
 template <typename T>
-__global__ void fe_prolong_f32_kernel(const Grid g, const float *__restrict__ cf, const Vol Vc, T *__restrict__ z,
-                                      const double *__restrict__ scale, double mult, int accumulate) {
+__global__ void __launch_bounds__(256) fe_prolong_f32_kernel(const Grid g, const float *__restrict__ cf,
+                                                             const Vol Vc, T *__restrict__ z,
+                                                             const double *__restrict__ scale, double mult,
+                                                             int accumulate) {
+    // native vectors of the coupled operators hold < 2^31 entries (checked by the host)
     const double sc = (scale ? scale[0] : 1.0) * mult;
-    const int64_t n = (int64_t)g.NIp * g.NJ * g.NK;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int I = (int)(i % g.NIp);
-        const int64_t row = i / g.NIp;
-        const int J = (int)(row % g.NJ), K = (int)(row / g.NJ);
+    const uint32_t n = (uint32_t)g.NIp * (uint32_t)g.NJ * (uint32_t)g.NK;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t row = i / (uint32_t)g.NIp;
+        const int I = (int)(i - row * (uint32_t)g.NIp);
+        const int J = (int)(row % (uint32_t)g.NJ), K = (int)(row / (uint32_t)g.NJ);
         double s = 0.0;
         if (I < g.NI && !g.is_ess(I, J, K)) {
-            for (int a = 0; a <= (K & 1); ++a)
-                for (int bb = 0; bb <= (J & 1); ++bb)
-                    for (int d = 0; d <= (I & 1); ++d) {
-                        const double w = ((K & 1) ? 0.5 : 1.0) * ((J & 1) ? 0.5 : 1.0) * ((I & 1) ? 0.5 : 1.0);
-                        s += w * (double)cf[((int64_t)((K >> 1) + a) * Vc.Y + (J >> 1) + bb) * Vc.X + (I >> 1) + d];
-                    }
-            s *= sc;
+            const int64_t c0 = ((int64_t)(K >> 1) * Vc.Y + (J >> 1)) * Vc.X + (I >> 1);
+            const int oz = (K & 1) ? Vc.Y * Vc.X : 0, oy = (J & 1) ? Vc.X : 0, ox = I & 1;
+            const double wz = (K & 1) ? 0.5 : 1.0, wy = (J & 1) ? 0.5 : 1.0, wx = (I & 1) ? 0.5 : 1.0;
+            // terms with a zero offset repeat the base value with weight 0 (same sum)
+            const double f000 = cf[c0], f001 = cf[c0 + ox], f010 = cf[c0 + oy], f011 = cf[c0 + oy + ox];
+            const double f100 = cf[c0 + oz], f101 = cf[c0 + oz + ox], f110 = cf[c0 + oz + oy],
+                         f111 = cf[c0 + oz + oy + ox];
+            const double ax = ox ? wx : 0.0, ay = oy ? wy : 0.0, az = oz ? wz : 0.0;
+            const double y0 = wx * f000 + ax * f001, y1 = wx * f010 + ax * f011;
+            const double y2 = wx * f100 + ax * f101, y3 = wx * f110 + ax * f111;
+            const double z0 = wy * y0 + ay * y1, z1 = wy * y2 + ay * y3;
+            s = sc * (wz * z0 + az * z1);
         }
         z[i] = accumulate ? (T)((double)z[i] + s) : (T)s;
     }
