@@ -20,6 +20,7 @@
 #include "fg_common.cuh"
 #include "pa_kernels.cuh"
 #include "vec_kernels.cuh"
+#include "form_kernels.cuh"
 
 
 using namespace fg;
@@ -493,21 +494,21 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
     };
     if (mesh->vcoord) {
         const size_t nb = sizeof(double) * 3 * (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
-        if (cudaMalloc(&d_vc, nb) || cudaMemcpy(d_vc, mesh->vcoord, nb, cudaMemcpyHostToDevice)) {
+        if (cudaMalloc(&d_vc, nb) || cudaMemcpy(d_vc, mesh->vcoord, nb, cudaMemcpyDefault)) {
             cleanup_in();
             return bail(fail(FG_CUDA_ERROR, "vertex upload failed"));
         }
     }
     if (kappa_q) {
         const size_t nb = sizeof(double) * E * Q3;
-        if (cudaMalloc(&d_kq, nb) || cudaMemcpy(d_kq, kappa_q, nb, cudaMemcpyHostToDevice)) {
+        if (cudaMalloc(&d_kq, nb) || cudaMemcpy(d_kq, kappa_q, nb, cudaMemcpyDefault)) {
             cleanup_in();
             return bail(fail(FG_CUDA_ERROR, "kappa upload failed"));
         }
     }
     if (rho_q) {
         const size_t nb = sizeof(double) * E * Q3;
-        if (cudaMalloc(&d_rq, nb) || cudaMemcpy(d_rq, rho_q, nb, cudaMemcpyHostToDevice)) {
+        if (cudaMalloc(&d_rq, nb) || cudaMemcpy(d_rq, rho_q, nb, cudaMemcpyDefault)) {
             cleanup_in();
             return bail(fail(FG_CUDA_ERROR, "rho upload failed"));
         }
@@ -1067,11 +1068,12 @@ static int fcg_nn_run(fg_op *op, const PcgBufs<double> &B, const ChebCoef &cc, i
     return FG_OK;
 }
 
-static void set_state(fg_op *op, SolverState *dst, double rtol, double atol, int max_iter) {
+static void set_state(fg_op *op, SolverState *dst, double rtol, double atol, int max_iter, int cgop = 0) {
     SolverState h{};
     h.rtol = rtol;
     h.atol = atol;
     h.max_iter = max_iter;
+    h.cgop = cgop;
     cudaMemcpyAsync(dst, &h, sizeof h, cudaMemcpyHostToDevice, op->stream);
 }
 
@@ -1194,7 +1196,8 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
     if (!ir) {
         PcgBufs<double> B{op->qd, op->face, dinv_use, op->xw, op->bw, op->r, op->z, op->pv,
                           op->ap, op->cres, op->cd, op->ct, op->st};
-        set_state(op, op->st, cfg.rtol, cfg.atol, cfg.max_iter);
+        // FG_PC_NONE is the operator CG of solve_cg_operator, with its stopping rule
+        set_state(op, op->st, cfg.rtol, cfg.atol, cfg.max_iter, cfg.precond == FG_PC_NONE ? 1 : 0);
         if (learned) {
             if ((rc = fcg_nn_run(op, B, cc, cfg.max_iter, cfg.check_interval, cfg.nn_budget, &h, &applies,
                                  &fell_back)))
@@ -2354,6 +2357,193 @@ FG_API int fg_unet_train_energy(fg_unet *u, fg_op *op, const double *d_res, int 
     }
     if (loss) *loss = (float)(L / B);
     return check_device_error(op);
+}
+
+// ---------------------------------------------------------------------------
+// Linear forms, L2 error and lumped mass (one-time work around the solve).
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+// n-point Gauss-Legendre rule on [-1, 1]: closed forms up to 4 points (the
+// operator's rules), Newton on the Legendre recurrence above
+static void gauss_rule(int n, double *x, double *w) {
+    if (n <= 4) {
+        gauss_legendre(n, x, w);
+        return;
+    }
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= n; ++k) {
+                const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1.0);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        x[n - 1 - i] = z;
+        w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+struct FormSetup {
+    FormArgs A{};
+    double *d_vc = nullptr;
+    int64_t E = 0, N = 0;
+    ~FormSetup() {
+        if (d_vc) cudaFree(d_vc);
+    }
+};
+
+static int form_setup(const fg_mesh *mesh, int order, int nq, FormSetup &F) {
+    if (!mesh) return fail(FG_INVALID_ARGUMENT, "NULL mesh");
+    if (mesh->nx < 1 || mesh->ny < 1 || mesh->nz < 1) return fail(FG_INVALID_ARGUMENT, "empty mesh");
+    if (order < 1 || order > FG_MAXP) return fail(FG_UNSUPPORTED, "order %d not supported (1..%d)", order, FG_MAXP);
+    if (nq < 1 || nq > FORM_MAXQ) return fail(FG_UNSUPPORTED, "%d quadrature points not supported (1..%d)", nq, FORM_MAXQ);
+    Grid &g = F.A.g;
+    g.nx = mesh->nx; g.ny = mesh->ny; g.nz = mesh->nz; g.p = order;
+    g.NI = mesh->nx * order + 1; g.NJ = mesh->ny * order + 1; g.NK = mesh->nz * order + 1;
+    F.E = (int64_t)g.nx * g.ny * g.nz;
+    F.N = (int64_t)g.NI * g.NJ * g.NK;
+    F.A.nq = nq;
+    gauss_rule(nq, F.A.gx, F.A.gw);
+    for (int q = 0; q < nq; ++q) {
+        double phi[FG_MAXP + 1], dphi[FG_MAXP + 1];
+        lagrange1d(order, F.A.gx[q], phi, dphi);
+        for (int d = 0; d <= order; ++d) F.A.B[q][d] = phi[d];
+    }
+    if (mesh->vcoord) {
+        const size_t nb = sizeof(double) * 3 * (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+        CK(cudaMalloc(&F.d_vc, nb));
+        CK(cudaMemcpy(F.d_vc, mesh->vcoord, nb, cudaMemcpyDefault));
+    }
+    F.A.vcoord = F.d_vc;
+    return FG_OK;
+}
+
+// device copy of n doubles from host or device memory (owned = allocated here)
+struct DevBuf {
+    double *p = nullptr;
+    bool owned = false;
+    ~DevBuf() {
+        if (owned && p) cudaFree(p);
+    }
+};
+static int dev_in(const double *src, int64_t n, int mem, DevBuf &d) {
+    if (!src) return FG_OK;
+    if (mem == FG_DEVICE) {
+        d.p = const_cast<double *>(src);
+        return FG_OK;
+    }
+    CK(cudaMalloc(&d.p, sizeof(double) * (size_t)std::max<int64_t>(n, 1)));
+    d.owned = true;
+    CK(cudaMemcpy(d.p, src, sizeof(double) * n, cudaMemcpyHostToDevice));
+    return FG_OK;
+}
+
+// out = M_f 1 with M_f the mass form of the coefficient f (sum_j phi_j = 1),
+// then the essential rows of ess_tags set to zero
+static int mass_times_ones(const fg_mesh *mesh, int order, const double *f_q, double f_const, int ess_tags,
+                           double *out, int mem) {
+    fg_op *op = nullptr;
+    int rc = fg_op_create(mesh, order, order + 1, FG_MASS, 1.0, 0.0, nullptr, 0.0, f_q, f_const, 0, &op);
+    if (rc) return rc;
+    struct Kill { fg_op *o; ~Kill() { fg_op_destroy(o); } } kill{op};
+    std::lock_guard<std::mutex> lk(op->mu);
+    double *ones = nullptr, *y = nullptr;
+    CK(cudaMalloc(&ones, sizeof(double) * op->Nn));
+    struct F1 { double *p; ~F1() { cudaFree(p); } } f1{ones};
+    CK(cudaMalloc(&y, sizeof(double) * op->Nn));
+    struct F2 { double *p; ~F2() { cudaFree(p); } } f2{y};
+    CK(cudaMemsetAsync(ones, 0, sizeof(double) * op->Nn, op->stream));
+    k_invert_diag<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->g, ones, ones);  // 1 on DOFs, 0 on pads
+    CK(cudaGetLastError());
+    if ((rc = apply_native(op, ones, y, 0, 0, nullptr))) return rc;
+    if (ess_tags) {
+        Grid g = op->g;
+        g.ess = ess_tags;
+        zero_ess_kernel<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(g, y);
+        CK(cudaGetLastError());
+    }
+    if ((rc = from_native(op, out, y, mem))) return rc;
+    CK(cudaStreamSynchronize(op->stream));
+    return check_device_error(op);
+}
+
+extern "C" {
+
+FG_API int fg_quadrature_points(const fg_mesh *mesh, int nq, double *xyz, int mem) {
+    if (!xyz) return fail(FG_INVALID_ARGUMENT, "NULL output");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    FormSetup F;
+    int rc;
+    if ((rc = form_setup(mesh, 1, nq, F))) return rc;
+    const int Q3 = nq * nq * nq;
+    const int64_t n = F.E * Q3 * 3;
+    double *out = xyz;
+    if (mem == FG_HOST) CK(cudaMalloc(&out, sizeof(double) * n));
+    struct F1 { double *p; bool own; ~F1() { if (own) cudaFree(p); } } f1{out, mem == FG_HOST};
+    qp_coords_kernel<<<VEC_GRID * 4, 256>>>(F.A, out);
+    CK(cudaGetLastError());
+    if (mem == FG_HOST) CK(cudaMemcpy(xyz, out, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CK(cudaDeviceSynchronize());
+    return FG_OK;
+}
+
+FG_API int fg_assemble_source(const fg_mesh *mesh, int order, const double *f_q, double f_const, int ess_tags,
+                              double *b, int mem) {
+    if (!b) return fail(FG_INVALID_ARGUMENT, "NULL output");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    if (ess_tags < 0 || ess_tags > 63) return fail(FG_INVALID_ARGUMENT, "bad ess_tags %d", ess_tags);
+    return mass_times_ones(mesh, order, f_q, f_const, ess_tags, b, mem);
+}
+
+FG_API int fg_lumped_mass(const fg_mesh *mesh, int order, const double *rho_q, double rho_const, double *diag,
+                          int mem) {
+    if (!diag) return fail(FG_INVALID_ARGUMENT, "NULL output");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    return mass_times_ones(mesh, order, rho_q, rho_const, 0, diag, mem);
+}
+
+FG_API int fg_lumped_apply(const double *diag, const double *x, double *y, int64_t n, int mode, int mem) {
+    if (!diag || !x || !y || n < 0) return fail(FG_INVALID_ARGUMENT, "bad arguments");
+    if (mode < 0 || mode > 2) return fail(FG_INVALID_ARGUMENT, "bad mode %d", mode);
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    if (n == 0) return FG_OK;
+    DevBuf dd, dx, dy;
+    int rc;
+    if ((rc = dev_in(diag, n, mem, dd)) || (rc = dev_in(x, n, mem, dx)) || (rc = dev_in(y, n, mem, dy))) return rc;
+    lumped_apply_kernel<<<VEC_GRID, 256>>>(dd.p, dx.p, dy.p, n, mode);
+    CK(cudaGetLastError());
+    if (mem == FG_HOST) CK(cudaMemcpy(y, dy.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CK(cudaDeviceSynchronize());
+    return FG_OK;
+}
+
+FG_API int fg_l2_error(const fg_mesh *mesh, int order, int nq, const double *u, const double *u_q, double *err,
+                       int mem) {
+    if (!u || !err) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    FormSetup F;
+    int rc;
+    if ((rc = form_setup(mesh, order, nq, F))) return rc;
+    DevBuf du, duq;
+    if ((rc = dev_in(u, F.N, mem, du)) || (rc = dev_in(u_q, F.E * nq * nq * nq, mem, duq))) return rc;
+    double *part = nullptr;
+    CK(cudaMalloc(&part, sizeof(double) * VEC_GRID));
+    struct F1 { double *p; ~F1() { cudaFree(p); } } f1{part};
+    l2_error_kernel<<<VEC_GRID, 256>>>(F.A, du.p, duq.p, part);
+    CK(cudaGetLastError());
+    std::vector<double> h(VEC_GRID);
+    CK(cudaMemcpy(h.data(), part, sizeof(double) * VEC_GRID, cudaMemcpyDeviceToHost));
+    double s = 0.0;
+    for (double v : h) s += v;  // block order: deterministic
+    *err = std::sqrt(s);
+    return FG_OK;
 }
 
 }  // extern "C"

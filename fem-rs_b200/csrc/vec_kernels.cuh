@@ -25,6 +25,11 @@ struct SolverState {
     int iter, done, converged, breakdown, max_iter;
     int trigger, skip_rel;     // reliable update pending / its kernels skip
     unsigned int ticket;
+    // operator-CG stopping rule (solve_cg_operator, crates/solver/src/lib.rs:229-278):
+    // converged when ||r|| <= stop_abs = max(atol, rtol*max(||b||, 1e-32)), also
+    // before the first iteration; breakdown |pAp| < 1e-32; res = ||r|| (absolute)
+    int cgop;
+    double stop_abs;
 };
 
 template <int NV>
@@ -138,7 +143,14 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_init(int64_t n, const T *__
         st->converged = 0;
         st->breakdown = 0;
         st->done = 0;
-        if (st->bnorm < 1e-30) {
+        if (st->cgop) {  // z = r here, so rz = ||r0||^2
+            st->stop_abs = fmax(st->atol, st->rtol * fmax(st->bnorm, 1e-32));
+            st->res = sqrt(tot[0]);
+            if (st->res <= st->stop_abs) {
+                st->converged = 1;
+                st->done = 1;
+            }
+        } else if (st->bnorm < 1e-30) {
             st->converged = 1;
             st->done = 1;
             st->res = 0.0;
@@ -160,7 +172,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_pap(int64_t n, const T *__r
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) {
         st->pap = tot[0];
-        if (fabs(tot[0]) < 1e-30) {
+        if (fabs(tot[0]) < (st->cgop ? 1e-32 : 1e-30)) {
             st->breakdown = 1;
             st->done = 1;
         } else {
@@ -204,8 +216,8 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_update(int64_t n, T *__rest
         st->iter += 1;
         st->rr = tot[0];
         const double rn = sqrt(tot[0]);
-        st->res = rn / st->bnorm;
-        if (st->res < st->rtol || rn < st->atol) {
+        st->res = st->cgop ? rn : rn / st->bnorm;
+        if (st->cgop ? rn <= st->stop_abs : (st->res < st->rtol || rn < st->atol)) {
             st->converged = 1;
             st->done = 1;
         } else if (st->iter >= st->max_iter) {

@@ -43,7 +43,8 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_unet_create", "fg_unet_destroy", "fg_unet_num_params", "fg_unet_get_params",
            "fg_unet_set_params", "fg_unet_get_grads", "fg_unet_forward", "fg_unet_loss_grad",
            "fg_unet_train_step", "fg_op_set_nodal_kappa", "fg_op_attach_unet", "fg_op_collect_pairs",
-           "fg_op_collect_residuals", "fg_unet_train_energy")
+           "fg_op_collect_residuals", "fg_unet_train_energy", "fg_quadrature_points",
+           "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply")
 
 
 class FgMesh(C.Structure):
@@ -117,6 +118,11 @@ def lib():
         L.fg_op_collect_pairs.argtypes = [vp, vp, vp, i, i, vp, vp, vp]
         L.fg_op_collect_residuals.argtypes = [vp, vp, vp, i, i, vp, vp]
         L.fg_unet_train_energy.argtypes = [vp, vp, vp, i, C.c_float, vp]
+        L.fg_quadrature_points.argtypes = [vp, i, vp, i]
+        L.fg_assemble_source.argtypes = [vp, i, vp, d, i, vp, i]
+        L.fg_l2_error.argtypes = [vp, i, i, vp, vp, vp, i]
+        L.fg_lumped_mass.argtypes = [vp, i, vp, d, vp, i]
+        L.fg_lumped_apply.argtypes = [vp, vp, vp, i64, i, i]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
@@ -594,6 +600,75 @@ def collect_residuals(op, b, every, max_res, cfg=None):
     _check(lib().fg_op_collect_residuals(op.handle, b.ctypes.data, C.byref(c), int(every), int(max_res),
                                          out.data_ptr(), C.byref(n)))
     return out[:n.value]
+
+
+def _mesh_struct(nx, ny, nz, vcoord):
+    vc = None if vcoord is None else np.ascontiguousarray(vcoord, dtype=np.float64)
+    m = FgMesh(int(nx), int(ny), int(nz), None if vc is None else vc.ctypes.data)
+    return m, vc
+
+
+def quadrature_points(nx, ny, nz, nq, vcoord=None):
+    """Physical Gauss points (nq per direction): [E, nq^3, 3]."""
+    m, _vc = _mesh_struct(nx, ny, nz, vcoord)
+    out = np.zeros((nx * ny * nz, nq ** 3, 3))
+    _check(lib().fg_quadrature_points(C.byref(m), int(nq), out.ctypes.data, HOST))
+    return out
+
+
+def assemble_source(nx, ny, nz, p, f_q=None, f=1.0, ess_tags=TAG_ALL, vcoord=None):
+    """b_i = sum_e sum_q w |det J| f(x_q) phi_i(x_q) (DomainSourceIntegrator +
+    assemble_linear), essential rows zeroed; f_q at quadrature_points(.., p+1)."""
+    m, _vc = _mesh_struct(nx, ny, nz, vcoord)
+    fq = None if f_q is None else np.ascontiguousarray(f_q, dtype=np.float64)
+    b = np.zeros((nx * p + 1) * (ny * p + 1) * (nz * p + 1))
+    _check(lib().fg_assemble_source(C.byref(m), int(p), None if fq is None else fq.ctypes.data, float(f),
+                                    int(ess_tags), b.ctypes.data, HOST))
+    return b
+
+
+def l2_error(nx, ny, nz, p, u, u_q=None, nq=None, vcoord=None):
+    """||u_h - u||_L2 with an nq-point Gauss rule per direction (default p+2
+    clamped to 4, as hex_rule does); u_q = exact values at the points of that
+    rule ([E, nq^3]) or None."""
+    nq = int(nq if nq is not None else min(p + 2, 4))
+    m, _vc = _mesh_struct(nx, ny, nz, vcoord)
+    uu = np.ascontiguousarray(u, dtype=np.float64)
+    uq = None if u_q is None else np.ascontiguousarray(u_q, dtype=np.float64)
+    err = C.c_double()
+    _check(lib().fg_l2_error(C.byref(m), int(p), nq, uu.ctypes.data, None if uq is None else uq.ctypes.data,
+                             C.byref(err), HOST))
+    return float(err.value)
+
+
+class LumpedMassOperator:
+    """LumpedMassOperator (crates/assembly/src/partial.rs:217-274): row-sum
+    lumped mass diagonal assembled on the GPU; apply / apply_zero /
+    apply_inverse run on the GPU."""
+
+    def __init__(self, nx, ny, nz, p, rho=1.0, rho_q=None, vcoord=None):
+        m, _vc = _mesh_struct(nx, ny, nz, vcoord)
+        rq = None if rho_q is None else np.ascontiguousarray(rho_q, dtype=np.float64)
+        self.diag = np.zeros((nx * p + 1) * (ny * p + 1) * (nz * p + 1))
+        _check(lib().fg_lumped_mass(C.byref(m), int(p), None if rq is None else rq.ctypes.data, float(rho),
+                                    self.diag.ctypes.data, HOST))
+
+    def _run(self, x, y, mode):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert y.dtype == np.float64 and y.flags.c_contiguous and len(x) == len(y) == len(self.diag)
+        _check(lib().fg_lumped_apply(self.diag.ctypes.data, x.ctypes.data, y.ctypes.data, len(x), mode, HOST))
+
+    def apply(self, x, y):
+        """y += diag * x"""
+        self._run(x, y, 1)
+
+    def apply_zero(self, x, y):
+        """y = diag * x"""
+        self._run(x, y, 0)
+
+    def apply_inverse(self, x, y):
+        """y = x / diag (0 where |diag| <= 1e-14)"""
+        self._run(x, y, 2)
 
 
 def nodal_kappa_from_q(kq, nx, ny, nz, p=1):

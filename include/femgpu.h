@@ -111,7 +111,8 @@ typedef struct {
 typedef struct {
     int32_t converged;
     int32_t iterations;      /* PCG iterations */
-    double final_residual;   /* ||r||/||b|| of the recurrence residual */
+    double final_residual;   /* ||r||/||b|| of the recurrence residual; ||r|| for FG_PC_NONE
+                                (the operator CG's stopping rule, lib.rs:229-278) */
     double true_residual;    /* ||b - A x||/||b|| recomputed in FP64 at exit */
     int32_t status;          /* fg_status */
     int32_t outer_iterations;/* FP32_IR: FP64 reliable updates of x and the residual */
@@ -298,6 +299,35 @@ FG_API int fg_op_collect_residuals(fg_op *op, const double *b, const fg_cfg *cfg
  * loss = (c.Ac/2 - c.r) / (s^2 64^L Nc), Nc = network voxels; its minimiser
  * over range(P^L) is the Galerkin coarse correction.  *loss = batch mean. */
 FG_API int fg_unet_train_energy(fg_unet *net, fg_op *op, const double *res, int B, float lr, float *loss);
+
+/* ---- one-time work around the solve ---------------------------------------- */
+/* Physical Gauss points (nq per direction, nq <= 8) of every element:
+ * xyz[E][qz][qy][qx][3].  With nq = p+1 these are the points at which
+ * kappa_q / rho_q / f_q tables are given. */
+FG_API int fg_quadrature_points(const fg_mesh *mesh, int nq, double *xyz, int mem);
+/* Linear form b_i = sum_e sum_q w_q |det J| f(x_q) phi_i(x_q) with the
+ * (p+1)^3 Gauss rule: DomainSourceIntegrator + Assembler::assemble_linear
+ * (crates/assembly/src/standard/source.rs:39-50, assembler.rs:251-333,
+ * 434-454; hex_rule n = p+1 as in examples/mfem_ex1_poisson.rs:81,87).  f at
+ * the Gauss points ([E][qz][qy][qx], host or device as mem) or NULL for the
+ * constant f_const; the rows of the essential DOFs of ess_tags are set to
+ * zero (apply_dirichlet with g = 0, crates/linalg/src/csr.rs:297-312). */
+FG_API int fg_assemble_source(const fg_mesh *mesh, int order, const double *f_q, double f_const,
+                              int ess_tags, double *b, int mem);
+/* L2 norm of u_h - u with an nq-point Gauss rule per direction (nq <= 8):
+ * u_h = the FE field of the DOF values u (plain layout), u at the Gauss points
+ * ([E][nq^3]) or NULL for ||u_h||; the error norm of
+ * examples/mfem_ex1_poisson.rs:119-162. */
+FG_API int fg_l2_error(const fg_mesh *mesh, int order, int nq, const double *u, const double *u_q,
+                       double *err, int mem);
+/* LumpedMassOperator::assemble (crates/assembly/src/partial.rs:222-248): row-sum
+ * lumped mass diag_i = sum_q w |det J| rho phi_i (sum_j phi_j), (p+1)^3 Gauss
+ * rule, rho at the Gauss points or NULL for rho_const. */
+FG_API int fg_lumped_mass(const fg_mesh *mesh, int order, const double *rho_q, double rho_const,
+                          double *diag, int mem);
+/* LumpedMassOperator apply (mode 1: y += d x), apply_zero (mode 0: y = d x) and
+ * apply_inverse (mode 2: y = x / d, 0 where |d| <= 1e-14), partial.rs:251-273. */
+FG_API int fg_lumped_apply(const double *diag, const double *x, double *y, int64_t n, int mode, int mem);
 
 /* Synchronise the handle's stream and report device-side errors
  * (FG_DEVICE_TIMEOUT, FG_BOUNDS). */

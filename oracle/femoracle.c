@@ -447,6 +447,7 @@ static double u_sin(const double x[3]) {
 /* standard/source.rs:39-50: f_elem[i] += w f(x) phi_i; assembler.rs:434-454 */
 int or_source(const or_mesh *m, int f_kind, int nq, const uint8_t *ess, double *b) {
     (void)f_kind;
+    if (nq < 1 || nq > MAXD) return -1; /* hex_rule clamps to 4 points (quadrature.rs:405-419) */
     int64_t N = or_ndofs(m);
     memset(b, 0, sizeof(double) * N);
     reftab t;
@@ -473,7 +474,38 @@ int or_source(const or_mesh *m, int f_kind, int nq, const uint8_t *ess, double *
     return 0;
 }
 
+/* partial.rs:222-248 (LumpedMassOperator::assemble) on hexahedra: per
+ * quadrature point diag_i += w |det J| rho phi_i (sum_j phi_j). */
+int or_lumped_mass(const or_mesh *m, const double *rho_q, double rho_c, int nq, double *diag) {
+    if (nq < 1 || nq > MAXD) return -1;
+    int64_t N = or_ndofs(m);
+    memset(diag, 0, sizeof(double) * N);
+    reftab t;
+    reftab_init(&t, m->p, nq);
+    int L = t.L;
+    FOR_COLOURED_ELEMENTS(m, {
+        int64_t dofs[MAXL];
+        double xv[8][3], de[MAXL];
+        or_elem_dofs(m, e, dofs);
+        elem_vertices(m, e, xv);
+        for (int i = 0; i < L; ++i) de[i] = 0.0;
+        for (int q = 0; q < t.Q3; ++q) {
+            double J[3][3], xp[3];
+            double det = iso_jacobian(xv, t.gq1 + 24 * q, t.pq1 + 8 * q, J, xp);
+            double rho = rho_q ? rho_q[e * t.Q3 + q] : rho_c;
+            double w = t.w[q] * fabs(det);
+            double psum = 0.0;
+            for (int j = 0; j < L; ++j) psum += t.phi[q * L + j];
+            for (int i = 0; i < L; ++i) de[i] += w * rho * t.phi[q * L + i] * psum;
+        }
+        for (int i = 0; i < L; ++i) diag[dofs[i]] += de[i];
+    })
+    reftab_free(&t);
+    return 0;
+}
+
 double or_l2_error_sin(const or_mesh *m, int nq, const double *u) {
+    if (nq < 1 || nq > MAXD) return -1.0;
     reftab t;
     reftab_init(&t, m->p, nq);
     int L = t.L;
@@ -590,8 +622,9 @@ double or_lambda_max(const or_mesh *m, int kind, double c_m, double c_k,
     return l;
 }
 
-/* par_solver.rs:262-342 (Jacobi) generalised to z = M r; precond 0 gives the
- * operator CG of solver/src/lib.rs:198-278 (stop on ||r|| <= max(atol, rtol*||b||)). */
+/* par_solver.rs:262-342 (Jacobi) generalised to z = M r; precond 0 is the
+ * operator CG of solver/src/lib.rs:198-278 with its own stopping rule
+ * (||r|| <= max(atol, rtol*max(||b||, 1e-32)), absolute final residual). */
 int or_pcg(const or_mesh *m, int kind, double c_m, double c_k,
            const double *kappa_q, double kappa_c, const double *rho_q, double rho_c,
            const uint8_t *ess, const double *b, double *x, const or_cfg *cfg,
@@ -631,14 +664,25 @@ int or_pcg(const or_mesh *m, int kind, double c_m, double c_k,
     double bnorm = sqrt(dot(N, b, b));
     int conv = 0, it_done = cfg->max_iter;
     double final_res = 0.0;
-    if (bnorm < 1e-30) {
+    /* precond 0 = solve_cg_operator (lib.rs:229-278): tol = max(atol,
+     * rtol*max(||b||, 1e-32)), converged when ||r|| <= tol (checked before the
+     * first iteration too), breakdown |pAp| < 1e-32, absolute final residual */
+    const int cgop = cfg->precond == 0;
+    const double tol_abs = fmax(cfg->atol, cfg->rtol * fmax(bnorm, 1e-32));
+    if (cgop) {
+        final_res = sqrt(rz);
+        if (final_res <= tol_abs) {
+            conv = 1; it_done = 0;
+            goto done;
+        }
+    } else if (bnorm < 1e-30) {
         conv = 1; it_done = 0; final_res = 0.0;
         goto done;
     }
     for (int iter = 0; iter < cfg->max_iter; ++iter) {
         op_apply(&o, p, ap);
         double pap = dot(N, p, ap);
-        if (fabs(pap) < 1e-30) break;
+        if (fabs(pap) < (cgop ? 1e-32 : 1e-30)) break;
         double alpha = rz / pap;
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; ++i) {
@@ -647,8 +691,8 @@ int or_pcg(const or_mesh *m, int kind, double c_m, double c_k,
         }
         double rr = dot(N, r, r);
         double rn = sqrt(rr) / bnorm;
-        final_res = rn;
-        if (rn < cfg->rtol || sqrt(rr) < cfg->atol) {
+        final_res = cgop ? sqrt(rr) : rn;
+        if (cgop ? sqrt(rr) <= tol_abs : (rn < cfg->rtol || sqrt(rr) < cfg->atol)) {
             conv = 1; it_done = iter + 1;
             goto done;
         }
@@ -659,7 +703,7 @@ int or_pcg(const or_mesh *m, int kind, double c_m, double c_k,
         for (int64_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
         rz = rz_new;
     }
-    final_res = sqrt(dot(N, r, r)) / bnorm;
+    final_res = cgop ? sqrt(dot(N, r, r)) : sqrt(dot(N, r, r)) / bnorm;
 done:
     res->converged = conv;
     res->iterations = it_done;

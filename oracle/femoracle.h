@@ -109,6 +109,9 @@ int or_source(const or_mesh *m, int f_kind, int nq, const uint8_t *ess, double *
 /* L2 error against u = sin(pi x) sin(pi y) sin(pi z) with nq points. */
 double or_l2_error_sin(const or_mesh *m, int nq, const double *u);
 
+/* Row-sum lumped mass (partial.rs:222-248); rho_q [E][q^3] or NULL for rho_c. */
+int or_lumped_mass(const or_mesh *m, const double *rho_q, double rho_c, int nq, double *diag);
+
 typedef struct {
     int precond;        /* 0 none (operator CG), 1 Jacobi, 2 Chebyshev(D^-1 A) */
     int cheb_degree;    /* Chebyshev sweeps (first sweep from zero needs no apply) */
@@ -120,7 +123,7 @@ typedef struct {
 typedef struct {
     int converged;
     int iterations;
-    double final_residual;   /* ||r||/||b|| of the recurrence residual */
+    double final_residual;   /* ||r||/||b|| of the recurrence residual (||r|| for precond 0) */
     double true_residual;    /* ||b - A x|| / ||b|| recomputed at exit */
     int64_t applies;
 } or_result;

@@ -65,6 +65,9 @@ def lib():
         L.or_source.argtypes = [vp, i, i, vp, vp]
         L.or_l2_error_sin.restype = d
         L.or_l2_error_sin.argtypes = [vp, i, vp]
+        L.or_lumped_mass.argtypes = [vp, vp, d, i, vp]
+        L.or_lumped_mass.restype = i
+        L.or_source.restype = i
         L.or_pcg.argtypes = [vp, i, d, d, vp, d, vp, d, vp, vp, vp, vp, vp, i]
         L.or_lambda_max.restype = d
         L.or_lambda_max.argtypes = [vp, i, d, d, vp, d, vp, d, vp, i, i]
@@ -161,13 +164,26 @@ def element_matrix(mesh, e, coef):
 
 def source(mesh, ess=None, nq=None):
     b = np.zeros(mesh.ndofs)
-    lib().or_source(mesh.ptr, 1, int(nq if nq else mesh.p + 1), _p(ess), _p(b))
+    if lib().or_source(mesh.ptr, 1, int(nq if nq else mesh.p + 1), _p(ess), _p(b)) != 0:
+        raise ValueError("the oracle's Gauss rules have 1 to 4 points")
     return b
 
 
 def l2_error_sin(mesh, u, nq=None):
+    """Default rule: p+2 points, clamped to 4 as hex_rule does (quadrature.rs:405-419)."""
     u = np.ascontiguousarray(u, dtype=np.float64)
-    return float(lib().or_l2_error_sin(mesh.ptr, int(nq if nq else mesh.p + 2), _p(u)))
+    e = float(lib().or_l2_error_sin(mesh.ptr, int(nq if nq else min(mesh.p + 2, 4)), _p(u)))
+    if e < 0:
+        raise ValueError("the oracle's Gauss rules have 1 to 4 points")
+    return e
+
+
+def lumped_mass(mesh, rho_q=None, rho=1.0, nq=None):
+    d = np.zeros(mesh.ndofs)
+    rq = None if rho_q is None else np.ascontiguousarray(rho_q, dtype=np.float64)
+    if lib().or_lumped_mass(mesh.ptr, _p(rq), C.c_double(rho), int(nq if nq else mesh.p + 1), _p(d)) != 0:
+        raise ValueError("the oracle's Gauss rules have 1 to 4 points")
+    return d
 
 
 def lambda_max(mesh, coef, ess, iters=20, nthreads=0):

@@ -14,6 +14,7 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 import femgpu  # noqa: E402
+from femgpu.fields import lognormal_kappa_q  # noqa: E402
 
 RTOL = 1e-12
 
@@ -193,3 +194,28 @@ def test_zero_rhs_returns_immediately():
     x = np.zeros(n)
     res = femgpu.solve_pcg_jacobi(op, np.zeros(n), x)
     assert res.converged and res.iterations == 0 and not x.any()
+
+
+@pytest.mark.parametrize("rtol,atol", [(1e-9, 0.0), (1e-12, 1e-4)])
+def test_cg_operator_stopping_rule_matches_oracle(rtol, atol):
+    """FG_PC_NONE is solve_cg_operator (crates/solver/src/lib.rs:229-278):
+    ||r|| <= max(atol, rtol*max(||b||, 1e-32)), absolute final residual,
+    exit before the first iteration when the start already meets it."""
+    need_gpu()
+    n, p = 6, 2
+    kq = lognormal_kappa_q(n, n, n, p, seed=8)
+    mesh = O.Mesh(n, n, n, p)
+    mask = O.ess_mask(mesh)
+    b = O.source(mesh, mask)
+    _, info = O.pcg(mesh, O.Coef(O.DIFF, kappa_q=kq), mask, b, precond=0, rtol=rtol, atol=atol, max_iter=5000)
+    op = femgpu.PADiffusionOperator((n, n, n), p, kappa=kq)
+    N = op.n_dofs()
+    x = np.zeros(N)
+    res = femgpu.solve_cg_operator(N, N, op, b, x, femgpu.SolverConfig(rtol=rtol, atol=atol, max_iter=5000))
+    assert res.converged and abs(res.iterations - info["iterations"]) <= 1
+    tol = max(atol, rtol * np.linalg.norm(b))
+    assert 0.05 * tol < res.final_residual <= tol
+    # restart from the solution with a tolerance it already meets
+    res0 = femgpu.solve_cg_operator(N, N, op, b, x.copy(),
+                                    femgpu.SolverConfig(rtol=0.0, atol=2.0 * res.final_residual))
+    assert res0.converged and res0.iterations == 0

@@ -176,6 +176,70 @@ def test_pcg_matches_dense_solve():
     assert np.abs(x - xd).max() < 1e-10 * np.abs(xd).max()
 
 
+def _cg_operator_numpy(A, b, x, rtol, atol, max_iter):
+    """crates/solver/src/lib.rs:198-278 restated on an assembled matrix:
+    (converged, iterations, final_residual) with the absolute residual."""
+    r = b - A @ x
+    p = r.copy()
+    tol = max(atol, rtol * max(np.linalg.norm(b), 1e-32))
+    rs_old = r @ r
+    res = np.sqrt(rs_old)
+    if res <= tol:
+        return True, 0, res
+    for it in range(max_iter):
+        ap = A @ p
+        pap = p @ ap
+        if abs(pap) < 1e-32:
+            return False, it, res
+        alpha = rs_old / pap
+        x += alpha * p
+        r -= alpha * ap
+        rs_new = r @ r
+        res = np.sqrt(rs_new)
+        if res <= tol:
+            return True, it + 1, res
+        p = r + (rs_new / rs_old) * p
+        rs_old = rs_new
+    return False, max_iter, res
+
+
+def _constrained_csr(m, coef, ess):
+    A = O.assemble_csr(m, coef).tolil()
+    fixed = np.nonzero(ess)[0]
+    A[fixed, :] = 0.0
+    A[:, fixed] = 0.0
+    A[fixed, fixed] = 1.0
+    return A.tocsr()
+
+
+@pytest.mark.parametrize("rtol,atol", [(1e-9, 0.0), (1e-3, 0.0), (1e-12, 1e-4)])
+def test_operator_cg_stopping_rule(rtol, atol):
+    """precond 0 follows solve_cg_operator: tol = max(atol, rtol*max(||b||,
+    1e-32)), ||r|| <= tol, absolute final residual."""
+    m = O.Mesh(5, 4, 3, 2)
+    ess = O.ess_mask(m)
+    coef = O.Coef(O.DIFF, kappa_q=np.exp(np.random.default_rng(7).normal(size=m.n_elem * 27)))
+    b = O.source(m, ess)
+    x, info = O.pcg(m, coef, ess, b, precond=0, rtol=rtol, atol=atol, max_iter=2000)
+    conv, its, res = _cg_operator_numpy(_constrained_csr(m, coef, ess), b, np.zeros(m.ndofs), rtol, atol, 2000)
+    assert info["converged"] and conv
+    assert abs(info["iterations"] - its) <= 1
+    tol = max(atol, rtol * np.linalg.norm(b))
+    # absolute residuals at the stop, both under the same tolerance
+    assert info["final_residual"] <= tol and res <= tol
+    assert info["final_residual"] > 0.05 * tol
+
+
+def test_operator_cg_exits_before_first_iteration():
+    m = O.Mesh(4, 4, 4, 1)
+    ess = O.ess_mask(m)
+    coef = O.Coef(O.DIFF)
+    b = O.source(m, ess)
+    x, _ = O.pcg(m, coef, ess, b, precond=1, rtol=1e-14, max_iter=2000)
+    _, info = O.pcg(m, coef, ess, b, x0=x, precond=0, rtol=1e-6)
+    assert info["converged"] and info["iterations"] == 0
+
+
 def test_chebyshev_pcg_converges_faster():
     m = O.Mesh(8, 8, 8, 2)
     ess = O.ess_mask(m)
