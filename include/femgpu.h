@@ -84,7 +84,7 @@ typedef struct fg_op fg_op;
 
 typedef struct {
     int32_t nx, ny, nz;    /* elements per direction */
-    const double *vcoord;  /* host, (nx+1)(ny+1)(nz+1)*3 vertex coordinates,
+    const double *vcoord;  /* host or device, (nx+1)(ny+1)(nz+1)*3 vertex coordinates,
                               lexicographic i fastest; NULL = unit cube */
 } fg_mesh;
 
@@ -129,7 +129,7 @@ FG_API void fg_cfg_default(fg_cfg *cfg);
 /* Build the operator: uploads the mesh, computes the quadrature data
  * (PAMassOperator::new / PADiffusionOperator::new + the libCEED-style
  * qdata build of crates/assembly/src/reed/qfunction.rs:155-192 in 3-D).
- * kappa_q / rho_q: host arrays [E][qz][qy][qx] (E = nx*ny*nz, element index
+ * kappa_q / rho_q: host or device arrays [E][qz][qy][qx] (E = nx*ny*nz, element index
  * (ez*ny + ey)*nx + ex) of per-quadrature-point coefficients, or NULL for the
  * constants.  nq1d must be order+1.  ess_tags: Dirichlet boundary tags used
  * when a call asks for the constrained operator. */
