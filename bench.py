@@ -472,10 +472,7 @@ def main():
             total += o.n_dofs()
         t_setup = time.perf_counter() - t_setup
         cfgb = femgpu.SolverConfig(rtol=1e-8, max_iter=5000, precision=femgpu.FP32_IR, check_interval=10)
-        bxs = [np.zeros_like(v) for v in bbs]
-        ok, bres = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
-        t_batch = bres[0].solve_ms / 1e3
-        # the same solves one after another (single-instance launches)
+        # the same solves one after another (single-instance launches, default tiles)
         t_seq = 0.0
         seq_iters = []
         for o, v in zip(bops, bbs):
@@ -483,14 +480,28 @@ def main():
             r1 = o.pcg(v, xs1, cfgb, femgpu.PC_CHEBYSHEV)
             t_seq += r1.solve_ms / 1e3
             seq_iters.append(r1.iterations)
-        batch = {"instances": len(bops), "total_dofs": total, "all_converged": bool(ok),
+        # batched with the default tiles
+        bxs = [np.zeros_like(v) for v in bbs]
+        ok0, bres0 = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
+        t_batch0 = bres0[0].solve_ms / 1e3
+        # autotuner: item depth per (order, size class) from timed batched applies
+        t_tune = time.perf_counter()
+        tune = femgpu.batch_autotune(bops, reps=3)
+        t_tune = time.perf_counter() - t_tune
+        bxs = [np.zeros_like(v) for v in bbs]
+        ok, bres = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
+        t_batch = bres[0].solve_ms / 1e3
+        batch = {"instances": len(bops), "total_dofs": total, "all_converged": bool(ok and ok0),
                  "max_true_residual": max(r.true_residual for r in bres),
                  "iterations_min_max": [min(r.iterations for r in bres), max(r.iterations for r in bres)],
                  "max_iteration_diff_vs_single": int(max(abs(a.iterations - b) for a, b in zip(bres, seq_iters))),
-                 "batched_solve_s": t_batch, "sequential_single_solves_s": t_seq,
-                 "speedup_batched_vs_sequential": t_seq / t_batch,
+                 "sequential_single_solves_s": t_seq, "batched_default_tiles_s": t_batch0,
+                 "batched_solve_s": t_batch, "speedup_batched_vs_sequential": t_seq / t_batch,
+                 "speedup_autotune": t_batch0 / t_batch,
                  "dof_iterations_per_s": sum(o.n_dofs() * r.iterations for o, r in zip(bops, bres)) / t_batch,
-                 "setup_s": t_setup}
+                 "setup_s": t_setup, "autotune_s": t_tune,
+                 "autotune": [{"order": e["order"], "size_class": e["size_class"], "instances": e["instances"],
+                               "tz": e["tz"], "us_per_candidate_tz": e["us"]} for e in tune]}
         for o in bops:
             o.close()
 

@@ -182,6 +182,9 @@ struct fg_op {
     std::vector<float *> nn_tmp;  // intermediate levels 1 .. nn_levels-1
     double *nn_scale = nullptr;
     int nn_levels = 1;  // coarsenings between the DOF lattice and the network volume
+    cudaStream_t nn_stream = nullptr;          // high-priority side stream of the network
+    cudaEvent_t nn_ev_r = nullptr, nn_ev_n = nullptr;
+    bool nn_overlap = true;                    // network beside the smoother (FG_NN_OVERLAP=0: in line)
     fg_unet *nn = nullptr;
     int fmt = 0;
     double *qa64 = nullptr;
@@ -223,6 +226,9 @@ static void free_op(fg_op *op) {
     if (op->ev1) cudaEventDestroy(op->ev1);
     if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
     if (op->cap_stream) cudaStreamDestroy(op->cap_stream);
+    if (op->nn_stream) cudaStreamDestroy(op->nn_stream);
+    if (op->nn_ev_r) cudaEventDestroy(op->nn_ev_r);
+    if (op->nn_ev_n) cudaEventDestroy(op->nn_ev_n);
     delete op;
 }
 
@@ -471,6 +477,8 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
     {
         const char *e = std::getenv("FG_SOLVER_GRAPHS");
         op->graphs = !(e && e[0] == '0');
+        const char *o = std::getenv("FG_NN_OVERLAP");
+        op->nn_overlap = !(o && o[0] == '0');
     }
     if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)))
         return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
@@ -975,11 +983,8 @@ template <typename T> static int nn_restrict(fg_op *op, const T *r, float *dst) 
     return FG_OK;
 }
 
-// fine native z (+)= scale[0] * mult * P^L (network-level FP32 field oc)
-template <typename T>
-static int nn_prolong(fg_op *op, const float *oc, T *z, const double *scale, double mult, int accumulate) {
-    Grid g = op->g;
-    g.ess = op->ess_tags;
+// level-1 FP32 field P^(L-1) oc of the network-level field oc (on op->stream)
+static const float *nn_prolong_to_level1(fg_op *op, const float *oc) {
     const float *f = oc;
     for (int l = op->nn_levels - 1; l >= 1; --l) {
         const Vol vc = nn_vol(op, l + 1), vf = nn_vol(op, l);
@@ -988,18 +993,58 @@ static int nn_prolong(fg_op *op, const float *oc, T *z, const double *scale, dou
         prolong_f32_kernel<<<blocks, 256, 0, op->stream>>>(f, vc, op->nn_tmp[l - 1], vf);
         f = op->nn_tmp[l - 1];
     }
-    fe_prolong_f32_kernel<T><<<VEC_GRID, 256, 0, op->stream>>>(g, f, nn_vol(op, 1), z, scale, mult, accumulate);
+    return f;
+}
+
+// fine native z (+)= scale[0] * mult * P f1 (level-1 FP32 field f1)
+template <typename T>
+static int nn_fe_prolong(fg_op *op, const float *f1, T *z, const double *scale, double mult, int accumulate) {
+    Grid g = op->g;
+    g.ess = op->ess_tags;
+    fe_prolong_f32_kernel<T><<<VEC_GRID, 256, 0, op->stream>>>(g, f1, nn_vol(op, 1), z, scale, mult, accumulate);
     CK(cudaGetLastError());
     return FG_OK;
 }
 
-// z += s 8^L P^L(UNet(R^L r / s, R^L log kappa)),  s = rms(R^L r)
-template <typename T> static int nn_precond_add(fg_op *op, const T *r, T *z) {
+// fine native z (+)= scale[0] * mult * P^L (network-level FP32 field oc)
+template <typename T>
+static int nn_prolong(fg_op *op, const float *oc, T *z, const double *scale, double mult, int accumulate) {
+    const float *f1 = nn_prolong_to_level1(op, oc);
+    CK(cudaGetLastError());
+    return nn_fe_prolong<T>(op, f1, z, scale, mult, accumulate);
+}
+
+// z += s 8^L P^L(UNet(R^L r / s, R^L log kappa)),  s = rms(R^L r), in two
+// halves around the Chebyshev smoother, which reads the same r:
+//   nn_begin: restriction, network and the coarse prolongations, issued on a
+//             high-priority side stream forked from op->stream (event), so the
+//             small latency-bound network kernels run beside the smoother's
+//             bandwidth-bound applies;
+//   nn_end:   op->stream waits for the side stream, then adds the last
+//             prolongation into z (after the smoother has written z).
+// The fork and join are events, so a chunk captured into a CUDA graph records
+// them as graph edges.  No buffer is shared between the two streams except r
+// (read by both) and the network's own buffers (side stream only).
+template <typename T> static int nn_begin(fg_op *op, const T *r, const float **f1) {
     fg_unet *u = op->nn;
-    u->stream = op->stream;
     const Vol Vc = nn_coarse_vol(op);
     int rc;
     if ((rc = unet_ensure_bufs(u, 1, Vc.Z, Vc.Y, Vc.X))) return rc;
+    const cudaStream_t main = op->stream;
+    struct Restore { fg_op *o; cudaStream_t s; ~Restore() { o->stream = s; } } restore{op, main};
+    if (op->nn_overlap) {
+        if (!op->nn_stream) {
+            int lo = 0, hi = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            CK(cudaStreamCreateWithPriority(&op->nn_stream, cudaStreamNonBlocking, hi));
+            CK(cudaEventCreateWithFlags(&op->nn_ev_r, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&op->nn_ev_n, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(op->nn_ev_r, main));
+        CK(cudaStreamWaitEvent(op->nn_stream, op->nn_ev_r, 0));
+        op->stream = op->nn_stream;
+    }
+    u->stream = op->stream;
     const int64_t nv = Vc.nvox();
     int blocks;
     grid_launch(nv, blocks);
@@ -1010,8 +1055,15 @@ template <typename T> static int nn_precond_add(fg_op *op, const T *r, T *z) {
     CK(cudaGetLastError());
     if ((rc = unet_forward(u))) return rc;
     out0_to_f32_kernel<<<blocks, 256, 0, op->stream>>>(TView{u->buf.out, 8, 0}, nv, op->nn_oc);
+    *f1 = nn_prolong_to_level1(op, op->nn_oc);
     CK(cudaGetLastError());
-    return nn_prolong<T>(op, op->nn_oc, z, op->nn_scale, nn_mult(op), 1);
+    if (op->nn_overlap) CK(cudaEventRecord(op->nn_ev_n, op->stream));
+    return FG_OK;
+}
+
+template <typename T> static int nn_end(fg_op *op, const float *f1, T *z) {
+    if (op->nn_overlap) CK(cudaStreamWaitEvent(op->stream, op->nn_ev_n, 0));
+    return nn_fe_prolong<T>(op, f1, z, op->nn_scale, nn_mult(op), 1);
 }
 
 // Flexible CG (FCG(1), Notay) with z = Chebyshev(r) [+ learned correction];
@@ -1031,9 +1083,11 @@ static int fcg_nn_run(fg_op *op, const PcgBufs<double> &B, const ChebCoef &cc, i
     k_pcg_init<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.b, B.ap, B.dinv, B.r, B.z, B.p,
                                                                  0, op->partials, B.st);
     auto direction = [&](int init) -> int {
-        int r2 = cheb_apply<double>(op, B, cc, B.r, B.z, skip);
-        if (r2) return r2;
-        if (nn_on && (r2 = nn_precond_add<double>(op, B.r, B.z))) return r2;
+        const float *f1 = nullptr;
+        int r2;
+        if (nn_on && (r2 = nn_begin<double>(op, B.r, &f1))) return r2;
+        if ((r2 = cheb_apply<double>(op, B, cc, B.r, B.z, skip))) return r2;
+        if (nn_on && (r2 = nn_end<double>(op, f1, B.z))) return r2;
         k_fcg_zap<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.ap, op->partials, B.st, init);
         k_pcg_pupdate<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.p, B.st, init);
         k_fcg_pr<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.r, op->partials, B.st);
@@ -1192,6 +1246,16 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
     int64_t applies = 0;
     SolverState h{};
     int outer = 1, inner_total = 0, status = FG_OK;
+    // one-time preparation (FP32 copies, network buffers) outside the timed solve
+    if (ir) {
+        if ((rc = ensure_fp32(op))) return rc;
+        if (cfg.precond != FG_PC_NONE && (rc = ensure_dinv32(op))) return rc;
+    }
+    if (learned) {
+        const Vol Vc = nn_coarse_vol(op);
+        if ((rc = unet_ensure_bufs(op->nn, 1, Vc.Z, Vc.Y, Vc.X))) return rc;
+    }
+    CK(cudaStreamSynchronize(op->stream));
     CK(cudaEventRecord(op->ev0, op->stream));
     if (!ir) {
         PcgBufs<double> B{op->qd, op->face, dinv_use, op->xw, op->bw, op->r, op->z, op->pv,
@@ -1240,9 +1304,11 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
         bool nn_on = learned;
         auto precond = [&](int init) -> int {
             if (learned) {  // flexible directions: z = Chebyshev(r) [+ learned correction]
-                int rc2 = cheb_apply<float>(op, B, cc, op->r32, op->z32, done);
-                if (rc2) return rc2;
-                if (nn_on && (rc2 = nn_precond_add<float>(op, op->r32, op->z32))) return rc2;
+                const float *f1 = nullptr;
+                int rc2;
+                if (nn_on && (rc2 = nn_begin<float>(op, op->r32, &f1))) return rc2;
+                if ((rc2 = cheb_apply<float>(op, B, cc, op->r32, op->z32, done))) return rc2;
+                if (nn_on && (rc2 = nn_end<float>(op, f1, op->z32))) return rc2;
                 k_fcg_zap<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z32, op->ap32, op->partials,
                                                                            op->st, init);
                 k_pcg_pupdate<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z32, op->p32, op->st, init);
@@ -1404,6 +1470,244 @@ template <typename T> static int dev_upload(T **dst, const std::vector<T> &v) {
     return FG_OK;
 }
 
+// ---- tile shape: items of 32 x WY x TZ elements -----------------------------
+template <int P, int OPK> static int relayout_t(fg_op *op, const Grid &gn, double *dst) {
+    const int64_t total = (int64_t)op->g.nx * op->g.ny * op->g.nz * (P + 1) * (P + 1) * (P + 1);
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+    qdata_relayout_kernel<P, OPK><<<blocks, 256, 0, op->stream>>>(op->g, gn, op->qd, dst);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+template <int P> static int relayout_p(fg_op *op, const Grid &gn, double **dst, int64_t *size) {
+    switch (op->kind) {
+    case FG_MASS: *size = qd_size<P, 1>(gn); break;
+    case FG_DIFF: *size = qd_size<P, 2>(gn); break;
+    default: *size = qd_size<P, 3>(gn); break;
+    }
+    int rc;
+    if ((rc = alloc_vec(dst, *size))) return rc;
+    switch (op->kind) {
+    case FG_MASS: return relayout_t<P, 1>(op, gn, *dst);
+    case FG_DIFF: return relayout_t<P, 2>(op, gn, *dst);
+    default: return relayout_t<P, 3>(op, gn, *dst);
+    }
+}
+
+// Move the operator to items of TZ = tz layers (caller holds op->mu): the
+// full quadrature data is re-laid out on the device, the face slots are
+// re-sized, and the FP32 / affine copies are dropped and rebuilt from the new
+// layout on next use (the affine FP64 copy at once if it is in use).
+static int set_tile_locked(fg_op *op, int tz) {
+    if (tz == op->g.TZ) return FG_OK;
+    Grid gn = op->g;
+    gn.TZ = tz;
+    gn.ntz = (gn.nz + tz - 1) / tz;
+    double *nq = nullptr, *nface = nullptr;
+    int64_t nsize = 0;
+    int rc;
+    switch (op->p) {
+    case 1: rc = relayout_p<1>(op, gn, &nq, &nsize); break;
+    case 2: rc = relayout_p<2>(op, gn, &nq, &nsize); break;
+    default: rc = relayout_p<3>(op, gn, &nq, &nsize); break;
+    }
+    if (!rc) rc = alloc_vec(&nface, (int64_t)gn.n_items() * gn.face_stride());
+    if (!rc && cudaStreamSynchronize(op->stream) != cudaSuccess)
+        rc = fail(FG_CUDA_ERROR, "quadrature-data re-layout failed: %s", cudaGetErrorString(cudaGetLastError()));
+    if (rc) {
+        if (nq) cudaFree(nq);
+        if (nface) cudaFree(nface);
+        return rc;
+    }
+    cudaFree(op->qd);
+    cudaFree(op->face);
+    float **f32[] = {&op->qd32, &op->face32, &op->qa32};
+    for (float **b : f32)
+        if (*b) { cudaFree(*b); *b = nullptr; }
+    if (op->qa64) { cudaFree(op->qa64); op->qa64 = nullptr; }
+    op->qd = nq;
+    op->face = nface;
+    op->qsize = nsize;
+    op->g = gn;
+    if (op->fmt == 1 && (rc = build_affine<double>(op, &op->qa64))) return rc;
+    return FG_OK;
+}
+
+// batched launches over a set of instances: block map with the instances
+// holding the most items first (fewer idle SMs at the end of a launch)
+static std::vector<int2> largest_first_bmap(fg_op *const *ops, const std::vector<int> &inst,
+                                            const std::vector<int> &slot_of) {
+    std::vector<int> order(inst.size());
+    for (size_t k = 0; k < inst.size(); ++k) order[k] = (int)k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return ops[inst[a]]->g.n_items() > ops[inst[b]]->g.n_items();
+    });
+    std::vector<int2> m;
+    for (int k : order)
+        for (int it = 0; it < ops[inst[k]]->g.n_items(); ++it) m.push_back(make_int2(slot_of[k], it));
+    return m;
+}
+
+static const int kTuneTZ[FG_TUNE_CANDIDATES] = {1, 2, 4, 8, 16};
+
+// time `reps` batched FP32 applies (apply + fix-up) of the instances `inst`
+// in their current tile shapes; microseconds per apply
+static int time_batched_apply(fg_op *const *ops, const std::vector<int> &inst, cudaStream_t bs, int reps,
+                              double *us) {
+    const int k = (int)inst.size();
+    std::vector<ApplyArgs<float>> a(k);
+    std::vector<CUtensorMap> t(k);
+    std::vector<FixArgs<float>> f(k);
+    std::vector<int> slot(k);
+    int rc;
+    for (int j = 0; j < k; ++j) {
+        fg_op *o = ops[inst[j]];
+        if ((rc = ensure_fp32(o))) return rc;
+        Grid g = o->g;
+        g.ess = o->ess_tags;
+        a[j] = ApplyArgs<float>{g, qdata_of<float>(o), o->ap32, o->face32, 0, o->d_err, nullptr};
+        if ((rc = encode_xmap<float>(o, o->p32, &t[j]))) return rc;
+        f[j] = FixArgs<float>{g, o->ap32, o->face32, nullptr};
+        slot[j] = j;
+        CK(cudaStreamSynchronize(o->stream));
+    }
+    fg_op *o0 = ops[inst[0]];
+    BatchGroup G{o0->p, o0->kind, o0->fmt, {}};
+    const std::vector<int2> m = largest_first_bmap(ops, inst, slot);
+    G.nblocks = (int)m.size();
+    ApplyArgs<float> *d_a = nullptr;
+    CUtensorMap *d_t = nullptr;
+    FixArgs<float> *d_f = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&]() {
+        void *ptrs[] = {G.bmap, d_a, d_t, d_f};
+        for (void *q : ptrs) if (q) cudaFree(q);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+    struct Guard { std::function<void()> f; ~Guard() { f(); } } guard{cleanup};
+    if ((rc = dev_upload(&G.bmap, m)) || (rc = dev_upload(&d_a, a)) || (rc = dev_upload(&d_t, t)) ||
+        (rc = dev_upload(&d_f, f)))
+        return rc;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const dim3 fgrid(64, k);
+    auto once = [&]() -> int {
+        int r2 = launch_batched<float>(bs, G, d_a, d_t, 1, 0);
+        if (r2) return r2;
+        fixup_batched_kernel<float><<<fgrid, 128, 0, bs>>>(d_f, 1, 0);
+        CK(cudaGetLastError());
+        return FG_OK;
+    };
+    for (int w = 0; w < 2; ++w)
+        if ((rc = once())) return rc;
+    CK(cudaEventRecord(e0, bs));
+    for (int r = 0; r < reps; ++r)
+        if ((rc = once())) return rc;
+    CK(cudaEventRecord(e1, bs));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    *us = 1e3 * ms / reps;
+    for (int j = 0; j < k; ++j)
+        if ((rc = check_device_error(ops[inst[j]]))) return rc;
+    return FG_OK;
+}
+
+extern "C" {
+
+FG_API int fg_op_set_tile(fg_op *op, int tz) {
+    if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
+    if (tz < 1 || tz > 64) return fail(FG_INVALID_ARGUMENT, "tile depth %d outside 1..64", tz);
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    return set_tile_locked(op, tz);
+}
+
+FG_API int fg_op_tile(const fg_op *op, int dims[3]) {
+    if (!op || !dims) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    dims[0] = 32;
+    dims[1] = op->g.WY;
+    dims[2] = op->g.TZ;
+    return FG_OK;
+}
+
+FG_API int fg_batch_autotune(fg_op *const *ops, int n, int reps, fg_tune_entry *out, int max_out, int *n_out) {
+    if (!ops || n <= 0 || reps < 1 || !n_out) return fail(FG_INVALID_ARGUMENT, "bad autotune arguments");
+    *n_out = 0;
+    std::vector<fg_op *> sorted(ops, ops + n);
+    for (int i = 0; i < n; ++i)
+        if (!ops[i]) return fail(FG_INVALID_ARGUMENT, "NULL instance %d", i);
+    std::sort(sorted.begin(), sorted.end());
+    if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+        return fail(FG_INVALID_ARGUMENT, "an operator appears twice in the batch");
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (fg_op *o : sorted) locks.emplace_back(o->mu);
+    const int dev = ops[0]->device;
+    for (int i = 0; i < n; ++i)
+        if (ops[i]->device != dev) return fail(FG_INVALID_ARGUMENT, "batch spans devices");
+    CK(cudaSetDevice(dev));
+    int rc;
+    for (int i = 0; i < n; ++i)
+        if ((rc = ensure_solver_buffers(ops[i])) || (rc = ensure_fp32(ops[i]))) return rc;
+    // classes of (order, kind, format, size): elements <= 16^3, <= 32^3, larger
+    struct Cls { int p, kind, fmt, sc; std::vector<int> inst; };
+    std::vector<Cls> cls;
+    for (int i = 0; i < n; ++i) {
+        const fg_op *o = ops[i];
+        const int64_t E = (int64_t)o->g.nx * o->g.ny * o->g.nz;
+        const int sc = E <= 4096 ? 0 : (E <= 32768 ? 1 : 2);
+        auto it = std::find_if(cls.begin(), cls.end(), [&](const Cls &c) {
+            return c.p == o->p && c.kind == o->kind && c.fmt == o->fmt && c.sc == sc;
+        });
+        if (it == cls.end()) { cls.push_back(Cls{o->p, o->kind, o->fmt, sc, {}}); it = cls.end() - 1; }
+        it->inst.push_back(i);
+    }
+    cudaStream_t bs;
+    CK(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+    struct SG { cudaStream_t s; ~SG() { cudaStreamDestroy(s); } } sg{bs};
+    // depth of a candidate for one instance: at most the largest power of two <= nz
+    auto depth = [&](const fg_op *o, int tz) {
+        int d = 1;
+        while (d * 2 <= tz && d * 2 <= o->g.nz) d *= 2;
+        return d;
+    };
+    int count = 0;
+    for (const Cls &c : cls) {
+        double us[FG_TUNE_CANDIDATES];
+        int best = -1;
+        int maxnz = 1;
+        for (int i : c.inst) maxnz = std::max(maxnz, ops[i]->g.nz);
+        for (int k = 0; k < FG_TUNE_CANDIDATES; ++k) {
+            us[k] = -1.0;
+            if (k > 0 && kTuneTZ[k] > maxnz) continue;  // same shapes as a smaller candidate
+            for (int i : c.inst)
+                if ((rc = set_tile_locked(ops[i], depth(ops[i], kTuneTZ[k])))) return rc;
+            if ((rc = time_batched_apply(ops, c.inst, bs, reps, &us[k]))) return rc;
+            if (best < 0 || us[k] < us[best]) best = k;
+        }
+        for (int i : c.inst) {
+            if ((rc = set_tile_locked(ops[i], depth(ops[i], kTuneTZ[best]))) || (rc = ensure_fp32(ops[i])))
+                return rc;
+            CK(cudaStreamSynchronize(ops[i]->stream));
+        }
+        if (out && count < max_out) {
+            fg_tune_entry &e = out[count];
+            e.order = c.p;
+            e.kind = c.kind;
+            e.size_class = c.sc;
+            e.instances = (int)c.inst.size();
+            e.tz = kTuneTZ[best];
+            e.format = c.fmt;
+            for (int k = 0; k < FG_TUNE_CANDIDATES; ++k) e.us[k] = us[k];
+        }
+        ++count;
+    }
+    *n_out = count;
+    return FG_OK;
+}
+
+}  // extern "C"
+
 extern "C" {
 
 FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, fg_result *res,
@@ -1556,9 +1860,7 @@ FG_API int fg_batch_pcg(fg_op *const *ops, int n, const double *const *b, double
     };
     struct Guard { std::function<void()> f; ~Guard() { f(); } } guard{cleanup};
     for (auto &G : groups) {
-        std::vector<int2> m;
-        for (int i : G.inst)
-            for (int it = 0; it < ops[i]->g.n_items(); ++it) m.push_back(make_int2(i, it));
+        const std::vector<int2> m = largest_first_bmap(ops, G.inst, G.inst);
         G.nblocks = (int)m.size();
         if ((rc = dev_upload(&G.bmap, m))) return rc;
     }

@@ -694,6 +694,30 @@ struct SetupArgs {
     int *err;
 };
 
+// Re-layout of full-format quadrature data for another z extent of the items
+// (TZ): the data of element e, point (col, qz), component c moves from its
+// place under grid go to its place under grid gn (same mesh, same WY).  One
+// thread per (element, point); pads of the new layout stay as initialised.
+template <int P, int OPK>
+__global__ void qdata_relayout_kernel(const Grid go, const Grid gn, const double *__restrict__ src,
+                                      double *__restrict__ dst) {
+    constexpr int Q = P + 1, NC = NComp<OPK>::v;
+    const int64_t total = (int64_t)go.nx * go.ny * go.nz * Q * Q * Q;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int cq = (int)(t % (Q * Q * Q));
+        const int64_t e = t / (Q * Q * Q);
+        const int col = cq / Q, qz = cq % Q;
+        const int ex = (int)(e % go.nx), ey = (int)((e / go.nx) % go.ny), ez = (int)(e / ((int64_t)go.nx * go.ny));
+        const int tx = ex / 32, lane = ex % 32, ty = ey / go.WY, wy = ey % go.WY;
+        const int io = ((ez / go.TZ) * go.nty + ty) * go.ntx + tx, lo = ez % go.TZ;
+        const int in = ((ez / gn.TZ) * gn.nty + ty) * gn.ntx + tx, ln = ez % gn.TZ;
+        const double *s = src + qd_index<P, OPK>(go, io, wy, lo, col, qz, 0, lane);
+        double *d = dst + qd_index<P, OPK>(gn, in, wy, ln, col, qz, 0, lane);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) d[c * 32] = s[c * 32];
+    }
+}
+
 // Affine-compressed quadrature data (FMT 1) derived from the full FP64 data:
 // on an element with constant J every D_q is w_q kappa_q times the same
 // symmetric matrix |detJ| J^-1 J^-T, so G_e = D_{q0} and s_q = tr(D_q)/tr(D_{q0})

@@ -44,7 +44,8 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_unet_set_params", "fg_unet_get_grads", "fg_unet_forward", "fg_unet_loss_grad",
            "fg_unet_train_step", "fg_op_set_nodal_kappa", "fg_op_attach_unet", "fg_op_collect_pairs",
            "fg_op_collect_residuals", "fg_unet_train_energy", "fg_quadrature_points",
-           "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply")
+           "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply", "fg_op_set_tile",
+           "fg_op_tile", "fg_batch_autotune")
 
 
 class FgMesh(C.Structure):
@@ -63,6 +64,14 @@ class FgSdirkResult(C.Structure):
     _fields_ = [("steps", C.c_int32), ("max_stage_iterations", C.c_int32), ("total_iterations", C.c_int64),
                 ("failed_solves", C.c_int32), ("reserved", C.c_int32), ("applies", C.c_int64),
                 ("time_ms", C.c_double)]
+
+
+TUNE_TZ = (1, 2, 4, 8, 16)
+
+
+class FgTuneEntry(C.Structure):
+    _fields_ = [("order", C.c_int32), ("kind", C.c_int32), ("format", C.c_int32), ("size_class", C.c_int32),
+                ("instances", C.c_int32), ("tz", C.c_int32), ("us", C.c_double * len(TUNE_TZ))]
 
 
 class FgResult(C.Structure):
@@ -123,6 +132,9 @@ def lib():
         L.fg_l2_error.argtypes = [vp, i, i, vp, vp, vp, i]
         L.fg_lumped_mass.argtypes = [vp, i, vp, d, vp, i]
         L.fg_lumped_apply.argtypes = [vp, vp, vp, i64, i, i]
+        L.fg_op_set_tile.argtypes = [vp, i]
+        L.fg_op_tile.argtypes = [vp, vp]
+        L.fg_batch_autotune.argtypes = [vp, i, i, vp, i, vp]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
@@ -336,6 +348,17 @@ class PAOperator:
     def set_stream(self, stream_ptr):
         _check(lib().fg_op_set_stream(self._h, stream_ptr))
 
+    @property
+    def tile(self):
+        """(32, WY, TZ): elements per apply work item in x, y, z."""
+        d = (C.c_int * 3)()
+        _check(lib().fg_op_tile(self._h, d))
+        return tuple(d)
+
+    def set_tile(self, tz):
+        """Re-lay out the quadrature data for items of TZ = tz element layers."""
+        _check(lib().fg_op_set_tile(self._h, int(tz)))
+
     # native layout helpers
     def to_native(self, v):
         out = np.zeros((self.NK, self.NJ, self.NIp))
@@ -449,6 +472,20 @@ def batch_pcg(ops, bs, xs, cfg=None, precond=PC_CHEBYSHEV):
                        int(r.applies), float(r.lmax), float(r.solve_ms), int(r.outer_iterations), int(r.status))
            for r in res]
     return rc == FG_OK, out
+
+
+def batch_autotune(ops, reps=5):
+    """Choose each batch class's item depth TZ by timing the batched FP32 apply
+    (fg_batch_autotune); the choice stays on the operators.  Returns one dict
+    per (order, kind, format, size class)."""
+    n = len(ops)
+    hs = (C.c_void_p * n)(*[o.handle for o in ops])
+    out = (FgTuneEntry * 64)()
+    cnt = C.c_int()
+    _check(lib().fg_batch_autotune(hs, n, int(reps), out, 64, C.byref(cnt)))
+    return [dict(order=e.order, kind=e.kind, format=e.format, size_class=e.size_class, instances=e.instances,
+                 tz=e.tz, us={tz: (e.us[k] if e.us[k] >= 0 else None) for k, tz in enumerate(TUNE_TZ)})
+            for e in out[:min(cnt.value, 64)]]
 
 
 SDIRK2_GAMMA = 1.0 - 2.0 ** -0.5  # crates/solver/src/ode.rs:441

@@ -300,6 +300,32 @@ FG_API int fg_op_collect_residuals(fg_op *op, const double *b, const fg_cfg *cfg
  * over range(P^L) is the Galerkin coarse correction.  *loss = batch mean. */
 FG_API int fg_unet_train_energy(fg_unet *net, fg_op *op, const double *res, int B, float lr, float *loss);
 
+/* ---- tile shape and the batched autotuner ------------------------------------ */
+/* An apply work item (one CTA's unit) is a box of 32 x WY x TZ elements; WY is
+ * fixed per order, TZ (layers per item) is chosen at creation (8, halved until
+ * there are >= 592 items) and can be changed: fg_op_set_tile re-lays out the
+ * quadrature data on the device.  fg_op_tile returns {32, WY, TZ}.  No
+ * reference counterpart (tuning of this library's kernels). */
+FG_API int fg_op_set_tile(fg_op *op, int tz);
+FG_API int fg_op_tile(const fg_op *op, int dims[3]);
+
+#define FG_TUNE_CANDIDATES 5 /* TZ = 1, 2, 4, 8, 16 */
+typedef struct {
+    int32_t order, kind, format;
+    int32_t size_class;  /* 0: <= 16^3 elements, 1: <= 32^3, 2: larger */
+    int32_t instances;   /* batch members in the class */
+    int32_t tz;          /* chosen layers per item */
+    double us[FG_TUNE_CANDIDATES]; /* batched FP32 apply time per candidate, -1 = not tried */
+} fg_tune_entry;
+/* Autotuner for fg_batch_pcg: instances are grouped by (order, kind, qdata
+ * format, size class); for each group every candidate TZ (clamped per
+ * instance to the largest power of two <= nz) is applied to all members, the
+ * group's batched FP32 apply (one launch + fix-up) is timed over `reps`
+ * launches with CUDA events, and the fastest is kept on the operators.
+ * Results per group in out[0 .. min(*n_out, max_out)). */
+FG_API int fg_batch_autotune(fg_op *const *ops, int n, int reps, fg_tune_entry *out, int max_out,
+                             int *n_out);
+
 /* ---- one-time work around the solve ---------------------------------------- */
 /* Physical Gauss points (nq per direction, nq <= 8) of every element:
  * xyz[E][qz][qy][qx][3].  With nq = p+1 these are the points at which

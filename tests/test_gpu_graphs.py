@@ -2,7 +2,8 @@
 direct chunks: solutions are bitwise identical and iteration counts equal
 with graphs on and off (FG_SOLVER_GRAPHS=0, read when a handle is created),
 for every solver loop (PCG-Jacobi, PCG-Chebyshev, mixed precision, learned
-flexible CG)."""
+flexible CG).  The learned correction computed on a side stream beside the
+smoother (default) equals the in-line order (FG_NN_OVERLAP=0) bit for bit."""
 import os
 
 import numpy as np
@@ -22,16 +23,18 @@ def need_gpu():
         pytest.skip("no CUDA device")
 
 
-def _op(n, p, kq, graphs):
-    old = os.environ.get("FG_SOLVER_GRAPHS")
-    os.environ["FG_SOLVER_GRAPHS"] = "1" if graphs else "0"
+def _op(n, p, kq, graphs, overlap=True):
+    env = {"FG_SOLVER_GRAPHS": "1" if graphs else "0", "FG_NN_OVERLAP": "1" if overlap else "0"}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         return femgpu.PADiffusionOperator((n, n, n), p, kappa=kq)
     finally:
-        if old is None:
-            del os.environ["FG_SOLVER_GRAPHS"]
-        else:
-            os.environ["FG_SOLVER_GRAPHS"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
 @pytest.mark.parametrize("precond,precision", [(femgpu.PC_JACOBI, femgpu.FP64),
@@ -71,8 +74,9 @@ def test_graph_replay_learned_fcg(precision):
     b[mask == 1] = 0.0
     net = femgpu.UNet(seed=2)
     xs, its = [], []
-    for graphs in (True, False):
-        op = _op(n, 1, kq, graphs)
+    # graphs + network beside the smoother, direct launches, network in line
+    for graphs, overlap in ((True, True), (False, True), (True, False)):
+        op = _op(n, 1, kq, graphs, overlap)
         femgpu.set_nodal_kappa(op, femgpu.nodal_kappa_from_q(kq, n, n, n), 1)
         femgpu.attach_unet(op, net)
         x = np.zeros(mesh.ndofs)
@@ -82,5 +86,5 @@ def test_graph_replay_learned_fcg(precision):
         xs.append(x)
         its.append(r.iterations)
         op.close()
-    assert its[0] == its[1]
-    assert np.array_equal(xs[0], xs[1])
+    assert its[0] == its[1] == its[2]
+    assert np.array_equal(xs[0], xs[1]) and np.array_equal(xs[0], xs[2])
