@@ -173,8 +173,9 @@ def main():
     ap.add_argument("--report", default=None)
     args = ap.parse_args()
     t0 = time.perf_counter()
+    init_meta = None
     if args.init:
-        net, _ = load(args.init)
+        net, init_meta = load(args.init)
     else:
         net = femgpu.UNet(tuple(int(c) for c in args.channels.split(",")), seed=1)
     seeds = list(range(args.first_seed, args.first_seed + args.train_fields))
@@ -189,6 +190,8 @@ def main():
             "train_s": t_train, "params": net.num_params, "channels": list(net.channels)}
     if seeds:
         save(net, args.out, meta)
+    elif init_meta is not None:  # evaluation of stored weights
+        meta = dict(init_meta, evaluation_only=True)
     forms = args.forms.split(",")
     eval_seeds = list(range(100_000, 100_000 + args.eval_fields))
     rows = evaluate(net, args.n, eval_seeds, args.levels, args.p, forms, args.eval_rhs)

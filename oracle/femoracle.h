@@ -153,4 +153,30 @@ double or_ref_spectral_radius_csr(int64_t n, const int64_t *rowptr, const int64_
 #ifdef __cplusplus
 }
 #endif
+/* ---- tetrahedra (femoracle_tet.c) ------------------------------------------
+ * tet_rule(order) of quadrature.rs:259-376: returns the point count (points
+ * [n][3] on the reference tet, weights summing to 1/6), -1 if cap is short. */
+int or_tet_rule(int order, double *pts, double *w, int cap);
+/* TetP1 / TetP2 basis values and reference gradients ([n][3]); returns n. */
+int or_tet_basis(int p, const double xi[3], double *phi, double *grad);
+/* partial.rs:85-130 / 154-208 on Tet4 elements: y (+)= A x.  coords
+ * [n_nodes][3]; elem_dofs [E][4 or 10], first 4 entries = vertex nodes;
+ * kappa_q / rho_q [E][nq] or NULL for the constants; kind bits 1 mass, 2
+ * diffusion; ess (or NULL): identity rows and columns on marked DOFs. */
+int or_tet_pa_apply(int p, int64_t n_dofs, const double *coords, int64_t n_elem, const int32_t *elem_dofs,
+                    int kind, double c_m, double c_k, const double *kappa_q, double kappa_c,
+                    const double *rho_q, double rho_c, int quad_order, const uint8_t *ess,
+                    const double *x, double *y, int accumulate);
+/* the diagonal of the same operator (1 on marked DOFs) */
+int or_tet_diagonal(int p, int64_t n_dofs, const double *coords, int64_t n_elem, const int32_t *elem_dofs,
+                    int kind, double c_m, double c_k, const double *kappa_q, double kappa_c,
+                    const double *rho_q, double rho_c, int quad_order, const uint8_t *ess, double *d);
+
+/* tests/poisson.rs:437-493 restated: the sin source form (ess rows zero) and
+ * the L2 error against sin(pi x) sin(pi y) sin(pi z) with tet_rule(quad_order). */
+int or_tet_source(int p, int64_t n_dofs, const double *coords, int64_t n_elem, const int32_t *elem_dofs,
+                  int quad_order, const uint8_t *ess, double *b);
+double or_tet_l2_error_sin(int p, const double *coords, int64_t n_elem, const int32_t *elem_dofs, int quad_order,
+                           const double *u);
+
 #endif

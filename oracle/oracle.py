@@ -66,6 +66,13 @@ def lib():
         L.or_l2_error_sin.restype = d
         L.or_l2_error_sin.argtypes = [vp, i, vp]
         L.or_lumped_mass.argtypes = [vp, vp, d, i, vp]
+        L.or_tet_rule.argtypes = [i, vp, vp, i]
+        L.or_tet_basis.argtypes = [i, vp, vp, vp]
+        L.or_tet_pa_apply.argtypes = [i, i64, vp, i64, vp, i, d, d, vp, d, vp, d, i, vp, vp, vp, i]
+        L.or_tet_diagonal.argtypes = [i, i64, vp, i64, vp, i, d, d, vp, d, vp, d, i, vp, vp]
+        L.or_tet_source.argtypes = [i, i64, vp, i64, vp, i, vp, vp]
+        L.or_tet_l2_error_sin.argtypes = [i, vp, i64, vp, i, vp]
+        L.or_tet_l2_error_sin.restype = d
         L.or_lumped_mass.restype = i
         L.or_source.restype = i
         L.or_pcg.argtypes = [vp, i, d, d, vp, d, vp, d, vp, vp, vp, vp, vp, i]
@@ -262,3 +269,75 @@ def ref_spectral_radius_csr(A, n_iter):
     ci = np.ascontiguousarray(A.indices, dtype=np.int64)
     v = np.ascontiguousarray(A.data, dtype=np.float64)
     return float(lib().or_ref_spectral_radius_csr(A.shape[0], _p(rp), _p(ci), _p(v), n_iter))
+
+
+# ---- tetrahedra (oracle/femoracle_tet.c) -------------------------------------
+def tet_rule(order):
+    pts = np.zeros((64, 3))
+    w = np.zeros(64)
+    n = lib().or_tet_rule(int(order), _p(pts), _p(w), 64)
+    assert n > 0
+    return pts[:n].copy(), w[:n].copy()
+
+
+def tet_basis(p, xi):
+    nl = 4 if p == 1 else 10
+    phi = np.zeros(nl)
+    g = np.zeros((nl, 3))
+    lib().or_tet_basis(int(p), _p(np.ascontiguousarray(xi, dtype=np.float64)), _p(phi), _p(g))
+    return phi, g
+
+
+class TetSpace:
+    """An order-p tet space: coords [n_nodes, 3], elem_dofs [E, 4|10] (first 4 =
+    vertex nodes), n_dofs, optional essential mask [n_dofs] uint8."""
+
+    def __init__(self, p, coords, elem_dofs, n_dofs, ess=None):
+        self.p = int(p)
+        self.coords = np.ascontiguousarray(coords, dtype=np.float64)
+        self.elem_dofs = np.ascontiguousarray(elem_dofs, dtype=np.int32)
+        self.n_dofs = int(n_dofs)
+        self.n_elem = self.elem_dofs.shape[0]
+        self.ess = None if ess is None else np.ascontiguousarray(ess, dtype=np.uint8)
+
+
+def _tet_coef(coef):
+    kq = None if coef.kappa_q is None else np.ascontiguousarray(coef.kappa_q, dtype=np.float64)
+    rq = None if coef.rho_q is None else np.ascontiguousarray(coef.rho_q, dtype=np.float64)
+    return kq, rq
+
+
+def tet_pa_apply(sp, coef, x, quad_order, constrained=False, y=None):
+    kq, rq = _tet_coef(coef)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    acc = y is not None
+    y = np.zeros(sp.n_dofs) if y is None else y
+    rc = lib().or_tet_pa_apply(sp.p, sp.n_dofs, _p(sp.coords), sp.n_elem, _p(sp.elem_dofs), coef.kind,
+                               coef.c_m, coef.c_k, _p(kq), coef.kappa, _p(rq), coef.rho, int(quad_order),
+                               _p(sp.ess) if constrained else None, _p(x), _p(y), int(acc))
+    assert rc == 0, rc
+    return y
+
+
+def tet_diagonal(sp, coef, quad_order, constrained=False):
+    kq, rq = _tet_coef(coef)
+    d = np.zeros(sp.n_dofs)
+    rc = lib().or_tet_diagonal(sp.p, sp.n_dofs, _p(sp.coords), sp.n_elem, _p(sp.elem_dofs), coef.kind,
+                               coef.c_m, coef.c_k, _p(kq), coef.kappa, _p(rq), coef.rho, int(quad_order),
+                               _p(sp.ess) if constrained else None, _p(d))
+    assert rc == 0, rc
+    return d
+
+
+def tet_source(sp, quad_order, constrained=True):
+    b = np.zeros(sp.n_dofs)
+    rc = lib().or_tet_source(sp.p, sp.n_dofs, _p(sp.coords), sp.n_elem, _p(sp.elem_dofs), int(quad_order),
+                             _p(sp.ess) if constrained else None, _p(b))
+    assert rc == 0, rc
+    return b
+
+
+def tet_l2_error_sin(sp, u, quad_order):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    return float(lib().or_tet_l2_error_sin(sp.p, _p(sp.coords), sp.n_elem, _p(sp.elem_dofs), int(quad_order),
+                                            _p(u)))
