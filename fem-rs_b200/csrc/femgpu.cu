@@ -50,6 +50,7 @@ static int fail(int status, const char *fmt, ...) {
     } while (0)
 
 #include "unet_host.cuh"
+#include "tet_host.cuh"
 
 // ---------------------------------------------------------------------------
 // 1-D tables: Gauss-Legendre (crates/element/src/quadrature.rs:12-32) and
@@ -2845,6 +2846,159 @@ FG_API int fg_l2_error(const fg_mesh *mesh, int order, int nq, const double *u, 
     double s = 0.0;
     for (double v : h) s += v;  // block order: deterministic
     *err = std::sqrt(s);
+    return FG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tetrahedral PA operator (TetP1 / TetP2 on unstructured Tet4 meshes)
+// ---------------------------------------------------------------------------
+FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64_t n_elem, const int32_t *elem_dofs,
+                         int64_t n_dofs, int kind, double c_mass, double c_diff, const double *kappa_q,
+                         double kappa_const, const double *rho_q, double rho_const, int quad_order,
+                         const uint8_t *ess, fg_tet **out) {
+    if (!out) return fail(FG_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (order != 1 && order != 2) return fail(FG_UNSUPPORTED, "tet order %d not supported (1, 2)", order);
+    if (kind < 1 || kind > 3) return fail(FG_INVALID_ARGUMENT, "bad operator kind %d", kind);
+    if (!coords || !elem_dofs || n_nodes < 4 || n_elem < 1 || n_dofs < n_nodes || n_dofs >= ((int64_t)1 << 31))
+        return fail(FG_INVALID_ARGUMENT, "bad tet mesh arguments");
+    if (n_elem * (order == 1 ? 4 : 10) >= ((int64_t)1 << 31))
+        return fail(FG_UNSUPPORTED, "too many elements for 32-bit element-local slots");
+    int rc;
+    fg_tet *t = new fg_tet();
+    struct Bail { fg_tet *t; bool armed = true; ~Bail() { if (armed) tet_free(t); } } bail{t};
+    CK(cudaGetDevice(&t->device));
+    t->p = order;
+    t->nl = order == 1 ? 4 : 10;
+    t->kind = kind;
+    t->E = n_elem;
+    t->N = n_dofs;
+    t->n_nodes = n_nodes;
+    const int nl = t->nl;
+    CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&t->d_err, sizeof(int)));
+    CK(cudaMemset(t->d_err, 0, sizeof(int)));
+    // element map: validate, transpose to [nl][E], CSR of element-local slots per DOF
+    std::vector<int32_t> h(n_elem * nl);
+    CK(cudaMemcpy(h.data(), elem_dofs, sizeof(int32_t) * h.size(), cudaMemcpyDefault));
+    std::vector<int32_t> soa(h.size());
+    std::vector<int64_t> offs(n_dofs + 1, 0);
+    for (int64_t e = 0; e < n_elem; ++e)
+        for (int i = 0; i < nl; ++i) {
+            const int32_t d = h[e * nl + i];
+            if (d < 0 || d >= n_dofs || (i < 4 && d >= n_nodes))
+                return fail(FG_BOUNDS, "element %lld local DOF %d out of range", (long long)e, i);
+            soa[(int64_t)i * n_elem + e] = d;
+            ++offs[d + 1];
+        }
+    for (int64_t d = 0; d < n_dofs; ++d) offs[d + 1] += offs[d];
+    std::vector<int32_t> slots(offs[n_dofs]);
+    {
+        std::vector<int64_t> pos(offs.begin(), offs.end() - 1);
+        for (int64_t e = 0; e < n_elem; ++e)  // (e, i) ascending within each DOF
+            for (int i = 0; i < nl; ++i) slots[pos[h[e * nl + i]]++] = (int32_t)((int64_t)i * n_elem + e);
+    }
+    if ((rc = tet_upload(&t->dofs, soa.data(), soa.size())) || (rc = tet_upload(&t->offs, offs.data(), offs.size())) ||
+        (rc = tet_upload(&t->slots, slots.data(), slots.size())) ||
+        (rc = tet_upload(&t->coords, coords, (size_t)n_nodes * 3)))
+        return rc;
+    if (ess && (rc = tet_upload(&t->ess, ess, (size_t)n_dofs))) return rc;
+    // rule tables
+    std::vector<double> pts, w;
+    t->nq = tet_rule_host(quad_order, pts, w);
+    if (t->nq > TET_MAXQ) return fail(FG_UNSUPPORTED, "quadrature order %d too high", quad_order);
+    std::vector<double> phi((size_t)t->nq * nl), grad((size_t)t->nq * nl * 3);
+    for (int q = 0; q < t->nq; ++q) tet_basis_host(order, &pts[3 * q], &phi[(size_t)q * nl], &grad[(size_t)q * nl * 3]);
+    double *d_w = nullptr;
+    if ((rc = tet_upload(&t->qp, pts.data(), pts.size())) || (rc = tet_upload(&t->phi, phi.data(), phi.size())) ||
+        (rc = tet_upload(&t->grad, grad.data(), grad.size())) || (rc = tet_upload(&d_w, w.data(), w.size())))
+        return rc;
+    struct FW { double *p; ~FW() { cudaFree(p); } } fw{d_w};
+    const double *d_kq = nullptr, *d_rq = nullptr;
+    double *tk = nullptr, *tr = nullptr;
+    struct FT { double **a, **b; ~FT() { if (*a) cudaFree(*a); if (*b) cudaFree(*b); } } ft{&tk, &tr};
+    if (kappa_q) { if ((rc = tet_upload(&tk, kappa_q, (size_t)n_elem * t->nq))) return rc; d_kq = tk; }
+    if (rho_q) { if ((rc = tet_upload(&tr, rho_q, (size_t)n_elem * t->nq))) return rc; d_rq = tr; }
+    CK(cudaMalloc(&t->G, sizeof(double) * 6 * n_elem));
+    if (kind & 2) CK(cudaMalloc(&t->sk, sizeof(double) * t->nq * n_elem));
+    if (kind & 1) CK(cudaMalloc(&t->sm, sizeof(double) * t->nq * n_elem));
+    CK(cudaMalloc(&t->Ye, sizeof(double) * nl * n_elem));
+    const TetArgs A = tet_args(t);
+    const int eb = (int)std::min<int64_t>((n_elem + 255) / 256, 148 * 16);
+    tet_setup_kernel<<<eb, 256, 0, t->stream>>>(A, nl, t->coords, d_w, d_kq, kappa_const, d_rq, rho_const, c_mass,
+                                                c_diff, t->G, t->sk, t->sm, t->d_err);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(t->stream));
+    int herr = 0;
+    CK(cudaMemcpy(&herr, t->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return fail(FG_BOUNDS, "degenerate tetrahedron (det J = 0)");
+    bail.armed = false;
+    *out = t;
+    return FG_OK;
+}
+
+FG_API void fg_tet_destroy(fg_tet *t) { tet_free(t); }
+
+FG_API int64_t fg_tet_ndofs(const fg_tet *t) { return t ? t->N : -1; }
+
+FG_API int fg_tet_nq(const fg_tet *t) { return t ? t->nq : -1; }
+
+FG_API int fg_tet_quadrature_points(fg_tet *t, double *xyz, int mem) {
+    if (!t || !xyz) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    std::lock_guard<std::mutex> lk(t->mu);
+    CK(cudaSetDevice(t->device));
+    const int64_t n = t->E * t->nq * 3;
+    double *out = xyz;
+    if (mem == FG_HOST) CK(cudaMalloc(&out, sizeof(double) * n));
+    struct F1 { double *p; bool own; ~F1() { if (own) cudaFree(p); } } f1{out, mem == FG_HOST};
+    const TetArgs A = tet_args(t);
+    tet_qp_coords_kernel<<<VEC_GRID * 4, 256, 0, t->stream>>>(A, t->coords, t->qp, out);
+    CK(cudaGetLastError());
+    if (mem == FG_HOST) CK(cudaMemcpyAsync(xyz, out, sizeof(double) * n, cudaMemcpyDeviceToHost, t->stream));
+    CK(cudaStreamSynchronize(t->stream));
+    return FG_OK;
+}
+
+FG_API int fg_tet_apply(fg_tet *t, const double *x, double *y, int accumulate, int constrained, int mem) {
+    if (!t || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    if (constrained && !t->ess) return fail(FG_INVALID_ARGUMENT, "constrained apply needs the essential mask");
+    std::lock_guard<std::mutex> lk(t->mu);
+    CK(cudaSetDevice(t->device));
+    const double *xd = x;
+    double *yd = y;
+    const size_t nb = sizeof(double) * t->N;
+    if (mem == FG_HOST) {
+        if (!t->xh) CK(cudaMalloc(&t->xh, nb));
+        if (!t->yh) CK(cudaMalloc(&t->yh, nb));
+        CK(cudaMemcpyAsync(t->xh, x, nb, cudaMemcpyHostToDevice, t->stream));
+        if (accumulate) CK(cudaMemcpyAsync(t->yh, y, nb, cudaMemcpyHostToDevice, t->stream));
+        xd = t->xh;
+        yd = t->yh;
+    }
+    int rc;
+    if ((rc = tet_launch_apply(t, xd, yd, accumulate, constrained, 0))) return rc;
+    if (mem == FG_HOST) CK(cudaMemcpyAsync(y, yd, nb, cudaMemcpyDeviceToHost, t->stream));
+    CK(cudaStreamSynchronize(t->stream));
+    return FG_OK;
+}
+
+FG_API int fg_tet_diagonal(fg_tet *t, double *d, int constrained, int mem) {
+    if (!t || !d) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);
+    if (constrained && !t->ess) return fail(FG_INVALID_ARGUMENT, "constrained diagonal needs the essential mask");
+    std::lock_guard<std::mutex> lk(t->mu);
+    CK(cudaSetDevice(t->device));
+    double *dd = d;
+    if (mem == FG_HOST) {
+        if (!t->yh) CK(cudaMalloc(&t->yh, sizeof(double) * t->N));
+        dd = t->yh;
+    }
+    int rc;
+    if ((rc = tet_launch_apply(t, nullptr, dd, 0, constrained, 1))) return rc;
+    if (mem == FG_HOST) CK(cudaMemcpyAsync(d, dd, sizeof(double) * t->N, cudaMemcpyDeviceToHost, t->stream));
+    CK(cudaStreamSynchronize(t->stream));
     return FG_OK;
 }
 

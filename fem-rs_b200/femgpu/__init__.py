@@ -45,7 +45,8 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_unet_train_step", "fg_op_set_nodal_kappa", "fg_op_attach_unet", "fg_op_collect_pairs",
            "fg_op_collect_residuals", "fg_unet_train_energy", "fg_quadrature_points",
            "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply", "fg_op_set_tile",
-           "fg_op_tile", "fg_batch_autotune")
+           "fg_op_tile", "fg_batch_autotune", "fg_tet_create", "fg_tet_destroy", "fg_tet_ndofs", "fg_tet_nq",
+           "fg_tet_quadrature_points", "fg_tet_apply", "fg_tet_diagonal")
 
 
 class FgMesh(C.Structure):
@@ -135,6 +136,15 @@ def lib():
         L.fg_op_set_tile.argtypes = [vp, i]
         L.fg_op_tile.argtypes = [vp, vp]
         L.fg_batch_autotune.argtypes = [vp, i, i, vp, i, vp]
+        L.fg_tet_create.argtypes = [i, i64, vp, i64, vp, i64, i, d, d, vp, d, vp, d, i, vp, C.POINTER(vp)]
+        L.fg_tet_destroy.argtypes = [vp]
+        L.fg_tet_destroy.restype = None
+        L.fg_tet_ndofs.argtypes = [vp]
+        L.fg_tet_ndofs.restype = i64
+        L.fg_tet_nq.argtypes = [vp]
+        L.fg_tet_quadrature_points.argtypes = [vp, vp, i]
+        L.fg_tet_apply.argtypes = [vp, vp, vp, i, i, i]
+        L.fg_tet_diagonal.argtypes = [vp, vp, i, i]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         _lib = L
     return _lib
@@ -637,6 +647,78 @@ def collect_residuals(op, b, every, max_res, cfg=None):
     _check(lib().fg_op_collect_residuals(op.handle, b.ctypes.data, C.byref(c), int(every), int(max_res),
                                          out.data_ptr(), C.byref(n)))
     return out[:n.value]
+
+
+class TetOperator:
+    """PA mass / diffusion operator on an unstructured Tet4 mesh with TetP1 or
+    TetP2 (fg_tet_*): the MatFreeOperator surface of partial.rs (apply =
+    y += A x, apply_zero = y = A x, n_dofs) plus the Jacobi diagonal.
+    coords [n_nodes, 3]; elem_dofs [E, 4|10] (first 4 = vertex nodes);
+    kappa / rho: constants or [E, nq] tables at quadrature_points()."""
+
+    def __init__(self, p, coords, elem_dofs, n_dofs, kind=DIFF, kappa=1.0, rho=1.0, c_mass=1.0, c_diff=1.0,
+                 quad_order=None, ess=None):
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        dofs = np.ascontiguousarray(elem_dofs, dtype=np.int32)
+        self.p, self.n = int(p), int(n_dofs)
+        self.quad_order = int(quad_order if quad_order is not None else 2 * p)
+        kq = None if np.isscalar(kappa) else np.ascontiguousarray(kappa, dtype=np.float64)
+        rq = None if np.isscalar(rho) else np.ascontiguousarray(rho, dtype=np.float64)
+        ms = None if ess is None else np.ascontiguousarray(ess, dtype=np.uint8)
+        self._keep = (coords, dofs, kq, rq, ms)
+        h = C.c_void_p()
+        _check(lib().fg_tet_create(self.p, coords.shape[0], coords.ctypes.data, dofs.shape[0], dofs.ctypes.data,
+                                   self.n, int(kind), float(c_mass), float(c_diff),
+                                   None if kq is None else kq.ctypes.data, float(kappa) if kq is None else 0.0,
+                                   None if rq is None else rq.ctypes.data, float(rho) if rq is None else 0.0,
+                                   self.quad_order, None if ms is None else ms.ctypes.data, C.byref(h)))
+        self._h = h
+        self.nq = int(lib().fg_tet_nq(h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fg_tet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def n_dofs(self):
+        return int(lib().fg_tet_ndofs(self._h))
+
+    def quadrature_points(self):
+        n_elem = self._keep[1].shape[0]
+        out = np.zeros((n_elem, self.nq, 3))
+        _check(lib().fg_tet_quadrature_points(self._h, out.ctypes.data, HOST))
+        return out
+
+    def _apply(self, x, y, accumulate, constrained):
+        px, mx = _as_f64(x)
+        py, my = _as_f64(y)
+        if mx != my:
+            raise TypeError("x and y must live in one memory space")
+        _check(lib().fg_tet_apply(self._h, px, py, int(accumulate), int(constrained), mx))
+        return y
+
+    def apply(self, x, y, constrained=False):
+        """y += A x"""
+        return self._apply(x, y, True, constrained)
+
+    def apply_zero(self, x, y, constrained=False):
+        """y = A x"""
+        return self._apply(x, y, False, constrained)
+
+    def matvec(self, x, constrained=False):
+        y = np.zeros(self.n)
+        return self.apply_zero(np.ascontiguousarray(x, dtype=np.float64), y, constrained)
+
+    def diagonal(self, constrained=False):
+        d = np.zeros(self.n)
+        _check(lib().fg_tet_diagonal(self._h, d.ctypes.data, int(constrained), HOST))
+        return d
 
 
 def _mesh_struct(nx, ny, nz, vcoord):

@@ -355,6 +355,35 @@ FG_API int fg_lumped_mass(const fg_mesh *mesh, int order, const double *rho_q, d
  * apply_inverse (mode 2: y = x / d, 0 where |d| <= 1e-14), partial.rs:251-273. */
 FG_API int fg_lumped_apply(const double *diag, const double *x, double *y, int64_t n, int mode, int mem);
 
+/* ---- tetrahedral PA operator -------------------------------------------------
+ * PAMassOperator / PADiffusionOperator on Tet4 meshes with TetP1 / TetP2
+ * (crates/assembly/src/partial.rs:85-130, 154-208 with ref_elem :277-288,
+ * simplex_jac :290-299, xform_grads :301-309; bases
+ * crates/element/src/lagrange/tet.rs; rule tet_rule(quad_order),
+ * crates/element/src/quadrature.rs:259-376).  coords [n_nodes][3]; elem_dofs
+ * [E][4 or 10] as DofManager numbers them (first 4 = vertex nodes,
+ * crates/space/src/dof_manager.rs:137-180, 628-700); kappa_q / rho_q
+ * [E][nq] at the rule's points (fg_tet_quadrature_points) or NULL for the
+ * constants; ess: essential-DOF mask [n_dofs] (boundary_dofs) or NULL.  All
+ * arrays in host or device memory.  The scatter is the transpose of the
+ * element map summed in a fixed order (no float atomics). */
+typedef struct fg_tet fg_tet;
+FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64_t n_elem,
+                         const int32_t *elem_dofs, int64_t n_dofs, int kind, double c_mass, double c_diff,
+                         const double *kappa_q, double kappa_const, const double *rho_q, double rho_const,
+                         int quad_order, const uint8_t *ess, fg_tet **out);
+FG_API void fg_tet_destroy(fg_tet *op);
+FG_API int64_t fg_tet_ndofs(const fg_tet *op);
+/* quadrature points per element of the operator's rule */
+FG_API int fg_tet_nq(const fg_tet *op);
+/* physical quadrature points xyz[E][nq][3] = x_0 + J xi_q */
+FG_API int fg_tet_quadrature_points(fg_tet *op, double *xyz, int mem);
+/* MatFreeOperator::apply (accumulate = 1) / apply_zero (0); constrained = 1:
+ * identity rows and columns on the essential DOFs. */
+FG_API int fg_tet_apply(fg_tet *op, const double *x, double *y, int accumulate, int constrained, int mem);
+/* Jacobi diagonal (1 on essential DOFs when constrained). */
+FG_API int fg_tet_diagonal(fg_tet *op, double *d, int constrained, int mem);
+
 /* Synchronise the handle's stream and report device-side errors
  * (FG_DEVICE_TIMEOUT, FG_BOUNDS). */
 FG_API int fg_op_check(fg_op *op);
