@@ -2896,7 +2896,7 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
     {
         std::vector<int64_t> pos(offs.begin(), offs.end() - 1);
         for (int64_t e = 0; e < n_elem; ++e)  // (e, i) ascending within each DOF
-            for (int i = 0; i < nl; ++i) slots[pos[h[e * nl + i]]++] = (int32_t)((int64_t)i * n_elem + e);
+            for (int i = 0; i < nl; ++i) slots[pos[h[e * nl + i]]++] = (int32_t)(e * nl + i);
     }
     if ((rc = tet_upload(&t->dofs, soa.data(), soa.size())) || (rc = tet_upload(&t->offs, offs.data(), offs.size())) ||
         (rc = tet_upload(&t->slots, slots.data(), slots.size())) ||
@@ -2909,6 +2909,8 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
     if (t->nq > TET_MAXQ) return fail(FG_UNSUPPORTED, "quadrature order %d too high", quad_order);
     std::vector<double> phi((size_t)t->nq * nl), grad((size_t)t->nq * nl * 3);
     for (int q = 0; q < t->nq; ++q) tet_basis_host(order, &pts[3 * q], &phi[(size_t)q * nl], &grad[(size_t)q * nl * 3]);
+    t->h_phi = phi;
+    t->h_grad = grad;
     double *d_w = nullptr;
     if ((rc = tet_upload(&t->qp, pts.data(), pts.size())) || (rc = tet_upload(&t->phi, phi.data(), phi.size())) ||
         (rc = tet_upload(&t->grad, grad.data(), grad.size())) || (rc = tet_upload(&d_w, w.data(), w.size())))

@@ -15,7 +15,8 @@ struct fg_tet {
     int64_t E = 0, N = 0, n_nodes = 0;
     int32_t *dofs = nullptr;  // [nl][E]
     double *G = nullptr, *sk = nullptr, *sm = nullptr, *Ye = nullptr, *coords = nullptr;
-    double *qp = nullptr, *phi = nullptr, *grad = nullptr;  // rule tables
+    double *qp = nullptr, *phi = nullptr, *grad = nullptr;  // rule tables (device)
+    std::vector<double> h_phi, h_grad;                       // rule tables (host, kernel parameters)
     int nq = 0;
     int64_t *offs = nullptr;
     int32_t *slots = nullptr;
@@ -158,11 +159,28 @@ template <typename T> static int tet_upload(T **dst, const T *src, size_t n) {
     return FG_OK;
 }
 
+template <int NL, int MQ>
+static void tet_launch_t(fg_tet *t, const TetArgs &A, int eb, const double *x, int constrained, int diag) {
+    TetTab<NL, MQ> R{};
+    for (int q = 0; q < t->nq; ++q)
+        for (int i = 0; i < NL; ++i) {
+            R.phi[q][i] = t->h_phi[(size_t)q * NL + i];
+            for (int c = 0; c < 3; ++c) R.grad[q][i][c] = t->h_grad[((size_t)q * NL + i) * 3 + c];
+        }
+    tet_apply_kernel<NL, MQ><<<eb, 128, 0, t->stream>>>(A, R, x, t->Ye, constrained, diag);
+}
+
 static int tet_launch_apply(fg_tet *t, const double *x, double *y, int accumulate, int constrained, int diag) {
     const TetArgs A = tet_args(t);
     const int eb = (int)std::min<int64_t>((t->E + 127) / 128, 148 * 16);
-    if (t->p == 1) tet_apply_kernel<4><<<eb, 128, 0, t->stream>>>(A, x, t->Ye, constrained, diag);
-    else tet_apply_kernel<10><<<eb, 128, 0, t->stream>>>(A, x, t->Ye, constrained, diag);
+    const bool small = t->nq <= 4;
+    if (t->p == 1) {
+        if (small) tet_launch_t<4, 4>(t, A, eb, x, constrained, diag);
+        else tet_launch_t<4, TET_MAXQ>(t, A, eb, x, constrained, diag);
+    } else {
+        if (small) tet_launch_t<10, 4>(t, A, eb, x, constrained, diag);
+        else tet_launch_t<10, TET_MAXQ>(t, A, eb, x, constrained, diag);
+    }
     const int db = (int)std::min<int64_t>((t->N + 255) / 256, 148 * 16);
     tet_scatter_kernel<<<db, 256, 0, t->stream>>>(A, t->offs, t->slots, t->Ye, diag ? nullptr : x, y, accumulate,
                                                   constrained);

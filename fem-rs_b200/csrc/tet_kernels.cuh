@@ -8,20 +8,21 @@
 //                 per element (affine map)
 //   sk   [nq][E]  w_q kappa_q c_k          (diffusion)
 //   sm   [nq][E]  w_q |det J| rho_q c_m    (mass)
-//   Ye   [nl][E]  element-local results (scratch)
+//   Ye   [E][nl]  element-local results (scratch; element-major so that the
+//                 slots of one DOF, which come from nearby elements, share sectors)
 // Per quadrature point the reference computes grad_phys = J^-T grad_ref and
 // y_i += w |det J| kappa (grad u . grad phi_i); with the affine map this is
 // y_i += (w kappa) grad_ref phi_i . G grad_ref u, which the apply evaluates.
 //
 // Scatter without float atomics: the transpose of the element-to-DOF map is a
-// CSR list per DOF of element-local slots (i*E + e) in increasing (e, i); one
+// CSR list per DOF of element-local slots (e*nl + i) in increasing (e, i); one
 // thread per DOF sums its slots in that order (deterministic).
 #pragma once
 #include "fg_common.cuh"
 
 namespace fg {
 
-constexpr int TET_MAXQ = 40;
+constexpr int TET_MAXQ = 35;  // Grundmann-Moller s = 3
 
 struct TetRule {
     int nq;
@@ -80,16 +81,27 @@ __global__ void tet_setup_kernel(TetArgs A, int nl, const double *__restrict__ c
     }
 }
 
-// Ye = A_e x_e (diag = 0) or the diagonal of A_e (diag = 1), one thread per element
-template <int NL>
-__global__ void __launch_bounds__(128) tet_apply_kernel(TetArgs A, const double *__restrict__ x,
-                                                        double *__restrict__ Ye, int constrained, int diag) {
+// Rule tables passed by value as a kernel parameter (constant bank): every
+// thread of a warp reads the same entry at the same time, so the reads are
+// broadcasts.  MQ = capacity in points (4 for tet_rule orders <= 2, 35 above).
+template <int NL, int MQ> struct TetTab {
+    double phi[MQ][NL];
+    double grad[MQ][NL][3];
+};
+
+// Ye[e][i] = (A_e x_e)_i (diag = 0) or (A_e)_ii (diag = 1), one thread per element
+template <int NL, int MQ>
+__global__ void __launch_bounds__(128) tet_apply_kernel(TetArgs A, const __grid_constant__ TetTab<NL, MQ> R,
+                                                        const double *__restrict__ x, double *__restrict__ Ye,
+                                                        int constrained, int diag) {
     const int64_t E = A.E;
+    const int nq = A.R.nq;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
         double xe[NL], ye[NL];
 #pragma unroll
         for (int i = 0; i < NL; ++i) {
             ye[i] = 0.0;
+            xe[i] = 0.0;
             if (!diag) {
                 const int32_t d = __ldg(A.dofs + (int64_t)i * E + e);
                 xe[i] = (constrained && A.ess && A.ess[d]) ? 0.0 : __ldg(x + d);
@@ -99,9 +111,7 @@ __global__ void __launch_bounds__(128) tet_apply_kernel(TetArgs A, const double 
         if (A.kind & 2)
 #pragma unroll
             for (int k = 0; k < 6; ++k) g[k] = __ldg(A.G + (int64_t)k * E + e);
-        for (int q = 0; q < A.R.nq; ++q) {
-            const double *gr = A.R.grad + (int64_t)q * NL * 3;
-            const double *ph = A.R.phi + (int64_t)q * NL;
+        for (int q = 0; q < nq; ++q) {
             if (A.kind & 2) {
                 const double s = __ldg(A.sk + (int64_t)q * E + e);
                 if (!diag) {
@@ -109,17 +119,17 @@ __global__ void __launch_bounds__(128) tet_apply_kernel(TetArgs A, const double 
 #pragma unroll
                     for (int j = 0; j < NL; ++j)
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) gu[c] += xe[j] * __ldg(gr + 3 * j + c);
+                        for (int c = 0; c < 3; ++c) gu[c] += xe[j] * R.grad[q][j][c];
                     const double v0 = s * (g[0] * gu[0] + g[1] * gu[1] + g[2] * gu[2]);
                     const double v1 = s * (g[1] * gu[0] + g[3] * gu[1] + g[4] * gu[2]);
                     const double v2 = s * (g[2] * gu[0] + g[4] * gu[1] + g[5] * gu[2]);
 #pragma unroll
                     for (int i = 0; i < NL; ++i)
-                        ye[i] += __ldg(gr + 3 * i) * v0 + __ldg(gr + 3 * i + 1) * v1 + __ldg(gr + 3 * i + 2) * v2;
+                        ye[i] += R.grad[q][i][0] * v0 + R.grad[q][i][1] * v1 + R.grad[q][i][2] * v2;
                 } else {
 #pragma unroll
                     for (int i = 0; i < NL; ++i) {
-                        const double a = __ldg(gr + 3 * i), b = __ldg(gr + 3 * i + 1), c = __ldg(gr + 3 * i + 2);
+                        const double a = R.grad[q][i][0], b = R.grad[q][i][1], c = R.grad[q][i][2];
                         ye[i] += s * (g[0] * a * a + g[3] * b * b + g[5] * c * c +
                                       2.0 * (g[1] * a * b + g[2] * a * c + g[4] * b * c));
                     }
@@ -130,21 +140,19 @@ __global__ void __launch_bounds__(128) tet_apply_kernel(TetArgs A, const double 
                 if (!diag) {
                     double u = 0.0;
 #pragma unroll
-                    for (int j = 0; j < NL; ++j) u += __ldg(ph + j) * xe[j];
+                    for (int j = 0; j < NL; ++j) u += R.phi[q][j] * xe[j];
                     const double t = m * u;
 #pragma unroll
-                    for (int i = 0; i < NL; ++i) ye[i] += __ldg(ph + i) * t;
+                    for (int i = 0; i < NL; ++i) ye[i] += R.phi[q][i] * t;
                 } else {
 #pragma unroll
-                    for (int i = 0; i < NL; ++i) {
-                        const double f = __ldg(ph + i);
-                        ye[i] += m * f * f;
-                    }
+                    for (int i = 0; i < NL; ++i) ye[i] += m * R.phi[q][i] * R.phi[q][i];
                 }
             }
         }
+        double *dst = Ye + e * NL;
 #pragma unroll
-        for (int i = 0; i < NL; ++i) Ye[(int64_t)i * E + e] = ye[i];
+        for (int i = 0; i < NL; ++i) dst[i] = ye[i];
     }
 }
 
