@@ -146,7 +146,16 @@ static int ensure_encode() {
 template <int P> struct KCfg;
 template <> struct KCfg<1> { static constexpr int WY = 4, S = 4, MINB = 3; };
 template <> struct KCfg<2> { static constexpr int WY = 4, S = 3, MINB = 2; };
-template <> struct KCfg<3> { static constexpr int WY = 2, S = 2, MINB = 1; };
+#ifndef FG_Q3_WY  // Q3 FP64 tile knobs (compile-time): row warps, qdata ring depth, CTAs/SM hint
+#define FG_Q3_WY 2
+#endif
+#ifndef FG_Q3_S
+#define FG_Q3_S 2
+#endif
+#ifndef FG_Q3_MINB
+#define FG_Q3_MINB 1
+#endif
+template <> struct KCfg<3> { static constexpr int WY = FG_Q3_WY, S = FG_Q3_S, MINB = FG_Q3_MINB; };
 
 static int cfg_wy(int p) { return p == 1 ? KCfg<1>::WY : p == 2 ? KCfg<2>::WY : KCfg<3>::WY; }
 
@@ -245,7 +254,7 @@ template <typename T> static int alloc_vec(T **p, int64_t n) {
 template <int P> struct KCfg32;  // FP32 apply: same tile (WY) as FP64, deeper rings
 template <> struct KCfg32<1> { static constexpr int WY = 4, S = 6, MINB = 4; };
 template <> struct KCfg32<2> { static constexpr int WY = 4, S = 4, MINB = 3; };
-template <> struct KCfg32<3> { static constexpr int WY = 2, S = 3, MINB = 2; };
+template <> struct KCfg32<3> { static constexpr int WY = FG_Q3_WY, S = 3, MINB = 2; };
 template <int P, typename T> struct KC;
 template <int P> struct KC<P, double> : KCfg<P> {};
 template <int P> struct KC<P, float> : KCfg32<P> {};

@@ -282,72 +282,221 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
         const T *xt = reinterpret_cast<const T *>(reinterpret_cast<const unsigned char *>(xs) +
                                                   xb * SM::XB);
 
-        // ---- gather (E) with essential-DOF masking -------------------------
-        T u[D][D][D];
-#pragma unroll
-        for (int c = 0; c < D; ++c)
-#pragma unroll
-            for (int b = 0; b < D; ++b)
-#pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    const T v = xt[(c * RY + warp * P + b) * XW + lane * P + a];
-                    const bool e = (a == 0 && fx0) || (a == P && fx1) || (b == 0 && fy0) ||
-                                   (b == P && fy1) || (c == 0 && fz0) || (c == P && fz1);
-                    u[c][b][a] = e ? T(0) : v;
-                }
-        // ---- B: contractions in x then y ----------------------------------
-        T C0[D][Q][Q], C1[D][Q][Q], C2[D][Q][Q];  // [c][qy][qx]
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-            T A0[D][Q], A1[D][Q];
-#pragma unroll
-            for (int b = 0; b < D; ++b)
-#pragma unroll
-                for (int qx = 0; qx < Q; ++qx) {
-                    T s0 = 0, s1 = 0;
-#pragma unroll
+        T out[D][D][D];
+        if constexpr (P != 3 || FMT == 1) {
+            // ---- gather (E) with essential-DOF masking -------------------------
+            T u[D][D][D];
+    #pragma unroll
+            for (int c = 0; c < D; ++c)
+    #pragma unroll
+                for (int b = 0; b < D; ++b)
+    #pragma unroll
                     for (int a = 0; a < D; ++a) {
-                        s0 += TB::B(P, qx, a) * u[c][b][a];
-                        if (HK) s1 += TB::G(P, qx, a) * u[c][b][a];
+                        const T v = xt[(c * RY + warp * P + b) * XW + lane * P + a];
+                        const bool e = (a == 0 && fx0) || (a == P && fx1) || (b == 0 && fy0) ||
+                                       (b == P && fy1) || (c == 0 && fz0) || (c == P && fz1);
+                        u[c][b][a] = e ? T(0) : v;
                     }
-                    A0[b][qx] = s0;
-                    A1[b][qx] = s1;
-                }
-#pragma unroll
+            // ---- B: contractions in x then y ----------------------------------
+            T C0[D][Q][Q], C1[D][Q][Q], C2[D][Q][Q];  // [c][qy][qx]
+    #pragma unroll
+            for (int c = 0; c < D; ++c) {
+                T A0[D][Q], A1[D][Q];
+    #pragma unroll
+                for (int b = 0; b < D; ++b)
+    #pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+                        T s0 = 0, s1 = 0;
+    #pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            s0 += TB::B(P, qx, a) * u[c][b][a];
+                            if (HK) s1 += TB::G(P, qx, a) * u[c][b][a];
+                        }
+                        A0[b][qx] = s0;
+                        A1[b][qx] = s1;
+                    }
+    #pragma unroll
+                for (int qy = 0; qy < Q; ++qy)
+    #pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+                        T s0 = 0, s1 = 0, s2 = 0;
+    #pragma unroll
+                        for (int b = 0; b < D; ++b) {
+                            s0 += TB::B(P, qy, b) * A0[b][qx];
+                            if (HK) {
+                                s1 += TB::G(P, qy, b) * A0[b][qx];
+                                s2 += TB::B(P, qy, b) * A1[b][qx];
+                            }
+                        }
+                        C0[c][qy][qx] = s0;
+                        C1[c][qy][qx] = s1;
+                        C2[c][qy][qx] = s2;
+                    }
+            }
+            // ---- per quadrature column: B in z, D, B^T in z (in place) --------
+            T Ge[6] = {0, 0, 0, 0, 0, 0};
+            const T *ql = nullptr;  // layer stage (FMT 1)
+            if (FMT == 1) {
+                const int j = lz;
+                const int s = j % S;
+                if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+                q_waited = j + 1;
+                ql = qsw + s * STAGE;
+    #pragma unroll
+                for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
+            }
+    #pragma unroll
             for (int qy = 0; qy < Q; ++qy)
-#pragma unroll
+    #pragma unroll
                 for (int qx = 0; qx < Q; ++qx) {
-                    T s0 = 0, s1 = 0, s2 = 0;
-#pragma unroll
-                    for (int b = 0; b < D; ++b) {
-                        s0 += TB::B(P, qy, b) * A0[b][qx];
-                        if (HK) {
-                            s1 += TB::G(P, qy, b) * A0[b][qx];
-                            s2 += TB::B(P, qy, b) * A1[b][qx];
+                    const int col = qy * Q + qx;
+                    const int j = lz * COLS + col;
+                    const int s = j % S;
+                    if (FMT == 0) {
+                        if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+                        q_waited = j + 1;
+                    }
+                    const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
+                    T vx[Q], vy[Q], vz[Q], vu[Q];
+    #pragma unroll
+                    for (int qz = 0; qz < Q; ++qz) {
+                        T gx = 0, gy = 0, gz = 0, ui = 0;
+    #pragma unroll
+                        for (int c = 0; c < D; ++c) {
+                            if (HK) {
+                                gx += TB::B(P, qz, c) * C2[c][qy][qx];
+                                gy += TB::B(P, qz, c) * C1[c][qy][qx];
+                                gz += TB::G(P, qz, c) * C0[c][qy][qx];
+                            }
+                            if (HM) ui += TB::B(P, qz, c) * C0[c][qy][qx];
+                        }
+                        if (FMT == 0) {
+                            const T *qq = qc + qz * (NC * 32) + lane;
+                            if (HK) {
+                                const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128],
+                                        d5 = qq[160];
+                                vx[qz] = d0 * gx + d1 * gy + d2 * gz;
+                                vy[qz] = d1 * gx + d3 * gy + d4 * gz;
+                                vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                            }
+                            if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
+                        } else {
+                            const T *qq = qc + (NCE + (col * Q + qz) * NCQ) * 32 + lane;
+                            if (HK) {
+                                const T sk = qq[0];
+                                const T hx = sk * gx, hy = sk * gy, hz = sk * gz;
+                                vx[qz] = Ge[0] * hx + Ge[1] * hy + Ge[2] * hz;
+                                vy[qz] = Ge[1] * hx + Ge[3] * hy + Ge[4] * hz;
+                                vz[qz] = Ge[2] * hx + Ge[4] * hy + Ge[5] * hz;
+                            }
+                            if (HM) vu[qz] = qq[(HK ? 1 : 0) * 32] * ui;
                         }
                     }
-                    C0[c][qy][qx] = s0;
-                    C1[c][qy][qx] = s1;
-                    C2[c][qy][qx] = s2;
+    #pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        T e0 = 0, e1 = 0, e2 = 0;
+    #pragma unroll
+                        for (int qz = 0; qz < Q; ++qz) {
+                            if (HK) {
+                                e2 += TB::B(P, qz, c) * vx[qz];
+                                e1 += TB::B(P, qz, c) * vy[qz];
+                                e0 += TB::G(P, qz, c) * vz[qz];
+                            }
+                            if (HM) e0 += TB::B(P, qz, c) * vu[qz];
+                        }
+                        C0[c][qy][qx] = e0;
+                        C1[c][qy][qx] = e1;
+                        C2[c][qy][qx] = e2;
+                    }
+                    if (FMT == 0) {
+                        __syncwarp();
+                        if (lane == 0 && ok && j + S < total_cols) {
+                            fence_proxy_async();
+                            mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                            bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                            q_issued = j + S + 1;
+                        }
+                    }
                 }
-        }
-        // ---- per quadrature column: B in z, D, B^T in z (in place) --------
-        T Ge[6] = {0, 0, 0, 0, 0, 0};
-        const T *ql = nullptr;  // layer stage (FMT 1)
-        if (FMT == 1) {
-            const int j = lz;
-            const int s = j % S;
-            if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-            q_waited = j + 1;
-            ql = qsw + s * STAGE;
+            if (FMT == 1) {
+                const int j = lz, s = j % S;
+                __syncwarp();
+                if (lane == 0 && ok && j + S < total_cols) {
+                    fence_proxy_async();
+                    mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                    bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                    q_issued = j + S + 1;
+                }
+            }
+            // ---- B^T: contractions in y then x --------------------------------
+    #pragma unroll
+            for (int c = 0; c < D; ++c) {
+                T F0[D][Q], F1[D][Q];
+    #pragma unroll
+                for (int b = 0; b < D; ++b)
+    #pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+                        T s0 = 0, s1 = 0;
+    #pragma unroll
+                        for (int qy = 0; qy < Q; ++qy) {
+                            if (HK) {
+                                s0 += TB::G(P, qy, b) * C1[c][qy][qx];
+                                s1 += TB::B(P, qy, b) * C2[c][qy][qx];
+                            }
+                            s0 += TB::B(P, qy, b) * C0[c][qy][qx];
+                        }
+                        F0[b][qx] = s0;
+                        F1[b][qx] = s1;
+                    }
+    #pragma unroll
+                for (int b = 0; b < D; ++b)
+    #pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        T s = 0;
+    #pragma unroll
+                        for (int qx = 0; qx < Q; ++qx) {
+                            s += TB::B(P, qx, a) * F0[b][qx];
+                            if (HK) s += TB::G(P, qx, a) * F1[b][qx];
+                        }
+                        out[c][b][a] = s;
+                    }
+            }
+        } else {
+            // Q3 (full qdata): column streaming.  Holding the element's 64 values and the
+            // 3 x 64 gradient intermediates at once exceeds the register file
+            // at Q3 in FP64, so each quadrature column (qy, qx) recomputes its
+            // x/y contractions from the element values in the shared-memory x
+            // tile, runs z, D and z^T for its Q points, and adds its transposed
+            // x/y contribution to out[] at once.  The column order and the data
+            // read per column are those of the stream above.
 #pragma unroll
-            for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
-        }
+            for (int c = 0; c < D; ++c)
 #pragma unroll
-        for (int qy = 0; qy < Q; ++qy)
+                for (int b = 0; b < D; ++b)
 #pragma unroll
-            for (int qx = 0; qx < Q; ++qx) {
-                const int col = qy * Q + qx;
+                    for (int a = 0; a < D; ++a) out[c][b][a] = T(0);
+            // (a per-element branch around the mask measured 24 % slower than the
+            // predicated form: it splits the unrolled column code in two)
+            const T *xe = xt + (warp * P) * XW + lane * P;
+            auto uval = [&](int c, int b, int a) -> T {
+                const T v = xe[(c * RY + b) * XW + a];
+                const bool e = (a == 0 && fx0) || (a == P && fx1) || (b == 0 && fy0) || (b == P && fy1) ||
+                               (c == 0 && fz0) || (c == P && fz1);
+                return e ? T(0) : v;
+            };
+            T Ge[6] = {0, 0, 0, 0, 0, 0};
+            const T *ql = nullptr;
+            if (FMT == 1) {
+                const int j = lz, s = j % S;
+                if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+                q_waited = j + 1;
+                ql = qsw + s * STAGE;
+#pragma unroll
+                for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
+            }
+#pragma unroll 1
+            for (int col = 0; col < COLS; ++col) {
+                const int qy = col / Q, qx = col % Q;
                 const int j = lz * COLS + col;
                 const int s = j % S;
                 if (FMT == 0) {
@@ -355,57 +504,95 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     q_waited = j + 1;
                 }
                 const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
-                T vx[Q], vy[Q], vz[Q], vu[Q];
+                T bx[D], gxa[D], by[D], gyb[D];
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    bx[k] = TB::B(P, qx, k);
+                    gxa[k] = TB::G(P, qx, k);
+                    by[k] = TB::B(P, qy, k);
+                    gyb[k] = TB::G(P, qy, k);
+                }
+                // forward x/y contractions of this column, per z layer c
+                T c0[D], c1[D], c2[D];
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+                    for (int b = 0; b < D; ++b) {
+                        T rb = 0, rg = 0;
+#pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            const T u = uval(c, b, a);
+                            rb += bx[a] * u;
+                            if (HK) rg += gxa[a] * u;
+                        }
+                        t0 += by[b] * rb;
+                        if (HK) {
+                            t1 += gyb[b] * rb;
+                            t2 += by[b] * rg;
+                        }
+                    }
+                    c0[c] = t0;
+                    c1[c] = t1;
+                    c2[c] = t2;
+                }
+                // z, D, z^T at the Q points of the column
+                T e0[D], e1[D], e2[D];
+#pragma unroll
+                for (int c = 0; c < D; ++c) e0[c] = e1[c] = e2[c] = 0;
 #pragma unroll
                 for (int qz = 0; qz < Q; ++qz) {
                     T gx = 0, gy = 0, gz = 0, ui = 0;
 #pragma unroll
                     for (int c = 0; c < D; ++c) {
                         if (HK) {
-                            gx += TB::B(P, qz, c) * C2[c][qy][qx];
-                            gy += TB::B(P, qz, c) * C1[c][qy][qx];
-                            gz += TB::G(P, qz, c) * C0[c][qy][qx];
+                            gx += TB::B(P, qz, c) * c2[c];
+                            gy += TB::B(P, qz, c) * c1[c];
+                            gz += TB::G(P, qz, c) * c0[c];
                         }
-                        if (HM) ui += TB::B(P, qz, c) * C0[c][qy][qx];
+                        if (HM) ui += TB::B(P, qz, c) * c0[c];
                     }
+                    T vx = 0, vy = 0, vz = 0, vu = 0;
                     if (FMT == 0) {
                         const T *qq = qc + qz * (NC * 32) + lane;
                         if (HK) {
-                            const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128],
-                                    d5 = qq[160];
-                            vx[qz] = d0 * gx + d1 * gy + d2 * gz;
-                            vy[qz] = d1 * gx + d3 * gy + d4 * gz;
-                            vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                            const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
+                            vx = d0 * gx + d1 * gy + d2 * gz;
+                            vy = d1 * gx + d3 * gy + d4 * gz;
+                            vz = d2 * gx + d4 * gy + d5 * gz;
                         }
-                        if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
+                        if (HM) vu = qq[(HK ? 6 : 0) * 32] * ui;
                     } else {
                         const T *qq = qc + (NCE + (col * Q + qz) * NCQ) * 32 + lane;
                         if (HK) {
                             const T sk = qq[0];
                             const T hx = sk * gx, hy = sk * gy, hz = sk * gz;
-                            vx[qz] = Ge[0] * hx + Ge[1] * hy + Ge[2] * hz;
-                            vy[qz] = Ge[1] * hx + Ge[3] * hy + Ge[4] * hz;
-                            vz[qz] = Ge[2] * hx + Ge[4] * hy + Ge[5] * hz;
+                            vx = Ge[0] * hx + Ge[1] * hy + Ge[2] * hz;
+                            vy = Ge[1] * hx + Ge[3] * hy + Ge[4] * hz;
+                            vz = Ge[2] * hx + Ge[4] * hy + Ge[5] * hz;
                         }
-                        if (HM) vu[qz] = qq[(HK ? 1 : 0) * 32] * ui;
+                        if (HM) vu = qq[(HK ? 1 : 0) * 32] * ui;
                     }
-                }
 #pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    T e0 = 0, e1 = 0, e2 = 0;
-#pragma unroll
-                    for (int qz = 0; qz < Q; ++qz) {
+                    for (int c = 0; c < D; ++c) {
                         if (HK) {
-                            e2 += TB::B(P, qz, c) * vx[qz];
-                            e1 += TB::B(P, qz, c) * vy[qz];
-                            e0 += TB::G(P, qz, c) * vz[qz];
+                            e2[c] += TB::B(P, qz, c) * vx;
+                            e1[c] += TB::B(P, qz, c) * vy;
+                            e0[c] += TB::G(P, qz, c) * vz;
                         }
-                        if (HM) e0 += TB::B(P, qz, c) * vu[qz];
+                        if (HM) e0[c] += TB::B(P, qz, c) * vu;
                     }
-                    C0[c][qy][qx] = e0;
-                    C1[c][qy][qx] = e1;
-                    C2[c][qy][qx] = e2;
                 }
+                // transposed y/x of this column into the element result
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+#pragma unroll
+                    for (int b = 0; b < D; ++b) {
+                        const T f0 = gyb[b] * e1[c] + by[b] * e0[c];
+                        const T f1 = by[b] * e2[c];
+#pragma unroll
+                        for (int a = 0; a < D; ++a) out[c][b][a] += bx[a] * f0 + gxa[a] * f1;
+                    }
                 if (FMT == 0) {
                     __syncwarp();
                     if (lane == 0 && ok && j + S < total_cols) {
@@ -416,49 +603,16 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     }
                 }
             }
-        if (FMT == 1) {
-            const int j = lz, s = j % S;
-            __syncwarp();
-            if (lane == 0 && ok && j + S < total_cols) {
-                fence_proxy_async();
-                mbar_arrive_expect_tx(&qbw[s], QBYTES);
-                bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
-                q_issued = j + S + 1;
+            if (FMT == 1) {
+                const int j = lz, s = j % S;
+                __syncwarp();
+                if (lane == 0 && ok && j + S < total_cols) {
+                    fence_proxy_async();
+                    mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                    bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                    q_issued = j + S + 1;
+                }
             }
-        }
-        // ---- B^T: contractions in y then x --------------------------------
-        T out[D][D][D];
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-            T F0[D][Q], F1[D][Q];
-#pragma unroll
-            for (int b = 0; b < D; ++b)
-#pragma unroll
-                for (int qx = 0; qx < Q; ++qx) {
-                    T s0 = 0, s1 = 0;
-#pragma unroll
-                    for (int qy = 0; qy < Q; ++qy) {
-                        if (HK) {
-                            s0 += TB::G(P, qy, b) * C1[c][qy][qx];
-                            s1 += TB::B(P, qy, b) * C2[c][qy][qx];
-                        }
-                        s0 += TB::B(P, qy, b) * C0[c][qy][qx];
-                    }
-                    F0[b][qx] = s0;
-                    F1[b][qx] = s1;
-                }
-#pragma unroll
-            for (int b = 0; b < D; ++b)
-#pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    T s = 0;
-#pragma unroll
-                    for (int qx = 0; qx < Q; ++qx) {
-                        s += TB::B(P, qx, a) * F0[b][qx];
-                        if (HK) s += TB::G(P, qx, a) * F1[b][qx];
-                    }
-                    out[c][b][a] = s;
-                }
         }
         // ---- E^T: merge + store --------------------------------------------
         merge_and_store<P, T, WY>(
