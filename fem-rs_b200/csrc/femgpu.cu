@@ -123,6 +123,18 @@ static int ensure_tables(int dev) {
     CK(cudaMemcpyToSymbol(c_G64, G, sizeof G));
     CK(cudaMemcpyToSymbol(c_B32, Bf, sizeof Bf));
     CK(cudaMemcpyToSymbol(c_G32, Gf, sizeof Gf));
+    float2 GB[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {}, BG[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {},
+           BB[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {};
+    for (int p = 0; p < FG_MAXP; ++p)
+        for (int q = 0; q <= FG_MAXP; ++q)
+            for (int d = 0; d <= FG_MAXP; ++d) {
+                GB[p][q][d] = make_float2(Gf[p][q][d], Bf[p][q][d]);
+                BG[p][q][d] = make_float2(Bf[p][q][d], Gf[p][q][d]);
+                BB[p][q][d] = make_float2(Bf[p][q][d], Bf[p][q][d]);
+            }
+    CK(cudaMemcpyToSymbol(c_GB32, GB, sizeof GB));
+    CK(cudaMemcpyToSymbol(c_BG32, BG, sizeof BG));
+    CK(cudaMemcpyToSymbol(c_BB32, BB, sizeof BB));
     g_tables_ready[dev] = true;
     return FG_OK;
 }

@@ -32,6 +32,10 @@ __constant__ double c_B64[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 __constant__ double c_G64[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 __constant__ float c_B32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 __constant__ float c_G32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
+// pairs for packed FP32 FMA (__ffma2_rn): (G, B), (B, G) and (B, B) per (p, q, d)
+__constant__ float2 c_GB32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
+__constant__ float2 c_BG32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
+__constant__ float2 c_BB32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 
 template <typename T> struct Tab;
 template <> struct Tab<double> {

@@ -31,6 +31,7 @@
 // of each layer is a 3-D TMA tensor load (cp.async.bulk.tensor, no multicast)
 // into a double buffer.
 #pragma once
+#include <type_traits>
 #include "fg_common.cuh"
 
 namespace fg {
@@ -283,7 +284,170 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                                                   xb * SM::XB);
 
         T out[D][D][D];
-        if constexpr (P != 3 || FMT == 1) {
+        if constexpr (std::is_same<T, float>::value && P == 2 && HK) {
+            // FP32 Q2 diffusion (+ mass): the contractions as packed pairs, two
+            // FP32 FMAs per instruction (__ffma2_rn).  Pairing: x gives
+            // (A1, A0) = (Gx, Bx)(u, u); y gives (C2, C1) = (By, Gy)(A1, A0) and
+            // C0 = By A0; z gives (gx, gy) = (Bz, Bz)(C2, C1), gz = Gz C0; the
+            // transposed passes pair the same way.  Per element 486 paired and
+            // 567 single FMAs instead of 1539 single ones.
+            float u[D][D][D];
+#pragma unroll
+            for (int c = 0; c < D; ++c)
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        const float v = xt[(c * RY + warp * P + b) * XW + lane * P + a];
+                        const bool e = (a == 0 && fx0) || (a == P && fx1) || (b == 0 && fy0) ||
+                                       (b == P && fy1) || (c == 0 && fz0) || (c == P && fz1);
+                        u[c][b][a] = e ? 0.f : v;
+                    }
+            float2 C21[D][Q][Q];  // (C2, C1) [c][qy][qx]
+            float C0[D][Q][Q];
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                float2 X[D][Q];  // (A1, A0) [b][qx]
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+                        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int a = 0; a < D; ++a)
+                            acc = __ffma2_rn(c_GB32[P - 1][qx][a], make_float2(u[c][b][a], u[c][b][a]), acc);
+                        X[b][qx] = acc;
+                    }
+#pragma unroll
+                for (int qy = 0; qy < Q; ++qy)
+#pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+                        float2 acc = make_float2(0.f, 0.f);
+                        float c0 = 0.f;
+#pragma unroll
+                        for (int b = 0; b < D; ++b) {
+                            acc = __ffma2_rn(c_BG32[P - 1][qy][b], X[b][qx], acc);
+                            c0 += TB::B(P, qy, b) * X[b][qx].y;
+                        }
+                        C21[c][qy][qx] = acc;
+                        C0[c][qy][qx] = c0;
+                    }
+            }
+            T Ge[6] = {0, 0, 0, 0, 0, 0};
+            const T *ql = nullptr;
+            if (FMT == 1) {
+                const int j = lz;
+                const int s = j % S;
+                if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+                q_waited = j + 1;
+                ql = qsw + s * STAGE;
+#pragma unroll
+                for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
+            }
+#pragma unroll
+            for (int qy = 0; qy < Q; ++qy)
+#pragma unroll
+                for (int qx = 0; qx < Q; ++qx) {
+                    const int col = qy * Q + qx;
+                    const int j = lz * COLS + col;
+                    const int s = j % S;
+                    if (FMT == 0) {
+                        if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+                        q_waited = j + 1;
+                    }
+                    const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
+                    float2 vxy[Q];
+                    float vz[Q], vu[Q];
+#pragma unroll
+                    for (int qz = 0; qz < Q; ++qz) {
+                        float2 g21 = make_float2(0.f, 0.f);
+                        float gz = 0.f, ui = 0.f;
+#pragma unroll
+                        for (int c = 0; c < D; ++c) {
+                            g21 = __ffma2_rn(c_BB32[P - 1][qz][c], C21[c][qy][qx], g21);
+                            gz += TB::G(P, qz, c) * C0[c][qy][qx];
+                            if (HM) ui += TB::B(P, qz, c) * C0[c][qy][qx];
+                        }
+                        const float gx = g21.x, gy = g21.y;
+                        float vx, vy;
+                        if (FMT == 0) {
+                            const T *qq = qc + qz * (NC * 32) + lane;
+                            const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
+                            vx = d0 * gx + d1 * gy + d2 * gz;
+                            vy = d1 * gx + d3 * gy + d4 * gz;
+                            vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                            vu[qz] = HM ? qq[6 * 32] * ui : 0.f;
+                        } else {
+                            const T *qq = qc + (NCE + (col * Q + qz) * NCQ) * 32 + lane;
+                            const T sk = qq[0];
+                            const T hx = sk * gx, hy = sk * gy, hz = sk * gz;
+                            vx = Ge[0] * hx + Ge[1] * hy + Ge[2] * hz;
+                            vy = Ge[1] * hx + Ge[3] * hy + Ge[4] * hz;
+                            vz[qz] = Ge[2] * hx + Ge[4] * hy + Ge[5] * hz;
+                            vu[qz] = HM ? qq[32] * ui : 0.f;
+                        }
+                        vxy[qz] = make_float2(vx, vy);
+                    }
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        float2 e21 = make_float2(0.f, 0.f);
+                        float e0 = 0.f;
+#pragma unroll
+                        for (int qz = 0; qz < Q; ++qz) {
+                            e21 = __ffma2_rn(c_BB32[P - 1][qz][c], vxy[qz], e21);
+                            e0 += TB::G(P, qz, c) * vz[qz];
+                            if (HM) e0 += TB::B(P, qz, c) * vu[qz];
+                        }
+                        C21[c][qy][qx] = e21;
+                        C0[c][qy][qx] = e0;
+                    }
+                    if (FMT == 0) {
+                        __syncwarp();
+                        if (lane == 0 && ok && j + S < total_cols) {
+                            fence_proxy_async();
+                            mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                            bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                            q_issued = j + S + 1;
+                        }
+                    }
+                }
+            if (FMT == 1) {
+                const int j = lz, s = j % S;
+                __syncwarp();
+                if (lane == 0 && ok && j + S < total_cols) {
+                    fence_proxy_async();
+                    mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                    bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                    q_issued = j + S + 1;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                float2 F[D][Q];  // (F1, F0) [b][qx]
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+                        float2 acc = make_float2(0.f, 0.f);
+                        float f0 = 0.f;
+#pragma unroll
+                        for (int qy = 0; qy < Q; ++qy) {
+                            acc = __ffma2_rn(c_BG32[P - 1][qy][b], C21[c][qy][qx], acc);
+                            f0 += TB::B(P, qy, b) * C0[c][qy][qx];
+                        }
+                        F[b][qx] = make_float2(acc.x, acc.y + f0);
+                    }
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int qx = 0; qx < Q; ++qx) acc = __ffma2_rn(c_GB32[P - 1][qx][a], F[b][qx], acc);
+                        out[c][b][a] = acc.x + acc.y;
+                    }
+            }
+        } else if constexpr (P != 3 || FMT == 1) {
             // ---- gather (E) with essential-DOF masking -------------------------
             T u[D][D][D];
     #pragma unroll
