@@ -158,6 +158,22 @@ def cpu_apply_sample(n, p, kq_full, reps=2, layers=None):
     return mesh.ndofs / dt / 1e9, cores, desc
 
 
+def cpu_ex1_pipeline(n=24):
+    """The mfem_ex1 pipeline through the oracle port on the host cores: source
+    form, PCG-Jacobi to rtol 1e-10, L2 error (24^3 Q1 Poisson)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    t0 = time.perf_counter()
+    mesh = O.Mesh(n, n, n, 1)
+    mask = O.ess_mask(mesh)
+    b = O.source(mesh, mask)
+    x, info = O.pcg(mesh, O.Coef(O.DIFF), mask, b, precond=1, rtol=1e-10, max_iter=2000)
+    err = O.l2_error_sin(mesh, x, nq=3)
+    return {"pipeline_s": time.perf_counter() - t0, "iterations": info["iterations"], "l2_error": err,
+            "threads": os.cpu_count()}
+
+
 def run_reference(args, n, p):
     world, rank, _ = dist_setup()
     if rank != 0:
@@ -209,6 +225,7 @@ def main():
     ap.add_argument("--no-heat", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-tet", action="store_true")
+    ap.add_argument("--no-ex1", action="store_true")
     ap.add_argument("--batch-n", type=int, default=256)
     ap.add_argument("--heat-steps", type=int, default=500)
     args = ap.parse_args()
@@ -537,11 +554,34 @@ def main():
             top.close()
             del xt, yt
 
+    # the mfem_ex1 pipeline on the 24^3 Q1 Poisson case (kappa = 1, f = 3 pi^2 sin sin sin,
+    # homogeneous Dirichlet, PCG-Jacobi, rtol 1e-10): source form, solve and L2 error on the GPU
+    ex1 = None
+    if not args.no_ex1:
+        n1 = 24
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        op1 = femgpu.PADiffusionOperator((n1, n1, n1), 1)
+        qp2 = femgpu.quadrature_points(n1, n1, n1, 2)
+        b1 = femgpu.assemble_source(n1, n1, n1, 1, 3 * np.pi ** 2 * np.prod(np.sin(np.pi * qp2), axis=-1))
+        x1 = np.zeros(op1.n_dofs())
+        r1 = femgpu.solve_pcg_jacobi(op1, b1, x1, femgpu.SolverConfig(rtol=1e-10, max_iter=2000))
+        qp3 = femgpu.quadrature_points(n1, n1, n1, 3)
+        err1 = femgpu.l2_error(n1, n1, n1, 1, x1, np.prod(np.sin(np.pi * qp3), axis=-1), nq=3)
+        t_ex1 = time.perf_counter() - t0
+        ex1 = {"workload": "mfem_ex1: 24^3 Q1 Poisson, PCG-Jacobi rtol 1e-10 (15,625 DOFs)",
+               "iterations": r1.iterations, "solve_ms": r1.solve_ms, "l2_error": err1,
+               "pipeline_s": t_ex1, "converged": r1.converged,
+               "timing": "host wall clock: operator setup, source form, solve, L2 error"}
+        op1.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             v, cores, desc = cpu_apply_sample(n, p, kq)
             cpu = {"value": v, "unit": "GDOF/s", "cores": cores, "kind": "port", "sample": desc}
+            if ex1 is not None:
+                cpu["ex1_pipeline"] = cpu_ex1_pipeline()
         except Exception as exc:  # keep the bench line even if the oracle is unavailable
             cpu = {"value": None, "unit": "GDOF/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"unavailable: {exc}"}
@@ -571,6 +611,7 @@ def main():
             "heat": heat,
             "batch": batch,
             "tet": tet,
+            "ex1": ex1,
         }
         print(json.dumps(out), flush=True)
     op.close()

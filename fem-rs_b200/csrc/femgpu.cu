@@ -2879,18 +2879,18 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
                          const uint8_t *ess, fg_tet **out) {
     if (!out) return fail(FG_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
-    if (order != 1 && order != 2) return fail(FG_UNSUPPORTED, "tet order %d not supported (1, 2)", order);
+    if (order < 1 || order > 3) return fail(FG_UNSUPPORTED, "tet order %d not supported (1..3)", order);
     if (kind < 1 || kind > 3) return fail(FG_INVALID_ARGUMENT, "bad operator kind %d", kind);
     if (!coords || !elem_dofs || n_nodes < 4 || n_elem < 1 || n_dofs < n_nodes || n_dofs >= ((int64_t)1 << 31))
         return fail(FG_INVALID_ARGUMENT, "bad tet mesh arguments");
-    if (n_elem * (order == 1 ? 4 : 10) >= ((int64_t)1 << 31))
+    if (n_elem * (order == 1 ? 4 : (order == 2 ? 10 : 20)) >= ((int64_t)1 << 31))
         return fail(FG_UNSUPPORTED, "too many elements for 32-bit element-local slots");
     int rc;
     fg_tet *t = new fg_tet();
     struct Bail { fg_tet *t; bool armed = true; ~Bail() { if (armed) tet_free(t); } } bail{t};
     CK(cudaGetDevice(&t->device));
     t->p = order;
-    t->nl = order == 1 ? 4 : 10;
+    t->nl = order == 1 ? 4 : (order == 2 ? 10 : 20);
     t->kind = kind;
     t->E = n_elem;
     t->N = n_dofs;

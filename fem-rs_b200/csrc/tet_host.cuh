@@ -106,10 +106,50 @@ static int tet_rule_host(int order, std::vector<double> &pts, std::vector<double
     return (int)w.size();
 }
 
-// TetP1 / TetP2 basis values and reference gradients (crates/element/src/lagrange/tet.rs)
+// TetP1 / TetP2 / TetP3 basis values and reference gradients (crates/element/src/lagrange/tet.rs)
 static void tet_basis_host(int p, const double *xi, double *phi, double *grad) {
     const double x = xi[0], y = xi[1], z = xi[2];
     const double l1 = 1.0 - x - y - z, l2 = x, l3 = y, l4 = z;
+    if (p == 3) {
+        // each function is c * f0 f1 f2 with linear factors f = alpha * lambda_i + beta:
+        // vertices 1/2 l(3l-1)(3l-2); edge DOFs 9/2 li lj (3li-1) (near i) / (3lj-1) (near j),
+        // edges (01, 02, 03, 12, 13, 23); faces 27 li lj lk, faces (012, 013, 023, 123)
+        const double L[4] = {l1, l2, l3, l4};
+        const double dL[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        struct F { int i; double a, b; };
+        F fac[20][3];
+        double cc[20];
+        for (int v = 0; v < 4; ++v) {
+            cc[v] = 0.5;
+            fac[v][0] = {v, 1, 0};
+            fac[v][1] = {v, 3, -1};
+            fac[v][2] = {v, 3, -2};
+        }
+        const int ed[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+        for (int k = 0; k < 6; ++k)
+            for (int h = 0; h < 2; ++h) {
+                const int d = 4 + 2 * k + h;
+                cc[d] = 4.5;
+                fac[d][0] = {ed[k][0], 1, 0};
+                fac[d][1] = {ed[k][1], 1, 0};
+                fac[d][2] = {h ? ed[k][1] : ed[k][0], 3, -1};
+            }
+        const int fc[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+        for (int k = 0; k < 4; ++k) {
+            cc[16 + k] = 27.0;
+            for (int m = 0; m < 3; ++m) fac[16 + k][m] = {fc[k][m], 1, 0};
+        }
+        for (int d = 0; d < 20; ++d) {
+            double f[3];
+            for (int m = 0; m < 3; ++m) f[m] = fac[d][m].a * L[fac[d][m].i] + fac[d][m].b;
+            phi[d] = cc[d] * f[0] * f[1] * f[2];
+            for (int c = 0; c < 3; ++c)
+                grad[3 * d + c] = cc[d] * (fac[d][0].a * dL[fac[d][0].i][c] * f[1] * f[2] +
+                                           f[0] * fac[d][1].a * dL[fac[d][1].i][c] * f[2] +
+                                           f[0] * f[1] * fac[d][2].a * dL[fac[d][2].i][c]);
+        }
+        return;
+    }
     if (p == 1) {
         const double f[4] = {l1, l2, l3, l4};
         const double g[12] = {-1, -1, -1, 1, 0, 0, 0, 1, 0, 0, 0, 1};
@@ -177,9 +217,12 @@ static int tet_launch_apply(fg_tet *t, const double *x, double *y, int accumulat
     if (t->p == 1) {
         if (small) tet_launch_t<4, 4>(t, A, eb, x, constrained, diag);
         else tet_launch_t<4, TET_MAXQ>(t, A, eb, x, constrained, diag);
-    } else {
+    } else if (t->p == 2) {
         if (small) tet_launch_t<10, 4>(t, A, eb, x, constrained, diag);
         else tet_launch_t<10, TET_MAXQ>(t, A, eb, x, constrained, diag);
+    } else {
+        if (small) tet_launch_t<20, 4>(t, A, eb, x, constrained, diag);
+        else tet_launch_t<20, TET_MAXQ>(t, A, eb, x, constrained, diag);
     }
     const int db = (int)std::min<int64_t>((t->N + 255) / 256, 148 * 16);
     tet_scatter_kernel<<<db, 256, 0, t->stream>>>(A, t->offs, t->slots, t->Ye, diag ? nullptr : x, y, accumulate,

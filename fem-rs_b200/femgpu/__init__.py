@@ -650,10 +650,10 @@ def collect_residuals(op, b, every, max_res, cfg=None):
 
 
 class TetOperator:
-    """PA mass / diffusion operator on an unstructured Tet4 mesh with TetP1 or
-    TetP2 (fg_tet_*): the MatFreeOperator surface of partial.rs (apply =
+    """PA mass / diffusion operator on an unstructured Tet4 mesh with TetP1, TetP2
+    or TetP3 (fg_tet_*): the MatFreeOperator surface of partial.rs (apply =
     y += A x, apply_zero = y = A x, n_dofs) plus the Jacobi diagonal.
-    coords [n_nodes, 3]; elem_dofs [E, 4|10] (first 4 = vertex nodes);
+    coords [n_nodes, 3]; elem_dofs [E, 4|10|20] (first 4 = vertex nodes);
     kappa / rho: constants or [E, nq] tables at quadrature_points()."""
 
     def __init__(self, p, coords, elem_dofs, n_dofs, kind=DIFF, kappa=1.0, rho=1.0, c_mass=1.0, c_diff=1.0,

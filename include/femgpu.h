@@ -356,7 +356,7 @@ FG_API int fg_lumped_mass(const fg_mesh *mesh, int order, const double *rho_q, d
 FG_API int fg_lumped_apply(const double *diag, const double *x, double *y, int64_t n, int mode, int mem);
 
 /* ---- tetrahedral PA operator -------------------------------------------------
- * PAMassOperator / PADiffusionOperator on Tet4 meshes with TetP1 / TetP2
+ * PAMassOperator / PADiffusionOperator on Tet4 meshes with TetP1 / TetP2 / TetP3
  * (crates/assembly/src/partial.rs:85-130, 154-208 with ref_elem :277-288,
  * simplex_jac :290-299, xform_grads :301-309; bases
  * crates/element/src/lagrange/tet.rs; rule tet_rule(quad_order),
@@ -364,7 +364,8 @@ FG_API int fg_lumped_apply(const double *diag, const double *x, double *y, int64
  * [E][4 or 10] as DofManager numbers them (first 4 = vertex nodes,
  * crates/space/src/dof_manager.rs:137-180, 628-700); kappa_q / rho_q
  * [E][nq] at the rule's points (fg_tet_quadrature_points) or NULL for the
- * constants; ess: essential-DOF mask [n_dofs] (boundary_dofs) or NULL.  All
+ * constants; ess: essential-DOF mask [n_dofs] (boundary_dofs) or NULL.  TetP3
+ * element maps: [E][20] as build_p3_tet (dof_manager.rs:484-600).  All
  * arrays in host or device memory.  The scatter is the transpose of the
  * element map summed in a fixed order (no float atomics). */
 typedef struct fg_tet fg_tet;

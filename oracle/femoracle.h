@@ -157,7 +157,7 @@ double or_ref_spectral_radius_csr(int64_t n, const int64_t *rowptr, const int64_
  * tet_rule(order) of quadrature.rs:259-376: returns the point count (points
  * [n][3] on the reference tet, weights summing to 1/6), -1 if cap is short. */
 int or_tet_rule(int order, double *pts, double *w, int cap);
-/* TetP1 / TetP2 basis values and reference gradients ([n][3]); returns n. */
+/* TetP1 / TetP2 / TetP3 basis values and reference gradients ([n][3]); returns n. */
 int or_tet_basis(int p, const double xi[3], double *phi, double *grad);
 /* partial.rs:85-130 / 154-208 on Tet4 elements: y (+)= A x.  coords
  * [n_nodes][3]; elem_dofs [E][4 or 10], first 4 entries = vertex nodes;

@@ -9,7 +9,7 @@
  *   J^-T by cofactors, grad_phys = J^-T grad_ref (xform_grads, :301-309);
  *   y_elem[i] += w |det J| kappa (grad u . grad phi_i)  /  w |det J| rho phi_i u;
  *   scatter y[gd[i]] += y_elem[i].
- * Bases: TetP1 / TetP2 (crates/element/src/lagrange/tet.rs:17-172, barycentric
+ * Bases: TetP1 / TetP2 / TetP3 (crates/element/src/lagrange/tet.rs:17-236, barycentric
  * formulas); quadrature: tet_rule (crates/element/src/quadrature.rs:259-376),
  * including the Grundmann-Moller construction with per-level weights solved
  * from the x^{2k} moments exactly as that function does.
@@ -150,11 +150,51 @@ int or_tet_basis(int p, const double xi[3], double *phi, double *grad) {
         memcpy(grad, g, sizeof g);
         return 10;
     }
+    if (p == 3) {
+        /* TetP3 (tet.rs:172-236): every basis function is c * prod of factors
+         * (alpha * lambda_i + beta); vertices 1/2 l(3l-1)(3l-2), edge DOFs near
+         * the first / second vertex 9/2 li lj (3li-1) / (3lj-1), faces 27 li lj lk;
+         * gradients by the product rule with grad l1 = (-1,-1,-1), l2..l4 = e_x, e_y, e_z */
+        const double L[4] = {l1, l2, l3, l4};
+        const double dL[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        int fi[20][3];
+        double fa[20][3], fb[20][3], cc[20];
+        for (int v = 0; v < 4; ++v) {
+            cc[v] = 0.5;
+            fi[v][0] = fi[v][1] = fi[v][2] = v;
+            fa[v][0] = 1; fb[v][0] = 0; fa[v][1] = 3; fb[v][1] = -1; fa[v][2] = 3; fb[v][2] = -2;
+        }
+        const int ed[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+        for (int k = 0; k < 6; ++k)
+            for (int h = 0; h < 2; ++h) {
+                const int d = 4 + 2 * k + h, i = ed[k][0], j = ed[k][1];
+                cc[d] = 4.5;
+                fi[d][0] = i; fa[d][0] = 1; fb[d][0] = 0;
+                fi[d][1] = j; fa[d][1] = 1; fb[d][1] = 0;
+                fi[d][2] = h ? j : i; fa[d][2] = 3; fb[d][2] = -1;
+            }
+        const int fc[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+        for (int k = 0; k < 4; ++k) {
+            const int d = 16 + k;
+            cc[d] = 27.0;
+            for (int m = 0; m < 3; ++m) { fi[d][m] = fc[k][m]; fa[d][m] = 1; fb[d][m] = 0; }
+        }
+        for (int d = 0; d < 20; ++d) {
+            double f[3];
+            for (int m = 0; m < 3; ++m) f[m] = fa[d][m] * L[fi[d][m]] + fb[d][m];
+            phi[d] = cc[d] * f[0] * f[1] * f[2];
+            for (int c = 0; c < 3; ++c)
+                grad[3 * d + c] = cc[d] * (fa[d][0] * dL[fi[d][0]][c] * f[1] * f[2] +
+                                           f[0] * fa[d][1] * dL[fi[d][1]][c] * f[2] +
+                                           f[0] * f[1] * fa[d][2] * dL[fi[d][2]][c]);
+        }
+        return 20;
+    }
     return -1;
 }
 
 /* ---- element loop ------------------------------------------------------ */
-#define TMAXL 10
+#define TMAXL 20
 #define TMAXQ 64
 
 static void tet_jac(const double *coords, const int32_t *nd, double J[3][3], double *det) {
@@ -190,7 +230,7 @@ static int tet_element(int p, int kind, double c_m, double c_k, const double *co
     tet_jac(coords, gd, J, &det);
     if (!(fabs(det) > 0.0)) return -1;
     inv_T(J, det, jit);
-    const int n = p == 1 ? 4 : 10;
+    const int n = p == 1 ? 4 : (p == 2 ? 10 : 20);
     for (int i = 0; i < n; ++i) ye[i] = 0.0;
     for (int q = 0; q < nq; ++q) {
         double phi[TMAXL], gr[3 * TMAXL], gp[3 * TMAXL];
@@ -226,11 +266,11 @@ int or_tet_pa_apply(int p, int64_t n_dofs, const double *coords, int64_t n_elem,
                     int kind, double c_m, double c_k, const double *kappa_q, double kappa_c,
                     const double *rho_q, double rho_c, int quad_order, const uint8_t *ess,
                     const double *x, double *y, int accumulate) {
-    if (p != 1 && p != 2) return -1;
+    if (p < 1 || p > 3) return -1;
     double qp[3 * TMAXQ], qw[TMAXQ];
     const int nq = or_tet_rule(quad_order, qp, qw, TMAXQ);
     if (nq <= 0) return -1;
-    const int n = p == 1 ? 4 : 10;
+    const int n = p == 1 ? 4 : (p == 2 ? 10 : 20);
     if (!accumulate) memset(y, 0, sizeof(double) * n_dofs);
     for (int64_t e = 0; e < n_elem; ++e) {
         const int32_t *gd = elem_dofs + e * n;
@@ -250,11 +290,11 @@ int or_tet_pa_apply(int p, int64_t n_dofs, const double *coords, int64_t n_elem,
 int or_tet_diagonal(int p, int64_t n_dofs, const double *coords, int64_t n_elem, const int32_t *elem_dofs,
                     int kind, double c_m, double c_k, const double *kappa_q, double kappa_c,
                     const double *rho_q, double rho_c, int quad_order, const uint8_t *ess, double *d) {
-    if (p != 1 && p != 2) return -1;
+    if (p < 1 || p > 3) return -1;
     double qp[3 * TMAXQ], qw[TMAXQ];
     const int nq = or_tet_rule(quad_order, qp, qw, TMAXQ);
     if (nq <= 0) return -1;
-    const int n = p == 1 ? 4 : 10;
+    const int n = p == 1 ? 4 : (p == 2 ? 10 : 20);
     memset(d, 0, sizeof(double) * n_dofs);
     for (int64_t e = 0; e < n_elem; ++e) {
         const int32_t *gd = elem_dofs + e * n;
@@ -280,11 +320,11 @@ static double tet_usin(const double *x) { return sin(M_PI * x[0]) * sin(M_PI * x
 
 int or_tet_source(int p, int64_t n_dofs, const double *coords, int64_t n_elem, const int32_t *elem_dofs,
                   int quad_order, const uint8_t *ess, double *b) {
-    if (p != 1 && p != 2) return -1;
+    if (p < 1 || p > 3) return -1;
     double qp[3 * TMAXQ], qw[TMAXQ];
     const int nq = or_tet_rule(quad_order, qp, qw, TMAXQ);
     if (nq <= 0) return -1;
-    const int n = p == 1 ? 4 : 10;
+    const int n = p == 1 ? 4 : (p == 2 ? 10 : 20);
     memset(b, 0, sizeof(double) * n_dofs);
     for (int64_t e = 0; e < n_elem; ++e) {
         const int32_t *gd = elem_dofs + e * n;
@@ -308,11 +348,11 @@ int or_tet_source(int p, int64_t n_dofs, const double *coords, int64_t n_elem, c
 
 double or_tet_l2_error_sin(int p, const double *coords, int64_t n_elem, const int32_t *elem_dofs, int quad_order,
                            const double *u) {
-    if (p != 1 && p != 2) return -1.0;
+    if (p < 1 || p > 3) return -1.0;
     double qp[3 * TMAXQ], qw[TMAXQ];
     const int nq = or_tet_rule(quad_order, qp, qw, TMAXQ);
     if (nq <= 0) return -1.0;
-    const int n = p == 1 ? 4 : 10;
+    const int n = p == 1 ? 4 : (p == 2 ? 10 : 20);
     double err2 = 0.0;
     for (int64_t e = 0; e < n_elem; ++e) {
         const int32_t *gd = elem_dofs + e * n;

@@ -281,7 +281,7 @@ def tet_rule(order):
 
 
 def tet_basis(p, xi):
-    nl = 4 if p == 1 else 10
+    nl = {1: 4, 2: 10, 3: 20}[p]
     phi = np.zeros(nl)
     g = np.zeros((nl, 3))
     lib().or_tet_basis(int(p), _p(np.ascontiguousarray(xi, dtype=np.float64)), _p(phi), _p(g))

@@ -1,6 +1,6 @@
 """Tetrahedral PA operator on the GPU (fg_tet_*) against the tetrahedral
 oracle, the restatement of partial.rs's element loop on Tet4 with TetP1 /
-TetP2: apply and diagonal <= 1e-12 relative (2-norm) on unit_cube_tet meshes
+TetP2 / TetP3: apply and diagonal <= 1e-12 relative (2-norm) on unit_cube_tet meshes
 with perturbed interior nodes and per-point lognormal coefficients, all
 operator kinds, accumulate / overwrite, constrained / raw, host and device
 vectors; bit-for-bit repeatable; the 3-D Poisson known answers of
@@ -38,11 +38,11 @@ def space(n, p, perturb=0.25, seed=0):
     return coords, dofs, nd, mask
 
 
-@pytest.mark.parametrize("p", [1, 2])
+@pytest.mark.parametrize("p", [1, 2, 3])
 @pytest.mark.parametrize("kind", [femgpu.MASS, femgpu.DIFF, femgpu.MASS_DIFF])
 def test_tet_apply_matches_oracle(p, kind):
     need_gpu()
-    coords, dofs, nd, mask = space(5, p, seed=p + kind)
+    coords, dofs, nd, mask = space(5 if p < 3 else 3, p, seed=p + kind)
     qo = 2 * p + (1 if kind & 1 else 0)
     nq = len(O.tet_rule(qo)[1])
     rng = np.random.default_rng(kind)
@@ -111,6 +111,7 @@ def test_tet_poisson_known_answers_with_gpu_apply():
     e4, e8 = _gpu_poisson_l2(4, 1), _gpu_poisson_l2(8, 1)
     assert e4 < 1e-1 and math.log2(e4 / e8) > 1.8
     assert _gpu_poisson_l2(4, 2) < 1e-2
+    assert _gpu_poisson_l2(4, 3) < 5e-3
 
 
 def test_tet_rejects_bad_input():
@@ -121,7 +122,7 @@ def test_tet_rejects_bad_input():
     with pytest.raises(femgpu.SolverError):
         femgpu.TetOperator(1, coords, bad, nd)
     with pytest.raises(femgpu.SolverError):
-        femgpu.TetOperator(3, coords, dofs, nd)
+        femgpu.TetOperator(4, coords, dofs, nd)
     op = femgpu.TetOperator(1, coords, dofs, nd)
     with pytest.raises(femgpu.SolverError):
         op.matvec(np.ones(nd), constrained=True)  # no essential mask given

@@ -5,7 +5,8 @@ the DOF points (crates/element/src/lagrange/tet.rs:451-497), the PA
 properties of partial.rs:322-412 (symmetry, K 1 = 0, linearity, 1^T M 1 =
 |Omega|), and the 3-D Poisson known answers of crates/assembly/tests/
 poisson.rs:495-533 on unit_cube_tet (TetP1 L2 < 1e-1 at n = 4, rate > 1.8;
-TetP2 L2 < 1e-2 at n = 4), solved here through the oracle's PA apply.
+TetP2 L2 < 1e-2 and TetP3 L2 < 5e-3 at n = 4), solved here through the
+oracle's PA apply.
 The mesh and the P2 DOF map come from femgpu.tet (simplex.rs:591-679,
 dof_manager.rs:628-700)."""
 import math
@@ -36,11 +37,23 @@ def test_tet_rule_exactness(order, deg):
             assert abs(got - exact) < 1e-13
 
 
-@pytest.mark.parametrize("p", [1, 2])
-def test_tet_basis_pou_grad_kronecker(p):
-    nodes = [[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]]
+def _ref_nodes(p):
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=float)
+    if p == 1:
+        return v
+    ed = [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]
     if p == 2:
-        nodes += [[.5, 0, 0], [0, .5, 0], [0, 0, .5], [.5, .5, 0], [.5, 0, .5], [0, .5, .5]]
+        return np.vstack([v] + [0.5 * (v[a] + v[b]) for a, b in ed])
+    out = [v]
+    for a, b in ed:
+        out += [(2 * v[a] + v[b]) / 3, (v[a] + 2 * v[b]) / 3]
+    out += [v[list(f)].mean(axis=0) for f in ((0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3))]
+    return np.vstack(out)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_tet_basis_pou_grad_kronecker(p):
+    nodes = _ref_nodes(p)
     pts, _ = O.tet_rule(7)
     for xi in pts:
         phi, g = O.tet_basis(p, xi)
@@ -60,7 +73,7 @@ def _space(n, p, perturb=0.0, seed=0):
     return O.TetSpace(p, coords, dofs, nd, mask)
 
 
-@pytest.mark.parametrize("p", [1, 2])
+@pytest.mark.parametrize("p", [1, 2, 3])
 def test_tet_pa_properties(p):
     sp = _space(3, p, perturb=0.2, seed=p)
     nq = sum(1 for _ in range(len(O.tet_rule(2 * p)[1])))
@@ -100,3 +113,31 @@ def test_poisson_tet_known_answers():
     e8 = _solve_poisson(8, 1)
     assert e4 < 1e-1 and math.log2(e4 / e8) > 1.8
     assert _solve_poisson(4, 2) < 1e-2
+    assert _solve_poisson(4, 3) < 5e-3  # tests/poisson.rs:536-541
+
+
+def test_p3_dof_map_matches_build_p3_tet():
+    """p3_dofs against a literal restatement of build_p3_tet's two passes."""
+    c, conn = T.unit_cube_tet(2)
+    d, nd = T.p3_dofs(conn, len(c))
+    nn = len(c)
+    em, fm, nxt, ref = {}, {}, nn, []
+    for e in conn:
+        n0, n1, n2, n3 = (int(v) for v in e)
+        row = [n0, n1, n2, n3]
+        for a, b in ((n0, n1), (n0, n2), (n0, n3), (n1, n2), (n1, n3), (n2, n3)):
+            k = (min(a, b), max(a, b))
+            if k not in em:
+                em[k] = [nxt, nxt + 1]
+                nxt += 2
+            row += em[k] if a == k[0] else em[k][::-1]
+        ref.append(row)
+    for i, e in enumerate(conn):
+        n0, n1, n2, n3 = (int(v) for v in e)
+        for f in ((n0, n1, n2), (n0, n1, n3), (n0, n2, n3), (n1, n2, n3)):
+            k = tuple(sorted(f))
+            if k not in fm:
+                fm[k] = nxt
+                nxt += 1
+            ref[i].append(fm[k])
+    assert np.array_equal(np.array(ref), d) and nxt == nd
