@@ -126,6 +126,10 @@ def test_lumped_mass_matches_oracle(p):
     assert np.array_equal(y, lm.diag * x)
     lm.apply_inverse(x, y)
     assert np.allclose(y, x / lm.diag, rtol=1e-15, atol=0)
+    # zero-length vectors are a no-op (no launch)
+    empty = np.zeros(0)
+    assert femgpu.lib().fg_lumped_apply(lm.diag.ctypes.data, empty.ctypes.data, empty.ctypes.data, 0, 0,
+                                        femgpu.HOST) == 0
 
 
 def test_ex1_known_answers_on_gpu():

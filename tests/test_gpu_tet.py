@@ -70,6 +70,30 @@ def test_tet_apply_matches_oracle(p, kind):
     assert rel(yd.cpu().numpy(), O.tet_pa_apply(sp, coef, x, qo, True)) <= 1e-12
 
 
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_tet_single_cube_and_single_element(p):
+    """Smallest meshes: the 6 tets of one cube, and one tetrahedron alone."""
+    need_gpu()
+    coords, dofs, nd, mask = space(1, p, perturb=0.0)
+    sp = O.TetSpace(p, coords, dofs, nd, mask)
+    op = femgpu.TetOperator(p, coords, dofs, nd, kind=femgpu.MASS_DIFF, quad_order=2 * p, ess=mask)
+    x = np.random.default_rng(p).standard_normal(nd)
+    coef = O.Coef(femgpu.MASS_DIFF)
+    for constrained in (False, True):
+        assert rel(op.matvec(x, constrained), O.tet_pa_apply(sp, coef, x, 2 * p, constrained)) <= 1e-12
+    one = dofs[:1]
+    used = np.unique(one)
+    remap = np.full(nd, -1)
+    remap[used] = np.arange(len(used))
+    c1 = coords[used[used < len(coords)]] if p == 1 else None
+    if p == 1:
+        d1 = remap[one].astype(np.int32)
+        op1 = femgpu.TetOperator(1, c1, d1, 4)
+        sp1 = O.TetSpace(1, c1, d1, 4)
+        x1 = np.arange(1.0, 5.0)
+        assert rel(op1.matvec(x1), O.tet_pa_apply(sp1, O.Coef(O.DIFF), x1, 2)) <= 1e-12
+
+
 def test_tet_quadrature_points():
     need_gpu()
     coords, dofs, nd, mask = space(3, 2, seed=9)
