@@ -133,6 +133,23 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(value, world, device):
+    """Max of a per-rank float over all ranks (timings are reported as the
+    slowest rank's); the identity on one rank."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gdofs(world, n_dofs, steps, t_ms):
+    """Whole-job throughput: every rank applies its own instance `steps` times."""
+    return world * n_dofs * steps / (t_ms / 1e3) / 1e9
+
+
 def cpu_apply_sample(n, p, kq_full, reps=2, layers=None):
     """Oracle (reference-algorithm port) apply on a z-slab of the workload, all
     host threads.  Returns (GDOF/s, threads, description)."""
@@ -280,13 +297,10 @@ def main():
     barrier()
     t_ms = e0.elapsed_time(e1)
     clk = clocks.stop()
-    if world > 1:
-        tt = torch.tensor([t_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = max_over_ranks(t_ms, world, dev)
     op.check()
     per_apply_s = t_ms / 1e3 / args.steps
-    value = world * N * args.steps / (t_ms / 1e3) / 1e9
+    value = whole_job_gdofs(world, N, args.steps, t_ms)
     bytes_canon, bytes_nomap = canonical_bytes(n, p)
     peak, peak_kind = measured_peak()
     achieved = bytes_canon / per_apply_s / 1e9
@@ -308,11 +322,8 @@ def main():
     f1.record(stream)
     torch.cuda.synchronize()
     te_ms = f0.elapsed_time(f1)
-    if world > 1:
-        tt = torch.tensor([te_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te_ms = float(tt.item())
-    e2e_val = world * N * k_e2e / (te_ms / 1e3) / 1e9
+    te_ms = max_over_ranks(te_ms, world, dev)
+    e2e_val = whole_job_gdofs(world, N, k_e2e, te_ms)
     _ = float(yh[0])
 
     solve = None
