@@ -34,6 +34,13 @@
 #include <type_traits>
 #include "fg_common.cuh"
 
+#ifndef FG_Q3_QH  // Q3 FP64 full-format slab width in quadrature columns (Q: a whole qy slab)
+#define FG_Q3_QH 2
+#endif
+#ifndef FG_Q3_NXB  // Q3 FP64 x tile buffers (1: single buffer, 3 CTAs per SM; 2: double, 2 CTAs)
+#define FG_Q3_NXB 1
+#endif
+
 namespace fg {
 
 template <int OPK> struct NComp { static constexpr int v = OPK == 1 ? 1 : (OPK == 2 ? 6 : 7); };
@@ -90,13 +97,16 @@ __host__ __device__ inline int64_t qd_size_fmt(const Grid &g) {
 // in units of 32-lane vectors.
 template <int P, typename T, int WY, int S, int NC> struct ApplySmem {
     static constexpr int D = P + 1, Q = P + 1;
+    // x tile buffers: two (the next layer's tile loads during this layer's
+    // math) except for Q3 in FP64, where one buffer lets 3 CTAs share an SM
+    static constexpr int NXB = (P == 3 && sizeof(T) == 8) ? FG_Q3_NXB : 2;
     static constexpr int XW = round_up(32 * P + 1, 16 / (int)sizeof(T));
     static constexpr int RY = WY * P + 1;
     static constexpr int XTILE = (P + 1) * RY * XW;               // elements
     static constexpr int XB = round_up(XTILE * (int)sizeof(T), 128);
     static constexpr int STAGE = NC * 32;                         // elements
     static constexpr int QB = STAGE * (int)sizeof(T);
-    static constexpr int off_q = 2 * XB;
+    static constexpr int off_q = NXB * XB;
     static constexpr int off_y = off_q + WY * S * QB;
     static constexpr int off_c = off_y + WY * D * D * 32 * (int)sizeof(T);
     static constexpr int off_b = round_up(off_c + D * D * WY * 32 * (int)sizeof(T), 8);
@@ -269,16 +279,19 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
     for (int lz = 0; lz < nl; ++lz) {
         const int ez = tz * g.TZ + lz;
         const bool fz0 = (ess & 1) && ez == 0, fz1 = (ess & 2) && ez == g.nz - 1;
-        const int xb = lz & 1;
-        if (threadIdx.x == 0 && ok && lz + 1 < nl) {
-            // buffer (lz+1)&1 was last read in layer lz-1, before the end-of-layer barrier
+        constexpr int NXB = SM::NXB;
+        const int xb = lz % NXB;
+        if (threadIdx.x == 0 && ok && (NXB == 2 ? lz + 1 < nl : lz > 0)) {
+            // double buffer: buffer (lz+1)&1 was last read in layer lz-1, before the
+            // end-of-layer barrier; single buffer: layer lz loads now, after that barrier
+            const int ln = NXB == 2 ? lz + 1 : lz, bn = ln % NXB;
             fence_proxy_async();
-            mbar_arrive_expect_tx(&xbar[(lz + 1) & 1], XBYTES);
-            tma_load_3d(reinterpret_cast<unsigned char *>(xs) + ((lz + 1) & 1) * SM::XB, &xmap, I0,
-                        J0, K0 + (lz + 1) * P, &xbar[(lz + 1) & 1]);
-            x_issued = lz + 2;
+            mbar_arrive_expect_tx(&xbar[bn], XBYTES);
+            tma_load_3d(reinterpret_cast<unsigned char *>(xs) + bn * SM::XB, &xmap, I0, J0, K0 + ln * P,
+                        &xbar[bn]);
+            x_issued = ln + 1;
         }
-        if (ok && !mbar_wait(&xbar[xb], (lz >> 1) & 1, A.err)) ok = false;
+        if (ok && !mbar_wait(&xbar[xb], (lz / NXB) & 1, A.err)) ok = false;
         x_waited = lz + 1;
         const T *xt = reinterpret_cast<const T *>(reinterpret_cast<const unsigned char *>(xs) +
                                                   xb * SM::XB);
@@ -447,7 +460,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                         out[c][b][a] = acc.x + acc.y;
                     }
             }
-        } else if constexpr (P != 3 || FMT == 1) {
+        } else if constexpr (P != 3 || (FMT == 1 && sizeof(T) == 4)) {
             // ---- gather (E) with essential-DOF masking -------------------------
             T u[D][D][D];
     #pragma unroll
@@ -626,21 +639,25 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     }
             }
         } else {
-            // Q3 (full qdata): column streaming.  Holding the element's 64 values and the
-            // 3 x 64 gradient intermediates at once exceeds the register file
-            // at Q3 in FP64, so each quadrature column (qy, qx) recomputes its
-            // x/y contractions from the element values in the shared-memory x
-            // tile, runs z, D and z^T for its Q points, and adds its transposed
-            // x/y contribution to out[] at once.  The column order and the data
-            // read per column are those of the stream above.
+            // Q3 (FP32 full format, FP64 both formats): slab sum factorisation.
+            // The element's 64 values and its 3 x 64 gradient intermediates do
+            // not fit the register file together in FP64, so the quadrature
+            // points are taken one qy slab (QH of its Q columns) at a time: the y
+            // contraction of the element values (read from the shared-memory x
+            // tile) for this qy, then x, then per column z, D and z^T, then the
+            // transposed x and y of the slab into the element result.  With
+            // QH = Q every contraction is done once (the flop count of the full
+            // sum factorisation, slab state 3 x Q x Q values); QH = Q/2 repeats
+            // the y contractions once per half slab for a smaller state.  The
+            // column order and the data read per column are those of the stream.
 #pragma unroll
             for (int c = 0; c < D; ++c)
 #pragma unroll
                 for (int b = 0; b < D; ++b)
 #pragma unroll
                     for (int a = 0; a < D; ++a) out[c][b][a] = T(0);
-            // (a per-element branch around the mask measured 24 % slower than the
-            // predicated form: it splits the unrolled column code in two)
+            // (a per-element branch around the mask measured slower than the
+            // predicated form: it splits the unrolled code in two)
             const T *xe = xt + (warp * P) * XW + lane * P;
             auto uval = [&](int c, int b, int a) -> T {
                 const T v = xe[(c * RY + b) * XW + a];
@@ -648,6 +665,8 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                                (c == 0 && fz0) || (c == P && fz1);
                 return e ? T(0) : v;
             };
+            constexpr int QH = (sizeof(T) == 8 && FMT == 0) ? FG_Q3_QH : Q;
+            static_assert(Q % QH == 0, "slab width must divide Q");
             T Ge[6] = {0, 0, 0, 0, 0, 0};
             const T *ql = nullptr;
             if (FMT == 1) {
@@ -659,111 +678,149 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                 for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
             }
 #pragma unroll 1
-            for (int col = 0; col < COLS; ++col) {
-                const int qy = col / Q, qx = col % Q;
-                const int j = lz * COLS + col;
-                const int s = j % S;
-                if (FMT == 0) {
-                    if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-                    q_waited = j + 1;
-                }
-                const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
-                T bx[D], gxa[D], by[D], gyb[D];
+            for (int qy = 0; qy < Q; ++qy) {
+                T by[D], gyb[D];
 #pragma unroll
                 for (int k = 0; k < D; ++k) {
-                    bx[k] = TB::B(P, qx, k);
-                    gxa[k] = TB::G(P, qx, k);
                     by[k] = TB::B(P, qy, k);
                     gyb[k] = TB::G(P, qy, k);
                 }
-                // forward x/y contractions of this column, per z layer c
-                T c0[D], c1[D], c2[D];
 #pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    T t0 = 0, t1 = 0, t2 = 0;
+                for (int h0 = 0; h0 < Q; h0 += QH) {
+                    // forward: y (this qy) then x, per z layer c -> slab [c][qx - h0]
+                    T C0[D][QH], C1[D][QH], C2[D][QH];
 #pragma unroll
-                    for (int b = 0; b < D; ++b) {
-                        T rb = 0, rg = 0;
+                    for (int c = 0; c < D; ++c) {
+                        T R[D], Rg[D];
 #pragma unroll
                         for (int a = 0; a < D; ++a) {
-                            const T u = uval(c, b, a);
-                            rb += bx[a] * u;
-                            if (HK) rg += gxa[a] * u;
+                            T s0 = 0, s1 = 0;
+#pragma unroll
+                            for (int b = 0; b < D; ++b) {
+                                const T u = uval(c, b, a);
+                                s0 += by[b] * u;
+                                if (HK) s1 += gyb[b] * u;
+                            }
+                            R[a] = s0;
+                            Rg[a] = s1;
                         }
-                        t0 += by[b] * rb;
-                        if (HK) {
-                            t1 += gyb[b] * rb;
-                            t2 += by[b] * rg;
+#pragma unroll
+                        for (int k = 0; k < QH; ++k) {
+                            const int qx = h0 + k;
+                            T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+                            for (int a = 0; a < D; ++a) {
+                                t0 += TB::B(P, qx, a) * R[a];
+                                if (HK) {
+                                    t1 += TB::B(P, qx, a) * Rg[a];
+                                    t2 += TB::G(P, qx, a) * R[a];
+                                }
+                            }
+                            C0[c][k] = t0;
+                            C1[c][k] = t1;
+                            C2[c][k] = t2;
                         }
                     }
-                    c0[c] = t0;
-                    c1[c] = t1;
-                    c2[c] = t2;
-                }
-                // z, D, z^T at the Q points of the column
-                T e0[D], e1[D], e2[D];
+                    // per column of the slab: z, D, z^T (in place)
 #pragma unroll
-                for (int c = 0; c < D; ++c) e0[c] = e1[c] = e2[c] = 0;
+                    for (int k = 0; k < QH; ++k) {
+                        const int qx = h0 + k;
+                        const int col = qy * Q + qx;
+                        const int j = lz * COLS + col;
+                        const int s = j % S;
+                        if (FMT == 0) {
+                            if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
+                            q_waited = j + 1;
+                        }
+                        const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
+                        T vx[Q], vy[Q], vz[Q], vu[Q];
 #pragma unroll
-                for (int qz = 0; qz < Q; ++qz) {
-                    T gx = 0, gy = 0, gz = 0, ui = 0;
+                        for (int qz = 0; qz < Q; ++qz) {
+                            T gx = 0, gy = 0, gz = 0, ui = 0;
+#pragma unroll
+                            for (int c = 0; c < D; ++c) {
+                                if (HK) {
+                                    gx += TB::B(P, qz, c) * C2[c][k];
+                                    gy += TB::B(P, qz, c) * C1[c][k];
+                                    gz += TB::G(P, qz, c) * C0[c][k];
+                                }
+                                if (HM) ui += TB::B(P, qz, c) * C0[c][k];
+                            }
+                            vx[qz] = vy[qz] = vz[qz] = vu[qz] = T(0);
+                            if (FMT == 0) {
+                                const T *qq = qc + qz * (NC * 32) + lane;
+                                if (HK) {
+                                    const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
+                                    vx[qz] = d0 * gx + d1 * gy + d2 * gz;
+                                    vy[qz] = d1 * gx + d3 * gy + d4 * gz;
+                                    vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                                }
+                                if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
+                            } else {
+                                const T *qq = qc + (NCE + (col * Q + qz) * NCQ) * 32 + lane;
+                                if (HK) {
+                                    const T sk = qq[0];
+                                    const T hx = sk * gx, hy = sk * gy, hz = sk * gz;
+                                    vx[qz] = Ge[0] * hx + Ge[1] * hy + Ge[2] * hz;
+                                    vy[qz] = Ge[1] * hx + Ge[3] * hy + Ge[4] * hz;
+                                    vz[qz] = Ge[2] * hx + Ge[4] * hy + Ge[5] * hz;
+                                }
+                                if (HM) vu[qz] = qq[(HK ? 1 : 0) * 32] * ui;
+                            }
+                        }
+#pragma unroll
+                        for (int c = 0; c < D; ++c) {
+                            T e0 = 0, e1 = 0, e2 = 0;
+#pragma unroll
+                            for (int qz = 0; qz < Q; ++qz) {
+                                if (HK) {
+                                    e2 += TB::B(P, qz, c) * vx[qz];
+                                    e1 += TB::B(P, qz, c) * vy[qz];
+                                    e0 += TB::G(P, qz, c) * vz[qz];
+                                }
+                                if (HM) e0 += TB::B(P, qz, c) * vu[qz];
+                            }
+                            C0[c][k] = e0;
+                            C1[c][k] = e1;
+                            C2[c][k] = e2;
+                        }
+                        if (FMT == 0) {
+                            __syncwarp();
+                            if (lane == 0 && ok && j + S < total_cols) {
+                                fence_proxy_async();
+                                mbar_arrive_expect_tx(&qbw[s], QBYTES);
+                                bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
+                                q_issued = j + S + 1;
+                            }
+                        }
+                    }
+                    // transposed x then y of the slab into the element result
 #pragma unroll
                     for (int c = 0; c < D; ++c) {
-                        if (HK) {
-                            gx += TB::B(P, qz, c) * c2[c];
-                            gy += TB::B(P, qz, c) * c1[c];
-                            gz += TB::G(P, qz, c) * c0[c];
-                        }
-                        if (HM) ui += TB::B(P, qz, c) * c0[c];
-                    }
-                    T vx = 0, vy = 0, vz = 0, vu = 0;
-                    if (FMT == 0) {
-                        const T *qq = qc + qz * (NC * 32) + lane;
-                        if (HK) {
-                            const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
-                            vx = d0 * gx + d1 * gy + d2 * gz;
-                            vy = d1 * gx + d3 * gy + d4 * gz;
-                            vz = d2 * gx + d4 * gy + d5 * gz;
-                        }
-                        if (HM) vu = qq[(HK ? 6 : 0) * 32] * ui;
-                    } else {
-                        const T *qq = qc + (NCE + (col * Q + qz) * NCQ) * 32 + lane;
-                        if (HK) {
-                            const T sk = qq[0];
-                            const T hx = sk * gx, hy = sk * gy, hz = sk * gz;
-                            vx = Ge[0] * hx + Ge[1] * hy + Ge[2] * hz;
-                            vy = Ge[1] * hx + Ge[3] * hy + Ge[4] * hz;
-                            vz = Ge[2] * hx + Ge[4] * hy + Ge[5] * hz;
-                        }
-                        if (HM) vu = qq[(HK ? 1 : 0) * 32] * ui;
-                    }
+                        T H0[D], H1[D];
 #pragma unroll
-                    for (int c = 0; c < D; ++c) {
-                        if (HK) {
-                            e2[c] += TB::B(P, qz, c) * vx;
-                            e1[c] += TB::B(P, qz, c) * vy;
-                            e0[c] += TB::G(P, qz, c) * vz;
+                        for (int a = 0; a < D; ++a) {
+                            T s0 = 0, s1 = 0;
+#pragma unroll
+                            for (int k = 0; k < QH; ++k) {
+                                const int qx = h0 + k;
+                                s0 += TB::B(P, qx, a) * C0[c][k];
+                                if (HK) {
+                                    s0 += TB::G(P, qx, a) * C2[c][k];
+                                    s1 += TB::B(P, qx, a) * C1[c][k];
+                                }
+                            }
+                            H0[a] = s0;
+                            H1[a] = s1;
                         }
-                        if (HM) e0[c] += TB::B(P, qz, c) * vu;
-                    }
-                }
-                // transposed y/x of this column into the element result
 #pragma unroll
-                for (int c = 0; c < D; ++c)
+                        for (int b = 0; b < D; ++b)
 #pragma unroll
-                    for (int b = 0; b < D; ++b) {
-                        const T f0 = gyb[b] * e1[c] + by[b] * e0[c];
-                        const T f1 = by[b] * e2[c];
-#pragma unroll
-                        for (int a = 0; a < D; ++a) out[c][b][a] += bx[a] * f0 + gxa[a] * f1;
-                    }
-                if (FMT == 0) {
-                    __syncwarp();
-                    if (lane == 0 && ok && j + S < total_cols) {
-                        fence_proxy_async();
-                        mbar_arrive_expect_tx(&qbw[s], QBYTES);
-                        bulk_g2s(qsw + s * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[s]);
-                        q_issued = j + S + 1;
+                            for (int a = 0; a < D; ++a) {
+                                T v = out[c][b][a] + by[b] * H0[a];
+                                if (HK) v += gyb[b] * H1[a];
+                                out[c][b][a] = v;
+                            }
                     }
                 }
             }
@@ -792,7 +849,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                 mbar_wait(&qbw[j % S], (j / S) & 1, nullptr, 100000000ull);
         if (threadIdx.x == 0)
             for (int j = x_waited; j < x_issued; ++j)
-                mbar_wait(&xbar[j & 1], (j >> 1) & 1, nullptr, 100000000ull);
+                mbar_wait(&xbar[j % SM::NXB], (j / SM::NXB) & 1, nullptr, 100000000ull);
     }
 }
 
