@@ -162,7 +162,7 @@ template <> struct KCfg<2> { static constexpr int WY = 4, S = 3, MINB = 2; };
 #define FG_Q3_WY 2
 #endif
 #ifndef FG_Q3_S
-#define FG_Q3_S 2
+#define FG_Q3_S 1
 #endif
 #ifndef FG_Q3_MINB
 #define FG_Q3_MINB 1
