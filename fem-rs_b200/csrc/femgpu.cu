@@ -48,6 +48,12 @@ static int fail(int status, const char *fmt, ...) {
             return fail(FG_CUDA_ERROR, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
                         __FILE__, __LINE__);                                               \
     } while (0)
+// cudaMemset, cudaMemcpy from pageable host memory and launches without a
+// stream go to the legacy default stream, which the library's non-blocking
+// streams (and the caller's) do not wait for, and the first two can still be
+// running when the call returns.  Set-up paths call this before any launch on
+// another stream reads what they wrote.
+#define FG_LEGACY_FENCE() CK(cudaStreamSynchronize(cudaStreamLegacy))
 
 #include "unet_host.cuh"
 #include "tet_host.cuh"
@@ -257,6 +263,7 @@ static void free_op(fg_op *op) {
 template <typename T> static int alloc_vec(T **p, int64_t n) {
     CK(cudaMalloc(p, sizeof(T) * std::max<int64_t>(n, 1)));
     CK(cudaMemset(*p, 0, sizeof(T) * std::max<int64_t>(n, 1)));
+    FG_LEGACY_FENCE();
     return FG_OK;
 }
 
@@ -326,16 +333,12 @@ static int launch_apply_p(fg_op *op, const Grid &g, const T *, T *face, const T 
     }
 }
 
-static dim3 fixup_grid(const Grid &g) {
-    const int planes = (g.ntx - 1) + (g.nty - 1) + (g.ntz - 1);
-    const int w = std::max(g.NI, g.NJ), h = std::max(g.NJ, g.NK);
-    return dim3((w + 127) / 128, h, planes);
-}
+static dim3 fixup_grid(const Grid &g) { return dim3(fixup_rows(g)); }
 
 template <typename T>
 static int launch_fixup(fg_op *op, const Grid &g, T *y, const T *face, const int *skip) {
     const dim3 grid = fixup_grid(g);
-    if (grid.z == 0) return FG_OK;
+    if (grid.x == 0) return FG_OK;
     fixup_kernel<T><<<grid, 128, 0, op->stream>>>(g, y, face, skip);
     CK(cudaGetLastError());
     return FG_OK;
@@ -542,6 +545,10 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
             cleanup_in();
             return bail(fail(FG_CUDA_ERROR, "rho upload failed"));
         }
+    }
+    if (cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess) {  // d_err/st memsets, uploads
+        cleanup_in();
+        return bail(fail(FG_CUDA_ERROR, "set-up copies failed"));
     }
     SetupArgs S{};
     S.g = g;
@@ -761,6 +768,7 @@ static int ensure_fp32(fg_op *op) {
     if (!op->st32) {
         CK(cudaMalloc(&op->st32, sizeof(SolverState)));
         CK(cudaMemset(op->st32, 0, sizeof(SolverState)));
+        FG_LEGACY_FENCE();
     }
     return FG_OK;
 }
@@ -1489,6 +1497,7 @@ static int launch_batched(cudaStream_t st, const BatchGroup &G, const ApplyArgs<
 template <typename T> static int dev_upload(T **dst, const std::vector<T> &v) {
     CK(cudaMalloc(dst, sizeof(T) * std::max<size_t>(v.size(), 1)));
     CK(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    FG_LEGACY_FENCE();
     return FG_OK;
 }
 
@@ -1891,6 +1900,7 @@ FG_API int fg_batch_pcg(fg_op *const *ops, int n, const double *const *b, double
         (rc = dev_upload(&d_bv, bv)))
         return rc;
     CK(cudaMemcpy(d_st, hst.data(), sizeof(SolverState) * n, cudaMemcpyHostToDevice));
+    FG_LEGACY_FENCE();
     const dim3 vgrid(VBX, n), fgrid(64, n);
     auto apply32 = [&](int slot) -> int {
         for (auto &G : groups) {
@@ -2228,7 +2238,7 @@ extern "C" FG_API int fg_op_apply_native_noalloc(fg_op *op, const double *x, dou
     }
     if (rc) return rc;
     const dim3 grid = fixup_grid(g);
-    if (grid.z > 0) {
+    if (grid.x > 0) {
         fixup_kernel<double><<<grid, 128, 0, op->stream>>>(g, y, face, nullptr);
         CK(cudaGetLastError());
     }
@@ -2263,6 +2273,7 @@ static int unet_copy_params(fg_unet *u, float *host, bool to_host, bool grads) {
             CK(cudaMemcpy(b, host + (int64_t)L.cout * K, L.cout * sizeof(float), cudaMemcpyHostToDevice));
             f32_to_bf16_kernel<<<64, 256>>>(L.w, L.wb, (int64_t)L.cout * L.kp);
             CK(cudaGetLastError());
+            FG_LEGACY_FENCE();
         }
         host += (int64_t)L.cout * K + L.cout;
     }
@@ -2744,6 +2755,7 @@ static int form_setup(const fg_mesh *mesh, int order, int nq, FormSetup &F) {
         const size_t nb = sizeof(double) * 3 * (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
         CK(cudaMalloc(&F.d_vc, nb));
         CK(cudaMemcpy(F.d_vc, mesh->vcoord, nb, cudaMemcpyDefault));
+        FG_LEGACY_FENCE();
     }
     F.A.vcoord = F.d_vc;
     return FG_OK;
@@ -2766,6 +2778,7 @@ static int dev_in(const double *src, int64_t n, int mem, DevBuf &d) {
     CK(cudaMalloc(&d.p, sizeof(double) * (size_t)std::max<int64_t>(n, 1)));
     d.owned = true;
     CK(cudaMemcpy(d.p, src, sizeof(double) * n, cudaMemcpyHostToDevice));
+    FG_LEGACY_FENCE();
     return FG_OK;
 }
 
@@ -2899,6 +2912,7 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
     CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
     CK(cudaMalloc(&t->d_err, sizeof(int)));
     CK(cudaMemset(t->d_err, 0, sizeof(int)));
+    FG_LEGACY_FENCE();
     // element map: validate, transpose to [nl][E], CSR of element-local slots per DOF
     std::vector<int32_t> h(n_elem * nl);
     CK(cudaMemcpy(h.data(), elem_dofs, sizeof(int32_t) * h.size(), cudaMemcpyDefault));

@@ -951,20 +951,18 @@ __global__ void __launch_bounds__(WY * 32) pa_diag_kernel(const ApplyArgs<T> A) 
 // ---------------------------------------------------------------------------
 // Fix-up: for every DOF on an item's lower face that a neighbour item also
 // touches, add the neighbours' face-slot partials to the owner's value, in a
-// fixed (dz, dy, dx) order.  Grid: x = position along a DOF row, y = the row
-// (K for x/y planes, J for z planes), z = plane (x planes first, then y, then
-// z).  x planes own all their DOFs, y planes skip DOFs on x planes, z planes
-// skip DOFs on x or y planes.  32-bit index arithmetic throughout.
+// fixed (dz, dy, dx) order.  The work is split into rows of DOFs on the shared
+// planes (fixup_rows).  x planes own all their DOFs, y planes skip DOFs on x
+// planes, z planes skip DOFs on x or y planes.  32-bit index arithmetic except
+// the DOF offset.
 // ---------------------------------------------------------------------------
+// The neighbours' face-slot partials of one shared DOF added to `own` in
+// (dz, dy, dx) order.  (tx, ty, tz): the owner item; (sx, sy, sz): whether the
+// DOF lies on an x / y / z plane between items.
 template <typename T>
-__device__ __forceinline__ T fixup_sum(const Grid &g, int I, int J, int K, T own,
-                                       const T *__restrict__ face) {
-    const int P = g.p;
-    const int SXe = 32 * P, SYe = g.WY * P, SZe = g.TZ * P;
-    const int sx = (I > 0 && I < g.NI - 1 && I % SXe == 0);
-    const int sy = (J > 0 && J < g.NJ - 1 && J % SYe == 0);
-    const int sz = (K > 0 && K < g.NK - 1 && K % SZe == 0);
-    const int tx = min(I / SXe, g.ntx - 1), ty = min(J / SYe, g.nty - 1), tz = min(K / SZe, g.ntz - 1);
+__device__ __forceinline__ T fixup_acc(const Grid &g, int I, int J, int K, int tx, int ty, int tz,
+                                       int sx, int sy, int sz, T own, const T *__restrict__ face) {
+    const int SXe = 32 * g.p, SYe = g.WY * g.p, SZe = g.TZ * g.p;
     const int fs = g.face_stride(), fxs = g.fx(), fys = g.fy();
     T sum = own;
     for (int dz = 0; dz <= sz; ++dz)
@@ -985,37 +983,98 @@ __device__ __forceinline__ T fixup_sum(const Grid &g, int I, int J, int K, T own
     return sum;
 }
 
+// The fix-up of any shared DOF (I, J, K), given the owner's value.
+template <typename T>
+__device__ __forceinline__ T fixup_sum(const Grid &g, int I, int J, int K, T own,
+                                       const T *__restrict__ face) {
+    const int P = g.p;
+    const int SXe = 32 * P, SYe = g.WY * P, SZe = g.TZ * P;
+    const int sx = (I > 0 && I < g.NI - 1 && I % SXe == 0);
+    const int sy = (J > 0 && J < g.NJ - 1 && J % SYe == 0);
+    const int sz = (K > 0 && K < g.NK - 1 && K % SZe == 0);
+    const int tx = min(I / SXe, g.ntx - 1), ty = min(J / SYe, g.nty - 1), tz = min(K / SZe, g.ntz - 1);
+    return fixup_acc<T>(g, I, J, K, tx, ty, tz, sx, sy, sz, own, face);
+}
+
+// Rows of shared-face DOFs: the x planes as NK rows of NJ DOFs (u -> J), the
+// y planes as NK rows of NI DOFs (u -> I), the z planes as NJ rows of NI DOFs
+// (u -> I); x planes first, then y, then z.
+__host__ __device__ inline int fixup_rows(const Grid &g) {
+    return (g.ntx - 1) * g.NK + (g.nty - 1) * g.NK + (g.ntz - 1) * g.NJ;
+}
+
+// One row of the fix-up, by the whole block.  Everything fixed along the row
+// (its plane, the owner item across the plane, the essential faces it lies on)
+// is worked out once; per DOF only the position along the row is classified,
+// by a division by the compile-time 32 P.  The sums are those of fixup_sum, in
+// the same order.  y planes skip DOFs on x planes, z planes skip DOFs on x or
+// y planes; essential DOFs keep the owner's value.
+template <typename T, int P>
+__device__ __forceinline__ void fixup_row_t(const Grid &g, int r, T *__restrict__ y,
+                                            const T *__restrict__ face) {
+    constexpr int SXe = 32 * P;
+    const int SYe = g.WY * P, SZe = g.TZ * P;
+    const int rx = (g.ntx - 1) * g.NK, ry = (g.nty - 1) * g.NK;
+    const int ess = g.ess;
+    if (r < rx) {  // x plane I = (pl + 1) SXe; u -> J, row -> K
+        const int pl = r / g.NK, K = r - pl * g.NK, I = (pl + 1) * SXe, tx = pl + 1;
+        if (((ess & 1) && K == 0) || ((ess & 2) && K == g.NK - 1)) return;
+        const int sz = (K > 0 && K < g.NK - 1 && K % SZe == 0), tz = min(K / SZe, g.ntz - 1);
+        T *yr = y + (int64_t)K * g.NJ * g.NIp + I;
+        for (int J = threadIdx.x; J < g.NJ; J += blockDim.x) {
+            if (((ess & 4) && J == 0) || ((ess & 8) && J == g.NJ - 1)) continue;
+            const int sy = (J > 0 && J < g.NJ - 1 && J % SYe == 0), ty = min(J / SYe, g.nty - 1);
+            T *yp = yr + (int64_t)J * g.NIp;
+            *yp = fixup_acc<T>(g, I, J, K, tx, ty, tz, 1, sy, sz, *yp, face);
+        }
+    } else if (r < rx + ry) {  // y plane J = (pl + 1) SYe; u -> I, row -> K
+        r -= rx;
+        const int pl = r / g.NK, K = r - pl * g.NK, J = (pl + 1) * SYe, ty = pl + 1;
+        if (((ess & 1) && K == 0) || ((ess & 2) && K == g.NK - 1)) return;
+        const int sz = (K > 0 && K < g.NK - 1 && K % SZe == 0), tz = min(K / SZe, g.ntz - 1);
+        T *yr = y + ((int64_t)K * g.NJ + J) * g.NIp;
+        for (int I = threadIdx.x; I < g.NI; I += blockDim.x) {
+            const int q = I / SXe;
+            if (I > 0 && I < g.NI - 1 && I == q * SXe) continue;  // on an x plane
+            if (((ess & 16) && I == 0) || ((ess & 32) && I == g.NI - 1)) continue;
+            yr[I] = fixup_acc<T>(g, I, J, K, min(q, g.ntx - 1), ty, tz, 0, 1, sz, yr[I], face);
+        }
+    } else {  // z plane K = (pl + 1) SZe; u -> I, row -> J
+        r -= rx + ry;
+        const int pl = r / g.NJ, J = r - pl * g.NJ, K = (pl + 1) * SZe, tz = pl + 1;
+        if (J > 0 && J < g.NJ - 1 && J % SYe == 0) return;  // on a y plane
+        if (((ess & 4) && J == 0) || ((ess & 8) && J == g.NJ - 1)) return;
+        const int ty = min(J / SYe, g.nty - 1);
+        T *yr = y + ((int64_t)K * g.NJ + J) * g.NIp;
+        for (int I = threadIdx.x; I < g.NI; I += blockDim.x) {
+            const int q = I / SXe;
+            if (I > 0 && I < g.NI - 1 && I == q * SXe) continue;  // on an x plane
+            if (((ess & 16) && I == 0) || ((ess & 32) && I == g.NI - 1)) continue;
+            yr[I] = fixup_acc<T>(g, I, J, K, min(q, g.ntx - 1), ty, tz, 0, 0, 1, yr[I], face);
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void fixup_row(const Grid &g, int r, T *__restrict__ y,
+                                          const T *__restrict__ face) {
+    switch (g.p) {
+    case 1: fixup_row_t<T, 1>(g, r, y, face); break;
+    case 2: fixup_row_t<T, 2>(g, r, y, face); break;
+    default: fixup_row_t<T, 3>(g, r, y, face); break;
+    }
+}
+
+// One block per row of shared-face DOFs (grid = fixup_rows(g)).
 template <typename T>
 __global__ void __launch_bounds__(128) fixup_kernel(const Grid g, T *__restrict__ y,
                                                     const T *__restrict__ face, const int *skip) {
     if (skip && *skip) return;
-    const int P = g.p;
-    const int SXe = 32 * P, SYe = g.WY * P, SZe = g.TZ * P;
-    const int pl = blockIdx.z;
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int row = blockIdx.y;
-    int I, J, K;
-    if (pl < g.ntx - 1) {            // x plane I = (pl+1) SXe: u -> J, row -> K
-        if (u >= g.NJ || row >= g.NK) return;
-        I = (pl + 1) * SXe; J = u; K = row;
-    } else if (pl < g.ntx - 1 + g.nty - 1) {  // y plane: u -> I, row -> K
-        if (u >= g.NI || row >= g.NK) return;
-        I = u; J = (pl - (g.ntx - 1) + 1) * SYe; K = row;
-        if (I > 0 && I < g.NI - 1 && I % SXe == 0) return;
-    } else {                          // z plane: u -> I, row -> J
-        if (u >= g.NI || row >= g.NJ) return;
-        I = u; J = row; K = (pl - (g.ntx - 1) - (g.nty - 1) + 1) * SZe;
-        if (I > 0 && I < g.NI - 1 && I % SXe == 0) return;
-        if (J > 0 && J < g.NJ - 1 && J % SYe == 0) return;
-    }
-    if (g.is_ess(I, J, K)) return;  // final value written by the owner item
-    const int64_t d = g.dof(I, J, K);
-    y[d] = fixup_sum<T>(g, I, J, K, y[d], face);
+    fixup_row<T>(g, blockIdx.x, y, face);
 }
 
 // Batched fix-up: blockIdx.y = instance; blocks stride over the instance's
-// rows of shared-face DOFs (x planes: rows K of J, y planes: rows K of I,
-// z planes: rows J of I), threads over the row.
+// rows of shared-face DOFs.
 template <typename T> struct FixArgs {
     Grid g;
     T *y;
@@ -1027,30 +1086,8 @@ __global__ void __launch_bounds__(128) fixup_batched_kernel(const FixArgs<T> *ar
                                                             int slot) {
     const FixArgs<T> &A = args[blockIdx.y * nslots + slot];
     if (A.skip && *A.skip) return;
-    const Grid &g = A.g;
-    const int SXe = 32 * g.p, SYe = g.WY * g.p, SZe = g.TZ * g.p;
-    const int rx = (g.ntx - 1) * g.NK, ry = (g.nty - 1) * g.NK, rz = (g.ntz - 1) * g.NJ;
-    for (int r = blockIdx.x; r < rx + ry + rz; r += gridDim.x) {
-        int fam, pl, row, len;
-        if (r < rx) { fam = 0; pl = r / g.NK; row = r % g.NK; len = g.NJ; }
-        else if (r < rx + ry) { fam = 1; pl = (r - rx) / g.NK; row = (r - rx) % g.NK; len = g.NI; }
-        else { fam = 2; pl = (r - rx - ry) / g.NJ; row = (r - rx - ry) % g.NJ; len = g.NI; }
-        for (int u = threadIdx.x; u < len; u += blockDim.x) {
-            int I, J, K;
-            if (fam == 0) { I = (pl + 1) * SXe; J = u; K = row; }
-            else if (fam == 1) {
-                I = u; J = (pl + 1) * SYe; K = row;
-                if (I > 0 && I < g.NI - 1 && I % SXe == 0) continue;
-            } else {
-                I = u; J = row; K = (pl + 1) * SZe;
-                if (I > 0 && I < g.NI - 1 && I % SXe == 0) continue;
-                if (J > 0 && J < g.NJ - 1 && J % SYe == 0) continue;
-            }
-            if (g.is_ess(I, J, K)) continue;
-            const int64_t d = g.dof(I, J, K);
-            A.y[d] = fixup_sum<T>(g, I, J, K, A.y[d], A.face);
-        }
-    }
+    const int rows = fixup_rows(A.g);
+    for (int r = blockIdx.x; r < rows; r += gridDim.x) fixup_row<T>(A.g, r, A.y, A.face);
 }
 
 // ---------------------------------------------------------------------------

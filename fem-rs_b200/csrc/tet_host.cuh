@@ -196,6 +196,7 @@ static void tet_free(fg_tet *t) {
 template <typename T> static int tet_upload(T **dst, const T *src, size_t n) {
     CK(cudaMalloc(dst, sizeof(T) * std::max<size_t>(n, 1)));
     if (n) CK(cudaMemcpy(*dst, src, sizeof(T) * n, cudaMemcpyDefault));
+    FG_LEGACY_FENCE();
     return FG_OK;
 }
 

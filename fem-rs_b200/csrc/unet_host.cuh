@@ -94,6 +94,7 @@ static int unet_layer_alloc(ConvLayer &l, int cin, int cout, uint64_t seed) {
     CK(cudaMemcpy(l.w, h.data(), nw * sizeof(float), cudaMemcpyHostToDevice));
     f32_to_bf16_kernel<<<64, 256>>>(l.w, l.wb, (int64_t)nw);
     CK(cudaGetLastError());
+    FG_LEGACY_FENCE();
     return FG_OK;
 }
 
@@ -122,6 +123,7 @@ static int unet_ensure_bufs(fg_unet *u, int B, int Z, int Y, int X) {
         const size_t n = (size_t)v.nvox() * c;
         CK(cudaMalloc(p, n * sizeof(__nv_bfloat16)));
         CK(cudaMemset(*p, 0, n * sizeof(__nv_bfloat16)));
+        FG_LEGACY_FENCE();
         b.all.push_back(*p);
         return FG_OK;
     };

@@ -510,22 +510,30 @@ double or_l2_error_sin(const or_mesh *m, int nq, const double *u) {
     reftab_init(&t, m->p, nq);
     int L = t.L;
     int64_t E = (int64_t)m->nx * m->ny * m->nz;
-    double err2 = 0.0;
-#pragma omp parallel for reduction(+ : err2) schedule(static)
-    for (int64_t e = 0; e < E; ++e) {
-        int64_t dofs[MAXL];
-        double xv[8][3];
-        or_elem_dofs(m, e, dofs);
-        elem_vertices(m, e, xv);
-        for (int q = 0; q < t.Q3; ++q) {
-            double J[3][3], xp[3];
-            double det = iso_jacobian(xv, t.gq1 + 24 * q, t.pq1 + 8 * q, J, xp);
-            double uh = 0.0;
-            for (int i = 0; i < L; ++i) uh += t.phi[q * L + i] * u[dofs[i]];
-            double df = uh - u_sin(xp);
-            err2 += t.w[q] * fabs(det) * df * df;
+    /* fixed element chunks summed in index order: the same result on any
+     * thread count (see dot() below) */
+    double part[64];
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < 64; ++c) {
+        double err2 = 0.0;
+        for (int64_t e = E * c / 64; e < E * (c + 1) / 64; ++e) {
+            int64_t dofs[MAXL];
+            double xv[8][3];
+            or_elem_dofs(m, e, dofs);
+            elem_vertices(m, e, xv);
+            for (int q = 0; q < t.Q3; ++q) {
+                double J[3][3], xp[3];
+                double det = iso_jacobian(xv, t.gq1 + 24 * q, t.pq1 + 8 * q, J, xp);
+                double uh = 0.0;
+                for (int i = 0; i < L; ++i) uh += t.phi[q * L + i] * u[dofs[i]];
+                double df = uh - u_sin(xp);
+                err2 += t.w[q] * fabs(det) * df * df;
+            }
         }
+        part[c] = err2;
     }
+    double err2 = 0.0;
+    for (int c = 0; c < 64; ++c) err2 += part[c];
     reftab_free(&t);
     return sqrt(err2);
 }
@@ -534,10 +542,23 @@ double or_l2_error_sin(const or_mesh *m, int nq, const double *u) {
 /* Krylov solvers on the constrained operator                             */
 /* ---------------------------------------------------------------------- */
 
+/* Dot product with a summation order that does not depend on the thread count
+ * or on which thread finishes first (an OpenMP reduction clause combines the
+ * per-thread sums in arrival order): fixed chunks, chunk sums added in index
+ * order.  The iteration counts of the Krylov solvers below are therefore the
+ * same on every host. */
+#define OR_DOT_CHUNKS 64
 static double dot(int64_t n, const double *a, const double *b) {
+    double part[OR_DOT_CHUNKS];
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < OR_DOT_CHUNKS; ++c) {
+        const int64_t i0 = n * c / OR_DOT_CHUNKS, i1 = n * (c + 1) / OR_DOT_CHUNKS;
+        double s = 0.0;
+        for (int64_t i = i0; i < i1; ++i) s += a[i] * b[i];
+        part[c] = s;
+    }
     double s = 0.0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    for (int c = 0; c < OR_DOT_CHUNKS; ++c) s += part[c];
     return s;
 }
 

@@ -41,5 +41,6 @@ def check(results, ref, tol_apply=1e-13):
         yl = r["y_local"].reshape(r["NK"], NJ, NI)
         np.testing.assert_allclose(yl, yg[r["K0"]:r["K0"] + r["NK"]], rtol=1e-12, atol=1e-12 * np.abs(yg).max())
     its = {r["it"] for r in results}
-    assert len(its) == 1 and all(r["conv"] for r in results)
-    assert abs(its.pop() - ref["it"]) <= 1
+    assert len(its) == 1 and all(r["conv"] for r in results), its
+    it = its.pop()
+    assert abs(it - ref["it"]) <= 1, (it, ref["it"])

@@ -139,3 +139,82 @@ def test_scatter_emulation_matches_oracle(shape, p, WY, TZ, ess):
     assert not np.isnan(y).any(), "a DOF was never written"
     ref = O.apply_constrained(mesh, coef, O.ess_mask(mesh, ess), x) if ess else O.pa_apply(mesh, coef, x)
     assert np.linalg.norm(y - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+def fixup_rows_visit(NI, NJ, NK, p, WY, TZ, ntx, nty, ntz, ess):
+    """The DOFs fixup_row_t visits, row by row, with the owner item and plane
+    flags it passes to fixup_acc: (I, J, K) -> (tx, ty, tz, sx, sy, sz)."""
+    SX, SY, SZ = 32 * p, WY * p, TZ * p
+    rx, ry, rz = (ntx - 1) * NK, (nty - 1) * NK, (ntz - 1) * NJ
+    ess_i = lambda I: (ess & 16 and I == 0) or (ess & 32 and I == NI - 1)  # noqa: E731
+    ess_j = lambda J: (ess & 4 and J == 0) or (ess & 8 and J == NJ - 1)  # noqa: E731
+    ess_k = lambda K: (ess & 1 and K == 0) or (ess & 2 and K == NK - 1)  # noqa: E731
+    on_x = lambda I: 0 < I < NI - 1 and I % SX == 0  # noqa: E731
+    seen = {}
+    for r in range(rx + ry + rz):
+        if r < rx:
+            pl, K = divmod(r, NK)
+            I, tx = (pl + 1) * SX, pl + 1
+            if ess_k(K):
+                continue
+            sz, tz = int(0 < K < NK - 1 and K % SZ == 0), min(K // SZ, ntz - 1)
+            for J in range(NJ):
+                if ess_j(J):
+                    continue
+                sy, ty = int(0 < J < NJ - 1 and J % SY == 0), min(J // SY, nty - 1)
+                assert (I, J, K) not in seen
+                seen[(I, J, K)] = (tx, ty, tz, 1, sy, sz)
+        elif r < rx + ry:
+            pl, K = divmod(r - rx, NK)
+            J, ty = (pl + 1) * SY, pl + 1
+            if ess_k(K):
+                continue
+            sz, tz = int(0 < K < NK - 1 and K % SZ == 0), min(K // SZ, ntz - 1)
+            for I in range(NI):
+                if on_x(I) or ess_i(I):
+                    continue
+                assert (I, J, K) not in seen
+                seen[(I, J, K)] = (min(I // SX, ntx - 1), ty, tz, 0, 1, sz)
+        else:
+            pl, J = divmod(r - rx - ry, NJ)
+            K, tz = (pl + 1) * SZ, pl + 1
+            if (0 < J < NJ - 1 and J % SY == 0) or ess_j(J):
+                continue
+            ty = min(J // SY, nty - 1)
+            for I in range(NI):
+                if on_x(I) or ess_i(I):
+                    continue
+                assert (I, J, K) not in seen
+                seen[(I, J, K)] = (min(I // SX, ntx - 1), ty, tz, 0, 0, 1)
+    return seen
+
+
+@pytest.mark.parametrize("shape,p,WY,TZ,ess", [
+    ((33, 5, 5), 1, 4, 2, 0),
+    ((70, 9, 7), 2, 4, 3, 63),
+    ((65, 7, 9), 3, 2, 2, 16 | 2 | 8),
+    ((3, 2, 2), 2, 4, 8, 0),
+    ((64, 8, 16), 2, 4, 8, 32 | 1 | 4),
+])
+def test_fixup_rows_cover_each_shared_dof_once(shape, p, WY, TZ, ess):
+    """The row decomposition of the fix-up kernel visits exactly the shared,
+    non-essential DOFs, once each, with the owner item and plane flags of the
+    per-DOF rule (fixup_sum)."""
+    nx, ny, nz = shape
+    NI, NJ, NK = nx * p + 1, ny * p + 1, nz * p + 1
+    ntx, nty, ntz = -(-nx // 32), -(-ny // WY), -(-nz // TZ)
+    SX, SY, SZ = 32 * p, WY * p, TZ * p
+    seen = fixup_rows_visit(NI, NJ, NK, p, WY, TZ, ntx, nty, ntz, ess)
+    want = {}
+    for K in range(NK):
+        for J in range(NJ):
+            for I in range(NI):
+                sx = int(0 < I < NI - 1 and I % SX == 0)
+                sy = int(0 < J < NJ - 1 and J % SY == 0)
+                sz = int(0 < K < NK - 1 and K % SZ == 0)
+                e = ((ess & 1 and K == 0) or (ess & 2 and K == NK - 1) or (ess & 4 and J == 0) or
+                     (ess & 8 and J == NJ - 1) or (ess & 16 and I == 0) or (ess & 32 and I == NI - 1))
+                if (sx or sy or sz) and not e:
+                    want[(I, J, K)] = (min(I // SX, ntx - 1), min(J // SY, nty - 1), min(K // SZ, ntz - 1),
+                                       sx, sy, sz)
+    assert seen == want
