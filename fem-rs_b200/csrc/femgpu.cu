@@ -189,6 +189,7 @@ struct fg_op {
     double *qd = nullptr, *face = nullptr;
     double *xs = nullptr, *ys = nullptr;
     double *dinv = nullptr, *ones = nullptr;
+    double *stage = nullptr;  // N values: contiguous device copy of a host vector
     bool have_dinv = false;
     double lmax_est = 0.0;
     bool have_lmax = false;
@@ -230,7 +231,7 @@ static void free_op(fg_op *op) {
     cudaSetDevice(op->device);
     if (op->stream) cudaStreamSynchronize(op->stream);
     double *bufs[] = {op->qd, op->face, op->xs, op->ys, op->dinv, op->ones, op->r, op->z, op->pv, op->ap,
-                      op->xw, op->bw, op->cres, op->cd, op->ct, op->partials};
+                      op->xw, op->bw, op->cres, op->cd, op->ct, op->partials, op->stage};
     for (double *b : bufs)
         if (b) cudaFree(b);
     float *fb[] = {op->qd32, op->face32, op->dinv32, op->r32, op->z32, op->p32, op->ap32, op->e32,
@@ -623,22 +624,55 @@ FG_API int fg_op_check(fg_op *op) {
     return check_device_error(op);
 }
 
-static int to_native(fg_op *op, double *dst, const double *src, int mem) {
-    const Grid &g = op->g;
-    CK(cudaMemcpy2DAsync(dst, sizeof(double) * g.NIp, src, sizeof(double) * g.NI,
-                         sizeof(double) * g.NI, (size_t)g.NJ * g.NK,
-                         mem == FG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
-                         op->stream));
+}  // extern "C"
+
+// Host vectors cross PCIe as one contiguous copy through the handle's staging
+// buffer; the change of row pitch (NI <-> NIp) is a device-to-device 2-D copy.
+// A 2-D copy straight from or to host memory moves one DOF row per transfer and
+// ran at about half the contiguous PCIe rate.
+template <typename T> static int stage_of(fg_op *op, T **st) {
+    static_assert(sizeof(T) <= sizeof(double), "staging holds N doubles");
+    if (!op->stage) {
+        int rc = alloc_vec(&op->stage, op->N);
+        if (rc) return rc;
+    }
+    *st = reinterpret_cast<T *>(op->stage);
     return FG_OK;
+}
+template <typename T> static int to_native_t(fg_op *op, T *dst, const T *src, int mem) {
+    const Grid &g = op->g;
+    if (mem == FG_HOST) {
+        T *st = nullptr;
+        int rc = stage_of(op, &st);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(st, src, sizeof(T) * op->N, cudaMemcpyHostToDevice, op->stream));
+        src = st;
+    }
+    CK(cudaMemcpy2DAsync(dst, sizeof(T) * g.NIp, src, sizeof(T) * g.NI, sizeof(T) * g.NI,
+                         (size_t)g.NJ * g.NK, cudaMemcpyDeviceToDevice, op->stream));
+    return FG_OK;
+}
+template <typename T> static int from_native_t(fg_op *op, T *dst, const T *src, int mem) {
+    const Grid &g = op->g;
+    T *out = dst;
+    if (mem == FG_HOST) {
+        int rc = stage_of(op, &out);
+        if (rc) return rc;
+    }
+    CK(cudaMemcpy2DAsync(out, sizeof(T) * g.NI, src, sizeof(T) * g.NIp, sizeof(T) * g.NI,
+                         (size_t)g.NJ * g.NK, cudaMemcpyDeviceToDevice, op->stream));
+    if (mem == FG_HOST)
+        CK(cudaMemcpyAsync(dst, out, sizeof(T) * op->N, cudaMemcpyDeviceToHost, op->stream));
+    return FG_OK;
+}
+static int to_native(fg_op *op, double *dst, const double *src, int mem) {
+    return to_native_t<double>(op, dst, src, mem);
 }
 static int from_native(fg_op *op, double *dst, const double *src, int mem) {
-    const Grid &g = op->g;
-    CK(cudaMemcpy2DAsync(dst, sizeof(double) * g.NI, src, sizeof(double) * g.NIp,
-                         sizeof(double) * g.NI, (size_t)g.NJ * g.NK,
-                         mem == FG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
-                         op->stream));
-    return FG_OK;
+    return from_native_t<double>(op, dst, src, mem);
 }
+
+extern "C" {
 
 FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, int constrained,
                        int mem) {
@@ -1164,18 +1198,10 @@ static void set_state(fg_op *op, SolverState *dst, double rtol, double atol, int
 extern "C" {
 
 static int to_native32(fg_op *op, float *dst, const float *src, int mem) {
-    const Grid &g = op->g;
-    CK(cudaMemcpy2DAsync(dst, sizeof(float) * g.NIp, src, sizeof(float) * g.NI, sizeof(float) * g.NI,
-                         (size_t)g.NJ * g.NK,
-                         mem == FG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, op->stream));
-    return FG_OK;
+    return to_native_t<float>(op, dst, src, mem);
 }
 static int from_native32(fg_op *op, float *dst, const float *src, int mem) {
-    const Grid &g = op->g;
-    CK(cudaMemcpy2DAsync(dst, sizeof(float) * g.NI, src, sizeof(float) * g.NIp, sizeof(float) * g.NI,
-                         (size_t)g.NJ * g.NK,
-                         mem == FG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, op->stream));
-    return FG_OK;
+    return from_native_t<float>(op, dst, src, mem);
 }
 
 FG_API int fg_op_set_qdata_format(fg_op *op, int format) {
