@@ -190,6 +190,12 @@ struct fg_op {
     double *xs = nullptr, *ys = nullptr;
     double *dinv = nullptr, *ones = nullptr;
     double *stage = nullptr;  // N values: contiguous device copy of a host vector
+    // fused fix-up (FG_FUSED_FIXUP=1; off by default, fixup_kernel runs after each apply):
+    // per-item arrival counters (FP64 applies, then FP32 applies), sized for the finest item
+    // tiling (one layer per item)
+    unsigned *fixcnt = nullptr;
+    int64_t fixcnt_items = 0;
+    bool fused_fixup = false;
     bool have_dinv = false;
     double lmax_est = 0.0;
     bool have_lmax = false;
@@ -232,6 +238,7 @@ static void free_op(fg_op *op) {
     if (op->stream) cudaStreamSynchronize(op->stream);
     double *bufs[] = {op->qd, op->face, op->xs, op->ys, op->dinv, op->ones, op->r, op->z, op->pv, op->ap,
                       op->xw, op->bw, op->cres, op->cd, op->ct, op->partials, op->stage};
+    if (op->fixcnt) cudaFree(op->fixcnt);
     for (double *b : bufs)
         if (b) cudaFree(b);
     float *fb[] = {op->qd32, op->face32, op->dinv32, op->r32, op->z32, op->p32, op->ap32, op->e32,
@@ -285,7 +292,7 @@ template <> struct TmapType<float> { static constexpr CUtensorMapDataType v = CU
 
 template <int P, int OPK, typename T, int FMT>
 static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const T *x, T *y,
-                          int accumulate, const int *skip) {
+                          int accumulate, const int *skip, unsigned *fixcnt = nullptr) {
     using C = KC<P, T>;
     static_assert(C::WY == KCfg<P>::WY, "FP32 and FP64 share the item tiling");
     constexpr int S = FMT == 0 ? C::S : 2;  // affine format: one element layer per stage
@@ -305,7 +312,7 @@ static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const 
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
-    ApplyArgs<T> A{g, qd, y, face, accumulate, op->d_err, skip};
+    ApplyArgs<T> A{g, qd, y, face, accumulate, op->d_err, skip, fixcnt};
     kern<<<g.n_items(), C::WY * 32, SM::bytes, op->stream>>>(tmap, A);
     CK(cudaGetLastError());
     return FG_OK;
@@ -317,20 +324,20 @@ template <> const float *qdata_of<float>(fg_op *op) { return op->fmt ? op->qa32 
 
 template <int P, typename T>
 static int launch_apply_p(fg_op *op, const Grid &g, const T *, T *face, const T *x, T *y,
-                          int accumulate, const int *skip) {
+                          int accumulate, const int *skip, unsigned *fixcnt) {
     const T *qd = qdata_of<T>(op);
     if (!qd) return fail(FG_INVALID_ARGUMENT, "quadrature data for this precision/format not built");
     if (op->fmt == 0) {
         switch (op->kind) {
-        case FG_MASS: return launch_apply_t<P, 1, T, 0>(op, g, qd, face, x, y, accumulate, skip);
-        case FG_DIFF: return launch_apply_t<P, 2, T, 0>(op, g, qd, face, x, y, accumulate, skip);
-        default: return launch_apply_t<P, 3, T, 0>(op, g, qd, face, x, y, accumulate, skip);
+        case FG_MASS: return launch_apply_t<P, 1, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
+        case FG_DIFF: return launch_apply_t<P, 2, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
+        default: return launch_apply_t<P, 3, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
         }
     }
     switch (op->kind) {
-    case FG_MASS: return launch_apply_t<P, 1, T, 1>(op, g, qd, face, x, y, accumulate, skip);
-    case FG_DIFF: return launch_apply_t<P, 2, T, 1>(op, g, qd, face, x, y, accumulate, skip);
-    default: return launch_apply_t<P, 3, T, 1>(op, g, qd, face, x, y, accumulate, skip);
+    case FG_MASS: return launch_apply_t<P, 1, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
+    case FG_DIFF: return launch_apply_t<P, 2, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
+    default: return launch_apply_t<P, 3, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
     }
 }
 
@@ -345,19 +352,31 @@ static int launch_fixup(fg_op *op, const Grid &g, T *y, const T *face, const int
     return FG_OK;
 }
 
+// Arrival counters of the fused fix-up for an apply into the handle's own face
+// buffer of this precision (one set per precision, so an FP64 and an FP32
+// apply never share them), or null: the separate fixup_kernel.
+template <typename T> static unsigned *fixcnt_for(fg_op *op, const T *face) {
+    if (!op->fused_fixup || !op->fixcnt) return nullptr;
+    if (std::is_same<T, double>::value && (const void *)face == (const void *)op->face) return op->fixcnt;
+    if (std::is_same<T, float>::value && (const void *)face == (const void *)op->face32)
+        return op->fixcnt + op->fixcnt_items;
+    return nullptr;
+}
+
 // y (+)= A x on native vectors with the given precision's quadrature data.
 template <typename T>
 static int apply_native_t(fg_op *op, const T *qd, T *face, const T *x, T *y, int accumulate,
                           int constrained, const int *skip) {
+    unsigned *fixcnt = fixcnt_for<T>(op, face);
     Grid g = op->g;
     g.ess = constrained ? op->ess_tags : 0;
     int rc;
     switch (op->p) {
-    case 1: rc = launch_apply_p<1, T>(op, g, qd, face, x, y, accumulate, skip); break;
-    case 2: rc = launch_apply_p<2, T>(op, g, qd, face, x, y, accumulate, skip); break;
-    default: rc = launch_apply_p<3, T>(op, g, qd, face, x, y, accumulate, skip); break;
+    case 1: rc = launch_apply_p<1, T>(op, g, qd, face, x, y, accumulate, skip, fixcnt); break;
+    case 2: rc = launch_apply_p<2, T>(op, g, qd, face, x, y, accumulate, skip, fixcnt); break;
+    default: rc = launch_apply_p<3, T>(op, g, qd, face, x, y, accumulate, skip, fixcnt); break;
     }
-    if (rc) return rc;
+    if (rc || fixcnt) return rc;
     return launch_fixup<T>(op, g, y, face, skip);
 }
 
@@ -505,6 +524,8 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
         op->graphs = !(e && e[0] == '0');
         const char *o = std::getenv("FG_NN_OVERLAP");
         op->nn_overlap = !(o && o[0] == '0');
+        const char *f = std::getenv("FG_FUSED_FIXUP");
+        op->fused_fixup = f && f[0] == '1';
     }
     if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)))
         return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
@@ -512,6 +533,8 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
         cudaMemset(op->st, 0, sizeof(SolverState)) != cudaSuccess)
         return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
     if ((rc = alloc_vec(&op->face, (int64_t)g.n_items() * g.face_stride()))) return bail(rc);
+    op->fixcnt_items = (int64_t)g.ntx * g.nty * g.nz;  // items at one layer each: any tiling fits
+    if ((rc = alloc_vec(&op->fixcnt, 2 * op->fixcnt_items))) return bail(rc);
     if ((rc = alloc_vec(&op->xs, op->Nn)) || (rc = alloc_vec(&op->ys, op->Nn))) return bail(rc);
     if ((rc = alloc_vec(&op->partials, VEC_GRID * 4))) return bail(rc);
     cudaEventCreate(&op->ev0);

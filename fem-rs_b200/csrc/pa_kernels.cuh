@@ -67,7 +67,13 @@ template <typename T> struct ApplyArgs {
     int accumulate;   // 1: y += A x, 0: y = A x
     int *err;         // device error word
     const int *skip;  // if non-null and *skip != 0 the kernel returns at once
+    unsigned *fixcnt; // non-null: fix-up fused into the apply (per-item arrival counters, all zero
+                      // between launches); null: fixup_kernel runs after the apply
 };
+
+template <typename T, int P>
+__device__ __forceinline__ void fused_fixup(const Grid &g, T *y, const T *face, unsigned *cnt,
+                                            int item, int *flag);
 
 // Quadrature-data formats.
 //  FMT 0 (full): NC components per quadrature point (6 symmetric w|detJ| kappa
@@ -851,6 +857,8 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
             for (int j = x_waited; j < x_issued; ++j)
                 mbar_wait(&xbar[j % SM::NXB], (j / SM::NXB) & 1, nullptr, 100000000ull);
     }
+    if (A.fixcnt)  // the y staging area is free after the last layer's barrier
+        fused_fixup<T, P>(g, A.y, A.face, A.fixcnt, item, reinterpret_cast<int *>(ybuf));
 }
 
 // Single operator: one CTA per item; the x tile map is a kernel parameter.
@@ -959,7 +967,11 @@ __global__ void __launch_bounds__(WY * 32) pa_diag_kernel(const ApplyArgs<T> A) 
 // The neighbours' face-slot partials of one shared DOF added to `own` in
 // (dz, dy, dx) order.  (tx, ty, tz): the owner item; (sx, sy, sz): whether the
 // DOF lies on an x / y / z plane between items.
-template <typename T>
+template <bool CG, typename T> __device__ __forceinline__ T ld_face(const T *p) {
+    if constexpr (CG) return __ldcg(p);  // written by other CTAs of the same launch: read at L2
+    else return *p;
+}
+template <typename T, bool CG = false>
 __device__ __forceinline__ T fixup_acc(const Grid &g, int I, int J, int K, int tx, int ty, int tz,
                                        int sx, int sy, int sz, T own, const T *__restrict__ face) {
     const int SXe = 32 * g.p, SYe = g.WY * g.p, SZe = g.TZ * g.p;
@@ -974,11 +986,11 @@ __device__ __forceinline__ T fixup_acc(const Grid &g, int I, int J, int K, int t
                 const int I0 = nx_ * SXe, J0 = ny_ * SYe, K0 = nz_ * SZe;
                 const T *fb = face + (int64_t)nb * fs;
                 if (dx)
-                    sum += fb[(K - K0) * (SYe + 1) + (J - J0)];
+                    sum += ld_face<CG>(fb + (K - K0) * (SYe + 1) + (J - J0));
                 else if (dy)
-                    sum += fb[fxs + (K - K0) * (SXe + 1) + (I - I0)];
+                    sum += ld_face<CG>(fb + fxs + (K - K0) * (SXe + 1) + (I - I0));
                 else
-                    sum += fb[fxs + fys + (J - J0) * (SXe + 1) + (I - I0)];
+                    sum += ld_face<CG>(fb + fxs + fys + (J - J0) * (SXe + 1) + (I - I0));
             }
     return sum;
 }
@@ -1062,6 +1074,84 @@ __device__ __forceinline__ void fixup_row(const Grid &g, int r, T *__restrict__ 
     case 1: fixup_row_t<T, 1>(g, r, y, face); break;
     case 2: fixup_row_t<T, 2>(g, r, y, face); break;
     default: fixup_row_t<T, 3>(g, r, y, face); break;
+    }
+}
+
+// The shared DOFs owned by item (ox, oy, oz): those on its lower x, y and z
+// faces that a lower neighbour item also touches (the same DOFs, owner and
+// plane flags as the rows of fixup_row_t), fixed up by the whole block.
+template <typename T, int P>
+__device__ __forceinline__ void fixup_owner(const Grid &g, T *y, const T *face, int ox, int oy,
+                                            int oz) {
+    constexpr int SXe = 32 * P;
+    const int SYe = g.WY * P, SZe = g.TZ * P;
+    const int I0 = ox * SXe, J0 = oy * SYe, K0 = oz * SZe;
+    const int I1 = ox == g.ntx - 1 ? g.NI - 1 : I0 + SXe - 1;
+    const int J1 = oy == g.nty - 1 ? g.NJ - 1 : J0 + SYe - 1;
+    const int K1 = oz == g.ntz - 1 ? g.NK - 1 : K0 + SZe - 1;
+    const int ia = I0 + (ox > 0), ja = J0 + (oy > 0);  // first I / J off the owner's x / y plane
+    const int nI = I1 - ia + 1, nJ = J1 - J0 + 1, nJy = J1 - ja + 1, nK = K1 - K0 + 1;
+    const int cx = ox > 0 ? nJ * nK : 0;   // x face (J, K)
+    const int cy = oy > 0 ? nI * nK : 0;   // y face (I, K), off the x plane
+    const int cz = oz > 0 ? nI * nJy : 0;  // z face (I, J), off the x and y planes
+    for (int t = threadIdx.x; t < cx + cy + cz; t += blockDim.x) {
+        int I, J, K, sx, sy, sz;
+        if (t < cx) {
+            const int k = t / nJ;
+            J = J0 + (t - k * nJ); K = K0 + k; I = I0;
+            sx = 1; sy = (J == J0 && oy > 0); sz = (K == K0 && oz > 0);
+        } else if (t < cx + cy) {
+            const int u = t - cx, k = u / nI;
+            I = ia + (u - k * nI); K = K0 + k; J = J0;
+            sx = 0; sy = 1; sz = (K == K0 && oz > 0);
+        } else {
+            const int u = t - cx - cy, j = u / nI;
+            I = ia + (u - j * nI); J = ja + j; K = K0;
+            sx = 0; sy = 0; sz = 1;
+        }
+        if (g.is_ess(I, J, K)) continue;
+        T *yp = y + g.dof(I, J, K);
+        *yp = fixup_acc<T, true>(g, I, J, K, ox, oy, oz, sx, sy, sz, __ldcg(yp), face);
+    }
+}
+
+// Fix-up fused into the apply (a run-time option, off by default: measured
+// slower than fixup_kernel, 0.657 against 0.503 ms for the 128^3 Q2 FP64
+// apply, because the last arriver's owner fix-up is a serial tail of
+// L2-latency-bound loads on an SM slot that would otherwise stream qdata).
+// Once an item has stored its values and face slots it arrives at the counter
+// of every item whose lower faces it touches (itself and its upper neighbours
+// in x, y and z).  The last of an owner's contributors to arrive (an arrival
+// count, not a wait: no CTA waits on another) resets the owner's counter for
+// the next launch and adds the face partials into the owner's lower-face DOFs:
+// the sums of fixup_sum in the same order, so the result is bit-identical to
+// fixup_kernel's.  `flag` is one int of shared memory that is free at this
+// point.
+template <typename T, int P>
+__device__ __forceinline__ void fused_fixup(const Grid &g, T *y, const T *face, unsigned *cnt,
+                                            int item, int *flag) {
+    const int tx = item % g.ntx, ty = (item / g.ntx) % g.nty, tz = item / (g.ntx * g.nty);
+    __threadfence();  // this thread's y and face-slot stores, before the arrival below
+    __syncthreads();
+    for (int o = 0; o < 8; ++o) {
+        const int ox = tx + (o & 1), oy = ty + ((o >> 1) & 1), oz = tz + (o >> 2);
+        if (ox >= g.ntx || oy >= g.nty || oz >= g.ntz) continue;
+        const unsigned need = (1u + (ox > 0)) * (1u + (oy > 0)) * (1u + (oz > 0));
+        if (need == 1u) continue;  // no lower neighbour: nothing shared below
+        const int owner = (oz * g.nty + oy) * g.ntx + ox;
+        if (threadIdx.x == 0) {
+            const unsigned prev = atomicAdd(&cnt[owner], 1u);
+            const int last = prev == need - 1u;
+            if (last) {
+                atomicExch(&cnt[owner], 0u);
+                __threadfence();  // the contributors' stores, before this block reads them
+            }
+            *flag = last;
+        }
+        __syncthreads();
+        const int last = *flag;
+        __syncthreads();
+        if (last) fixup_owner<T, P>(g, y, face, ox, oy, oz);
     }
 }
 

@@ -205,6 +205,12 @@ def test_fixup_rows_cover_each_shared_dof_once(shape, p, WY, TZ, ess):
     ntx, nty, ntz = -(-nx // 32), -(-ny // WY), -(-nz // TZ)
     SX, SY, SZ = 32 * p, WY * p, TZ * p
     seen = fixup_rows_visit(NI, NJ, NK, p, WY, TZ, ntx, nty, ntz, ess)
+    assert seen == per_dof_rule(NI, NJ, NK, SX, SY, SZ, ntx, nty, ntz, ess)
+
+
+def per_dof_rule(NI, NJ, NK, SX, SY, SZ, ntx, nty, ntz, ess):
+    """fixup_sum's classification of every DOF: shared (on a plane between
+    items) and not essential -> owner item and plane flags."""
     want = {}
     for K in range(NK):
         for J in range(NJ):
@@ -217,4 +223,66 @@ def test_fixup_rows_cover_each_shared_dof_once(shape, p, WY, TZ, ess):
                 if (sx or sy or sz) and not e:
                     want[(I, J, K)] = (min(I // SX, ntx - 1), min(J // SY, nty - 1), min(K // SZ, ntz - 1),
                                        sx, sy, sz)
-    assert seen == want
+    return want
+
+
+def fixup_owner_visit(NI, NJ, NK, p, WY, TZ, ntx, nty, ntz, ess):
+    """The DOFs the fused fix-up (fixup_owner, run once per item by the last of
+    its contributors to arrive) visits, with the flags it passes to fixup_acc."""
+    SX, SY, SZ = 32 * p, WY * p, TZ * p
+    seen = {}
+    for oz in range(ntz):
+        for oy in range(nty):
+            for ox in range(ntx):
+                if (1 + (ox > 0)) * (1 + (oy > 0)) * (1 + (oz > 0)) == 1:
+                    continue
+                I0, J0, K0 = ox * SX, oy * SY, oz * SZ
+                I1 = NI - 1 if ox == ntx - 1 else I0 + SX - 1
+                J1 = NJ - 1 if oy == nty - 1 else J0 + SY - 1
+                K1 = NK - 1 if oz == ntz - 1 else K0 + SZ - 1
+                ia, ja = I0 + (ox > 0), J0 + (oy > 0)
+                nI, nJ, nJy, nK = I1 - ia + 1, J1 - J0 + 1, J1 - ja + 1, K1 - K0 + 1
+                cx = nJ * nK if ox > 0 else 0
+                cy = nI * nK if oy > 0 else 0
+                cz = nI * nJy if oz > 0 else 0
+                for t in range(cx + cy + cz):
+                    if t < cx:
+                        k, j = divmod(t, nJ)
+                        I, J, K = I0, J0 + j, K0 + k
+                        f = (1, int(J == J0 and oy > 0), int(K == K0 and oz > 0))
+                    elif t < cx + cy:
+                        k, i = divmod(t - cx, nI)
+                        I, J, K = ia + i, J0, K0 + k
+                        f = (0, 1, int(K == K0 and oz > 0))
+                    else:
+                        j, i = divmod(t - cx - cy, nI)
+                        I, J, K = ia + i, ja + j, K0
+                        f = (0, 0, 1)
+                    e = ((ess & 1 and K == 0) or (ess & 2 and K == NK - 1) or (ess & 4 and J == 0) or
+                         (ess & 8 and J == NJ - 1) or (ess & 16 and I == 0) or (ess & 32 and I == NI - 1))
+                    if e:
+                        continue
+                    assert 0 <= I < NI and 0 <= J < NJ and 0 <= K < NK
+                    assert (I, J, K) not in seen
+                    seen[(I, J, K)] = (ox, oy, oz) + f
+    return seen
+
+
+@pytest.mark.parametrize("shape,p,WY,TZ,ess", [
+    ((33, 5, 5), 1, 4, 2, 0),
+    ((70, 9, 7), 2, 4, 3, 63),
+    ((65, 7, 9), 3, 2, 2, 16 | 2 | 8),
+    ((3, 2, 2), 2, 4, 8, 0),
+    ((64, 8, 16), 2, 4, 8, 32 | 1 | 4),
+    ((4, 4, 4), 1, 4, 1, 63),
+    ((96, 12, 8), 1, 4, 4, 63),
+])
+def test_fused_fixup_owners_match_rows(shape, p, WY, TZ, ess):
+    """The per-owner enumeration of the fused fix-up and the row decomposition
+    of fixup_kernel visit the same DOFs with the same owner and plane flags."""
+    nx, ny, nz = shape
+    NI, NJ, NK = nx * p + 1, ny * p + 1, nz * p + 1
+    ntx, nty, ntz = -(-nx // 32), -(-ny // WY), -(-nz // TZ)
+    rows = fixup_rows_visit(NI, NJ, NK, p, WY, TZ, ntx, nty, ntz, ess)
+    owners = fixup_owner_visit(NI, NJ, NK, p, WY, TZ, ntx, nty, ntz, ess)
+    assert owners == rows == per_dof_rule(NI, NJ, NK, 32 * p, WY * p, TZ * p, ntx, nty, ntz, ess)
