@@ -163,12 +163,12 @@ def cpu_apply_sample(n, p, kq_full, reps=2, layers=None):
     coef = O.Coef(O.DIFF, kappa_q=kq)
     x = np.random.default_rng(1).standard_normal(mesh.ndofs)
     y = np.zeros(mesh.ndofs)
-    O.pa_apply(mesh, coef, x, y)  # warm
+    cores = host_threads()
+    O.pa_apply(mesh, coef, x, y, nthreads=cores)  # warm
     t0 = time.perf_counter()
     for _ in range(reps):
-        O.pa_apply(mesh, coef, x, y)
+        O.pa_apply(mesh, coef, x, y, nthreads=cores)
     dt = (time.perf_counter() - t0) / reps
-    cores = os.cpu_count()
     desc = (f"oracle port of the reference PA element loop (partial.rs:154-208 + assembler.rs:96-143), "
             f"{n}x{n}x{nzs} Q{p} z-slab of the workload ({mesh.ndofs} DOFs), {reps} applies, "
             f"OpenMP {cores} threads")
@@ -181,14 +181,24 @@ def cpu_ex1_pipeline(n=24):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
+    cores = host_threads()
     t0 = time.perf_counter()
     mesh = O.Mesh(n, n, n, 1)
     mask = O.ess_mask(mesh)
     b = O.source(mesh, mask)
-    x, info = O.pcg(mesh, O.Coef(O.DIFF), mask, b, precond=1, rtol=1e-10, max_iter=2000)
+    x, info = O.pcg(mesh, O.Coef(O.DIFF), mask, b, precond=1, rtol=1e-10, max_iter=2000, nthreads=cores)
     err = O.l2_error_sin(mesh, x, nq=3)
     return {"pipeline_s": time.perf_counter() - t0, "iterations": info["iterations"], "l2_error": err,
-            "threads": os.cpu_count()}
+            "threads": cores}
+
+
+def host_threads():
+    """Host threads this process may run on (the CPU baseline uses all of
+    them, whatever OMP_NUM_THREADS a launcher such as torchrun has set)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
 def run_reference(args, n, p):
@@ -207,14 +217,14 @@ def run_reference(args, n, p):
     coef = O.Coef(O.DIFF, kappa_q=kq)
     x = np.random.default_rng(1).standard_normal(mesh.ndofs)
     y = np.zeros(mesh.ndofs)
+    cores = host_threads()
     for _ in range(args.warmup):
-        O.pa_apply(mesh, coef, x, y)
+        O.pa_apply(mesh, coef, x, y, nthreads=cores)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.pa_apply(mesh, coef, x, y)
+        O.pa_apply(mesh, coef, x, y, nthreads=cores)
     dt = time.perf_counter() - t0
     val = mesh.ndofs * args.steps / dt / 1e9
-    cores = os.cpu_count()
     out = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "GDOF/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
@@ -594,7 +604,7 @@ def main():
             if ex1 is not None:
                 cpu["ex1_pipeline"] = cpu_ex1_pipeline()
         except Exception as exc:  # keep the bench line even if the oracle is unavailable
-            cpu = {"value": None, "unit": "GDOF/s", "cores": os.cpu_count(), "kind": "port",
+            cpu = {"value": None, "unit": "GDOF/s", "cores": host_threads(), "kind": "port",
                    "sample": f"unavailable: {exc}"}
 
     if rank == 0:
