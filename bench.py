@@ -471,8 +471,14 @@ def main():
         u0.reshape(hn * hp + 1, hn * hp + 1, hn * hp + 1)[:, :, [0, -1]] = 0.0
         heat = {"workload": f"{hn}^3 Q2 SDIRK-2, dt={dt}, {args.heat_steps} steps, stage rtol 1e-10, warm start"}
         finals = {}
-        for name, prec, pc in (("fp64_chebyshev4", femgpu.FP64, femgpu.PC_CHEBYSHEV),
-                               ("fp32_chebyshev4", femgpu.FP32_IR, femgpu.PC_CHEBYSHEV)):
+        # _affine: the quadrature data of both operators in the affine-compressed
+        # format (constant-J elements: |detJ| J^-1 J^-T per element, kappa per point)
+        for name, prec, pc, fmt in (("fp64_chebyshev4", femgpu.FP64, femgpu.PC_CHEBYSHEV, femgpu.QDATA_FULL),
+                                    ("fp32_chebyshev4", femgpu.FP32_IR, femgpu.PC_CHEBYSHEV, femgpu.QDATA_FULL),
+                                    ("fp32_chebyshev4_affine", femgpu.FP32_IR, femgpu.PC_CHEBYSHEV,
+                                     femgpu.QDATA_AFFINE)):
+            K.set_qdata_format(fmt)
+            S.set_qdata_format(fmt)
             u = u0.copy()
             info = femgpu.sdirk2(K, S, u, dt, args.heat_steps,
                                  femgpu.SolverConfig(rtol=1e-10, max_iter=5000, precision=prec), pc)
