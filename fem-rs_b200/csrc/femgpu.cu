@@ -201,6 +201,8 @@ struct fg_op {
     bool have_lmax = false;
     double *r = nullptr, *z = nullptr, *pv = nullptr, *ap = nullptr, *xw = nullptr, *bw = nullptr;
     double *cres = nullptr, *cd = nullptr, *ct = nullptr;
+    double *cdk[CHEB_MAXD] = {};   // Chebyshev d_1 .. d_{s-1} (d_0 is cd)
+    float *cdk32[CHEB_MAXD] = {};
     double *partials = nullptr;
     SolverState *st = nullptr;
     // FP32 operator data and inner-solve work vectors (iterative refinement)
@@ -239,6 +241,10 @@ static void free_op(fg_op *op) {
     double *bufs[] = {op->qd, op->face, op->xs, op->ys, op->dinv, op->ones, op->r, op->z, op->pv, op->ap,
                       op->xw, op->bw, op->cres, op->cd, op->ct, op->partials, op->stage};
     if (op->fixcnt) cudaFree(op->fixcnt);
+    for (int k = 0; k < CHEB_MAXD; ++k) {
+        if (op->cdk[k]) cudaFree(op->cdk[k]);
+        if (op->cdk32[k]) cudaFree(op->cdk32[k]);
+    }
     for (double *b : bufs)
         if (b) cudaFree(b);
     float *fb[] = {op->qd32, op->face32, op->dinv32, op->r32, op->z32, op->p32, op->ap32, op->e32,
@@ -893,12 +899,51 @@ template <typename T> struct PcgBufs {
     SolverState *st;
 };
 
+template <typename T> static T **cheb_dk(fg_op *op);
+template <> double **cheb_dk<double>(fg_op *op) { return op->cdk; }
+template <> float **cheb_dk<float>(fg_op *op) { return op->cdk32; }
+
 // z = Chebyshev(D^-1 A) r (Saad Alg. 12.1, zero start, k sweeps)
 template <typename T>
 static int cheb_apply(fg_op *op, const PcgBufs<T> &B, const ChebCoef &cc, const T *r, T *z,
                       const int *skip) {
     const int64_t n = op->Nn;
     const SolverState *sst = skip ? B.st : nullptr;
+    const int s = (int)cc.c1.size();
+    if (s >= 1 && s <= CHEB_MAXD) {
+        // d_k in their own vectors (d_0 = cd), z formed once in the last sweep.
+        // The vectors are allocated by the first call, which a solver makes
+        // outside graph capture (its first chunk runs directly).
+        T **dk = cheb_dk<T>(op);
+        for (int k = 1; k < s; ++k)
+            if (!dk[k - 1]) {
+                int rc = alloc_vec(&dk[k - 1], n);
+                if (rc) return rc;
+            }
+        k_cheb_first_d<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, r, B.dinv, B.cres, B.cd,
+                                                                    cc.inv_theta, sst);
+        CK(cudaGetLastError());
+        const T *dprev = B.cd;
+        for (int k = 1; k <= s; ++k) {
+            int rc = apply_native_t<T>(op, B.qd, B.face, dprev, B.ct, 0, 1, skip);
+            if (rc) return rc;
+            if (k < s) {
+                k_cheb_mid<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.ct, B.dinv, B.cres, dprev,
+                                                                        dk[k - 1], cc.c1[k - 1],
+                                                                        cc.c2[k - 1], sst);
+                dprev = dk[k - 1];
+            } else {
+                ChebSum<T> earlier{};
+                earlier.n = s - 1;  // d_0 .. d_{s-2}
+                for (int j = 0; j < s - 1; ++j) earlier.d[j] = j == 0 ? B.cd : dk[j - 1];
+                k_cheb_last<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.ct, B.dinv, B.cres, dprev,
+                                                                         earlier, z, cc.c1[k - 1],
+                                                                         cc.c2[k - 1], sst);
+            }
+            CK(cudaGetLastError());
+        }
+        return FG_OK;
+    }
     k_cheb_first<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, r, B.dinv, B.cres, B.cd, z,
                                                               cc.inv_theta, sst);
     CK(cudaGetLastError());

@@ -309,6 +309,86 @@ __global__ void __launch_bounds__(VEC_THREADS) k_cheb_step(int64_t n, const T *_
     }
 }
 
+// The same sweeps with each d_k kept in its own vector and z formed once, in
+// the last sweep: z = d_0 + d_1 + ... + d_s added in that order, the order in
+// which k_cheb_step accumulates it, so z is bit-identical.  Per application of
+// degree s + 1 this moves 6 s + 5 vector passes instead of 8 s + 5 -- the last
+// sweep writes neither res nor d, and z is written once instead of s + 1 times.
+constexpr int CHEB_MAXD = 16;  // longest list of earlier d_k the last sweep sums
+template <typename T> struct ChebSum {
+    const T *d[CHEB_MAXD];  // d_0 .. d_{s-2}
+    int n;
+};
+
+// sweep 1 from zero: res = dinv r ; d_0 = res / theta
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_cheb_first_d(int64_t n, const T *__restrict__ r,
+                                                              const T *__restrict__ dinv,
+                                                              T *__restrict__ res, T *__restrict__ d,
+                                                              double inv_theta, const SolverState *st) {
+    if (st && st->done) return;
+    const T it = (T)inv_theta;
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> rv = ld4(r, q), dv = ld4(dinv, q);
+        V4<T> sv, dd;
+        FG_K4 {
+            sv.a[k] = dv.a[k] * rv.a[k];
+            dd.a[k] = sv.a[k] * it;
+        }
+        st4(res, q, sv);
+        st4(d, q, dd);
+    }
+}
+
+// middle sweep: res -= dinv t ; d_k = c1 d_{k-1} + c2 res
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_cheb_mid(int64_t n, const T *__restrict__ t,
+                                                          const T *__restrict__ dinv,
+                                                          T *__restrict__ res,
+                                                          const T *__restrict__ dprev,
+                                                          T *__restrict__ dnext, double c1, double c2,
+                                                          const SolverState *st) {
+    if (st && st->done) return;
+    const T a1 = (T)c1, a2 = (T)c2;
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> tv = ld4(t, q), dv = ld4(dinv, q), pv = ld4(dprev, q);
+        V4<T> sv = ld4(res, q), dd;
+        FG_K4 {
+            sv.a[k] = sv.a[k] - dv.a[k] * tv.a[k];
+            dd.a[k] = a1 * pv.a[k] + a2 * sv.a[k];
+        }
+        st4(res, q, sv);
+        st4(dnext, q, dd);
+    }
+}
+
+// last sweep: d_s = c1 d_{s-1} + c2 (res - dinv t) ; z = d_0 + ... + d_{s-1} + d_s
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_cheb_last(int64_t n, const T *__restrict__ t,
+                                                           const T *__restrict__ dinv,
+                                                           const T *__restrict__ res,
+                                                           const T *__restrict__ dprev,
+                                                           const ChebSum<T> earlier, T *__restrict__ z,
+                                                           double c1, double c2, const SolverState *st) {
+    if (st && st->done) return;
+    const T a1 = (T)c1, a2 = (T)c2;
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> tv = ld4(t, q), dv = ld4(dinv, q), pv = ld4(dprev, q), sv = ld4(res, q);
+        V4<T> zv = earlier.n > 0 ? ld4(earlier.d[0], q) : pv;
+        for (int j = 1; j < earlier.n; ++j) {
+            const V4<T> w = ld4(earlier.d[j], q);
+            FG_K4 zv.a[k] += w.a[k];
+        }
+        FG_K4 {
+            if (earlier.n > 0) zv.a[k] += pv.a[k];
+            const T rs = sv.a[k] - dv.a[k] * tv.a[k];
+            const T dk = a1 * pv.a[k] + a2 * rs;
+            zv.a[k] += dk;
+        }
+        st4(z, q, zv);
+    }
+}
+
 // ||b - ap|| / bnorm into st->tmp[0] (true residual)
 __global__ void __launch_bounds__(VEC_THREADS) k_true_residual(int64_t n, const double *__restrict__ b,
                                                                const double *__restrict__ ap,
