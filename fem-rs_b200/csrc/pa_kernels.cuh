@@ -995,19 +995,6 @@ __device__ __forceinline__ T fixup_acc(const Grid &g, int I, int J, int K, int t
     return sum;
 }
 
-// The fix-up of any shared DOF (I, J, K), given the owner's value.
-template <typename T>
-__device__ __forceinline__ T fixup_sum(const Grid &g, int I, int J, int K, T own,
-                                       const T *__restrict__ face) {
-    const int P = g.p;
-    const int SXe = 32 * P, SYe = g.WY * P, SZe = g.TZ * P;
-    const int sx = (I > 0 && I < g.NI - 1 && I % SXe == 0);
-    const int sy = (J > 0 && J < g.NJ - 1 && J % SYe == 0);
-    const int sz = (K > 0 && K < g.NK - 1 && K % SZe == 0);
-    const int tx = min(I / SXe, g.ntx - 1), ty = min(J / SYe, g.nty - 1), tz = min(K / SZe, g.ntz - 1);
-    return fixup_acc<T>(g, I, J, K, tx, ty, tz, sx, sy, sz, own, face);
-}
-
 // Rows of shared-face DOFs: the x planes as NK rows of NJ DOFs (u -> J), the
 // y planes as NK rows of NI DOFs (u -> I), the z planes as NJ rows of NI DOFs
 // (u -> I); x planes first, then y, then z.
@@ -1018,8 +1005,9 @@ __host__ __device__ inline int fixup_rows(const Grid &g) {
 // One row of the fix-up, by the whole block.  Everything fixed along the row
 // (its plane, the owner item across the plane, the essential faces it lies on)
 // is worked out once; per DOF only the position along the row is classified,
-// by a division by the compile-time 32 P.  The sums are those of fixup_sum, in
-// the same order.  y planes skip DOFs on x planes, z planes skip DOFs on x or
+// by a division by the compile-time 32 P.  A DOF (I, J, K) with sx = (0 < I < NI-1
+// and I % 32P == 0), sy, sz alike, owned by item (min(I / 32P, ntx-1), ...), gets
+// the sum of fixup_acc.  y planes skip DOFs on x planes, z planes skip DOFs on x or
 // y planes; essential DOFs keep the owner's value.
 template <typename T, int P>
 __device__ __forceinline__ void fixup_row_t(const Grid &g, int r, T *__restrict__ y,
@@ -1124,7 +1112,7 @@ __device__ __forceinline__ void fixup_owner(const Grid &g, T *y, const T *face, 
 // in x, y and z).  The last of an owner's contributors to arrive (an arrival
 // count, not a wait: no CTA waits on another) resets the owner's counter for
 // the next launch and adds the face partials into the owner's lower-face DOFs:
-// the sums of fixup_sum in the same order, so the result is bit-identical to
+// the sums of fixup_acc in the same order, so the result is bit-identical to
 // fixup_kernel's.  `flag` is one int of shared memory that is free at this
 // point.
 template <typename T, int P>

@@ -199,7 +199,7 @@ def fixup_rows_visit(NI, NJ, NK, p, WY, TZ, ntx, nty, ntz, ess):
 def test_fixup_rows_cover_each_shared_dof_once(shape, p, WY, TZ, ess):
     """The row decomposition of the fix-up kernel visits exactly the shared,
     non-essential DOFs, once each, with the owner item and plane flags of the
-    per-DOF rule (fixup_sum)."""
+    per-DOF rule (the plane flags and owner item fixup_acc is given)."""
     nx, ny, nz = shape
     NI, NJ, NK = nx * p + 1, ny * p + 1, nz * p + 1
     ntx, nty, ntz = -(-nx // 32), -(-ny // WY), -(-nz // TZ)
@@ -209,7 +209,7 @@ def test_fixup_rows_cover_each_shared_dof_once(shape, p, WY, TZ, ess):
 
 
 def per_dof_rule(NI, NJ, NK, SX, SY, SZ, ntx, nty, ntz, ess):
-    """fixup_sum's classification of every DOF: shared (on a plane between
+    """The per-DOF classification of the fix-up: shared (on a plane between
     items) and not essential -> owner item and plane flags."""
     want = {}
     for K in range(NK):
