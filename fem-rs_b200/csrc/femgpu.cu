@@ -286,7 +286,10 @@ template <typename T> static int alloc_vec(T **p, int64_t n) {
 // ---------------------------------------------------------------------------
 template <int P> struct KCfg32;  // FP32 apply: same tile (WY) as FP64, deeper rings
 template <> struct KCfg32<1> { static constexpr int WY = 4, S = 6, MINB = 4; };
-template <> struct KCfg32<2> { static constexpr int WY = 4, S = 4, MINB = 3; };
+#ifndef FG_F32_Q2_S  // FP32 Q2 full-format qdata ring depth (stages of one quadrature column per warp)
+#define FG_F32_Q2_S 4
+#endif
+template <> struct KCfg32<2> { static constexpr int WY = 4, S = FG_F32_Q2_S, MINB = 3; };
 template <> struct KCfg32<3> { static constexpr int WY = FG_Q3_WY, S = 3, MINB = 2; };
 template <int P, typename T> struct KC;
 template <int P> struct KC<P, double> : KCfg<P> {};
