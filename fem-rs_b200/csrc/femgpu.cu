@@ -1136,7 +1136,11 @@ template <typename T>
 static int nn_fe_prolong(fg_op *op, const float *f1, T *z, const double *scale, double mult, int accumulate) {
     Grid g = op->g;
     g.ess = op->ess_tags;
-    fe_prolong_f32_kernel<T><<<VEC_GRID, 256, 0, op->stream>>>(g, f1, nn_vol(op, 1), z, scale, mult, accumulate);
+    if (g.NJ > 65535 || g.NK > 65535) return fail(FG_UNSUPPORTED, "prolongation grid: more than 65535 DOF rows");
+    const int pairs = g.NIp / 2;
+    const int bd = std::min(256, (pairs + 31) / 32 * 32);
+    const dim3 grid((pairs + bd - 1) / bd, g.NJ, g.NK);
+    fe_prolong_f32_kernel<T><<<grid, bd, 0, op->stream>>>(g, f1, nn_vol(op, 1), z, scale, mult, accumulate);
     CK(cudaGetLastError());
     return FG_OK;
 }

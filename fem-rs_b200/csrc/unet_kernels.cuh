@@ -647,35 +647,47 @@ __global__ void prolong_f32_kernel(const float *__restrict__ c, const Vol Vc, fl
 }
 
 // z (native, T) (+)= scale[0] * mult * P(cf) for an FP32 field cf on the
-// first coarse level; zero on essential DOFs and pads
+// first coarse level; zero on essential DOFs and pads.  Grid: x over pairs of
+// DOFs along a row (2m, 2m+1), y = J, z = K, so a thread does no index
+// division and every DOF of the vector has its own thread (a grid-stride loop
+// over 17M DOFs left each thread ~115 dependent iterations: 135 us instead of
+// the ~25 us its bytes take).
 template <typename T>
 __global__ void __launch_bounds__(256) fe_prolong_f32_kernel(const Grid g, const float *__restrict__ cf,
                                                              const Vol Vc, T *__restrict__ z,
                                                              const double *__restrict__ scale, double mult,
                                                              int accumulate) {
-    // native vectors of the coupled operators hold < 2^31 entries (checked by the host)
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J = blockIdx.y, K = blockIdx.z;
+    if (2 * m >= g.NIp) return;
     const double sc = (scale ? scale[0] : 1.0) * mult;
-    const uint32_t n = (uint32_t)g.NIp * (uint32_t)g.NJ * (uint32_t)g.NK;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t row = i / (uint32_t)g.NIp;
-        const int I = (int)(i - row * (uint32_t)g.NIp);
-        const int J = (int)(row % (uint32_t)g.NJ), K = (int)(row / (uint32_t)g.NJ);
+    const int64_t row = ((int64_t)K * g.NJ + J) * g.NIp;
+    const int64_t crow = ((int64_t)(K >> 1) * Vc.Y + (J >> 1)) * Vc.X;
+    const int oz = (K & 1) ? Vc.Y * Vc.X : 0, oy = (J & 1) ? Vc.X : 0;
+    const double wz = (K & 1) ? 0.5 : 1.0, wy = (J & 1) ? 0.5 : 1.0;
+    const double ay = oy ? wy : 0.0, az = oz ? wz : 0.0;
+    const bool ess_jk = ((g.ess & 1) && K == 0) || ((g.ess & 2) && K == g.NK - 1) ||
+                        ((g.ess & 4) && J == 0) || ((g.ess & 8) && J == g.NJ - 1);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {  // NIp is a multiple of 4: both DOFs of the pair exist
+        const int I = 2 * m + h;
         double s = 0.0;
-        if (I < g.NI && !g.is_ess(I, J, K)) {
-            const int64_t c0 = ((int64_t)(K >> 1) * Vc.Y + (J >> 1)) * Vc.X + (I >> 1);
-            const int oz = (K & 1) ? Vc.Y * Vc.X : 0, oy = (J & 1) ? Vc.X : 0, ox = I & 1;
-            const double wz = (K & 1) ? 0.5 : 1.0, wy = (J & 1) ? 0.5 : 1.0, wx = (I & 1) ? 0.5 : 1.0;
+        if (I < g.NI && !ess_jk && !(((g.ess & 16) && I == 0) || ((g.ess & 32) && I == g.NI - 1))) {
+            const int64_t c0 = crow + (I >> 1);
+            const int ox = I & 1;
+            const double wx = ox ? 0.5 : 1.0;
             // terms with a zero offset repeat the base value with weight 0 (same sum)
             const double f000 = cf[c0], f001 = cf[c0 + ox], f010 = cf[c0 + oy], f011 = cf[c0 + oy + ox];
             const double f100 = cf[c0 + oz], f101 = cf[c0 + oz + ox], f110 = cf[c0 + oz + oy],
                          f111 = cf[c0 + oz + oy + ox];
-            const double ax = ox ? wx : 0.0, ay = oy ? wy : 0.0, az = oz ? wz : 0.0;
+            const double ax = ox ? wx : 0.0;
             const double y0 = wx * f000 + ax * f001, y1 = wx * f010 + ax * f011;
             const double y2 = wx * f100 + ax * f101, y3 = wx * f110 + ax * f111;
             const double z0 = wy * y0 + ay * y1, z1 = wy * y2 + ay * y3;
             s = sc * (wz * z0 + az * z1);
         }
-        z[i] = accumulate ? (T)((double)z[i] + s) : (T)s;
+        T *zp = z + row + I;
+        *zp = accumulate ? (T)((double)*zp + s) : (T)s;
     }
 }
 
