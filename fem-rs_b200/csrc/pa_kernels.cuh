@@ -964,13 +964,15 @@ __global__ void __launch_bounds__(WY * 32) pa_diag_kernel(const ApplyArgs<T> A) 
 // planes, z planes skip DOFs on x or y planes.  32-bit index arithmetic except
 // the DOF offset.
 // ---------------------------------------------------------------------------
-// The neighbours' face-slot partials of one shared DOF added to `own` in
-// (dz, dy, dx) order.  (tx, ty, tz): the owner item; (sx, sy, sz): whether the
-// DOF lies on an x / y / z plane between items.
 template <bool CG, typename T> __device__ __forceinline__ T ld_face(const T *p) {
     if constexpr (CG) return __ldcg(p);  // written by other CTAs of the same launch: read at L2
     else return *p;
 }
+
+// The neighbours' face-slot partials of one shared DOF added to `own` in
+// (dz, dy, dx) order.  (tx, ty, tz): the owner item; (sx, sy, sz): whether the
+// DOF lies on an x / y / z plane between items.  CG: loads at L2 (the fused
+// fix-up reads slots other CTAs of the same launch wrote).
 template <typename T, bool CG = false>
 __device__ __forceinline__ T fixup_acc(const Grid &g, int I, int J, int K, int tx, int ty, int tz,
                                        int sx, int sy, int sz, T own, const T *__restrict__ face) {
