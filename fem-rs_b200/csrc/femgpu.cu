@@ -1228,8 +1228,8 @@ static int fcg_nn_run(fg_op *op, const PcgBufs<double> &B, const ChebCoef &cc, i
         if ((r2 = cheb_apply<double>(op, B, cc, B.r, B.z, skip))) return r2;
         if (nn_on && (r2 = nn_end<double>(op, f1, B.z))) return r2;
         k_fcg_zap<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.ap, op->partials, B.st, init);
-        k_pcg_pupdate<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.p, B.st, init);
-        k_fcg_pr<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.r, op->partials, B.st);
+        k_fcg_pupdate_pr<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.z, B.p, B.r, op->partials,
+                                                                            B.st, init);
         CK(cudaGetLastError());
         return FG_OK;
     };
@@ -1442,8 +1442,8 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
                 if (nn_on && (rc2 = nn_end<float>(op, f1, op->z32))) return rc2;
                 k_fcg_zap<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z32, op->ap32, op->partials,
                                                                            op->st, init);
-                k_pcg_pupdate<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z32, op->p32, op->st, init);
-                k_fcg_pr<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->p32, op->r32, op->partials, op->st);
+                k_fcg_pupdate_pr<float><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->z32, op->p32, op->r32,
+                                                                                   op->partials, op->st, init);
                 CK(cudaGetLastError());
                 return FG_OK;
             }
