@@ -967,8 +967,9 @@ __global__ void __launch_bounds__(VEC_THREADS) k_fcg_zap(int64_t n, const T *__r
 }
 
 // p = z + beta p (init: p = z) and rz = p . r in one pass: the values of
-// k_pcg_pupdate followed by k_fcg_pr (same loop order, same sums), one vector
-// pass and one launch fewer
+// k_pcg_pupdate followed by a separate p . r pass (same loop order, same sums),
+// one vector pass and one launch fewer.  rz is the FCG step numerator (alpha =
+// rz / pap in k_pcg_pap)
 template <typename T>
 __global__ void __launch_bounds__(VEC_THREADS) k_fcg_pupdate_pr(int64_t n, const T *__restrict__ z,
                                                                 T *__restrict__ p,
@@ -982,21 +983,6 @@ __global__ void __launch_bounds__(VEC_THREADS) k_fcg_pupdate_pr(int64_t n, const
         V4<T> pv = ld4(p, q);
         FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
         st4(p, q, pv);
-        FG_K4 v[0] += (double)pv.a[k] * (double)rv.a[k];
-    }
-    double tot[1];
-    if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0) st->rz = tot[0];
-}
-
-// rz = p . r (the FCG step numerator; alpha = rz / pap in k_pcg_pap)
-template <typename T>
-__global__ void __launch_bounds__(VEC_THREADS) k_fcg_pr(int64_t n, const T *__restrict__ p,
-                                                        const T *__restrict__ r, double *partials,
-                                                        SolverState *st) {
-    if (st->done) return;
-    double v[1] = {0.0};
-    FG_VEC4_LOOP(q, n) {
-        const V4<T> pv = ld4(p, q), rv = ld4(r, q);
         FG_K4 v[0] += (double)pv.a[k] * (double)rv.a[k];
     }
     double tot[1];
