@@ -106,6 +106,31 @@ def test_apply_is_deterministic_and_device_pointers_work():
     assert np.array_equal(yt.cpu().numpy(), a)
 
 
+@pytest.mark.parametrize("p,shape", [(1, (70, 9, 11)), (2, (40, 9, 17)), (3, (33, 5, 6))])
+def test_fused_fixup_option_is_bit_identical(p, shape, monkeypatch):
+    """FG_FUSED_FIXUP=1 (the fix-up done by the last contributing item inside
+    the apply kernel, a run-time option) gives the same bits as the separate
+    fix-up kernel, FP64 and FP32, raw and constrained, on multi-item grids."""
+    need_gpu()
+    mesh, coef, op = make_pair(shape, p, femgpu.MASS_DIFF, seed=9)
+    monkeypatch.setenv("FG_FUSED_FIXUP", "1")
+    _, _, fused = make_pair(shape, p, femgpu.MASS_DIFF, seed=9)
+    monkeypatch.delenv("FG_FUSED_FIXUP")
+    x = np.random.default_rng(3).normal(size=mesh.ndofs)
+    for constrained in (False, True):
+        for _ in range(2):  # the arrival counters reset themselves between launches
+            assert np.array_equal(fused.matvec(x, constrained=constrained), op.matvec(x, constrained=constrained))
+    xn = torch.from_numpy(op.to_native(x)).float().cuda()
+    ya, yb = torch.zeros_like(xn), torch.zeros_like(xn)
+    torch.cuda.synchronize()
+    op.apply_native_f32(xn.data_ptr(), ya.data_ptr())
+    fused.apply_native_f32(xn.data_ptr(), yb.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(ya, yb)
+    op.close()
+    fused.close()
+
+
 def test_native_layout_apply_matches_plain():
     need_gpu()
     mesh, coef, op = make_pair((33, 5, 6), 2, femgpu.MASS_DIFF, seed=2)
