@@ -2027,7 +2027,7 @@ FG_API int fg_batch_pcg(fg_op *const *ops, int n, const double *const *b, double
             for (int sidx = 0; sidx + 1 < cfg.cheb_degree; ++sidx) {
                 int r2 = apply32(1);
                 if (r2) return r2;
-                kb_cheb_step<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, sidx);
+                kb_cheb_step<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, sidx, sidx + 2 == cfg.cheb_degree ? 1 : 0);
             }
             kb_rz<<<vgrid, VEC_THREADS, 0, bs>>>(d_bv, init, 0);
         } else {

@@ -823,7 +823,9 @@ __global__ void __launch_bounds__(VEC_THREADS) kb_cheb_first(const BatchVec *bv)
     }
 }
 
-__global__ void __launch_bounds__(VEC_THREADS) kb_cheb_step(const BatchVec *bv, int s) {
+// last: the final sweep, whose residual and d are not needed afterwards (two
+// stores fewer; z is the same)
+__global__ void __launch_bounds__(VEC_THREADS) kb_cheb_step(const BatchVec *bv, int s, int last) {
     const BatchVec &B = bv[blockIdx.y];
     if (B.st->done) return;
     const float a1 = (float)B.c1[s], a2 = (float)B.c2[s];
@@ -835,8 +837,10 @@ __global__ void __launch_bounds__(VEC_THREADS) kb_cheb_step(const BatchVec *bv, 
             dd.a[k] = a1 * dd.a[k] + a2 * sv.a[k];
             zv.a[k] += dd.a[k];
         }
-        st4(B.cres, q, sv);
-        st4(B.cd, q, dd);
+        if (!last) {
+            st4(B.cres, q, sv);
+            st4(B.cd, q, dd);
+        }
         st4(B.z, q, zv);
     }
 }
