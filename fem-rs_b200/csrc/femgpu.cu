@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <functional>
 #include <cmath>
@@ -306,11 +307,13 @@ static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const 
     static_assert(C::WY == KCfg<P>::WY, "FP32 and FP64 share the item tiling");
     constexpr int S = FMT == 0 ? C::S : 2;  // affine format: one element layer per stage
     using SM = ApplySmem<P, T, C::WY, S, stage_elems<P, OPK, FMT>() / 32>;
-    static bool attr_set[64] = {};
+    // per device, set once; handles on several host threads may race here, and
+    // setting the same attribute twice is harmless
+    static std::atomic<bool> attr_set[64];
     auto kern = pa_apply_kernel<P, OPK, T, C::WY, S, C::MINB, FMT>;
-    if (!attr_set[op->device]) {
+    if (!attr_set[op->device].load(std::memory_order_acquire)) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
-        attr_set[op->device] = true;
+        attr_set[op->device].store(true, std::memory_order_release);
     }
     CUtensorMap tmap;
     cuuint64_t gdim[3] = {(cuuint64_t)g.NI, (cuuint64_t)g.NJ, (cuuint64_t)g.NK};
@@ -1569,12 +1572,13 @@ static int launch_batched_t(cudaStream_t st, const BatchGroup &G, const ApplyArg
     constexpr int S = FMT == 0 ? C::S : 2;
     using SM = ApplySmem<P, T, C::WY, S, stage_elems<P, OPK, FMT>() / 32>;
     auto kern = pa_apply_batched_kernel<P, OPK, T, C::WY, S, C::MINB, FMT>;
-    static bool attr_set[64] = {};
+    static std::atomic<bool> attr_set[64];
     int dev = 0;
     CK(cudaGetDevice(&dev));
-    if (!attr_set[dev]) {  // set once, before any capture (see fg_batch_pcg)
+    if (dev < 0 || dev >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", dev);
+    if (!attr_set[dev].load(std::memory_order_acquire)) {  // set once, before any capture (see fg_batch_pcg)
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
-        attr_set[dev] = true;
+        attr_set[dev].store(true, std::memory_order_release);
     }
     if (!args) return FG_OK;  // attribute preparation only
     BatchApply<T> B{args, tm, G.bmap, nslots, slot};
