@@ -154,7 +154,10 @@ FG_API int fg_op_set_stream(fg_op *op, void *stream);
  * constrained = 1 applies the Dirichlet elimination of the ess_tags DOFs
  * (rows and columns of essential DOFs replaced by the identity), the form the
  * solver uses.  x, y: plain lexicographic vectors of n_dofs doubles in host
- * (mem = FG_HOST) or device (FG_DEVICE) memory.  Synchronous. */
+ * (mem = FG_HOST) or device (FG_DEVICE) memory.  Synchronous.  Host vectors
+ * go through a device staging buffer of n_dofs values that the first
+ * host-memory call allocates; page-locked host memory runs the copies at full
+ * PCIe rate. */
 FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, int constrained,
                        int mem);
 
