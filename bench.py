@@ -10,11 +10,17 @@ vector; `value` is whole-job GDOF/s (DOFs of all ranks x steps / max-over-ranks
 device time).  `e2e` is the same metric through the public C ABI call
 (fg_op_apply on pinned host buffers: H2D copy of x, apply, D2H copy of y each
 step).  `solve` reports time to FP64 true relative residual 1e-8 of plain FP64
-PCG (Chebyshev(4) on D^-1 A, and Jacobi).
+PCG (Chebyshev(4) on D^-1 A) and of the chosen forms (FP32 applies inside FP64
+reliable updates, affine-compressed quadrature data, the learned coarse
+correction), for 128^3 Q2 and 64^3 Q3.
+
+The JSON line carries summaries; the full record (per-form iteration counts,
+autotuner table, heat, batch, tet details) goes to --detail (default
+gpurun_out/bench_detail.json when that folder exists).
 
 --impl reference times the reference's algorithm (the oracle port of
 crates/assembly/src/partial.rs's element loop with the Hex8 isoparametric
-Jacobian) on the host cores, on a z-slab sample of the same workload.
+Jacobian) on the host cores, on the same full mesh as the GPU arm.
 
 Multi-GPU: one independent instance per rank (its own seeded kappa), no
 data-path collective; scaling is weak.
@@ -150,16 +156,53 @@ def whole_job_gdofs(world, n_dofs, steps, t_ms):
     return world * n_dofs * steps / (t_ms / 1e3) / 1e9
 
 
-def cpu_apply_sample(n, p, kq_full, reps=2, layers=None):
-    """Oracle (reference-algorithm port) apply on a z-slab of the workload, all
-    host threads.  Returns (GDOF/s, threads, description)."""
+def host_threads():
+    """Host threads this process may run on (the CPU baseline uses all of
+    them, whatever OMP_NUM_THREADS a launcher such as torchrun has set)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def bench_config(n, p, world):
+    """The workload description shared by both arms of the bench."""
+    N = (n * p + 1) ** 3
+    return {"workload": f"{n}^3 Q{p} unit-cube hex, FP64 PA diffusion apply (constrained), {N} DOFs per rank",
+            "order": p, "n_elem_1d": n,
+            "l2": "inputs larger than L2 (qdata %.2f GB per apply)" % (6 * (p + 1) ** 3 * n ** 3 * 8 / 1e9),
+            "parallelism": f"{world} independent instances"}
+
+
+def dirichlet_rhs(n, p):
+    """Load of the scale-up configuration: M sin(pi x) sin(pi y) sin(pi z) with
+    the Dirichlet rows zeroed."""
+    import femgpu
+    from femgpu.fields import sin_nodal
+
+    mass = femgpu.PAMassOperator((n, n, n), p)
+    b = mass.matvec(sin_nodal(n, n, n, p))
+    mass.close()
+    s = n * p + 1
+    bb = b.reshape(s, s, s)
+    bb[0], bb[-1], bb[:, 0], bb[:, -1], bb[:, :, 0], bb[:, :, -1] = 0, 0, 0, 0, 0, 0
+    return b
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (the oracle port of the reference algorithm; outside every timed
+# GPU region)
+# ---------------------------------------------------------------------------
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
+    return O
 
-    nzs = layers or max(1, n // 8)
-    q3 = (p + 1) ** 3
-    kq = np.ascontiguousarray(kq_full[: n * n * nzs * q3])
-    mesh = O.Mesh(n, n, nzs, p)
+
+def cpu_apply_time(n, p, kq, reps):
+    """Seconds per oracle apply on the full mesh, all host threads."""
+    O = _oracle()
+    mesh = O.Mesh(n, n, n, p)
     coef = O.Coef(O.DIFF, kappa_q=kq)
     x = np.random.default_rng(1).standard_normal(mesh.ndofs)
     y = np.zeros(mesh.ndofs)
@@ -168,19 +211,41 @@ def cpu_apply_sample(n, p, kq_full, reps=2, layers=None):
     t0 = time.perf_counter()
     for _ in range(reps):
         O.pa_apply(mesh, coef, x, y, nthreads=cores)
-    dt = (time.perf_counter() - t0) / reps
-    desc = (f"oracle port of the reference PA element loop (partial.rs:154-208 + assembler.rs:96-143), "
-            f"{n}x{n}x{nzs} Q{p} z-slab of the workload ({mesh.ndofs} DOFs), {reps} applies, "
-            f"OpenMP {cores} threads")
-    return mesh.ndofs / dt / 1e9, cores, desc
+    return (time.perf_counter() - t0) / reps, mesh.ndofs, cores
+
+
+def cpu_solve_extrapolated(n, p, kq, gpu_iterations, t_apply):
+    """Time to 1e-8 of the reference algorithm's Chebyshev(4)-PCG on the host
+    cores, extrapolated: the per-iteration time measured over 2 iterations of
+    the oracle's PCG on the full mesh (difference of 3 and 1 iterations, so
+    set-up cancels), times the GPU plain solve's iteration count, plus the 20
+    power-iteration applies of the lambda_max estimate at the measured apply
+    time."""
+    O = _oracle()
+    mesh = O.Mesh(n, n, n, p)
+    coef = O.Coef(O.DIFF, kappa_q=kq)
+    mask = O.ess_mask(mesh)
+    b = dirichlet_rhs(n, p)
+    cores = host_threads()
+    lm = 1.0  # any bounds: the iteration cost does not depend on them
+    ts = []
+    for k in (1, 3):
+        t0 = time.perf_counter()
+        O.pcg(mesh, coef, mask, b, precond=2, cheb_degree=4, lmin=lm / 30, lmax=lm, rtol=1e-30,
+              max_iter=k, nthreads=cores)
+        ts.append(time.perf_counter() - t0)
+    t_iter = max(ts[1] - ts[0], 0.0) / 2
+    total = 20 * t_apply + gpu_iterations * t_iter
+    return {"kind": "extrapolated", "t_iter_s": t_iter, "t_apply_s": t_apply, "iterations": gpu_iterations,
+            "time_to_1e8_s": total, "cores": cores,
+            "method": "oracle Chebyshev(4)-PCG (par_solver.rs:262-342 loop) per-iteration time on the full "
+                      "mesh x the GPU plain FP64 iteration count + 20 lambda_max applies"}
 
 
 def cpu_ex1_pipeline(n=24):
     """The mfem_ex1 pipeline through the oracle port on the host cores: source
     form, PCG-Jacobi to rtol 1e-10, L2 error (24^3 Q1 Poisson)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-
+    O = _oracle()
     cores = host_threads()
     t0 = time.perf_counter()
     mesh = O.Mesh(n, n, n, 1)
@@ -192,52 +257,349 @@ def cpu_ex1_pipeline(n=24):
             "threads": cores}
 
 
-def host_threads():
-    """Host threads this process may run on (the CPU baseline uses all of
-    them, whatever OMP_NUM_THREADS a launcher such as torchrun has set)."""
-    try:
-        return len(os.sched_getaffinity(0))
-    except AttributeError:
-        return os.cpu_count() or 1
-
-
 def run_reference(args, n, p):
+    """The reference arm: the oracle port of the reference PA element loop on
+    the host cores, on the GPU arm's full mesh and kappa (seed 0).  If the
+    warm-up shows that --steps full applies would take longer than about four
+    minutes, each step is a z-slab of the mesh instead (stated in `sample`)."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return
     from femgpu.fields import lognormal_kappa_q
 
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-
-    nzs = max(1, n // 32)
-    q3 = (p + 1) ** 3
-    kq = lognormal_kappa_q(n, n, n, p, seed=0)[: n * n * nzs * q3].copy()
-    mesh = O.Mesh(n, n, nzs, p)
-    coef = O.Coef(O.DIFF, kappa_q=kq)
-    x = np.random.default_rng(1).standard_normal(mesh.ndofs)
-    y = np.zeros(mesh.ndofs)
+    O = _oracle()
+    kq_full = lognormal_kappa_q(n, n, n, p, seed=0)
     cores = host_threads()
+    q3 = (p + 1) ** 3
+
+    def setup(nz):
+        kq = kq_full if nz == n else np.ascontiguousarray(kq_full[: n * n * nz * q3])
+        mesh = O.Mesh(n, n, nz, p)
+        coef = O.Coef(O.DIFF, kappa_q=kq)
+        x = np.random.default_rng(1).standard_normal(mesh.ndofs)
+        return mesh, coef, x, np.zeros(mesh.ndofs)
+
+    nzs = n
+    mesh, coef, x, y = setup(nzs)
+    t0 = time.perf_counter()
     for _ in range(args.warmup):
+        O.pa_apply(mesh, coef, x, y, nthreads=cores)
+    t_w = (time.perf_counter() - t0) / max(args.warmup, 1)
+    if t_w * args.steps > 240.0:
+        nzs = max(1, int(n * 240.0 / (t_w * args.steps)))
+        mesh, coef, x, y = setup(nzs)
         O.pa_apply(mesh, coef, x, y, nthreads=cores)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         O.pa_apply(mesh, coef, x, y, nthreads=cores)
     dt = time.perf_counter() - t0
     val = mesh.ndofs * args.steps / dt / 1e9
+    sample = (f"the full {n}^3 Q{p} mesh ({mesh.ndofs} DOFs) per step" if nzs == n else
+              f"{n}x{n}x{nzs} Q{p} z-slab ({mesh.ndofs} DOFs) per step (full-mesh steps would exceed 4 min)")
     out = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "GDOF/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: lognormal kappa GRF (sigma2=1, ell=0.1, seed 0) at Gauss points, x ~ N(0,1)",
-        "config": {"workload": f"{n}^3 Q{p} FP64 PA diffusion apply (sample: {n}x{n}x{nzs} z-slab)",
-                   "order": p, "n_elem_1d": n, "l2": "inputs larger than L2 not applicable on CPU"},
+        "config": bench_config(n, p, world),
         "cpu_baseline": {"value": val, "unit": "GDOF/s", "cores": cores, "kind": "port",
-                         "sample": f"{n}x{n}x{nzs} Q{p} z-slab ({mesh.ndofs} DOFs) per step, OpenMP {cores} threads; "
-                                   "the reference (Rust) cannot be built here, so this is the C restatement of its algorithm"},
+                         "sample": f"{sample}, OpenMP {cores} threads; the reference (Rust) cannot be built "
+                                   "here, so this is the C restatement of its algorithm"},
         "e2e": {"value": val, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU sections
+# ---------------------------------------------------------------------------
+def learned_weights(n, p):
+    return os.path.join(ROOT, "fem-rs_b200", "femgpu", "weights", f"unet_q{p}_{n}.npz")
+
+
+def run_solves(op, n, p, kq, rank):
+    """Time to FP64 true relative residual 1e-8 for every form on one operator.
+    Returns (summary, detail)."""
+    import femgpu
+
+    b = dirichlet_rhs(n, p)
+    N = op.n_dofs()
+    detail = {}
+    x_plain = None
+    runs = (("plain_fp64_chebyshev4", femgpu.PC_CHEBYSHEV, femgpu.FP64, femgpu.QDATA_FULL),
+            ("plain_fp64_jacobi", femgpu.PC_JACOBI, femgpu.FP64, femgpu.QDATA_FULL),
+            ("fp32_ir_chebyshev4", femgpu.PC_CHEBYSHEV, femgpu.FP32_IR, femgpu.QDATA_FULL),
+            ("plain_fp64_chebyshev4_affine", femgpu.PC_CHEBYSHEV, femgpu.FP64, femgpu.QDATA_AFFINE),
+            ("fp32_ir_chebyshev4_affine", femgpu.PC_CHEBYSHEV, femgpu.FP32_IR, femgpu.QDATA_AFFINE))
+    for name, pc, prec, fmt in runs:
+        op.set_qdata_format(fmt)
+        xs = np.zeros(N)
+        r = op.pcg(b, xs, femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec), pc)
+        if x_plain is None:
+            x_plain = xs.copy()
+        detail[name] = {"iterations": r.iterations, "reliable_updates": r.outer_iterations if prec else 0,
+                        "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual, "converged": r.converged,
+                        "applies": r.applies, "lmax": r.lmax if pc == femgpu.PC_CHEBYSHEV else None,
+                        "rel_err_vs_plain_fp64": float(np.linalg.norm(xs - x_plain) / np.linalg.norm(x_plain))}
+    op.set_qdata_format(femgpu.QDATA_FULL)
+
+    # learned coarse correction (flexible CG, z = Chebyshev(r) + network
+    # correction) with the committed weights trained for this mesh and order on
+    # other kappa seeds; budget = the plain iteration count of the same form
+    wpath = learned_weights(n, p)
+    if os.path.exists(wpath):
+        from femgpu import learned as learned_mod
+        net, meta = learned_mod.load(wpath)
+        if meta["first_seed"] <= rank < meta["first_seed"] + meta["train_fields"]:
+            detail["learned_skipped"] = f"kappa seed {rank} is a training seed of {os.path.basename(wpath)}"
+        else:
+            femgpu.set_nodal_kappa(op, femgpu.nodal_kappa_from_q(kq, n, n, n, p), int(meta["levels"]))
+            femgpu.attach_unet(op, net)
+            for name, prec, fmt, plain_key in (
+                    ("learned_fp64_chebyshev4", femgpu.FP64, femgpu.QDATA_FULL, "plain_fp64_chebyshev4"),
+                    ("learned_fp32_ir_chebyshev4", femgpu.FP32_IR, femgpu.QDATA_FULL, "fp32_ir_chebyshev4"),
+                    ("learned_fp32_ir_chebyshev4_affine", femgpu.FP32_IR, femgpu.QDATA_AFFINE,
+                     "fp32_ir_chebyshev4_affine")):
+                op.set_qdata_format(fmt)
+                xs = np.zeros(N)
+                cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec,
+                                          nn_budget=detail[plain_key]["iterations"])
+                r = op.pcg(b, xs, cfg, femgpu.PC_CHEB_NN)
+                detail[name] = {
+                    "iterations": r.iterations, "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual,
+                    "converged": r.converged, "nn_fallback": r.extra["nn_fallback"],
+                    "iterations_of_plain_same_form": detail[plain_key]["iterations"],
+                    "rel_err_vs_plain_fp64": float(np.linalg.norm(xs - x_plain) / np.linalg.norm(x_plain))}
+            femgpu.attach_unet(op, None)
+            op.set_qdata_format(femgpu.QDATA_FULL)
+            detail["learned_weights"] = {"file": os.path.relpath(wpath, ROOT), "levels": meta["levels"],
+                                         "train_fields": meta["train_fields"], "first_seed": meta["first_seed"],
+                                         "params": meta["params"]}
+        del net
+
+    plain = detail["plain_fp64_chebyshev4"]["solve_s"]
+    short = {"plain_fp64_chebyshev4": "plain", "plain_fp64_jacobi": "plain_jacobi", "fp32_ir_chebyshev4": "fp32",
+             "plain_fp64_chebyshev4_affine": "fp64_affine", "fp32_ir_chebyshev4_affine": "fp32_affine",
+             "learned_fp64_chebyshev4": "nn_fp64", "learned_fp32_ir_chebyshev4": "nn_fp32",
+             "learned_fp32_ir_chebyshev4_affine": "nn_fp32_affine"}
+    summary = {"dofs": N}
+    for k, s in short.items():
+        if k in detail:
+            d = detail[k]
+            summary[s] = [round(d["solve_s"], 4), d["iterations"]]
+    summary["max_rel_err_vs_plain"] = max(d["rel_err_vs_plain_fp64"] for k, d in detail.items() if k in short)
+    summary["all_converged"] = all(d["converged"] for k, d in detail.items() if k in short)
+    sp = {}
+    for k, s in short.items():
+        if k in detail and s != "plain":
+            sp[s] = round(plain / detail[k]["solve_s"], 3)
+    if "learned_fp32_ir_chebyshev4" in detail:
+        # like-for-like: learned vs plain in the same precision and qdata format
+        sp["nn_fp32_vs_fp32"] = round(detail["fp32_ir_chebyshev4"]["solve_s"]
+                                      / detail["learned_fp32_ir_chebyshev4"]["solve_s"], 3)
+        sp["nn_fp32_affine_vs_fp32_affine"] = round(
+            detail["fp32_ir_chebyshev4_affine"]["solve_s"] / detail["learned_fp32_ir_chebyshev4_affine"]["solve_s"], 3)
+    summary["speedup_vs_plain"] = sp
+    summary["format"] = "[solve_s, iterations]; plain = drop-in FP64 Chebyshev(4) PCG on full qdata"
+    return summary, detail
+
+
+def time_apply_variants(op, n, p, x, steps, peak, stream):
+    """FP64 / FP32 applies on the full and the affine-compressed quadrature
+    data, CUDA events on the launching stream."""
+    import torch
+
+    import femgpu
+
+    x32 = x.float()
+    y = torch.zeros_like(x)
+    y32 = torch.zeros_like(x32)
+
+    def time_apply(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(steps):
+            fn()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        return g0.elapsed_time(g1) / steps
+
+    E, q3, N = n ** 3, (p + 1) ** 3, op.n_dofs()
+    out = {}
+    for fmt, tag in ((femgpu.QDATA_FULL, "full"), (femgpu.QDATA_AFFINE, "affine")):
+        op.set_qdata_format(fmt)
+        for prec, es in (("fp64", 8), ("fp32", 4)):
+            if prec == "fp64":
+                t = time_apply(lambda: op.apply_native(x.data_ptr(), y.data_ptr()))
+            else:
+                t = time_apply(lambda: op.apply_native_f32(x32.data_ptr(), y32.data_ptr()))
+            qbytes = (6 * q3 * E if tag == "full" else (6 + q3) * E) * es
+            nbytes = qbytes + 2 * N * es
+            out[f"{prec}_{tag}"] = {"ms": round(t, 5), "gdof_s": round(N / (t / 1e3) / 1e9, 3),
+                                    "frac": round(nbytes / (t / 1e3) / 1e9 / peak, 4)}
+    op.set_qdata_format(femgpu.QDATA_FULL)
+    return out
+
+
+def run_heat(rank, steps, stream):
+    """SDIRK-2 heat stepping, 64^3 Q2, lognormal kappa, dt = 1e-3, u0 = sin sin sin."""
+    import femgpu
+    from femgpu.fields import lognormal_kappa_q
+
+    hn, hp, dt = 64, 2, 1e-3
+    hk = lognormal_kappa_q(hn, hn, hn, hp, sigma2=1.0, ell=0.1, seed=rank)
+    K = femgpu.PADiffusionOperator((hn, hn, hn), hp, kappa=hk)
+    S = femgpu.PAMassDiffusionOperator((hn, hn, hn), hp, 1.0, femgpu.SDIRK2_GAMMA * dt, kappa=hk)
+    K.set_stream(stream.cuda_stream)
+    S.set_stream(stream.cuda_stream)
+    xs1 = np.linspace(0, 1, hn * hp + 1)
+    u0 = (np.sin(np.pi * xs1)[:, None, None] * np.sin(np.pi * xs1)[None, :, None]
+          * np.sin(np.pi * xs1)[None, None, :])
+    u0[[0, -1]], u0[:, [0, -1]], u0[:, :, [0, -1]] = 0.0, 0.0, 0.0
+    u0 = u0.ravel()
+    detail = {"workload": f"{hn}^3 Q2 SDIRK-2, dt={dt}, {steps} steps, stage rtol 1e-10, warm start"}
+    finals = {}
+    for name, prec, fmt in (("fp64", femgpu.FP64, femgpu.QDATA_FULL),
+                            ("fp32", femgpu.FP32_IR, femgpu.QDATA_FULL),
+                            ("fp32_affine", femgpu.FP32_IR, femgpu.QDATA_AFFINE)):
+        K.set_qdata_format(fmt)
+        S.set_qdata_format(fmt)
+        u = u0.copy()
+        info = femgpu.sdirk2(K, S, u, dt, steps, femgpu.SolverConfig(rtol=1e-10, max_iter=5000, precision=prec),
+                             femgpu.PC_CHEBYSHEV)
+        finals[name] = u
+        detail[name] = {"time_s": info["time_ms"] / 1e3, "stage_iterations": info["total_iterations"],
+                        "max_stage_iterations": info["max_stage_iterations"], "applies": info["applies"]}
+    ref = finals["fp64"]
+    for name in finals:
+        detail[name]["rel_l2_diff_vs_fp64"] = float(np.linalg.norm(finals[name] - ref) / np.linalg.norm(ref))
+    K.close()
+    S.close()
+    summary = {k: [round(detail[k]["time_s"], 3), detail[k]["stage_iterations"], detail[k]["rel_l2_diff_vs_fp64"]]
+               for k in ("fp64", "fp32", "fp32_affine")}
+    summary["format"] = "[time_s, stage_iterations, rel_l2_diff_vs_fp64]"
+    summary["speedup_fp32_affine"] = round(detail["fp64"]["time_s"] / detail["fp32_affine"]["time_s"], 3)
+    return summary, detail
+
+
+def run_batch(rank, batch_n, dev):
+    """256 uneven solves, n ~ U{8..48}, p ~ U{1,2,3}, own lognormal kappa
+    (sigma2 ~ U[0.25,2], ell ~ U[0.05,0.3]) and RHS M xi, FP32 mixed precision."""
+    import femgpu
+    from femgpu.fields import lognormal_kappa_q
+
+    brng = np.random.default_rng(7000 + rank)
+    bops, bbs = [], []
+    total = 0
+    t_setup = time.perf_counter()
+    for i in range(batch_n):
+        bn, bp = int(brng.integers(8, 49)), int(brng.integers(1, 4))
+        kq = lognormal_kappa_q(bn, bn, bn, bp, sigma2=float(brng.uniform(0.25, 2.0)),
+                               ell=float(brng.uniform(0.05, 0.3)), seed=100000 * rank + i, device=dev)
+        o = femgpu.PADiffusionOperator((bn, bn, bn), bp, kappa=kq)
+        m = femgpu.PAMassOperator((bn, bn, bn), bp)
+        bb = m.matvec(brng.standard_normal(o.n_dofs()))
+        m.close()
+        bb3 = bb.reshape(o.NK, o.NJ, o.NI)
+        bb3[[0, -1]], bb3[:, [0, -1]], bb3[:, :, [0, -1]] = 0.0, 0.0, 0.0
+        bops.append(o)
+        bbs.append(bb)
+        total += o.n_dofs()
+    t_setup = time.perf_counter() - t_setup
+    cfgb = femgpu.SolverConfig(rtol=1e-8, max_iter=5000, precision=femgpu.FP32_IR, check_interval=10)
+
+    def sequential():
+        t, its = 0.0, []
+        for o, v in zip(bops, bbs):
+            r1 = o.pcg(v, np.zeros_like(v), cfgb, femgpu.PC_CHEBYSHEV)
+            t += r1.solve_ms / 1e3
+            its.append(r1.iterations)
+        return t, its
+
+    t_seq0, seq_iters = sequential()  # default tiles
+    bxs = [np.zeros_like(v) for v in bbs]
+    ok0, bres0 = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
+    t_batch0 = bres0[0].solve_ms / 1e3
+    t_tune = time.perf_counter()
+    tune = femgpu.batch_autotune(bops, reps=3)
+    t_tune = time.perf_counter() - t_tune
+    t_seq, _ = sequential()  # tuned tiles: the batching gain alone
+    bxs = [np.zeros_like(v) for v in bbs]
+    ok, bres = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
+    t_batch = bres[0].solve_ms / 1e3
+    for o in bops:
+        o.close()
+    summary = {"instances": len(bops), "total_dofs": total, "all_converged": bool(ok and ok0),
+               "max_true_residual": max(r.true_residual for r in bres),
+               "iterations_min_max": [min(r.iterations for r in bres), max(r.iterations for r in bres)],
+               "max_iteration_diff_vs_single": int(max(abs(a.iterations - b) for a, b in zip(bres, seq_iters))),
+               "sequential_default_tiles_s": round(t_seq0, 3), "sequential_tuned_tiles_s": round(t_seq, 3),
+               "batched_default_tiles_s": round(t_batch0, 3), "batched_tuned_s": round(t_batch, 3),
+               "speedup_batching_same_tiles": round(t_seq / t_batch, 3),
+               "speedup_autotune_batched": round(t_batch0 / t_batch, 3)}
+    detail = dict(summary, setup_s=t_setup, autotune_s=t_tune,
+                  dof_iterations_per_s=sum(o.n_dofs() * r.iterations for o, r in zip(bops, bres)) / t_batch,
+                  autotune=[{"order": e["order"], "size_class": e["size_class"], "instances": e["instances"],
+                             "tz": e["tz"], "us_per_candidate_tz": e["us"]} for e in tune])
+    return summary, detail
+
+
+def run_tet(dev, peak):
+    """Tetrahedral PA apply (TetP1/TetP2 on unit_cube_tet, partial.rs on Tet4)."""
+    import torch
+
+    import femgpu
+    from femgpu import tet as tetmesh
+
+    out = {}
+    for tn, tp in ((64, 2), (96, 1)):
+        coords, dofs, nd, mask = tetmesh.unit_cube_space(tn, tp)
+        top = femgpu.TetOperator(tp, coords, dofs, nd, quad_order=2 * tp, ess=mask)
+        xt = torch.randn(nd, dtype=torch.float64, device=dev)
+        yt = torch.zeros_like(xt)
+        for _ in range(3):
+            top.apply_zero(xt, yt, True)
+        torch.cuda.synchronize()
+        reps = 20
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            top.apply_zero(xt, yt, True)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / reps
+        E, nl, nqt = dofs.shape[0], dofs.shape[1], top.nq
+        # algorithmic bytes: element map, geometry, per-point scalars, x gathered once, y written once
+        ab = E * (nl * 4 + 6 * 8 + nqt * 8) + nd * (8 + 8)
+        out[f"p{tp}_n{tn}"] = {"elements": int(E), "dofs": int(nd), "ms": round(dt * 1e3, 4),
+                               "gdof_s": round(nd / dt / 1e9, 3), "frac_algorithmic": round(ab / dt / 1e9 / peak, 4)}
+        top.close()
+        del xt, yt
+    out["timing"] = "host wall clock over 20 synchronised applies"
+    return out
+
+
+def run_ex1():
+    """mfem_ex1 on 24^3 Q1: source form, PCG-Jacobi rtol 1e-10, L2 error, on the GPU."""
+    import torch
+
+    import femgpu
+
+    n1 = 24
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    op1 = femgpu.PADiffusionOperator((n1, n1, n1), 1)
+    qp2 = femgpu.quadrature_points(n1, n1, n1, 2)
+    b1 = femgpu.assemble_source(n1, n1, n1, 1, 3 * np.pi ** 2 * np.prod(np.sin(np.pi * qp2), axis=-1))
+    x1 = np.zeros(op1.n_dofs())
+    r1 = femgpu.solve_pcg_jacobi(op1, b1, x1, femgpu.SolverConfig(rtol=1e-10, max_iter=2000))
+    qp3 = femgpu.quadrature_points(n1, n1, n1, 3)
+    err1 = femgpu.l2_error(n1, n1, n1, 1, x1, np.prod(np.sin(np.pi * qp3), axis=-1), nq=3)
+    t_ex1 = time.perf_counter() - t0
+    op1.close()
+    return {"iterations": r1.iterations, "l2_error": err1, "pipeline_s": round(t_ex1, 4),
+            "converged": r1.converged}
 
 
 def main():
@@ -247,12 +609,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="q2_128", choices=sorted(WORKLOADS))
-    ap.add_argument("--no-solve", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-heat", action="store_true")
-    ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--no-tet", action="store_true")
-    ap.add_argument("--no-ex1", action="store_true")
+    ap.add_argument("--detail", default=None, help="file for the full record (default: gpurun_out/bench_detail.json "
+                                                   "if that folder exists)")
+    for opt in ("solve", "q3", "cpu", "heat", "batch", "tet", "ex1"):
+        ap.add_argument(f"--no-{opt}", action="store_true")
     ap.add_argument("--batch-n", type=int, default=256)
     ap.add_argument("--heat-steps", type=int, default=500)
     args = ap.parse_args()
@@ -267,7 +627,7 @@ def main():
     import torch.distributed as dist
 
     import femgpu
-    from femgpu.fields import lognormal_kappa_q, sin_nodal
+    from femgpu.fields import lognormal_kappa_q
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
@@ -331,284 +691,59 @@ def main():
         op.apply_zero(xh, yh, constrained=True)
     f1.record(stream)
     torch.cuda.synchronize()
-    te_ms = f0.elapsed_time(f1)
-    te_ms = max_over_ranks(te_ms, world, dev)
+    te_ms = max_over_ranks(f0.elapsed_time(f1), world, dev)
     e2e_val = whole_job_gdofs(world, N, k_e2e, te_ms)
     _ = float(yh[0])
 
+    detail = {}
+    variants = time_apply_variants(op, n, p, x, args.steps, peak, stream)
     solve = None
     if not args.no_solve:
         solve = {}
-        mass = femgpu.PAMassOperator((n, n, n), p)
-        mass.set_stream(stream.cuda_stream)
-        b = np.zeros(N)
-        mass.apply_zero(sin_nodal(n, n, n, p), b, constrained=False)
-        # homogeneous Dirichlet: zero boundary rows of the RHS
-        bb = b.reshape(op.NK, op.NJ, op.NI)
-        bb[0], bb[-1], bb[:, 0], bb[:, -1], bb[:, :, 0], bb[:, :, -1] = 0, 0, 0, 0, 0, 0
-        mass.close()
-        runs = (("plain_fp64_chebyshev4", femgpu.PC_CHEBYSHEV, femgpu.FP64),
-                ("plain_fp64_jacobi", femgpu.PC_JACOBI, femgpu.FP64),
-                ("fp32_ir_chebyshev4", femgpu.PC_CHEBYSHEV, femgpu.FP32_IR),
-                ("fp32_ir_jacobi", femgpu.PC_JACOBI, femgpu.FP32_IR))
-        x_plain = None
-        for fmt, suffix in ((femgpu.QDATA_FULL, ""), (femgpu.QDATA_AFFINE, "_affine")):
-            op.set_qdata_format(fmt)
-            for name, pc, prec in runs:
-                xs = np.zeros(N)
-                cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec)
-                r = op.pcg(b, xs, cfg, pc)
-                if x_plain is None:
-                    x_plain = xs.copy()
-                solve[name + suffix] = {
-                    "iterations": r.iterations, "reliable_updates": r.outer_iterations if prec else 0,
-                    "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual, "converged": r.converged,
-                    "applies": r.applies, "lmax": r.lmax if pc == femgpu.PC_CHEBYSHEV else None,
-                    "rel_err_vs_plain_fp64_chebyshev": float(np.linalg.norm(xs - x_plain) / np.linalg.norm(x_plain))}
-        op.set_qdata_format(femgpu.QDATA_FULL)
+        solve[args.workload], detail["solve_" + args.workload] = run_solves(op, n, p, kq, rank)
+    del x, y
 
-        def best(keys):
-            return min(solve[k]["solve_s"] for k in keys)
-        plain = best(["plain_fp64_chebyshev4", "plain_fp64_jacobi"])
-        solve["speedup"] = {
-            "fp32_vs_plain_same_full_qdata": plain / best(["fp32_ir_chebyshev4", "fp32_ir_jacobi"]),
-            "fp32_affine_vs_plain_full_qdata": plain / best(["fp32_ir_chebyshev4_affine", "fp32_ir_jacobi_affine"]),
-            "fp32_affine_vs_plain_affine": best(["plain_fp64_chebyshev4_affine", "plain_fp64_jacobi_affine"])
-            / best(["fp32_ir_chebyshev4_affine", "fp32_ir_jacobi_affine"]),
-            "note": "plain = drop-in FP64 PCG with the full (general-geometry) quadrature data; "
-                    "_affine = compressed qdata valid for constant-J elements, reported as such"}
+    # the 64^3 Q3 configuration beside the headline mesh: applies and solves
+    q3 = None
+    if not args.no_q3 and (n, p) == (128, 2):
+        qn, qp = WORKLOADS["q3_64"]
+        kq3 = lognormal_kappa_q(qn, qn, qn, qp, sigma2=1.0, ell=0.1, seed=rank)
+        op3 = femgpu.PADiffusionOperator((qn, qn, qn), qp, kappa=kq3)
+        op3.set_stream(stream.cuda_stream)
+        x3 = torch.from_numpy(op3.to_native(gen.standard_normal(op3.n_dofs()))).to(dev)
+        q3 = {"apply": time_apply_variants(op3, qn, qp, x3, args.steps, peak, stream)}
+        del x3
+        if solve is not None:
+            solve["q3_64"], detail["solve_q3_64"] = run_solves(op3, qn, qp, kq3, rank)
+        op3.close()
+        del kq3
 
-        # learned coarse correction (flexible CG, z = Chebyshev(r) + network
-        # correction) with the committed weights trained for this mesh and order
-        # on other kappa seeds; budget = the plain iteration count of the same
-        # form, beyond which the solve falls back to plain Chebyshev-PCG
-        wpath = os.path.join(ROOT, "fem-rs_b200", "femgpu", "weights", f"unet_q{p}_{n}.npz")
-        meta = None
-        if os.path.exists(wpath):
-            from femgpu import learned as learned_mod
-            net, meta = learned_mod.load(wpath)
-            if meta["first_seed"] <= rank < meta["first_seed"] + meta["train_fields"]:
-                # this rank's kappa seed was a training field: no held-out number
-                solve["learned_skipped"] = f"kappa seed {rank} is among the training seeds of {os.path.basename(wpath)}"
-                meta = None
-        if meta is not None:
-            femgpu.set_nodal_kappa(op, femgpu.nodal_kappa_from_q(kq, n, n, n, p), int(meta["levels"]))
-            femgpu.attach_unet(op, net)
-            for name, prec, fmt, plain_key in (
-                    ("learned_fp64_chebyshev4", femgpu.FP64, femgpu.QDATA_FULL, "plain_fp64_chebyshev4"),
-                    ("learned_fp32_ir_chebyshev4_affine", femgpu.FP32_IR, femgpu.QDATA_AFFINE,
-                     "fp32_ir_chebyshev4_affine")):
-                op.set_qdata_format(fmt)
-                xs = np.zeros(N)
-                cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec,
-                                          nn_budget=solve[plain_key]["iterations"])
-                r = op.pcg(b, xs, cfg, femgpu.PC_CHEB_NN)
-                solve[name] = {
-                    "iterations": r.iterations, "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual,
-                    "converged": r.converged, "nn_fallback": r.extra["nn_fallback"],
-                    "iterations_of_plain_same_form": solve[plain_key]["iterations"],
-                    "rel_err_vs_plain_fp64_chebyshev": float(np.linalg.norm(xs - x_plain) / np.linalg.norm(x_plain))}
-            femgpu.attach_unet(op, None)
-            op.set_qdata_format(femgpu.QDATA_FULL)
-            solve["learned_weights"] = {"file": os.path.relpath(wpath, ROOT), "levels": meta["levels"],
-                                        "train_fields": meta["train_fields"], "first_seed": meta["first_seed"],
-                                        "params": meta["params"]}
-            solve["speedup"]["learned_fp64_vs_plain_fp64"] = plain / solve["learned_fp64_chebyshev4"]["solve_s"]
-            solve["speedup"]["learned_fp32_affine_vs_plain_fp64"] = (
-                plain / solve["learned_fp32_ir_chebyshev4_affine"]["solve_s"])
-            del net
-
-    # FP32 apply throughput (chosen precision form) and the affine-compressed
-    # format, same workload
-    x32 = x.float()
-    y32 = torch.zeros_like(x32)
-
-    def time_apply(fn):
-        for _ in range(3):
-            fn()
-        torch.cuda.synchronize()
-        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        g0.record(stream)
-        for _ in range(args.steps):
-            fn()
-        g1.record(stream)
-        torch.cuda.synchronize()
-        return g0.elapsed_time(g1) / args.steps
-
-    E = n ** 3
-    q3 = (p + 1) ** 3
-    variants = {}
-    for fmt, tag in ((femgpu.QDATA_FULL, "full"), (femgpu.QDATA_AFFINE, "affine")):
-        op.set_qdata_format(fmt)
-        for prec, es in (("fp64", 8), ("fp32", 4)):
-            if prec == "fp64":
-                t = time_apply(lambda: op.apply_native(x.data_ptr(), y.data_ptr()))
-            else:
-                t = time_apply(lambda: op.apply_native_f32(x32.data_ptr(), y32.data_ptr()))
-            qbytes = (6 * q3 * E if tag == "full" else (6 + q3) * E) * es
-            nbytes = qbytes + 2 * N * es
-            variants[f"{prec}_{tag}"] = {"ms": t, "gdof_s": N / (t / 1e3) / 1e9, "bytes_per_apply": nbytes,
-                                         "achieved_gbs": nbytes / (t / 1e3) / 1e9,
-                                         "frac": nbytes / (t / 1e3) / 1e9 / peak}
-    op.set_qdata_format(femgpu.QDATA_FULL)
-    fp32_apply = variants
-
-    # SDIRK-2 heat stepping, 64^3 Q2, lognormal kappa, dt = 1e-3,
-    # u0 = sin sin sin; FP64 stage solves vs FP32 (reliable-update) stage solves
     heat = None
     if not args.no_heat:
-        hn, hp, dt = 64, 2, 1e-3
-        hk = lognormal_kappa_q(hn, hn, hn, hp, sigma2=1.0, ell=0.1, seed=rank)
-        K = femgpu.PADiffusionOperator((hn, hn, hn), hp, kappa=hk)
-        S = femgpu.PAMassDiffusionOperator((hn, hn, hn), hp, 1.0, femgpu.SDIRK2_GAMMA * dt, kappa=hk)
-        K.set_stream(stream.cuda_stream)
-        S.set_stream(stream.cuda_stream)
-        xs1 = np.linspace(0, 1, hn * hp + 1)
-        u0 = (np.sin(np.pi * xs1)[:, None, None] * np.sin(np.pi * xs1)[None, :, None]
-              * np.sin(np.pi * xs1)[None, None, :]).ravel()
-        u0.reshape(hn * hp + 1, hn * hp + 1, hn * hp + 1)[[0, -1], :, :] = 0.0
-        u0.reshape(hn * hp + 1, hn * hp + 1, hn * hp + 1)[:, [0, -1], :] = 0.0
-        u0.reshape(hn * hp + 1, hn * hp + 1, hn * hp + 1)[:, :, [0, -1]] = 0.0
-        heat = {"workload": f"{hn}^3 Q2 SDIRK-2, dt={dt}, {args.heat_steps} steps, stage rtol 1e-10, warm start"}
-        finals = {}
-        # _affine: the quadrature data of both operators in the affine-compressed
-        # format (constant-J elements: |detJ| J^-1 J^-T per element, kappa per point)
-        for name, prec, pc, fmt in (("fp64_chebyshev4", femgpu.FP64, femgpu.PC_CHEBYSHEV, femgpu.QDATA_FULL),
-                                    ("fp32_chebyshev4", femgpu.FP32_IR, femgpu.PC_CHEBYSHEV, femgpu.QDATA_FULL),
-                                    ("fp32_chebyshev4_affine", femgpu.FP32_IR, femgpu.PC_CHEBYSHEV,
-                                     femgpu.QDATA_AFFINE)):
-            K.set_qdata_format(fmt)
-            S.set_qdata_format(fmt)
-            u = u0.copy()
-            info = femgpu.sdirk2(K, S, u, dt, args.heat_steps,
-                                 femgpu.SolverConfig(rtol=1e-10, max_iter=5000, precision=prec), pc)
-            finals[name] = u
-            heat[name] = {"time_s": info["time_ms"] / 1e3, "stage_iterations": info["total_iterations"],
-                          "max_stage_iterations": info["max_stage_iterations"], "applies": info["applies"]}
-        ref = finals["fp64_chebyshev4"]
-        for name in finals:
-            heat[name]["rel_l2_diff_vs_fp64_chebyshev"] = float(np.linalg.norm(finals[name] - ref) / np.linalg.norm(ref))
-        K.close()
-        S.close()
-
-    # batched uneven solves, n ~ U{8..48}, p ~ U{1,2,3}, own lognormal
-    # kappa (sigma2 ~ U[0.25,2], ell ~ U[0.05,0.3]) and RHS M xi, FP32 mixed precision
+        heat, detail["heat"] = run_heat(rank, args.heat_steps, stream)
     batch = None
     if not args.no_batch:
-        brng = np.random.default_rng(7000 + rank)
-        bops, bbs = [], []
-        total = 0
-        t_setup = time.perf_counter()
-        for i in range(args.batch_n):
-            bn, bp = int(brng.integers(8, 49)), int(brng.integers(1, 4))
-            kq = lognormal_kappa_q(bn, bn, bn, bp, sigma2=float(brng.uniform(0.25, 2.0)),
-                                   ell=float(brng.uniform(0.05, 0.3)), seed=100000 * rank + i, device=dev)
-            o = femgpu.PADiffusionOperator((bn, bn, bn), bp, kappa=kq)
-            m = femgpu.PAMassOperator((bn, bn, bn), bp)
-            xi = brng.standard_normal(o.n_dofs())
-            bb = m.matvec(xi)
-            m.close()
-            bb3 = bb.reshape(o.NK, o.NJ, o.NI)
-            bb3[[0, -1]] = 0.0
-            bb3[:, [0, -1]] = 0.0
-            bb3[:, :, [0, -1]] = 0.0
-            bops.append(o)
-            bbs.append(bb)
-            total += o.n_dofs()
-        t_setup = time.perf_counter() - t_setup
-        cfgb = femgpu.SolverConfig(rtol=1e-8, max_iter=5000, precision=femgpu.FP32_IR, check_interval=10)
-        # the same solves one after another (single-instance launches, default tiles)
-        t_seq = 0.0
-        seq_iters = []
-        for o, v in zip(bops, bbs):
-            xs1 = np.zeros_like(v)
-            r1 = o.pcg(v, xs1, cfgb, femgpu.PC_CHEBYSHEV)
-            t_seq += r1.solve_ms / 1e3
-            seq_iters.append(r1.iterations)
-        # batched with the default tiles
-        bxs = [np.zeros_like(v) for v in bbs]
-        ok0, bres0 = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
-        t_batch0 = bres0[0].solve_ms / 1e3
-        # autotuner: item depth per (order, size class) from timed batched applies
-        t_tune = time.perf_counter()
-        tune = femgpu.batch_autotune(bops, reps=3)
-        t_tune = time.perf_counter() - t_tune
-        bxs = [np.zeros_like(v) for v in bbs]
-        ok, bres = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
-        t_batch = bres[0].solve_ms / 1e3
-        batch = {"instances": len(bops), "total_dofs": total, "all_converged": bool(ok and ok0),
-                 "max_true_residual": max(r.true_residual for r in bres),
-                 "iterations_min_max": [min(r.iterations for r in bres), max(r.iterations for r in bres)],
-                 "max_iteration_diff_vs_single": int(max(abs(a.iterations - b) for a, b in zip(bres, seq_iters))),
-                 "sequential_single_solves_s": t_seq, "batched_default_tiles_s": t_batch0,
-                 "batched_solve_s": t_batch, "speedup_batched_vs_sequential": t_seq / t_batch,
-                 "speedup_autotune": t_batch0 / t_batch,
-                 "dof_iterations_per_s": sum(o.n_dofs() * r.iterations for o, r in zip(bops, bres)) / t_batch,
-                 "setup_s": t_setup, "autotune_s": t_tune,
-                 "autotune": [{"order": e["order"], "size_class": e["size_class"], "instances": e["instances"],
-                               "tz": e["tz"], "us_per_candidate_tz": e["us"]} for e in tune]}
-        for o in bops:
-            o.close()
-
-    # tetrahedral PA apply (TetP1/TetP2 on unit_cube_tet, partial.rs on Tet4):
-    # element gather + per-point contraction + CSR transpose scatter
-    tet = None
-    if not args.no_tet:
-        from femgpu import tet as tetmesh
-        tet = {}
-        for tn, tp in ((64, 2), (96, 1)):
-            coords, dofs, nd, mask = tetmesh.unit_cube_space(tn, tp)
-            qo = 2 * tp
-            top = femgpu.TetOperator(tp, coords, dofs, nd, quad_order=qo, ess=mask)
-            xt = torch.randn(nd, dtype=torch.float64, device=dev)
-            yt = torch.zeros_like(xt)
-            for _ in range(3):
-                top.apply_zero(xt, yt, True)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            reps = 20
-            for _ in range(reps):
-                top.apply_zero(xt, yt, True)
-            torch.cuda.synchronize()
-            dt = (time.perf_counter() - t0) / reps
-            E, nl, nqt = dofs.shape[0], dofs.shape[1], top.nq
-            # element map + geometry + per-point scalars + local results (write, read) + slots; offsets, x, y
-            tb = E * (nl * 4 + 6 * 8 + nqt * 8 + 2 * nl * 8 + nl * 4) + nd * (8 + 8 + 8)
-            tet[f"p{tp}_n{tn}"] = {"elements": int(E), "dofs": int(nd), "ms_per_apply": dt * 1e3,
-                                   "gdof_s": nd / dt / 1e9, "bytes_per_apply": int(tb),
-                                   "achieved_gbs": tb / dt / 1e9, "frac": tb / dt / 1e9 / peak,
-                                   "timing": "host wall clock over 20 synchronised applies"}
-            top.close()
-            del xt, yt
-
-    # the mfem_ex1 pipeline on the 24^3 Q1 Poisson case (kappa = 1, f = 3 pi^2 sin sin sin,
-    # homogeneous Dirichlet, PCG-Jacobi, rtol 1e-10): source form, solve and L2 error on the GPU
-    ex1 = None
-    if not args.no_ex1:
-        n1 = 24
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        op1 = femgpu.PADiffusionOperator((n1, n1, n1), 1)
-        qp2 = femgpu.quadrature_points(n1, n1, n1, 2)
-        b1 = femgpu.assemble_source(n1, n1, n1, 1, 3 * np.pi ** 2 * np.prod(np.sin(np.pi * qp2), axis=-1))
-        x1 = np.zeros(op1.n_dofs())
-        r1 = femgpu.solve_pcg_jacobi(op1, b1, x1, femgpu.SolverConfig(rtol=1e-10, max_iter=2000))
-        qp3 = femgpu.quadrature_points(n1, n1, n1, 3)
-        err1 = femgpu.l2_error(n1, n1, n1, 1, x1, np.prod(np.sin(np.pi * qp3), axis=-1), nq=3)
-        t_ex1 = time.perf_counter() - t0
-        ex1 = {"workload": "mfem_ex1: 24^3 Q1 Poisson, PCG-Jacobi rtol 1e-10 (15,625 DOFs)",
-               "iterations": r1.iterations, "solve_ms": r1.solve_ms, "l2_error": err1,
-               "pipeline_s": t_ex1, "converged": r1.converged,
-               "timing": "host wall clock: operator setup, source form, solve, L2 error"}
-        op1.close()
+        batch, detail["batch"] = run_batch(rank, args.batch_n, dev)
+    tet = None if args.no_tet else run_tet(dev, peak)
+    ex1 = None if args.no_ex1 else run_ex1()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            v, cores, desc = cpu_apply_sample(n, p, kq)
-            cpu = {"value": v, "unit": "GDOF/s", "cores": cores, "kind": "port", "sample": desc}
+            t_apply, ndof, cores = cpu_apply_time(n, p, kq, reps=2)
+            cpu = {"value": ndof / t_apply / 1e9, "unit": "GDOF/s", "cores": cores, "kind": "port",
+                   "sample": f"oracle port of the reference PA element loop (partial.rs:154-208 + "
+                             f"assembler.rs:96-143) on the full {n}^3 Q{p} mesh ({ndof} DOFs), 2 applies, "
+                             f"OpenMP {cores} threads"}
+            if solve is not None:
+                gpu_it = detail["solve_" + args.workload]["plain_fp64_chebyshev4"]["iterations"]
+                ext = cpu_solve_extrapolated(n, p, kq, gpu_it, t_apply)
+                cpu["time_to_1e8_s_extrapolated"] = ext["time_to_1e8_s"]
+                cpu["time_to_1e8_vs_gpu_plain"] = ext["time_to_1e8_s"] / (
+                    detail["solve_" + args.workload]["plain_fp64_chebyshev4"]["solve_s"])
+                detail["cpu_solve_extrapolated"] = ext
             if ex1 is not None:
-                cpu["ex1_pipeline"] = cpu_ex1_pipeline()
+                cpu["ex1_pipeline_s"] = cpu_ex1_pipeline()["pipeline_s"]
         except Exception as exc:  # keep the bench line even if the oracle is unavailable
             cpu = {"value": None, "unit": "GDOF/s", "cores": host_threads(), "kind": "port",
                    "sample": f"unavailable: {exc}"}
@@ -619,14 +754,11 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: lognormal kappa GRF (sigma2=1, ell=0.1, seed=rank) at Gauss points, x ~ N(0,1)",
-            "config": {"workload": f"{n}^3 Q{p} unit-cube hex, FP64 PA diffusion apply (constrained), "
-                                   f"{N} DOFs per rank", "order": p, "n_elem_1d": n,
-                       "l2": "inputs larger than L2 (qdata %.2f GB per apply)" % (6 * (p + 1) ** 3 * n ** 3 * 8 / 1e9),
-                       "parallelism": f"{world} independent instances"},
+            "config": bench_config(n, p, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": tr,
-                         "bytes_per_apply_canonical": bytes_canon, "bytes_per_apply_no_map": bytes_nomap,
-                         "frac_no_map": bytes_nomap / per_apply_s / 1e9 / peak, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": tr, "peak_kind": peak_kind,
+                         "bytes_per_apply_canonical": bytes_canon,
+                         "frac_no_map": bytes_nomap / per_apply_s / 1e9 / peak,
                          "kernel": "pa_apply_kernel + fixup_kernel (timed together per apply)"},
             "e2e": {"value": e2e_val, "unit": "GDOF/s", "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
                     "steps": k_e2e},
@@ -634,13 +766,20 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "solve": solve,
-            "apply_variants": fp32_apply,
+            "apply": variants,
+            "q3_64": q3,
             "heat": heat,
             "batch": batch,
             "tet": tet,
             "ex1": ex1,
         }
         print(json.dumps(out), flush=True)
+        path = args.detail
+        if path is None and os.path.isdir(os.path.join(ROOT, "gpurun_out")):
+            path = os.path.join(ROOT, "gpurun_out", "bench_detail.json")
+        if path:
+            with open(path, "w") as f:
+                json.dump(dict(out, detail=detail), f, indent=1)
     op.close()
     if world > 1:
         dist.destroy_process_group()

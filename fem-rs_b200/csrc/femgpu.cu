@@ -2262,22 +2262,41 @@ FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_ste
 // ---------------------------------------------------------------------------
 #define FG_NOALLOC_FACE_DOUBLES (4u << 20)  // 4 Mi doubles = 32 MiB
 static __device__ __align__(256) double g_noalloc_face[FG_NOALLOC_FACE_DOUBLES];
-static double *g_noalloc_face_ptr[64];  // device address of g_noalloc_face, per device
+// device address of g_noalloc_face per device, with the context it was resolved in
+static double *g_noalloc_face_ptr[64];
+static CUcontext g_noalloc_ctx[64];
 static std::mutex g_noalloc_mu;
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+static CtxGetCurrentFn g_ctx_get_current = nullptr;
 
 // Host code cannot use g_noalloc_face directly (its host-side name is only a
-// stand-in for the symbol); resolve the device address once per device, with
-// that device current.
+// stand-in for the symbol); resolve the device address with that device
+// current.  The address belongs to the context the module was loaded in: it
+// is resolved again when the current context differs from the one it was
+// resolved in (after cudaDeviceReset, or when the primary context was released
+// and created anew), so a stale address is never passed to a kernel.
 static int noalloc_scratch(int dev, double **out) {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (dev < 0 || dev >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", dev);
-    if (!g_noalloc_face_ptr[dev]) {
+    if (!g_ctx_get_current) {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        CK(cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn)
+            return fail(FG_CUDA_ERROR, "cuCtxGetCurrent entry point not found");
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx)
+        return fail(FG_CUDA_ERROR, "no current CUDA context on device %d", dev);
+    if (!g_noalloc_face_ptr[dev] || g_noalloc_ctx[dev] != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_face);
         if (e != cudaSuccess || !p)
             return fail(FG_CUDA_ERROR, "cudaGetSymbolAddress(g_noalloc_face) failed: %s",
                         cudaGetErrorString(e));
         g_noalloc_face_ptr[dev] = static_cast<double *>(p);
+        g_noalloc_ctx[dev] = ctx;
     }
     *out = g_noalloc_face_ptr[dev];
     return FG_OK;
@@ -2289,7 +2308,13 @@ static int noalloc_launch_apply_t(fg_op *op, const Grid &g, const double *x, dou
     using C = KCfg<P>;
     using SM = ApplySmem<P, double, C::WY, C::S, stage_elems<P, OPK, 0>() / 32>;
     auto kern = pa_apply_kernel<P, OPK, double, C::WY, C::S, C::MINB>;
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
+    // per device, set once (as launch_apply_t does); racing setters are harmless
+    static std::atomic<bool> attr_set[64];
+    if (op->device < 0 || op->device >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", op->device);
+    if (!attr_set[op->device].load(std::memory_order_acquire)) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
+        attr_set[op->device].store(true, std::memory_order_release);
+    }
     CUtensorMap tmap;
     cuuint64_t gdim[3] = {(cuuint64_t)g.NI, (cuuint64_t)g.NJ, (cuuint64_t)g.NK};
     cuuint64_t gstr[2] = {(cuuint64_t)g.NIp * sizeof(double),

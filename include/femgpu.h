@@ -200,7 +200,10 @@ FG_API int fg_op_apply_native_f32(fg_op *op, const float *x, float *y, int accum
  * (about 0.22 * n_dofs doubles for Q2) exceeds it are rejected with
  * FG_INVALID_ARGUMENT.  The call allocates and frees nothing.  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture.  All calls share the one
+ * make that first call before any stream capture.  The address is tied to the
+ * CUDA context: a call made in a different context of the device than the
+ * last lookup (after cudaDeviceReset, or after the primary context was
+ * released and created again) looks it up again.  All calls share the one
  * array: calls whose GPU work overlaps in time (other streams, other handles,
  * other threads) race on it and give wrong results; calls on one stream are
  * ordered and safe.  Nothing needs clearing between calls: every slot read is
