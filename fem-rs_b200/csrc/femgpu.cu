@@ -228,6 +228,7 @@ struct fg_op {
     double *qa64 = nullptr;
     float *qa32 = nullptr;
     int *d_err = nullptr;
+    uint64_t wait_ns = 0;  // limit of the apply kernels' device-side waits (0: 1 s)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t cap_stream = nullptr;  // private stream for CUDA-graph capture
@@ -324,7 +325,7 @@ static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const 
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
-    ApplyArgs<T> A{g, qd, y, face, accumulate, op->d_err, skip, fixcnt};
+    ApplyArgs<T> A{g, qd, y, face, accumulate, op->d_err, skip, fixcnt, op->wait_ns};
     kern<<<g.n_items(), C::WY * 32, SM::bytes, op->stream>>>(tmap, A);
     CK(cudaGetLastError());
     return FG_OK;
@@ -637,6 +638,15 @@ FG_API int fg_op_set_stream(fg_op *op, void *stream) {
     if (op->own_stream) cudaStreamDestroy(op->stream);
     op->own_stream = false;
     op->stream = reinterpret_cast<cudaStream_t>(stream);
+    return FG_OK;
+}
+
+FG_API int fg_op_set_wait_limit(fg_op *op, double seconds) {
+    if (!op) return fail(FG_INVALID_ARGUMENT, "NULL operator");
+    if (!(seconds == seconds)) return fail(FG_INVALID_ARGUMENT, "wait limit is NaN");
+    std::lock_guard<std::mutex> lk(op->mu);
+    op->wait_ns = seconds <= 0.0 ? 0 : std::max<uint64_t>(1, (uint64_t)std::min(seconds * 1e9, 6e10));
+    t_last_status = FG_OK;
     return FG_OK;
 }
 
@@ -2326,7 +2336,7 @@ static int noalloc_launch_apply_t(fg_op *op, const Grid &g, const double *x, dou
                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
-    ApplyArgs<double> A{g, op->qd, y, face, accumulate, op->d_err, nullptr};
+    ApplyArgs<double> A{g, op->qd, y, face, accumulate, op->d_err, nullptr, nullptr, op->wait_ns};
     kern<<<g.n_items(), C::WY * 32, SM::bytes, op->stream>>>(tmap, A);
     CK(cudaGetLastError());
     return FG_OK;

@@ -124,6 +124,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
         }
     }
 }
+// Wait for stream stage `next - 1` of a producer's bulk copies while `ok`
+// holds.  `waited` counts the stages whose data arrived; a stage whose wait ran
+// out stays uncounted, so the drain after a timeout (drain_stages) still waits
+// for the copy that was in flight.
+__device__ __forceinline__ void wait_stage(uint64_t *bar, uint32_t parity, int *err, uint64_t limit_ns,
+                                           bool &ok, int &waited, int next) {
+    if (!ok) return;
+    if (mbar_wait(bar, parity, err, limit_ns)) waited = next;
+    else ok = false;
+}
+// After a timeout: wait (with the normal 1 s limit each) for every copy in
+// [waited, issued) of a ring of `depth` mbarriers, so that no CTA exits while
+// a bulk copy into its shared memory is still in flight.
+__device__ __forceinline__ void drain_stages(uint64_t *bars, int depth, int waited, int issued) {
+    for (int j = waited; j < issued; ++j) mbar_wait(&bars[j % depth], (j / depth) & 1, nullptr);
+}
 // 1-D bulk copy global -> shared, completing on an mbarrier (sizes/addresses
 // must be multiples of 16 bytes).
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,

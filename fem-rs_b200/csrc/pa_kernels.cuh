@@ -69,6 +69,7 @@ template <typename T> struct ApplyArgs {
     const int *skip;  // if non-null and *skip != 0 the kernel returns at once
     unsigned *fixcnt; // non-null: fix-up fused into the apply (per-item arrival counters, all zero
                       // between launches); null: fixup_kernel runs after the apply
+    uint64_t wait_ns; // limit of each wait for a copy into shared memory; 0: 1 s
 };
 
 template <typename T, int P>
@@ -231,6 +232,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
 
     if (A.skip && *A.skip) return;
     const Grid g = A.g;
+    const uint64_t wlim = A.wait_ns ? A.wait_ns : 1000000000ull;
     const CUtensorMap &xmap = *xmap_ptr;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T *xs = reinterpret_cast<T *>(smem_raw);
@@ -297,8 +299,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                         &xbar[bn]);
             x_issued = ln + 1;
         }
-        if (ok && !mbar_wait(&xbar[xb], (lz / NXB) & 1, A.err)) ok = false;
-        x_waited = lz + 1;
+        wait_stage(&xbar[xb], (lz / NXB) & 1, A.err, wlim, ok, x_waited, lz + 1);
         const T *xt = reinterpret_cast<const T *>(reinterpret_cast<const unsigned char *>(xs) +
                                                   xb * SM::XB);
 
@@ -357,8 +358,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
             if (FMT == 1) {
                 const int j = lz;
                 const int s = j % S;
-                if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-                q_waited = j + 1;
+                wait_stage(&qbw[s], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
                 ql = qsw + s * STAGE;
 #pragma unroll
                 for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
@@ -371,8 +371,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     const int j = lz * COLS + col;
                     const int s = j % S;
                     if (FMT == 0) {
-                        if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-                        q_waited = j + 1;
+                        wait_stage(&qbw[s], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
                     }
                     const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
                     float2 vxy[Q];
@@ -522,8 +521,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
             if (FMT == 1) {
                 const int j = lz;
                 const int s = j % S;
-                if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-                q_waited = j + 1;
+                wait_stage(&qbw[s], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
                 ql = qsw + s * STAGE;
     #pragma unroll
                 for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
@@ -536,8 +534,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     const int j = lz * COLS + col;
                     const int s = j % S;
                     if (FMT == 0) {
-                        if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-                        q_waited = j + 1;
+                        wait_stage(&qbw[s], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
                     }
                     const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
                     T vx[Q], vy[Q], vz[Q], vu[Q];
@@ -677,8 +674,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
             const T *ql = nullptr;
             if (FMT == 1) {
                 const int j = lz, s = j % S;
-                if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-                q_waited = j + 1;
+                wait_stage(&qbw[s], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
                 ql = qsw + s * STAGE;
 #pragma unroll
                 for (int k = 0; k < NCE; ++k) Ge[k] = ql[k * 32 + lane];
@@ -735,8 +731,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                         const int j = lz * COLS + col;
                         const int s = j % S;
                         if (FMT == 0) {
-                            if (ok && !mbar_wait(&qbw[s], (j / S) & 1, A.err)) ok = false;
-                            q_waited = j + 1;
+                            wait_stage(&qbw[s], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
                         }
                         const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
                         T vx[Q], vy[Q], vz[Q], vu[Q];
@@ -848,14 +843,11 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
             [&](int c, int b, int a) { return xt[(c * RY + warp * P + b) * XW + lane * P + a]; });
         __syncthreads();
     }
-    // Drain copies still in flight after a timeout (bounded waits).
+    // After a timeout, drain the copies this thread issued and has not seen
+    // arrive (the one whose wait ran out included), with bounded waits.
     if (!ok) {
-        if (lane == 0)
-            for (int j = q_waited; j < q_issued; ++j)
-                mbar_wait(&qbw[j % S], (j / S) & 1, nullptr, 100000000ull);
-        if (threadIdx.x == 0)
-            for (int j = x_waited; j < x_issued; ++j)
-                mbar_wait(&xbar[j % SM::NXB], (j / SM::NXB) & 1, nullptr, 100000000ull);
+        if (lane == 0) drain_stages(qbw, S, q_waited, q_issued);
+        if (threadIdx.x == 0) drain_stages(xbar, SM::NXB, x_waited, x_issued);
     }
     if (A.fixcnt)  // the y staging area is free after the last layer's barrier
         fused_fixup<T, P>(g, A.y, A.face, A.fixcnt, item, reinterpret_cast<int *>(ybuf));

@@ -46,7 +46,7 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_op_collect_residuals", "fg_unet_train_energy", "fg_quadrature_points",
            "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply", "fg_op_set_tile",
            "fg_op_tile", "fg_batch_autotune", "fg_tet_create", "fg_tet_destroy", "fg_tet_ndofs", "fg_tet_nq",
-           "fg_tet_quadrature_points", "fg_tet_apply", "fg_tet_diagonal")
+           "fg_tet_quadrature_points", "fg_tet_apply", "fg_tet_diagonal", "fg_op_set_wait_limit")
 
 
 class FgMesh(C.Structure):
@@ -146,6 +146,7 @@ def lib():
         L.fg_tet_apply.argtypes = [vp, vp, vp, i, i, i]
         L.fg_tet_diagonal.argtypes = [vp, vp, i, i]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
+        L.fg_op_set_wait_limit.argtypes = [vp, d]
         _lib = L
     return _lib
 
@@ -354,6 +355,10 @@ class PAOperator:
 
     def check(self):
         _check(lib().fg_op_check(self._h))
+
+    def set_wait_limit(self, seconds):
+        """Limit of each device-side wait of the apply kernels (<= 0: the 1 s default)."""
+        _check(lib().fg_op_set_wait_limit(self._h, C.c_double(seconds)))
 
     def set_stream(self, stream_ptr):
         _check(lib().fg_op_set_stream(self._h, stream_ptr))

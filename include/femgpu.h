@@ -391,6 +391,16 @@ FG_API int fg_tet_apply(fg_tet *op, const double *x, double *y, int accumulate, 
 /* Jacobi diagonal (1 on essential DOFs when constrained). */
 FG_API int fg_tet_diagonal(fg_tet *op, double *d, int constrained, int mem);
 
+/* Limit of each device-side wait of this handle's apply kernels for a copy
+ * into shared memory (default 1 s; seconds <= 0 restores it, at most 60 s).
+ * A wait that runs out sets the handle's device error word, the kernel stops
+ * issuing copies, waits (1 s at most each) for the copies it has in flight and
+ * returns; fg_op_check then reports FG_DEVICE_TIMEOUT and clears the word.
+ * The results of an apply that timed out are not defined.  No reference
+ * counterpart (the reference has no device code); a watchdog for the hosts of
+ * this library. */
+FG_API int fg_op_set_wait_limit(fg_op *op, double seconds);
+
 /* Synchronise the handle's stream and report device-side errors
  * (FG_DEVICE_TIMEOUT, FG_BOUNDS). */
 FG_API int fg_op_check(fg_op *op);

@@ -103,3 +103,35 @@ def test_collapsed_hex_is_rejected(order):
     op = femgpu.PADiffusionOperator((nx, ny, nz), order)
     assert np.abs(op.matvec(np.ones(op.n_dofs()))).max() < 1e-12
     op.close()
+
+
+def test_device_wait_limit_runs_out_and_handle_recovers():
+    """A 1 ns limit on the apply kernel's waits for its bulk copies makes them
+    run out (a copy from HBM takes far longer): the kernel stops issuing,
+    waits out the copies it has in flight with the normal limit, returns, and
+    fg_op_check reports FG_DEVICE_TIMEOUT.  With the default limit restored
+    the same handle applies correctly again."""
+    need_gpu()
+    n, p = 64, 2
+    op = femgpu.PADiffusionOperator((n, n, n), p)
+    x = np.random.default_rng(4).standard_normal(op.n_dofs())
+    xt = torch.from_numpy(op.to_native(x)).cuda()
+    yt = torch.zeros_like(xt)
+    torch.cuda.synchronize()
+    op.set_wait_limit(1e-9)
+    status = femgpu.FG_OK
+    for _ in range(10):
+        op.apply_native(xt.data_ptr(), yt.data_ptr(), accumulate=False, constrained=True)
+        try:
+            op.check()
+        except femgpu.SolverError as exc:
+            status = exc.status
+            break
+    assert status == femgpu.FG_DEVICE_TIMEOUT, status
+    op.set_wait_limit(0)
+    mesh = O.Mesh(n, n, n, p)
+    y_ref = O.apply_constrained(mesh, O.Coef(O.DIFF), O.ess_mask(mesh), x)
+    y = op.matvec(x, constrained=True)
+    op.check()
+    assert np.linalg.norm(y - y_ref) <= 1e-12 * np.linalg.norm(y_ref)
+    op.close()
