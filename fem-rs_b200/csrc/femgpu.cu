@@ -55,6 +55,13 @@ static int fail(int status, const char *fmt, ...) {
 // running when the call returns.  Set-up paths call this before any launch on
 // another stream reads what they wrote.
 #define FG_LEGACY_FENCE() CK(cudaStreamSynchronize(cudaStreamLegacy))
+// Entry points built on the structured box (its DOF lattice, item tiles or
+// compressed qdata) refuse operators of an unstructured Hex8 mesh.
+#define FG_NEED_BOX(op, what)                                                                  \
+    do {                                                                                       \
+        if ((op) && (op)->unstr)                                                               \
+            return fail(FG_UNSUPPORTED, "%s needs a structured hex box (fg_op_create)", what); \
+    } while (0)
 
 #include "unet_host.cuh"
 #include "tet_host.cuh"
@@ -225,6 +232,13 @@ struct fg_op {
     bool nn_overlap = true;                    // network beside the smoother (FG_NN_OVERLAP=0: in line)
     fg_unet *nn = nullptr;
     int fmt = 0;
+    // unstructured Hex8 mesh (fg_op_create_hex): element maps sorted by colour,
+    // colour starts, essential-DOF mask; vectors are plain (no pads)
+    bool unstr = false;
+    int64_t u_E = 0;
+    std::vector<int64_t> u_col;
+    int32_t *u_dofs = nullptr;
+    uint8_t *u_ess = nullptr;
     double *qa64 = nullptr;
     float *qa32 = nullptr;
     int *d_err = nullptr;
@@ -243,6 +257,8 @@ static void free_op(fg_op *op) {
     double *bufs[] = {op->qd, op->face, op->xs, op->ys, op->dinv, op->ones, op->r, op->z, op->pv, op->ap,
                       op->xw, op->bw, op->cres, op->cd, op->ct, op->partials, op->stage};
     if (op->fixcnt) cudaFree(op->fixcnt);
+    if (op->u_dofs) cudaFree(op->u_dofs);
+    if (op->u_ess) cudaFree(op->u_ess);
     for (int k = 0; k < CHEB_MAXD; ++k) {
         if (op->cdk[k]) cudaFree(op->cdk[k]);
         if (op->cdk32[k]) cudaFree(op->cdk32[k]);
@@ -282,6 +298,8 @@ template <typename T> static int alloc_vec(T **p, int64_t n) {
     FG_LEGACY_FENCE();
     return FG_OK;
 }
+
+#include "hex_host.cuh"
 
 // ---------------------------------------------------------------------------
 // launchers
@@ -380,6 +398,7 @@ template <typename T> static unsigned *fixcnt_for(fg_op *op, const T *face) {
 template <typename T>
 static int apply_native_t(fg_op *op, const T *qd, T *face, const T *x, T *y, int accumulate,
                           int constrained, const int *skip) {
+    if (op->unstr) return hex_apply<T>(op, qd, x, y, accumulate, constrained, skip);
     unsigned *fixcnt = fixcnt_for<T>(op, face);
     Grid g = op->g;
     g.ess = constrained ? op->ess_tags : 0;
@@ -413,6 +432,7 @@ template <int P> static int launch_diag_p(fg_op *op, const Grid &g, double *y) {
     }
 }
 static int diag_native(fg_op *op, double *y, int constrained) {
+    if (op->unstr) return hex_diag(op, y, constrained);
     Grid g = op->g;
     g.ess = constrained ? op->ess_tags : 0;
     int rc;
@@ -1293,6 +1313,7 @@ static int from_native32(fg_op *op, float *dst, const float *src, int mem) {
 }
 
 FG_API int fg_op_set_qdata_format(fg_op *op, int format) {
+    if (format != FG_QDATA_FULL) FG_NEED_BOX(op, "the affine quadrature-data format");
     if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
     if (format != FG_QDATA_FULL && format != FG_QDATA_AFFINE)
         return fail(FG_INVALID_ARGUMENT, "bad quadrature-data format %d", format);
@@ -1762,6 +1783,7 @@ static int time_batched_apply(fg_op *const *ops, const std::vector<int> &inst, c
 extern "C" {
 
 FG_API int fg_op_set_tile(fg_op *op, int tz) {
+    FG_NEED_BOX(op, "fg_op_set_tile");
     if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
     if (tz < 1 || tz > 64) return fail(FG_INVALID_ARGUMENT, "tile depth %d outside 1..64", tz);
     std::lock_guard<std::mutex> lk(op->mu);
@@ -1770,6 +1792,7 @@ FG_API int fg_op_set_tile(fg_op *op, int tz) {
 }
 
 FG_API int fg_op_tile(const fg_op *op, int dims[3]) {
+    FG_NEED_BOX(op, "fg_op_tile");
     if (!op || !dims) return fail(FG_INVALID_ARGUMENT, "NULL argument");
     dims[0] = 32;
     dims[1] = op->g.WY;
@@ -1778,6 +1801,8 @@ FG_API int fg_op_tile(const fg_op *op, int dims[3]) {
 }
 
 FG_API int fg_batch_autotune(fg_op *const *ops, int n, int reps, fg_tune_entry *out, int max_out, int *n_out) {
+    if (ops)
+        for (int i_ = 0; i_ < n; ++i_) FG_NEED_BOX(ops[i_], "fg_batch_autotune");
     if (!ops || n <= 0 || reps < 1 || !n_out) return fail(FG_INVALID_ARGUMENT, "bad autotune arguments");
     *n_out = 0;
     std::vector<fg_op *> sorted(ops, ops + n);
@@ -1886,6 +1911,8 @@ FG_API int fg_pcg(fg_op *op, const double *b, double *x, const fg_cfg *cfg_in, f
 // check_interval iterations are captured once in a CUDA graph and replayed.
 FG_API int fg_batch_pcg(fg_op *const *ops, int n, const double *const *b, double *const *x,
                         const fg_cfg *cfg_in, fg_result *results, int mem) {
+    if (ops)
+        for (int i_ = 0; i_ < n; ++i_) FG_NEED_BOX(ops[i_], "fg_batch_pcg");
     if (!ops || n <= 0 || !b || !x) return fail(FG_INVALID_ARGUMENT, "bad batch arguments");
     fg_cfg cfg;
     if (cfg_in) cfg = *cfg_in; else fg_cfg_default(&cfg);
@@ -2138,6 +2165,8 @@ FG_API int fg_batch_pcg(fg_op *const *ops, int n, const double *const *b, double
 // previous stage's k (the reference starts every solve from zero).
 FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_steps,
                      const fg_cfg *cfg_in, fg_sdirk_result *out, int mem) {
+    FG_NEED_BOX(stiff, "fg_sdirk2");
+    FG_NEED_BOX(stage, "fg_sdirk2");
     if (!stiff || !stage || !u) return fail(FG_INVALID_ARGUMENT, "NULL argument");
     if (stiff == stage) return fail(FG_INVALID_ARGUMENT, "stiff and stage must be distinct handles");
     if (n_steps < 0 || !(dt > 0)) return fail(FG_INVALID_ARGUMENT, "bad dt or n_steps");
@@ -2354,6 +2383,7 @@ static int noalloc_launch_apply_p(fg_op *op, const Grid &g, const double *x, dou
 
 extern "C" FG_API int fg_op_apply_native_noalloc(fg_op *op, const double *x, double *y,
                                                  int accumulate, int constrained) {
+    FG_NEED_BOX(op, "fg_op_apply_native_noalloc");
     if (!op || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
     if (x == y) return fail(FG_INVALID_ARGUMENT, "x and y must not alias");
     std::lock_guard<std::mutex> lk(op->mu);
@@ -2601,6 +2631,7 @@ FG_API int fg_unet_train_step(fg_unet *u, const float *in, const float *target, 
 // and >= 5, so the DOF lattice's cell counts (p times the element counts) must
 // be multiples of 4 * 2^levels.
 FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal, int levels) {
+    FG_NEED_BOX(op, "fg_op_set_nodal_kappa");
     if (!op || !kappa_nodal) return fail(FG_INVALID_ARGUMENT, "NULL argument");
     if (levels < 1 || levels > 4) return fail(FG_INVALID_ARGUMENT, "levels must be 1 to 4");
     const int m = 4 << levels;
@@ -2644,6 +2675,7 @@ FG_API int fg_op_set_nodal_kappa(fg_op *op, const double *kappa_nodal, int level
 }
 
 FG_API int fg_op_attach_unet(fg_op *op, fg_unet *net) {
+    FG_NEED_BOX(op, "fg_op_attach_unet");
     if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
     std::lock_guard<std::mutex> lk(op->mu);
     if (net && net->device != op->device) return fail(FG_INVALID_ARGUMENT, "network on another device");
@@ -2658,6 +2690,7 @@ FG_API int fg_op_attach_unet(fg_op *op, fg_unet *net) {
 // s_k = rms(R (b - A x_k)); device FP32 outputs, up to max_pairs.
 FG_API int fg_op_collect_pairs(fg_op *op, const double *b, const fg_cfg *cfg_in, int every, int max_pairs,
                                float *d_in, float *d_target, int *n_pairs) {
+    FG_NEED_BOX(op, "fg_op_collect_pairs");
     if (!op || !b || !d_in || !d_target || !n_pairs || every < 1 || max_pairs < 1)
         return fail(FG_INVALID_ARGUMENT, "bad arguments");
     if (!op->nn_lk) return fail(FG_INVALID_ARGUMENT, "call fg_op_set_nodal_kappa first");
@@ -2727,6 +2760,7 @@ FG_API int fg_op_collect_pairs(fg_op *op, const double *b, const fg_cfg *cfg_in,
 // d_out ([max_res][fg_op_native_len], device); the count in *n_res.
 FG_API int fg_op_collect_residuals(fg_op *op, const double *b, const fg_cfg *cfg_in, int every, int max_res,
                                    double *d_out, int *n_res) {
+    FG_NEED_BOX(op, "fg_op_collect_residuals");
     if (!op || !b || !d_out || !n_res || every < 1 || max_res < 1)
         return fail(FG_INVALID_ARGUMENT, "bad arguments");
     fg_cfg cfg;
@@ -2780,6 +2814,7 @@ FG_API int fg_op_collect_residuals(fg_op *op, const double *b, const fg_cfg *cfg
 // d loss_b / d n = R^L (A c - r) / (s Nc)  (P^T = 8 R per level).  The
 // reported loss is the batch mean.
 FG_API int fg_unet_train_energy(fg_unet *u, fg_op *op, const double *d_res, int B, float lr, float *loss) {
+    FG_NEED_BOX(op, "fg_unet_train_energy");
     if (!u || !op || !d_res || B < 1) return fail(FG_INVALID_ARGUMENT, "bad arguments");
     if (!op->nn_lk) return fail(FG_INVALID_ARGUMENT, "call fg_op_set_nodal_kappa first");
     if (u->device != op->device) return fail(FG_INVALID_ARGUMENT, "network on another device");

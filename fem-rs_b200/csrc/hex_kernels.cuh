@@ -1,0 +1,316 @@
+// hex_kernels.cuh -- partial-assembly mass / diffusion operator on an
+// unstructured Hex8 mesh of order P (Q = P+1 Gauss points per direction): the
+// element loop of crates/assembly/src/partial.rs:85-130, 154-208 with the
+// Hex8 geometry of crates/assembly/src/assembler.rs:96-143, for any element
+// connectivity and any DOF numbering (a DofManager's element maps).
+//
+// Data layout (elements sorted by colour, element-major structure of arrays,
+// so a warp of consecutive elements reads each entry in one coalesced load):
+//   dofs [nl][E]         int32 element-to-DOF map, local DOF (c,b,a) at
+//                        k = (c*D + b)*D + a (tensor order on the reference cube)
+//   qd   [Q^3*NC][E]     quadrature data of point pt = (qy*Q + qx)*Q + qz,
+//                        component c at (pt*NC + c)*E + e: 6 symmetric
+//                        w|detJ| kappa J^-1 J^-T and/or w|detJ| rho
+//   ess  [N]             essential-DOF mask (constrained applies)
+//
+// Scatter without float atomics: the elements are coloured so that no two
+// elements of a colour share a DOF; one launch per colour adds each element's
+// result into y directly.  Every DOF receives its element contributions in
+// colour order, so the sums are the same from run to run.
+//
+// Element math: slab sum factorisation (one qy slab of QH quadrature columns
+// at a time: y then x contraction of the element values, per column z, D, z^T,
+// then the transposed x and y into the element result).  The element values
+// are staged in shared memory, one column per thread.
+#pragma once
+#include "fg_common.cuh"
+#include "pa_kernels.cuh"
+
+namespace fg {
+
+template <typename T> struct HexApply {
+    int64_t E, N;          // elements, DOFs
+    int64_t e0, e1;        // element range of this launch (one colour)
+    const int32_t *dofs;   // [nl][E]
+    const T *qd;           // [Q^3*NC][E]
+    const uint8_t *ess;    // [N] or null
+    const T *x;            // null: diagonal
+    T *y;
+    int constrained;
+    const int *skip;       // if non-null and *skip != 0 the kernel returns at once
+};
+
+// y = (accumulate ? y : 0) + (identity rows of the essential DOFs of a
+// constrained call: x, or 1 for the diagonal); the colour launches add the
+// element contributions to the other DOFs.
+template <typename T>
+__global__ void hex_init_kernel(const HexApply<T> A, int accumulate) {
+    if (A.skip && *A.skip) return;
+    for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < A.N; d += (int64_t)gridDim.x * blockDim.x) {
+        T v = accumulate ? A.y[d] : T(0);
+        if (A.constrained && A.ess && A.ess[d]) v += A.x ? A.x[d] : T(1);
+        A.y[d] = v;
+    }
+}
+
+template <int P, int OPK, typename T, int BS>
+__global__ void __launch_bounds__(BS) hex_apply_kernel(const HexApply<T> A) {
+    constexpr int D = P + 1, Q = P + 1, NL = D * D * D, NC = NComp<OPK>::v;
+    constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
+    constexpr int QH = (P == 3 && sizeof(T) == 8) ? 2 : Q;  // half slabs bound the Q3 FP64 state
+    using TB = Tab<T>;
+    __shared__ T xs[NL * BS];
+    if (A.skip && *A.skip) return;
+    const int64_t e = A.e0 + (int64_t)blockIdx.x * BS + threadIdx.x;
+    if (e >= A.e1) return;
+    const int64_t E = A.E;
+    const int tid = threadIdx.x;
+    // gather (E) with the essential columns masked
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int32_t d = __ldg(A.dofs + (int64_t)k * E + e);
+        const bool ess = A.constrained && A.ess && A.ess[d];
+        xs[k * BS + tid] = ess ? T(0) : __ldg(A.x + d);
+    }
+    auto uval = [&](int c, int b, int a) -> T { return xs[((c * D + b) * D + a) * BS + tid]; };
+    auto qdv = [&](int pt, int comp) -> T { return __ldg(A.qd + ((int64_t)pt * NC + comp) * E + e); };
+    T out[D][D][D];
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+#pragma unroll
+        for (int b = 0; b < D; ++b)
+#pragma unroll
+            for (int a = 0; a < D; ++a) out[c][b][a] = T(0);
+#pragma unroll 1
+    for (int qy = 0; qy < Q; ++qy) {
+        T by[D], gyb[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            by[k] = TB::B(P, qy, k);
+            gyb[k] = TB::G(P, qy, k);
+        }
+#pragma unroll
+        for (int h0 = 0; h0 < Q; h0 += QH) {
+            T C0[D][QH], C1[D][QH], C2[D][QH];  // [c][qx - h0]
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                T R[D], Rg[D];
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    T s0 = 0, s1 = 0;
+#pragma unroll
+                    for (int b = 0; b < D; ++b) {
+                        const T u = uval(c, b, a);
+                        s0 += by[b] * u;
+                        if (HK) s1 += gyb[b] * u;
+                    }
+                    R[a] = s0;
+                    Rg[a] = s1;
+                }
+#pragma unroll
+                for (int k = 0; k < QH; ++k) {
+                    const int qx = h0 + k;
+                    T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        t0 += TB::B(P, qx, a) * R[a];
+                        if (HK) {
+                            t1 += TB::B(P, qx, a) * Rg[a];
+                            t2 += TB::G(P, qx, a) * R[a];
+                        }
+                    }
+                    C0[c][k] = t0;
+                    C1[c][k] = t1;
+                    C2[c][k] = t2;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < QH; ++k) {
+                const int col = qy * Q + h0 + k;
+                T vx[Q], vy[Q], vz[Q], vu[Q];
+#pragma unroll
+                for (int qz = 0; qz < Q; ++qz) {
+                    const int pt = col * Q + qz;
+                    T gx = 0, gy = 0, gz = 0, ui = 0;
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        if (HK) {
+                            gx += TB::B(P, qz, c) * C2[c][k];
+                            gy += TB::B(P, qz, c) * C1[c][k];
+                            gz += TB::G(P, qz, c) * C0[c][k];
+                        }
+                        if (HM) ui += TB::B(P, qz, c) * C0[c][k];
+                    }
+                    vx[qz] = vy[qz] = vz[qz] = vu[qz] = T(0);
+                    if (HK) {
+                        const T d0 = qdv(pt, 0), d1 = qdv(pt, 1), d2 = qdv(pt, 2), d3 = qdv(pt, 3),
+                                d4 = qdv(pt, 4), d5 = qdv(pt, 5);
+                        vx[qz] = d0 * gx + d1 * gy + d2 * gz;
+                        vy[qz] = d1 * gx + d3 * gy + d4 * gz;
+                        vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                    }
+                    if (HM) vu[qz] = qdv(pt, HK ? 6 : 0) * ui;
+                }
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    T e0 = 0, e1 = 0, e2 = 0;
+#pragma unroll
+                    for (int qz = 0; qz < Q; ++qz) {
+                        if (HK) {
+                            e2 += TB::B(P, qz, c) * vx[qz];
+                            e1 += TB::B(P, qz, c) * vy[qz];
+                            e0 += TB::G(P, qz, c) * vz[qz];
+                        }
+                        if (HM) e0 += TB::B(P, qz, c) * vu[qz];
+                    }
+                    C0[c][k] = e0;
+                    C1[c][k] = e1;
+                    C2[c][k] = e2;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                T H0[D], H1[D];
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    T s0 = 0, s1 = 0;
+#pragma unroll
+                    for (int k = 0; k < QH; ++k) {
+                        const int qx = h0 + k;
+                        s0 += TB::B(P, qx, a) * C0[c][k];
+                        if (HK) {
+                            s0 += TB::G(P, qx, a) * C2[c][k];
+                            s1 += TB::B(P, qx, a) * C1[c][k];
+                        }
+                    }
+                    H0[a] = s0;
+                    H1[a] = s1;
+                }
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+                        T v = out[c][b][a] + by[b] * H0[a];
+                        if (HK) v += gyb[b] * H1[a];
+                        out[c][b][a] = v;
+                    }
+            }
+        }
+    }
+    // E^T: add into the non-essential DOFs (no other element of this colour
+    // touches them)
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+#pragma unroll
+        for (int b = 0; b < D; ++b)
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                const int32_t d = __ldg(A.dofs + (int64_t)((c * D + b) * D + a) * E + e);
+                if (!(A.constrained && A.ess && A.ess[d])) A.y[d] += out[c][b][a];
+            }
+}
+
+// Jacobi diagonal: element diagonal sum_q g_i^T D_q g_i (+ m_q phi_i^2) added
+// into the non-essential DOFs, one launch per colour (after hex_init_kernel
+// with x = null, which puts 1 on the essential DOFs of a constrained call).
+template <int P, int OPK>
+__global__ void __launch_bounds__(128) hex_diag_kernel(const HexApply<double> A) {
+    constexpr int D = P + 1, Q = P + 1, NC = NComp<OPK>::v;
+    constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
+    using TB = Tab<double>;
+    const int64_t e = A.e0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= A.e1) return;
+    const int64_t E = A.E;
+    double out[D][D][D];
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+#pragma unroll
+        for (int b = 0; b < D; ++b)
+#pragma unroll
+            for (int a = 0; a < D; ++a) out[c][b][a] = 0.0;
+    for (int qy = 0; qy < Q; ++qy)
+        for (int qx = 0; qx < Q; ++qx)
+            for (int qz = 0; qz < Q; ++qz) {
+                const int pt = (qy * Q + qx) * Q + qz;
+                double d[7];
+#pragma unroll
+                for (int k = 0; k < NC; ++k) d[k] = __ldg(A.qd + ((int64_t)pt * NC + k) * E + e);
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+#pragma unroll
+                    for (int b = 0; b < D; ++b)
+#pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            const double Bx = TB::B(P, qx, a), By = TB::B(P, qy, b), Bz = TB::B(P, qz, c);
+                            double s = 0.0;
+                            if (HK) {
+                                const double gx = TB::G(P, qx, a) * By * Bz;
+                                const double gy = Bx * TB::G(P, qy, b) * Bz;
+                                const double gz = Bx * By * TB::G(P, qz, c);
+                                s = d[0] * gx * gx + d[3] * gy * gy + d[5] * gz * gz +
+                                    2.0 * (d[1] * gx * gy + d[2] * gx * gz + d[4] * gy * gz);
+                            }
+                            if (HM) {
+                                const double ph = Bx * By * Bz;
+                                s += d[HK ? 6 : 0] * ph * ph;
+                            }
+                            out[c][b][a] += s;
+                        }
+            }
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+#pragma unroll
+        for (int b = 0; b < D; ++b)
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                const int32_t d = __ldg(A.dofs + (int64_t)((c * D + b) * D + a) * E + e);
+                if (!(A.constrained && A.ess && A.ess[d])) A.y[d] += out[c][b][a];
+            }
+}
+
+// Quadrature-data setup of the unstructured mesh: one thread per (element,
+// point).  Sorted element s is the caller's element eid[s]; its vertices are
+// conn[eid*8 .. +8] in HexQ1 order; kappa_q / rho_q are indexed by the
+// caller's element and the tensor point (qz, qy, qx).
+struct HexSetup {
+    int64_t E;
+    const int32_t *eid;     // [E] sorted -> caller element
+    const uint32_t *conn;   // [E][8]
+    const double *coords;   // [n_nodes][3]
+    const double *kappa_q, *rho_q;
+    double kappa_c, rho_c, c_m, c_k;
+    double gx[4], gw[4];
+    int *err;
+};
+
+template <int P, int OPK, typename T>
+__global__ void hex_setup_kernel(const HexSetup S, T *__restrict__ qd) {
+    constexpr int Q = P + 1, Q3 = Q * Q * Q, NC = NComp<OPK>::v;
+    constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
+    const int64_t total = S.E * Q3;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = t / Q3;
+        const int q = (int)(t % Q3);  // tensor point index (qz, qy, qx), qx fastest
+        const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
+        const int64_t e = S.eid[s];
+        double xv[8][3];
+        for (int k = 0; k < 8; ++k) {
+            const int64_t v = S.conn[e * 8 + k];
+            xv[k][0] = S.coords[3 * v];
+            xv[k][1] = S.coords[3 * v + 1];
+            xv[k][2] = S.coords[3 * v + 2];
+        }
+        const double xi[3] = {S.gx[qx], S.gx[qy], S.gx[qz]};
+        const double w = S.gw[qx] * S.gw[qy] * S.gw[qz];
+        const double kap = S.kappa_q ? S.kappa_q[e * Q3 + q] : S.kappa_c;
+        const double rho = S.rho_q ? S.rho_q[e * Q3 + q] : S.rho_c;
+        double D[6], m;
+        if (!hex_point_qdata(xv, xi, w, kap, S.c_k, rho, S.c_m, D, m) && S.err) atomicOr(S.err, FG_DERR_BOUNDS);
+        const int pt = (qy * Q + qx) * Q + qz;
+        if (HK)
+            for (int k = 0; k < 6; ++k) qd[((int64_t)pt * NC + k) * S.E + s] = (T)D[k];
+        if (HM) qd[((int64_t)pt * NC + (HK ? 6 : 0)) * S.E + s] = (T)m;
+    }
+}
+
+}  // namespace fg

@@ -1250,6 +1250,48 @@ __global__ void qdata_compress_kernel(const Grid g, const double *__restrict__ q
     }
 }
 
+// Quadrature data of one point from the element's 8 vertices xv (HexQ1 node
+// order of crates/element/src/lagrange/hex.rs:27-36) at the reference point xi
+// with weight w: J_id = sum_k x_k[i] dphi_k/dxi_d (assembler.rs:96-123),
+// D = w |detJ| kappa c_k J^-1 J^-T (6 symmetric components xx xy xz yy yz zz),
+// m = w |detJ| rho c_m.  Returns false when det J = 0.
+__device__ __forceinline__ bool hex_point_qdata(const double (&xv)[8][3], const double (&xi)[3], double w,
+                                                double kap, double c_k, double rho, double c_m, double (&D)[6],
+                                                double &m) {
+    const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                           {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int k = 0; k < 8; ++k) {
+        const double sx = off[k][0] ? 1.0 : -1.0, sy = off[k][1] ? 1.0 : -1.0, sz = off[k][2] ? 1.0 : -1.0;
+        const double fx = 1.0 + sx * xi[0], fy = 1.0 + sy * xi[1], fz = 1.0 + sz * xi[2];
+        const double gr[3] = {0.125 * sx * fy * fz, 0.125 * sy * fx * fz, 0.125 * sz * fx * fy};
+        for (int i = 0; i < 3; ++i)
+            for (int d = 0; d < 3; ++d) J[i][d] += xv[k][i] * gr[d];
+    }
+    const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                       J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                       J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+    const double wd = w * fabs(det);
+    double inv[3][3];
+    inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+    inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+    inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+    inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+    inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+    inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+    inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+    inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+    inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    const double s = wd * kap * c_k;
+    const int mi[6] = {0, 0, 0, 1, 1, 2}, ni[6] = {0, 1, 2, 1, 2, 2};
+    for (int k = 0; k < 6; ++k) {
+        const int a = mi[k], b = ni[k];
+        D[k] = s * (inv[a][0] * inv[b][0] + inv[a][1] * inv[b][1] + inv[a][2] * inv[b][2]);
+    }
+    m = wd * rho * c_m;
+    return fabs(det) > 0.0;
+}
+
 template <int P, int OPK, typename T>
 __global__ void qdata_setup_kernel(const SetupArgs S, T *__restrict__ qd) {
     constexpr int Q = P + 1, NC = NComp<OPK>::v;
@@ -1267,62 +1309,31 @@ __global__ void qdata_setup_kernel(const SetupArgs S, T *__restrict__ qd) {
         const double w = S.gw[qx] * S.gw[qy] * S.gw[qz];
         const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
                                {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
-        double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        double xv[8][3];
         for (int k = 0; k < 8; ++k) {
-            const double sx = off[k][0] ? 1.0 : -1.0, sy = off[k][1] ? 1.0 : -1.0,
-                         sz = off[k][2] ? 1.0 : -1.0;
-            const double fx = 1.0 + sx * xi[0], fy = 1.0 + sy * xi[1], fz = 1.0 + sz * xi[2];
-            const double gr[3] = {0.125 * sx * fy * fz, 0.125 * sy * fx * fz, 0.125 * sz * fx * fy};
             const int vi = ex + off[k][0], vj = ey + off[k][1], vk = ez + off[k][2];
-            double xv[3];
             if (S.vcoord) {
                 const int64_t id = ((int64_t)vk * (g.ny + 1) + vj) * (g.nx + 1) + vi;
-                xv[0] = S.vcoord[3 * id];
-                xv[1] = S.vcoord[3 * id + 1];
-                xv[2] = S.vcoord[3 * id + 2];
+                xv[k][0] = S.vcoord[3 * id];
+                xv[k][1] = S.vcoord[3 * id + 1];
+                xv[k][2] = S.vcoord[3 * id + 2];
             } else {
-                xv[0] = (double)vi / g.nx;
-                xv[1] = (double)vj / g.ny;
-                xv[2] = (double)vk / g.nz;
+                xv[k][0] = (double)vi / g.nx;
+                xv[k][1] = (double)vj / g.ny;
+                xv[k][2] = (double)vk / g.nz;
             }
-            for (int i = 0; i < 3; ++i)
-                for (int d = 0; d < 3; ++d) J[i][d] += xv[i] * gr[d];
         }
-        const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
-                           J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
-                           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
-        if (!(fabs(det) > 0.0)) {
-            if (S.err) atomicOr(S.err, FG_DERR_BOUNDS);
-        }
-        const double wd = w * fabs(det);
+        const double kap = S.kappa_q ? S.kappa_q[e * (Q * Q * Q) + q] : S.kappa_c;
+        const double rho = S.rho_q ? S.rho_q[e * (Q * Q * Q) + q] : S.rho_c;
+        double D[6], m;
+        if (!hex_point_qdata(xv, xi, w, kap, S.c_k, rho, S.c_m, D, m) && S.err) atomicOr(S.err, FG_DERR_BOUNDS);
         const int tx = ex / 32, lane = ex % 32, ty = ey / g.WY, wy = ey % g.WY, tz = ez / g.TZ,
                   lz = ez % g.TZ;
         const int item = (tz * g.nty + ty) * g.ntx + tx;
         T *dst = qd + qd_index<P, OPK>(g, item, wy, lz, qy * Q + qx, qz, 0, lane);
-        if (HK) {
-            double inv[3][3];
-            inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
-            inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
-            inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
-            inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
-            inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
-            inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
-            inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
-            inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
-            inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
-            const double kap = S.kappa_q ? S.kappa_q[e * (Q * Q * Q) + q] : S.kappa_c;
-            const double s = wd * kap * S.c_k;
-            const int mi[6] = {0, 0, 0, 1, 1, 2}, ni[6] = {0, 1, 2, 1, 2, 2};
-            for (int k = 0; k < 6; ++k) {
-                const int m = mi[k], n = ni[k];
-                const double v = inv[m][0] * inv[n][0] + inv[m][1] * inv[n][1] + inv[m][2] * inv[n][2];
-                dst[k * 32] = (T)(s * v);
-            }
-        }
-        if (HM) {
-            const double rho = S.rho_q ? S.rho_q[e * (Q * Q * Q) + q] : S.rho_c;
-            dst[(HK ? 6 : 0) * 32] = (T)(wd * rho * S.c_m);
-        }
+        if (HK)
+            for (int k = 0; k < 6; ++k) dst[k * 32] = (T)D[k];
+        if (HM) dst[(HK ? 6 : 0) * 32] = (T)m;
         (void)NC;
     }
 }

@@ -256,8 +256,12 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_pupdate(int64_t n, const T 
     const T beta = init ? T(0) : (T)st->beta;
     FG_VEC4_LOOP(q, n) {
         const V4<T> zv = ld4(z, q);
-        V4<T> pv = ld4(p, q);
-        FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        // the first direction is z itself: the previous contents of p (a
+        // finished solve's, possibly not finite) are not read
+        V4<T> pv = init ? zv : ld4(p, q);
+        if (!init) {
+            FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        }
         st4(p, q, pv);
     }
 }
@@ -876,8 +880,10 @@ __global__ void __launch_bounds__(VEC_THREADS) kb_pupdate(const BatchVec *bv, in
     const float beta = init ? 0.0f : (float)B.st->beta;
     FG_VEC4_LOOP(q, B.n) {
         const V4<float> zv = ld4(B.z, q);
-        V4<float> pv = ld4(B.p, q);
-        FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        V4<float> pv = init ? zv : ld4(B.p, q);  // first direction: p is not read
+        if (!init) {
+            FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        }
         st4(B.p, q, pv);
     }
 }
@@ -984,8 +990,10 @@ __global__ void __launch_bounds__(VEC_THREADS) k_fcg_pupdate_pr(int64_t n, const
     double v[1] = {0.0};
     FG_VEC4_LOOP(q, n) {
         const V4<T> zv = ld4(z, q), rv = ld4(r, q);
-        V4<T> pv = ld4(p, q);
-        FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        V4<T> pv = init ? zv : ld4(p, q);  // first direction: p is not read
+        if (!init) {
+            FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        }
         st4(p, q, pv);
         FG_K4 v[0] += (double)pv.a[k] * (double)rv.a[k];
     }

@@ -46,7 +46,8 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_op_collect_residuals", "fg_unet_train_energy", "fg_quadrature_points",
            "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply", "fg_op_set_tile",
            "fg_op_tile", "fg_batch_autotune", "fg_tet_create", "fg_tet_destroy", "fg_tet_ndofs", "fg_tet_nq",
-           "fg_tet_quadrature_points", "fg_tet_apply", "fg_tet_diagonal", "fg_op_set_wait_limit")
+           "fg_tet_quadrature_points", "fg_tet_apply", "fg_tet_diagonal", "fg_op_set_wait_limit",
+           "fg_op_create_hex", "fg_op_colours")
 
 
 class FgMesh(C.Structure):
@@ -147,6 +148,9 @@ def lib():
         L.fg_tet_diagonal.argtypes = [vp, vp, i, i]
         L.fg_op_apply_native_f32.argtypes = [vp, vp, vp, i, i]
         L.fg_op_set_wait_limit.argtypes = [vp, d]
+        L.fg_op_create_hex.argtypes = [i, i64, vp, i64, vp, vp, i64, i, d, d, vp, d, vp, d, vp, i64,
+                                       C.POINTER(vp)]
+        L.fg_op_colours.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -401,6 +405,57 @@ class PAOperator:
         if rc not in (FG_OK, FG_CONVERGENCE_FAILED):
             _check(rc)
         return res
+
+
+class HexMeshOperator(PAOperator):
+    """PA operator on an unstructured Hex8 mesh: PAMassOperator /
+    PADiffusionOperator::new over any connectivity and DOF numbering
+    (partial.rs:65-80, 138-149 with the Hex8 geometry of assembler.rs:96-143).
+
+    ``coords``: (n_nodes, 3); ``conn``: (E, 8) vertex ids in HexQ1 order
+    (hex.rs:27-36); ``elem_dofs``: (E, (p+1)^3) element DOF maps (order 1: None
+    means DOF = node, as DofManager::build_p1; orders 2-3: tensor order on the
+    reference cube, local DOF (c, b, a) at (c*(p+1) + b)*(p+1) + a);
+    ``kappa`` / ``rho``: scalar or (E, (p+1)^3) at the tensor Gauss points;
+    ``ess_dofs``: the essential-DOF list (boundary_dofs, constraints.rs:53-60).
+    Vectors are plain (native layout = plain numbering).  The scatter is a
+    coloured element loop (no float atomics, same sums every run).
+    """
+
+    def __init__(self, order, coords, conn, elem_dofs=None, n_dofs=None, kind=DIFF, kappa=1.0, rho=1.0,
+                 c_mass=1.0, c_diff=1.0, ess_dofs=None):
+        self.order, self.kind = int(order), kind
+        xyz = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+        cn = np.ascontiguousarray(conn, dtype=np.uint32).reshape(-1, 8)
+        E = cn.shape[0]
+        nl = (self.order + 1) ** 3
+        ed = None if elem_dofs is None else np.ascontiguousarray(elem_dofs, dtype=np.uint32).reshape(E, nl)
+        if n_dofs is None:
+            n_dofs = xyz.shape[0] if ed is None else int(ed.max()) + 1
+        kq = None if np.isscalar(kappa) else np.ascontiguousarray(kappa, dtype=np.float64)
+        rq = None if np.isscalar(rho) else np.ascontiguousarray(rho, dtype=np.float64)
+        for arr in (kq, rq):
+            if arr is not None and arr.size != E * nl:
+                raise DimensionMismatch(FG_DIMENSION_MISMATCH, "coefficient array has wrong size")
+        ess = None if ess_dofs is None else np.ascontiguousarray(ess_dofs, dtype=np.uint32)
+        h = C.c_void_p()
+        rc = lib().fg_op_create_hex(self.order, xyz.shape[0], xyz.ctypes.data, E, cn.ctypes.data,
+                                    None if ed is None else ed.ctypes.data, int(n_dofs), kind, float(c_mass),
+                                    float(c_diff), None if kq is None else kq.ctypes.data,
+                                    float(kappa) if kq is None else 0.0, None if rq is None else rq.ctypes.data,
+                                    float(rho) if rq is None else 0.0, None if ess is None else ess.ctypes.data,
+                                    0 if ess is None else ess.size, C.byref(h))
+        _check(rc)
+        self._h = h
+        self.nx = self.ny = self.nz = None
+        dims = (C.c_int64 * 4)()
+        lib().fg_op_layout(self._h, dims)
+        self.NI, self.NJ, self.NK, self.NIp = (int(v) for v in dims)
+
+    @property
+    def colours(self):
+        """Element colours of the deterministic scatter (one launch each)."""
+        return int(lib().fg_op_colours(self._h))
 
 
 class PADiffusionOperator(PAOperator):

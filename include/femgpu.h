@@ -138,6 +138,38 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
                         const double *rho_q, double rho_const, int ess_tags, fg_op **out);
 FG_API void fg_op_destroy(fg_op *op);
 
+/* Build the operator on an unstructured Hex8 mesh with the caller's DOF
+ * numbering: PAMassOperator::new / PADiffusionOperator::new(space, ...)
+ * (crates/assembly/src/partial.rs:65-80, 138-149) for a space whose element
+ * maps come from a DofManager (crates/space/src/dof_manager.rs:119-128), with
+ * the essential DOFs of boundary_dofs (crates/space/src/constraints.rs:53-60)
+ * as a list.  coords [n_nodes][3]; conn [n_elem][8] vertex ids in HexQ1 order
+ * (crates/element/src/lagrange/hex.rs:27-36); elem_dofs [n_elem][(p+1)^3]:
+ * order 1 in the HexQ1 vertex order, or NULL for DOF = node
+ * (DofManager::build_p1); orders 2-3 in tensor order on the reference cube,
+ * local DOF (c, b, a) at (c*(p+1) + b)*(p+1) + a, node (a, b, c) at
+ * reference point (-1 + 2a/p, -1 + 2b/p, -1 + 2c/p) (the reference has no Q2/Q3
+ * hex element; this is the equispaced tensor Lagrange element of this
+ * library).  kappa_q / rho_q [n_elem][qz][qy][qx] at the tensor Gauss points
+ * or NULL for the constants; ess_dofs [n_ess] (may repeat, order free).  All
+ * arrays in host or device memory.  Geometry is trilinear from the 8
+ * vertices (assembler.rs:96-143); a degenerate element gives FG_BOUNDS.
+ * Vectors of the handle are plain (fg_op_layout: {n_dofs, 1, 1, n_dofs}), so
+ * the *_native entry points take plain device vectors.  fg_op_apply,
+ * fg_op_apply_native(_f32), fg_op_diagonal and fg_pcg (FG_PC_NONE, JACOBI,
+ * CHEBYSHEV; FP64 and FG_FP32_IR) work as for a box; entry points that need
+ * the box's lattice or tiles (affine format, tiles, batches, SDIRK-2, the
+ * learned correction, the no-alloc apply) return FG_UNSUPPORTED.  The scatter
+ * is coloured: elements that share no DOF form a colour and each colour is
+ * one launch adding into y (no float atomics; the same sums every run). */
+FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double *coords, int64_t n_elem,
+                            const uint32_t *conn, const uint32_t *elem_dofs, int64_t n_dofs, int kind,
+                            double c_mass, double c_diff, const double *kappa_q, double kappa_const,
+                            const double *rho_q, double rho_const, const uint32_t *ess_dofs, int64_t n_ess,
+                            fg_op **out);
+/* Element colours of an operator from fg_op_create_hex (0 for a box). */
+FG_API int fg_op_colours(const fg_op *op);
+
 /* MatFreeOperator::n_dofs / LinearOperator::{nrows,ncols}. */
 FG_API int64_t fg_op_ndofs(const fg_op *op);
 
