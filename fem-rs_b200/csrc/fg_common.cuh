@@ -93,14 +93,28 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  "r"(bytes)
                  : "memory");
 }
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+// Non-blocking test of a phase of an mbarrier.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, P1;\n\t}"
         : "=r"(ok)
         : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Potentially blocking test: the thread may be suspended until the phase
+// completes or for at most about hint_ns nanoseconds.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
         : "memory");
     return ok != 0;
 }
@@ -111,13 +125,15 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 // Wait for a phase of an mbarrier with a time limit.  On timeout the error
 // word gets FG_DERR_TIMEOUT and false is returned; the caller stops issuing
-// work and drains what it has in flight.
+// work and drains what it has in flight.  The first test does not block, and
+// a suspended try never outlasts the limit, so a short limit is honoured.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err,
                                           uint64_t limit_ns = 1000000000ull) {
-    if (mbar_try_wait(bar, parity)) return true;
-    uint64_t t0 = globaltimer_ns();
+    if (mbar_test_wait(bar, parity)) return true;
+    const uint32_t hint = (uint32_t)(limit_ns < 0xffffffffull ? limit_ns : 0xffffffffull);
+    const uint64_t t0 = globaltimer_ns();
     while (true) {
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait(bar, parity, hint)) return true;
         if (globaltimer_ns() - t0 > limit_ns) {
             if (err) atomicOr(err, FG_DERR_TIMEOUT);
             return false;

@@ -38,7 +38,7 @@ static int hex_apply_t(fg_op *op, HexApply<T> A) {
     return FG_OK;
 }
 
-// y (+)= A x on plain vectors (the native layout of an unstructured operator).
+// y (+)= A x on native vectors of an unstructured operator (the plain values, then zero pads).
 template <typename T>
 static int hex_apply(fg_op *op, const T *qd, const T *x, T *y, int accumulate, int constrained, const int *skip) {
     HexApply<T> A = hex_args<T>(op, qd, x, y, constrained, skip);
@@ -128,7 +128,7 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
         return fail(FG_INVALID_ARGUMENT, "empty mesh or NULL coordinates / connectivity");
     if (order > 1 && !elem_dofs) return fail(FG_INVALID_ARGUMENT, "order %d needs the element DOF maps", order);
     if (n_ess < 0 || (n_ess > 0 && !ess_dofs)) return fail(FG_INVALID_ARGUMENT, "bad essential-DOF list");
-    if (n_dofs >= ((int64_t)1 << 31) || n_elem >= ((int64_t)1 << 31))
+    if (n_dofs >= ((int64_t)1 << 31) - 4 || n_elem >= ((int64_t)1 << 31))
         return fail(FG_INVALID_ARGUMENT, "more than 2^31 DOFs or elements");
     const int D = order + 1, nl = D * D * D, Q3 = nl;
     const int64_t E = n_elem, N = n_dofs;
@@ -194,12 +194,14 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
     op->u_E = E;
     op->u_col = start;
     op->N = N;
-    op->Nn = N;
-    Grid &g = op->g;  // plain vectors: one row of N values, no pads, no tiles
+    // native vectors: one row of the N plain values padded with zeros to a
+    // multiple of 4 (the solver's vector kernels work in 4-wide groups); no tiles
+    op->Nn = round_up((int)N, 4);
+    Grid &g = op->g;
     g.p = order;
     g.NI = (int)N;
     g.NJ = g.NK = 1;
-    g.NIp = (int)N;
+    g.NIp = (int)op->Nn;
     g.WY = 1;
     g.TZ = 1;
     auto bail = [&](int s) { free_op(op); return s; };
@@ -214,7 +216,7 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
         cudaMalloc(&op->st, sizeof(SolverState)) != cudaSuccess ||
         cudaMemset(op->st, 0, sizeof(SolverState)) != cudaSuccess)
         return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
-    if ((rc = alloc_vec(&op->xs, N)) || (rc = alloc_vec(&op->ys, N)) || (rc = alloc_vec(&op->face, 1)) ||
+    if ((rc = alloc_vec(&op->xs, op->Nn)) || (rc = alloc_vec(&op->ys, op->Nn)) || (rc = alloc_vec(&op->face, 1)) ||
         (rc = alloc_vec(&op->partials, VEC_GRID * 4)))
         return bail(rc);
     cudaEventCreate(&op->ev0);

@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_true_residual(int64_t n, const 
     }
     double tot[1];
     if (grid_sum<1>(v, partials, st, tot) && threadIdx.x == 0)
-        st->tmp[0] = st->bnorm > 0.0 ? sqrt(tot[0]) / st->bnorm : 0.0;
+        st->tmp[0] = st->bnorm == 0.0 ? 0.0 : sqrt(tot[0]) / st->bnorm;
 }
 
 // Deterministic splitmix64 start vector in [-1,1) on the plain DOF index
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_ir_residual(int64_t n, const do
         }
         st->rr = tot[0];
         const double rn = sqrt(tot[0]);
-        st->res = st->bnorm > 0.0 ? rn / st->bnorm : 0.0;
+        st->res = st->bnorm == 0.0 ? 0.0 : rn / st->bnorm;
         if (st->bnorm < 1e-30 || st->res < st->rtol || rn < st->atol) {
             st->converged = 1;
             st->done = 1;
@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_rel_residual(int64_t n, const d
         const double rn = sqrt(tot[0]);
         st->rr = tot[0];
         st->maxr = rn;
-        st->res = st->bnorm > 0.0 ? rn / st->bnorm : 0.0;
+        st->res = st->bnorm == 0.0 ? 0.0 : rn / st->bnorm;
         st->trigger = 0;
         st->skip_rel = 1;
         if (st->bnorm < 1e-30 || st->res < st->rtol || rn < st->atol) {
@@ -798,7 +798,7 @@ __global__ void __launch_bounds__(VEC_THREADS) kb_rel_residual(const BatchVec *b
         const double rn = sqrt(tot[0]);
         st->rr = tot[0];
         st->maxr = rn;
-        st->res = st->bnorm > 0.0 ? rn / st->bnorm : 0.0;
+        st->res = st->bnorm == 0.0 ? 0.0 : rn / st->bnorm;
         st->trigger = 0;
         st->skip_rel = 1;
         if (st->bnorm < 1e-30 || st->res < st->rtol || rn < st->atol) {
@@ -906,7 +906,7 @@ __global__ void __launch_bounds__(VEC_THREADS) kb_true_residual(const BatchVec *
     }
     double tot[1];
     if (grid_sum<1>(v, B.partials, st, tot) && threadIdx.x == 0)
-        st->tmp[0] = st->bnorm > 0.0 ? sqrt(tot[0]) / st->bnorm : 0.0;
+        st->tmp[0] = st->bnorm == 0.0 ? 0.0 : sqrt(tot[0]) / st->bnorm;
 }
 
 // st->tmp[2] = ||v|| (FP64)

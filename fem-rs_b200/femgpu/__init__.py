@@ -418,7 +418,7 @@ class HexMeshOperator(PAOperator):
     reference cube, local DOF (c, b, a) at (c*(p+1) + b)*(p+1) + a);
     ``kappa`` / ``rho``: scalar or (E, (p+1)^3) at the tensor Gauss points;
     ``ess_dofs``: the essential-DOF list (boundary_dofs, constraints.rs:53-60).
-    Vectors are plain (native layout = plain numbering).  The scatter is a
+    Native vectors are the plain numbering padded with zeros to a multiple of 4.  The scatter is a
     coloured element loop (no float atomics, same sums every run).
     """
 

@@ -154,8 +154,8 @@ FG_API void fg_op_destroy(fg_op *op);
  * or NULL for the constants; ess_dofs [n_ess] (may repeat, order free).  All
  * arrays in host or device memory.  Geometry is trilinear from the 8
  * vertices (assembler.rs:96-143); a degenerate element gives FG_BOUNDS.
- * Vectors of the handle are plain (fg_op_layout: {n_dofs, 1, 1, n_dofs}), so
- * the *_native entry points take plain device vectors.  fg_op_apply,
+ * The native layout of the handle is the plain numbering padded with zeros
+ * to a multiple of 4 values (fg_op_layout: {n_dofs, 1, 1, round_up(n_dofs, 4)}).  fg_op_apply,
  * fg_op_apply_native(_f32), fg_op_diagonal and fg_pcg (FG_PC_NONE, JACOBI,
  * CHEBYSHEV; FP64 and FG_FP32_IR) work as for a box; entry points that need
  * the box's lattice or tiles (affine format, tiles, batches, SDIRK-2, the

@@ -55,8 +55,10 @@ def perturbed_vertices(nx, ny, nz, amp, rng):
 def scrambled_mesh(nx, ny, nz, p, kq, seed):
     """The box (nx, ny, nz) of order p as an unstructured Hex8 mesh with random
     node / DOF / element numbering and a random reference-frame symmetry per
-    element.  Returns the arrays of fg_op_create_hex, the DOF permutation
-    (new id of box DOF d) and the permuted kappa table."""
+    element.  Returns the arrays of fg_op_create_hex (element DOF maps in the
+    tensor order of the new frame, or in HexQ1 vertex order for p = 1), the
+    node and DOF permutations (new id of box vertex / DOF d) and the kappa
+    table at the new frames' Gauss points."""
     rng = np.random.default_rng(seed)
     q = p + 1
     NI, NJ, NK = nx * p + 1, ny * p + 1, nz * p + 1
@@ -88,6 +90,8 @@ def scrambled_mesh(nx, ny, nz, p, kq, seed):
             ed[s, k] = pd[((ez * p + t[2]) * NJ + ey * p + t[1]) * NI + ex * p + t[0]]
             if kq is not None:
                 kq_new[s, k] = kq[e * q ** 3 + (t[2] * q + t[1]) * q + t[0]]
+    if p == 1:  # order-1 element DOF maps are given in the HexQ1 vertex order
+        ed = np.ascontiguousarray(ed[:, [(c * 2 + b) * 2 + a for a, b, c in HEXQ1]])
     return conn, ed, pn, pd, kq_new
 
 
