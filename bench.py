@@ -363,7 +363,8 @@ def run_solves(op, n, p, kq, rank):
                 op.set_qdata_format(fmt)
                 xs = np.zeros(N)
                 cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=20000, cheb_degree=4, precision=prec,
-                                          nn_budget=detail[plain_key]["iterations"])
+                                          nn_budget=detail[plain_key]["iterations"],
+                                          nn_iter_ratio=float(meta.get("iter_ratio", 0.0)))
                 r = op.pcg(b, xs, cfg, femgpu.PC_CHEB_NN)
                 detail[name] = {
                     "iterations": r.iterations, "solve_s": r.solve_ms / 1e3, "true_residual": r.true_residual,

@@ -231,6 +231,10 @@ struct fg_op {
     cudaEvent_t nn_ev_r = nullptr, nn_ev_n = nullptr;
     bool nn_overlap = true;                    // network beside the smoother (FG_NN_OVERLAP=0: in line)
     fg_unet *nn = nullptr;
+    // per-iteration device times (ms) of the plain and the learned
+    // preconditioned iteration, per (precision, qdata format, Chebyshev degree)
+    struct NnTimes { int ir, fmt, degree; double plain_ms, learned_ms; };
+    std::vector<NnTimes> nn_times;
     int fmt = 0;
     // unstructured Hex8 mesh (fg_op_create_hex): element maps sorted by colour,
     // colour starts, essential-DOF mask; vectors are plain (no pads)
@@ -1238,6 +1242,43 @@ template <typename T> static int nn_end(fg_op *op, const float *f1, T *z) {
     return nn_fe_prolong<T>(op, f1, z, op->nn_scale, nn_mult(op), 1);
 }
 
+// Device time of one preconditioned iteration without and with the learned
+// correction (the operator apply, then the Chebyshev smoother, the network
+// beside it), in storage precision T, on the solve's own buffers: r holds the
+// right-hand side (the network sees a residual-like input) and p a copy of it.
+// Three timed repetitions after one warm-up each, CUDA events on the handle's
+// stream.  Used before the timed solve to decide whether the network pays.
+template <typename T>
+static int nn_iteration_times(fg_op *op, const PcgBufs<T> &B, const ChebCoef &cc, T *r, T *z, T *p, T *ap,
+                              double *plain_ms, double *learned_ms) {
+    auto plain = [&]() -> int {
+        int rc = apply_native_t<T>(op, B.qd, B.face, p, ap, 0, 1, nullptr);
+        return rc ? rc : cheb_apply<T>(op, B, cc, r, z, nullptr);
+    };
+    auto learned = [&]() -> int {
+        const float *f1 = nullptr;
+        int rc = apply_native_t<T>(op, B.qd, B.face, p, ap, 0, 1, nullptr);
+        if (!rc) rc = nn_begin<T>(op, r, &f1);
+        if (!rc) rc = cheb_apply<T>(op, B, cc, r, z, nullptr);
+        return rc ? rc : nn_end<T>(op, f1, z);
+    };
+    auto timed = [&](const std::function<int()> &fn, double *ms) -> int {
+        int rc = fn();
+        if (rc) return rc;
+        CK(cudaEventRecord(op->ev0, op->stream));
+        for (int k = 0; k < 3; ++k)
+            if ((rc = fn())) return rc;
+        CK(cudaEventRecord(op->ev1, op->stream));
+        CK(cudaEventSynchronize(op->ev1));
+        float m = 0.f;
+        CK(cudaEventElapsedTime(&m, op->ev0, op->ev1));
+        *ms = m / 3.0;
+        return FG_OK;
+    };
+    int rc = timed(plain, plain_ms);
+    return rc ? rc : timed(learned, learned_ms);
+}
+
 // Flexible CG (FCG(1), Notay) with z = Chebyshev(r) [+ learned correction];
 // once `budget` iterations pass without convergence the learned term is
 // dropped and the solve continues as plain Chebyshev-preconditioned CG from
@@ -1420,6 +1461,47 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
         const Vol Vc = nn_coarse_vol(op);
         if ((rc = unet_ensure_bufs(op->nn, 1, Vc.Z, Vc.Y, Vc.X))) return rc;
     }
+    // Whether the network pays: with the plain iteration count (nn_budget) and
+    // the network's expected iteration ratio (nn_iter_ratio) given, the learned
+    // solve is predicted to take ratio * budget iterations of the learned cost
+    // against budget iterations of the plain cost; the per-iteration costs are
+    // measured once per handle, format and degree (outside the timed solve).
+    // When the prediction is not faster the solve runs as plain Chebyshev-PCG
+    // from the start (nn_fallback = 2).
+    bool use_nn = learned;
+    if (learned && cfg.nn_budget > 0 && cfg.nn_iter_ratio > 0.0) {
+        const int deg = cfg.cheb_degree;
+        const fg_op::NnTimes *t = nullptr;
+        for (const auto &e : op->nn_times)
+            if (e.ir == (int)ir && e.fmt == op->fmt && e.degree == deg) t = &e;
+        if (!t) {
+            fg_op::NnTimes e{(int)ir, op->fmt, deg, 0.0, 0.0};
+            set_state(op, op->st, cfg.rtol, cfg.atol, cfg.max_iter);
+            if (!ir) {
+                PcgBufs<double> B{op->qd, op->face, dinv_use, op->xw, op->bw, op->r, op->z, op->pv,
+                                  op->ap, op->cres, op->cd, op->ct, op->st};
+                CK(cudaMemcpyAsync(op->r, op->bw, sizeof(double) * n, cudaMemcpyDeviceToDevice, op->stream));
+                CK(cudaMemcpyAsync(op->pv, op->bw, sizeof(double) * n, cudaMemcpyDeviceToDevice, op->stream));
+                rc = nn_iteration_times<double>(op, B, cc, op->r, op->z, op->pv, op->ap, &e.plain_ms,
+                                                &e.learned_ms);
+            } else {
+                PcgBufs<float> B{op->qd32, op->face32, op->dinv32, op->e32, nullptr, op->r32, op->z32, op->p32,
+                                 op->ap32, op->cres32, op->cd32, op->ct32, op->st};
+                k_to_f32<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->r32);
+                k_to_f32<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->p32);
+                CK(cudaGetLastError());
+                rc = nn_iteration_times<float>(op, B, cc, op->r32, op->z32, op->p32, op->ap32, &e.plain_ms,
+                                               &e.learned_ms);
+            }
+            if (rc) return rc;
+            op->nn_times.push_back(e);
+            t = &op->nn_times.back();
+        }
+        if (cfg.nn_iter_ratio * t->learned_ms >= t->plain_ms) {
+            use_nn = false;
+            fell_back = 2;
+        }
+    }
     CK(cudaStreamSynchronize(op->stream));
     CK(cudaEventRecord(op->ev0, op->stream));
     if (!ir) {
@@ -1427,7 +1509,7 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
                           op->ap, op->cres, op->cd, op->ct, op->st};
         // FG_PC_NONE is the operator CG of solve_cg_operator, with its stopping rule
         set_state(op, op->st, cfg.rtol, cfg.atol, cfg.max_iter, cfg.precond == FG_PC_NONE ? 1 : 0);
-        if (learned) {
+        if (learned && use_nn) {
             if ((rc = fcg_nn_run(op, B, cc, cfg.max_iter, cfg.check_interval, cfg.nn_budget, &h, &applies,
                                  &fell_back)))
                 return rc;
@@ -1466,9 +1548,9 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
         k_rel_residual<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, op->bw, op->ap, op->r32,
                                                                  op->partials, op->st, 1);
         // z = M r_lo ; p = z ; rz
-        bool nn_on = learned;
+        bool nn_on = learned && use_nn;
         auto precond = [&](int init) -> int {
-            if (learned) {  // flexible directions: z = Chebyshev(r) [+ learned correction]
+            if (learned && use_nn) {  // flexible directions: z = Chebyshev(r) [+ learned correction]
                 const float *f1 = nullptr;
                 int rc2;
                 if (nn_on && (rc2 = nn_begin<float>(op, op->r32, &f1))) return rc2;
@@ -2680,6 +2762,7 @@ FG_API int fg_op_attach_unet(fg_op *op, fg_unet *net) {
     std::lock_guard<std::mutex> lk(op->mu);
     if (net && net->device != op->device) return fail(FG_INVALID_ARGUMENT, "network on another device");
     op->nn = net;
+    op->nn_times.clear();
     return FG_OK;
 }
 

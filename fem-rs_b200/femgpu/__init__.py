@@ -59,7 +59,7 @@ class FgCfg(C.Structure):
                 ("print_level", C.c_int32), ("precond", C.c_int32), ("cheb_degree", C.c_int32),
                 ("precision", C.c_int32), ("power_iters", C.c_int32), ("lmax", C.c_double),
                 ("lmin_ratio", C.c_double), ("lmax_safety", C.c_double), ("inner_rtol", C.c_double),
-                ("check_interval", C.c_int32), ("nn_budget", C.c_int32)]
+                ("check_interval", C.c_int32), ("nn_budget", C.c_int32), ("nn_iter_ratio", C.c_double)]
 
 
 class FgSdirkResult(C.Structure):
@@ -214,6 +214,7 @@ class SolverConfig:
     inner_rtol: float = 0.1
     check_interval: int = 10
     nn_budget: int = 0
+    nn_iter_ratio: float = 0.0
 
     def to_c(self, precond):
         c = FgCfg()
@@ -223,7 +224,7 @@ class SolverConfig:
         c.precond, c.cheb_degree, c.precision = precond, self.cheb_degree, self.precision
         c.power_iters, c.lmax, c.lmin_ratio = self.power_iters, self.lmax, self.lmin_ratio
         c.lmax_safety, c.inner_rtol, c.check_interval = self.lmax_safety, self.inner_rtol, self.check_interval
-        c.nn_budget = self.nn_budget
+        c.nn_budget, c.nn_iter_ratio = self.nn_budget, self.nn_iter_ratio
         return c
 
 

@@ -98,10 +98,36 @@ FORMS = {  # name: (precision, qdata format)
 }
 
 
-def evaluate(net, n, seeds, levels=2, p=1, forms=("fp64",), rhs="random", rtol=1e-8):
+def calibrate(net, n, seeds, levels=2, p=1, form="fp32_mixed", rhs="random", rtol=1e-8):
+    """Expected ratio of learned to plain iterations of the network on its
+    problem family, measured on validation fields (seeds disjoint from the
+    training and the held-out test seeds) with the network always on.  The
+    solver uses it (SolverConfig.nn_iter_ratio) to decide whether the network
+    pays on a given operator and form."""
+    prec, fmt = FORMS[form]
+    plain, learned = [], []
+    for s in seeds:
+        op, b = make_problem(n, s, levels, p, rhs)
+        op.set_qdata_format(fmt)
+        r0 = op.pcg(b, np.zeros(op.n_dofs()), femgpu.SolverConfig(rtol=rtol, max_iter=20000, precision=prec),
+                    femgpu.PC_CHEBYSHEV)
+        femgpu.attach_unet(op, net)
+        r1 = op.pcg(b, np.zeros(op.n_dofs()), femgpu.SolverConfig(rtol=rtol, max_iter=20000, precision=prec),
+                    femgpu.PC_CHEB_NN)
+        femgpu.attach_unet(op, None)
+        plain.append(r0.iterations)
+        learned.append(r1.iterations)
+        op.close()
+    return float(np.sum(learned) / np.sum(plain)), {"seeds": [int(s) for s in seeds], "form": form,
+                                                      "plain_iterations": plain, "learned_iterations": learned}
+
+
+def evaluate(net, n, seeds, levels=2, p=1, forms=("fp64",), rhs="random", rtol=1e-8, iter_ratio=0.0):
     """Per held-out field: plain FP64 Chebyshev(4)-PCG (full qdata) against
     plain and learned flexible CG in each form; the learned solve's budget is
-    the plain iteration count of the same form."""
+    the plain iteration count of the same form, and with iter_ratio > 0 the
+    solver decides from measured per-iteration costs whether the network pays
+    (fallback 2: not used)."""
     rows = []
     for s in seeds:
         op, b = make_problem(n, s, levels, p, rhs)
@@ -117,7 +143,8 @@ def evaluate(net, n, seeds, levels=2, p=1, forms=("fp64",), rhs="random", rtol=1
                 x_ref = x0.copy()
             femgpu.attach_unet(op, net)
             x1 = np.zeros(op.n_dofs())
-            cfg1 = femgpu.SolverConfig(rtol=rtol, max_iter=20000, precision=prec, nn_budget=r0.iterations)
+            cfg1 = femgpu.SolverConfig(rtol=rtol, max_iter=20000, precision=prec, nn_budget=r0.iterations,
+                                       nn_iter_ratio=iter_ratio)
             r1 = op.pcg(b, x1, cfg1, femgpu.PC_CHEB_NN)
             femgpu.attach_unet(op, None)
             row[form] = {"plain_iterations": r0.iterations, "plain_s": r0.solve_ms / 1e3,
@@ -149,7 +176,9 @@ def summarise(rows, form):
             "mean_learned_iterations": float(np.mean([x["learned_iterations"] for x in r])),
             "mean_plain_s": float(np.mean([x["plain_s"] for x in r])),
             "mean_learned_s": float(np.mean([x["learned_s"] for x in r])),
-            "fallbacks": int(sum(x["fallback"] for x in r))}
+            "learned_not_slower": int(sum(x["learned_s"] <= x["plain_s"] for x in r)),
+            "fallbacks": int(sum(x["fallback"] == 1 for x in r)),
+            "network_not_used": int(sum(x["fallback"] == 2 for x in r))}
 
 
 def main():
@@ -171,6 +200,9 @@ def main():
     ap.add_argument("--init", default=None, help="start from these weights")
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--calibrate-fields", type=int, default=0,
+                    help="validation fields (seeds 50000+) for the expected iteration ratio stored with the weights")
+    ap.add_argument("--calibrate-form", default="fp32_mixed")
     args = ap.parse_args()
     t0 = time.perf_counter()
     init_meta = None
@@ -192,9 +224,19 @@ def main():
         save(net, args.out, meta)
     elif init_meta is not None:  # evaluation of stored weights
         meta = dict(init_meta, evaluation_only=True)
+    if args.calibrate_fields > 0:
+        ratio, cal = calibrate(net, args.n, list(range(50_000, 50_000 + args.calibrate_fields)), args.levels,
+                               args.p, args.calibrate_form, args.eval_rhs)
+        meta = {k: v for k, v in meta.items() if k != "evaluation_only"}
+        meta["iter_ratio"] = ratio
+        meta["calibration"] = cal
+        save(net, args.out, meta)
+        if not seeds:
+            meta = dict(meta, evaluation_only=True)
     forms = args.forms.split(",")
     eval_seeds = list(range(100_000, 100_000 + args.eval_fields))
-    rows = evaluate(net, args.n, eval_seeds, args.levels, args.p, forms, args.eval_rhs)
+    rows = evaluate(net, args.n, eval_seeds, args.levels, args.p, forms, args.eval_rhs,
+                    iter_ratio=float(meta.get("iter_ratio", 0.0)))
     summary = {"meta": meta, **{f: summarise(rows, f) for f in forms}, "eval": rows}
     print(json.dumps(summary))
     if args.report:

@@ -105,7 +105,14 @@ typedef struct {
     int32_t check_interval;/* iterations between host polls of the device flag */
     int32_t nn_budget;     /* FG_PC_CHEB_NN: iterations after which an unconverged solve
                               drops the learned term and continues as plain Chebyshev-
-                              preconditioned CG (0 = never) */
+                              preconditioned CG (0 = never); the plain solve's count */
+    double nn_iter_ratio;  /* FG_PC_CHEB_NN with nn_budget > 0: the network's expected
+                              ratio of learned to plain iterations (measured on
+                              validation problems of its family; 0 = not known).  The
+                              solver measures one plain and one learned iteration on the
+                              handle (once per precision, format and degree, outside the
+                              timed solve) and runs plain Chebyshev-PCG from the start
+                              when ratio * learned cost >= plain cost (nn_fallback = 2) */
 } fg_cfg;
 
 typedef struct {
@@ -119,7 +126,9 @@ typedef struct {
     int64_t applies;         /* operator applications */
     double lmax;             /* Chebyshev upper bound used */
     double solve_ms;         /* device time of the solve */
-    int32_t nn_fallback;     /* FG_PC_CHEB_NN: 1 if the solve fell back to plain Chebyshev */
+    int32_t nn_fallback;     /* FG_PC_CHEB_NN: 1 if the solve fell back to plain Chebyshev
+                                after nn_budget iterations, 2 if the network was not used
+                                because it was predicted not to pay (see nn_iter_ratio) */
     int32_t reserved;
 } fg_result;
 
