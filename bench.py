@@ -22,8 +22,12 @@ gpurun_out/bench_detail.json when that folder exists).
 crates/assembly/src/partial.rs's element loop with the Hex8 isoparametric
 Jacobian) on the host cores, on the same full mesh as the GPU arm.
 
-Multi-GPU: one independent instance per rank (its own seeded kappa), no
-data-path collective; scaling is weak.
+Multi-GPU (--mode): "sharded" (the default for N > 1) splits ONE global
+problem into z slabs, one per rank: a step is one sharded apply (local apply
++ halo sum of the interface planes over NCCL), value = global DOFs x steps /
+max-over-ranks time (strong scaling), plus a sharded Jacobi-PCG solve to
+1e-8 with the vector work in the library's kernels.  "replicas" (the default
+for N = 1) runs one independent instance per rank (weak scaling).
 """
 from __future__ import annotations
 
@@ -603,6 +607,103 @@ def run_ex1():
             "converged": r1.converged}
 
 
+def run_sharded(args, n, p, world, rank, local, dev):
+    """One global n^3 Q{p} problem over all ranks (z slabs): the sharded apply
+    as the step, and a sharded Jacobi-PCG solve to 1e-8 (the solve of
+    crates/parallel/src/par_solver.rs:262-342)."""
+    import torch
+    import torch.distributed as dist
+
+    from femgpu import SolverConfig
+    from femgpu import sharded as S
+    from femgpu.fields import lognormal_kappa_q
+
+    comm = S.TorchComm() if world > 1 else S.ThreadGroup(1).comm(0)
+    kq = lognormal_kappa_q(n, n, n, p, sigma2=1.0, ell=0.1, seed=0)  # one global field
+    A = S.ShardedPAOperator(comm, (n, n, n), p, kappa=kq)
+    del kq
+    stream = torch.cuda.current_stream(dev)
+    N = (n * p + 1) ** 3
+    x = A.scatter(np.random.default_rng(1000).standard_normal(N))
+    y = A.zeros()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        A.apply(x, y)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        A.apply(x, y)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    t_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    value = N * args.steps / (t_ms / 1e3) / 1e9
+    # e2e: the rank's slab vector from pinned host memory, apply, result back
+    xh = x.cpu().pin_memory()
+    yh = torch.zeros_like(xh).pin_memory()
+    k_e2e = max(3, min(args.steps, 20))
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(k_e2e):
+        x.copy_(xh, non_blocking=True)
+        A.apply(x, y)
+        yh.copy_(y, non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    te_ms = max_over_ranks(f0.elapsed_time(f1), world, dev)
+    solve = None
+    if not args.no_solve:
+        b = A.scatter(dirichlet_rhs(n, p))
+        xs = A.zeros()
+        barrier()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        res = S.par_solve_pcg_jacobi(A, b, xs, SolverConfig(rtol=1e-8, max_iter=5000))
+        s1.record(stream)
+        torch.cuda.synchronize()
+        t_s = max_over_ranks(s0.elapsed_time(s1), world, dev) / 1e3
+        solve = {"jacobi_pcg_s": t_s, "iterations": res.iterations, "converged": res.converged,
+                 "final_residual": res.final_residual}
+    bytes_canon, _ = canonical_bytes(n, p)
+    peak, peak_kind = measured_peak()
+    achieved = bytes_canon / world / (t_ms / 1e3 / args.steps) / 1e9  # per GPU
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "GDOF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: one lognormal kappa GRF (sigma2=1, ell=0.1, seed 0) at Gauss points, x ~ N(0,1)",
+            "config": {"workload": f"{n}^3 Q{p} unit-cube hex, FP64 PA diffusion apply (constrained), {N} DOFs "
+                                   f"split into {world} z slabs", "order": p, "n_elem_1d": n,
+                       "l2": "inputs larger than L2 (qdata %.2f GB over all ranks)" % (6 * (p + 1) ** 3 * n ** 3 * 8 / 1e9),
+                       "parallelism": f"sharded over {world} ranks: slab apply + halo sum of the interface planes"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "per-rank pa_apply_kernel + fixup_kernel + plane exchange (per-GPU share of the "
+                                   "canonical bytes)"},
+            "e2e": {"value": N * k_e2e / (te_ms / 1e3) / 1e9, "unit": "GDOF/s",
+                    "h2d_bytes_per_step": int(xh.numel() * 8 * world), "d2h_bytes_per_step": int(yh.numel() * 8 * world),
+                    "steps": k_e2e},
+            "gpu_launches": 2 * args.steps, "clocks": clk, "cpu_baseline": None, "sharded_solve": solve,
+        }
+        print(json.dumps(out), flush=True)
+    A.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -614,6 +715,8 @@ def main():
                                                    "if that folder exists)")
     for opt in ("solve", "q3", "cpu", "heat", "batch", "tet", "ex1"):
         ap.add_argument(f"--no-{opt}", action="store_true")
+    ap.add_argument("--mode", default=None, choices=["replicas", "sharded"],
+                    help="multi-GPU form (default: replicas for 1 GPU, sharded for more)")
     ap.add_argument("--batch-n", type=int, default=256)
     ap.add_argument("--heat-steps", type=int, default=500)
     args = ap.parse_args()
@@ -636,6 +739,12 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
+    mode = args.mode or ("sharded" if world > 1 else "replicas")
+    if mode == "sharded":
+        run_sharded(args, n, p, world, rank, local, dev)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     kq = lognormal_kappa_q(n, n, n, p, sigma2=1.0, ell=0.1, seed=rank)
     op = femgpu.PADiffusionOperator((n, n, n), p, kappa=kq)

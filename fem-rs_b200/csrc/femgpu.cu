@@ -2373,6 +2373,63 @@ FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_ste
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Solver steps on caller-owned device vectors of a handle's native layout, for
+// loops whose dot products are completed outside the library (the sharded
+// PCG of crates/parallel/src/par_solver.rs:262-342: each rank's owned-DOF dots,
+// then the caller's allreduce, ParVector::global_dot, par_vector.rs:182-194).
+// The scalars stay in device memory; everything runs on the handle's stream.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+FG_API int fg_vec_dots(fg_op *op, int64_t n_own, int npairs, const double *const *a, const double *const *b,
+                       double *out) {
+    if (!op || !a || !b || !out) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (npairs < 1 || npairs > 3) return fail(FG_INVALID_ARGUMENT, "1 to 3 pairs");
+    if (n_own < 0 || n_own > op->Nn || n_own % 4) return fail(FG_INVALID_ARGUMENT, "n_own must be a multiple "
+                                                             "of 4 within the native length");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    VecPairs P{};
+    for (int j = 0; j < npairs; ++j) {
+        if (!a[j] || !b[j]) return fail(FG_INVALID_ARGUMENT, "NULL vector");
+        P.a[j] = a[j];
+        P.b[j] = b[j];
+    }
+    switch (npairs) {
+    case 1: k_sh_dots<1><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n_own, P, op->partials, op->st, out); break;
+    case 2: k_sh_dots<2><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n_own, P, op->partials, op->st, out); break;
+    default: k_sh_dots<3><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n_own, P, op->partials, op->st, out); break;
+    }
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+FG_API int fg_vec_pcg_update(fg_op *op, int64_t n_own, double *x, double *r, const double *p, const double *ap,
+                             const double *dinv, double *z, const double *rz_pap, double *rr_rz) {
+    if (!op || !x || !r || !p || !ap || !dinv || !z || !rz_pap || !rr_rz)
+        return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (n_own < 0 || n_own > op->Nn || n_own % 4) return fail(FG_INVALID_ARGUMENT, "n_own must be a multiple "
+                                                             "of 4 within the native length");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    k_sh_update<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->Nn, n_own, x, r, p, ap, dinv, z, rz_pap,
+                                                          op->partials, op->st, rr_rz);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+FG_API int fg_vec_pupdate(fg_op *op, const double *z, double *p, const double *num, const double *den) {
+    if (!op || !z || !p || !num || !den) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    std::lock_guard<std::mutex> lk(op->mu);
+    CK(cudaSetDevice(op->device));
+    k_sh_pupdate<<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(op->Nn, z, p, num, den);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Allocation-free apply.
 //
 // Same kernels as fg_op_apply_native, but the face-slot scratch that the

@@ -1002,3 +1002,84 @@ __global__ void __launch_bounds__(VEC_THREADS) k_fcg_pupdate_pr(int64_t n, const
 }
 
 }  // namespace fg
+
+// ---- steps of a solve whose dots are completed outside the library ----------
+// (the sharded PCG: each rank reduces over the DOFs it owns, the caller's
+// allreduce adds the ranks' partial sums, and the scalars stay on the
+// device).  The owned DOFs are the prefix [0, n_own) of the local vector (a
+// multiple of 4).  Same deterministic block-order sums as above.
+namespace fg {
+struct VecPairs {
+    const double *a[3];
+    const double *b[3];
+};
+
+// out[j] = sum_{i < n_own} a_j[i] b_j[i], j < NV
+template <int NV>
+__global__ void __launch_bounds__(VEC_THREADS) k_sh_dots(int64_t n_own, const VecPairs P, double *partials,
+                                                         SolverState *st, double *out) {
+    double v[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = 0.0;
+    FG_VEC4_LOOP(q, n_own) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const V4<double> av = ld4(P.a[j], q), bv = ld4(P.b[j], q);
+            FG_K4 v[j] += av.a[k] * bv.a[k];
+        }
+    }
+    double tot[NV];
+    if (grid_sum<NV>(v, partials, st, tot) && threadIdx.x == 0)
+#pragma unroll
+        for (int j = 0; j < NV; ++j) out[j] = tot[j];
+}
+
+// alpha = s[0] / s[1] (r.z / p.Ap after the allreduce); x += alpha p,
+// r -= alpha Ap, z = dinv r on the whole local vector; out = (r.r, r.z) over
+// the owned prefix
+__global__ void __launch_bounds__(VEC_THREADS) k_sh_update(int64_t n, int64_t n_own, double *__restrict__ x,
+                                                           double *__restrict__ r, const double *__restrict__ p,
+                                                           const double *__restrict__ ap,
+                                                           const double *__restrict__ dinv, double *__restrict__ z,
+                                                           const double *s, double *partials, SolverState *st,
+                                                           double *out) {
+    const double alpha = s[0] / s[1];
+    double v[2] = {0.0, 0.0};
+    FG_VEC4_LOOP(q, n) {
+        V4<double> xv = ld4(x, q), rv = ld4(r, q), zv;
+        const V4<double> pv = ld4(p, q), av = ld4(ap, q), dv = ld4(dinv, q);
+        FG_K4 {
+            xv.a[k] += alpha * pv.a[k];
+            rv.a[k] -= alpha * av.a[k];
+            zv.a[k] = dv.a[k] * rv.a[k];
+        }
+        st4(x, q, xv);
+        st4(r, q, rv);
+        st4(z, q, zv);
+        if (4 * q < n_own) {
+            FG_K4 {
+                v[0] += rv.a[k] * rv.a[k];
+                v[1] += rv.a[k] * zv.a[k];
+            }
+        }
+    }
+    double tot[2];
+    if (grid_sum<2>(v, partials, st, tot) && threadIdx.x == 0) {
+        out[0] = tot[0];
+        out[1] = tot[1];
+    }
+}
+
+// p = z + (num / den) p
+__global__ void __launch_bounds__(VEC_THREADS) k_sh_pupdate(int64_t n, const double *__restrict__ z,
+                                                            double *__restrict__ p, const double *num,
+                                                            const double *den) {
+    const double beta = *num / *den;
+    FG_VEC4_LOOP(q, n) {
+        const V4<double> zv = ld4(z, q);
+        V4<double> pv = ld4(p, q);
+        FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        st4(p, q, pv);
+    }
+}
+}  // namespace fg

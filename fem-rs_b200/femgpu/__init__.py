@@ -47,7 +47,7 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply", "fg_op_set_tile",
            "fg_op_tile", "fg_batch_autotune", "fg_tet_create", "fg_tet_destroy", "fg_tet_ndofs", "fg_tet_nq",
            "fg_tet_quadrature_points", "fg_tet_apply", "fg_tet_diagonal", "fg_op_set_wait_limit",
-           "fg_op_create_hex", "fg_op_colours")
+           "fg_op_create_hex", "fg_op_colours", "fg_vec_dots", "fg_vec_pcg_update", "fg_vec_pupdate")
 
 
 class FgMesh(C.Structure):
@@ -151,6 +151,9 @@ def lib():
         L.fg_op_create_hex.argtypes = [i, i64, vp, i64, vp, vp, i64, i, d, d, vp, d, vp, d, vp, i64,
                                        C.POINTER(vp)]
         L.fg_op_colours.argtypes = [vp]
+        L.fg_vec_dots.argtypes = [vp, i64, i, vp, vp, vp]
+        L.fg_vec_pcg_update.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.fg_vec_pupdate.argtypes = [vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 

@@ -26,15 +26,20 @@ rank, the z0 tag only on the first rank and the z1 tag only on the last;
 on an interface plane the essential rows are the identity on both sides
 and are not summed.
 
-Local work (apply, diagonal) runs through the C ABI on torch's current CUDA
-stream, with vectors in the native padded layout of fg_op_layout.
-Communication goes through a ``Comm``: ``TorchComm`` (torch.distributed;
-NCCL between GPUs, gloo between CPU processes) or ``ThreadGroup`` ranks
-(threads of one process, each with its own stream).  Vector updates are
-plain torch tensor arithmetic.
+Local work runs through the C ABI on torch's current CUDA stream, with
+vectors in the native padded layout of fg_op_layout: the apply, the
+diagonal, and in the PCG loop the owned-DOF dots, the x / r / z update and
+the direction update (fg_vec_dots, fg_vec_pcg_update, fg_vec_pupdate:
+deterministic block-order sums, scalars kept on the device, one allreduce
+per reduction step).  Communication goes through a ``Comm``: ``TorchComm``
+(torch.distributed; NCCL between GPUs, gloo between CPU processes) or
+``ThreadGroup`` ranks (threads of one process, each with its own stream).
+Local operators without those entry points (the CPU oracle slabs of the
+tests) take the same loop with torch tensor arithmetic.
 """
 from __future__ import annotations
 
+import ctypes as C
 import threading
 
 import numpy as np
@@ -81,13 +86,21 @@ class Comm:
 
 
 class TorchComm(Comm):
-    """torch.distributed process group (NCCL for CUDA tensors, gloo for CPU)."""
+    """torch.distributed process group (NCCL for CUDA tensors, gloo for CPU).
+    ``rank`` / ``size`` are positions within ``group``; the neighbours of the
+    plane exchange are translated to global ranks for the point-to-point
+    operations, so any group works, not only the default one."""
 
     def __init__(self, group=None):
         import torch.distributed as dist
 
         self._dist, self._group = dist, group
         self.rank, self.size = dist.get_rank(group), dist.get_world_size(group)
+
+    def _peer(self, group_rank):
+        if self._group is None:
+            return group_rank
+        return self._dist.get_global_rank(self._group, group_rank)
 
     def allreduce_sum(self, t):
         self._dist.all_reduce(t, op=self._dist.ReduceOp.SUM, group=self._group)
@@ -98,12 +111,14 @@ class TorchComm(Comm):
         ops, rlo, rhi = [], None, None
         if send_lo is not None:
             rlo = torch.empty_like(send_lo)
-            ops += [dist.P2POp(dist.isend, send_lo, self.rank - 1, self._group),
-                    dist.P2POp(dist.irecv, rlo, self.rank - 1, self._group)]
+            lo = self._peer(self.rank - 1)
+            ops += [dist.P2POp(dist.isend, send_lo, lo, self._group),
+                    dist.P2POp(dist.irecv, rlo, lo, self._group)]
         if send_hi is not None:
             rhi = torch.empty_like(send_hi)
-            ops += [dist.P2POp(dist.isend, send_hi, self.rank + 1, self._group),
-                    dist.P2POp(dist.irecv, rhi, self.rank + 1, self._group)]
+            hi = self._peer(self.rank + 1)
+            ops += [dist.P2POp(dist.isend, send_hi, hi, self._group),
+                    dist.P2POp(dist.irecv, rhi, hi, self._group)]
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
@@ -191,6 +206,24 @@ class GpuSlab:
         out = torch.zeros(self.NK, self.NJ, self.pitch, dtype=torch.float64, device=self.device)
         out[:, :, :self.NI] = d.view(self.NK, self.NJ, self.NI)
         return out.view(-1)
+
+    # solver steps on native vectors, owned prefix [0, n_own) ------------
+    def vec_dots(self, n_own, pairs, out):
+        """out[j] = a_j . b_j over the owned prefix (device tensor out)."""
+        self._stream()
+        a = (C.c_void_p * 3)(*([pa.data_ptr() for pa, _ in pairs] + [None] * (3 - len(pairs))))
+        b = (C.c_void_p * 3)(*([pb.data_ptr() for _, pb in pairs] + [None] * (3 - len(pairs))))
+        _check(lib().fg_vec_dots(self.op.handle, int(n_own), len(pairs), a, b, out.data_ptr()))
+
+    def vec_pcg_update(self, n_own, x, r, p, ap, dinv, z, rz_pap, rr_rz):
+        self._stream()
+        _check(lib().fg_vec_pcg_update(self.op.handle, int(n_own), x.data_ptr(), r.data_ptr(), p.data_ptr(),
+                                       ap.data_ptr(), dinv.data_ptr(), z.data_ptr(), rz_pap.data_ptr(),
+                                       rr_rz.data_ptr()))
+
+    def vec_pupdate(self, z, p, num, den):
+        self._stream()
+        _check(lib().fg_vec_pupdate(self.op.handle, z.data_ptr(), p.data_ptr(), num.data_ptr(), den.data_ptr()))
 
     def close(self):
         self.op.close()
@@ -325,6 +358,8 @@ def par_solve_pcg_jacobi(A: ShardedPAOperator, b, x, cfg: SolverConfig | None = 
     allreduce (same values).  b, x: consistent local vectors; x holds the
     guess on entry and the solution on exit."""
     cfg = cfg or SolverConfig()
+    if hasattr(A.local, "vec_pcg_update"):
+        return _pcg_jacobi_device(A, b, x, cfg)
     d = A.diagonal()
     inv = d.clone()
     big = d.abs() > 1e-30
@@ -356,5 +391,50 @@ def par_solve_pcg_jacobi(A: ShardedPAOperator, b, x, cfg: SolverConfig | None = 
         beta = rz_new / rz
         p.mul_(beta).add_(z)
         rz = rz_new
+    rr = A.dot(r, r)
+    return SolveResult(False, cfg.max_iter, rr ** 0.5 / b_norm, applies=cfg.max_iter + 1)
+
+
+def _pcg_jacobi_device(A: ShardedPAOperator, b, x, cfg: SolverConfig) -> SolveResult:
+    """par_solve_pcg_jacobi with the vector work in the library's kernels
+    (GPU slabs): the same iteration and stopping rule as the torch form
+    above; the scalars live on the device and the host reads p.Ap (the
+    breakdown test) and r.r (the stopping test) once per iteration, as the
+    reference's loop does."""
+    L, n_own = A.local, A.n_own
+    d = A.diagonal()
+    inv = torch.ones_like(d)
+    big = d.abs() > 1e-30
+    inv[big] = 1.0 / d[big]
+    ax = A.zeros()
+    A.apply(x, ax)
+    r = b - ax
+    z = inv * r
+    p = z.clone()
+    dev = r.device
+    init = torch.zeros(2, dtype=torch.float64, device=dev)
+    L.vec_dots(n_own, [(r, z), (b, b)], init)
+    A.comm.allreduce_sum(init)
+    b_norm = float(init[1]) ** 0.5
+    if b_norm < 1e-30:
+        return SolveResult(True, 0, 0.0)
+    rz_pap = torch.zeros(2, dtype=torch.float64, device=dev)
+    rr_rz = torch.zeros(2, dtype=torch.float64, device=dev)
+    rz_pap[0:1].copy_(init[0:1])
+    ap = A.zeros()
+    for it in range(cfg.max_iter):
+        A.apply(p, ap)
+        L.vec_dots(n_own, [(p, ap)], rz_pap[1:2])
+        A.comm.allreduce_sum(rz_pap[1:2])
+        if abs(float(rz_pap[1])) < 1e-30:
+            break
+        L.vec_pcg_update(n_own, x, r, p, ap, inv, z, rz_pap, rr_rz)
+        A.comm.allreduce_sum(rr_rz)
+        rn = float(rr_rz[0]) ** 0.5
+        res = rn / b_norm
+        if res < cfg.rtol or rn < cfg.atol:
+            return SolveResult(True, it + 1, res, applies=it + 2)
+        L.vec_pupdate(z, p, rr_rz[1:2], rz_pap[0:1])
+        rz_pap[0:1].copy_(rr_rz[1:2])
     rr = A.dot(r, r)
     return SolveResult(False, cfg.max_iter, rr ** 0.5 / b_norm, applies=cfg.max_iter + 1)

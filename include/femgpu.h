@@ -442,6 +442,25 @@ FG_API int fg_tet_diagonal(fg_tet *op, double *d, int constrained, int mem);
  * this library. */
 FG_API int fg_op_set_wait_limit(fg_op *op, double seconds);
 
+/* Steps of a PCG whose dot products are completed by the caller, on device
+ * vectors of the handle's native layout (fg_op_native_len values), on the
+ * handle's stream, scalars in device memory: the sharded solve of
+ * par_solve_pcg_jacobi (crates/parallel/src/par_solver.rs:262-342), where each
+ * rank reduces over the DOFs it owns and an allreduce adds the ranks' sums
+ * (ParVector::global_dot, crates/parallel/src/par_vector.rs:182-194).  The
+ * owned DOFs are the prefix [0, n_own) of the local vector, n_own a multiple
+ * of 4.  Reductions are summed in a fixed order (the same bits every run).
+ *   fg_vec_dots:       out[j] = a_j . b_j over the owned prefix, j < npairs <= 3
+ *   fg_vec_pcg_update: alpha = rz_pap[0] / rz_pap[1]; x += alpha p,
+ *                      r -= alpha ap, z = dinv r (whole vector);
+ *                      rr_rz = (r . r, r . z) over the owned prefix
+ *   fg_vec_pupdate:    p = z + (*num / *den) p */
+FG_API int fg_vec_dots(fg_op *op, int64_t n_own, int npairs, const double *const *a, const double *const *b,
+                       double *out);
+FG_API int fg_vec_pcg_update(fg_op *op, int64_t n_own, double *x, double *r, const double *p, const double *ap,
+                             const double *dinv, double *z, const double *rz_pap, double *rr_rz);
+FG_API int fg_vec_pupdate(fg_op *op, const double *z, double *p, const double *num, const double *den);
+
 /* Synchronise the handle's stream and report device-side errors
  * (FG_DEVICE_TIMEOUT, FG_BOUNDS). */
 FG_API int fg_op_check(fg_op *op);

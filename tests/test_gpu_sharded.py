@@ -4,7 +4,9 @@ Ranks run as threads of this process on cuda:0, each with its own stream;
 their kernels never wait on one another (the exchanges and sums meet on the
 host), so one GPU carries them.  A one-rank NCCL group checks the
 torch.distributed path.  Everything is compared with the oracle on the whole
-mesh: assembled apply and diagonal <= 1e-12, PCG iterations within 1."""
+mesh: assembled apply and diagonal <= 1e-12, PCG iterations within 1.  The
+PCG's dots and vector updates run in the library's kernels (fg_vec_dots,
+fg_vec_pcg_update, fg_vec_pupdate) with the scalars on the device."""
 import os
 import threading
 
@@ -22,6 +24,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _rank_work(A, x, b):
+    assert hasattr(A.local, "vec_pcg_update")  # the PCG's vector work runs in the library's kernels
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
         yl = A.zeros()

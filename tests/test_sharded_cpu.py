@@ -143,3 +143,37 @@ def test_gloo_ranks(world):
         assert pr.exitcode == 0
     mesh, p, kq = problem()
     check(res, reference(mesh, p, kq, 63))
+
+
+def _gloo_subgroup_worker(rank, world, port, q):
+    # global ranks 1 and 2 form the group of a 2-rank sharded solve; rank 0
+    # only takes part in creating the group
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sub = dist.new_group([1, 2])
+        if rank in (1, 2):
+            mesh, p, kq = problem()
+            ref = reference(mesh, p, kq, 63)
+            q.put(rank_work(S.TorchComm(sub), mesh, p, kq, 63, ref["x"], ref["b"]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_non_default_group():
+    """TorchComm on a subgroup: the plane exchange addresses its neighbours
+    by global rank (dist.get_global_rank), so a group that does not start at
+    global rank 0 gives the same answer as the default group."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29650 + os.getpid() % 1000
+    procs = [ctx.Process(target=_gloo_subgroup_worker, args=(r, 3, port, q)) for r in range(3)]
+    for pr in procs:
+        pr.start()
+    res = [q.get(timeout=180) for _ in range(2)]
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    mesh, p, kq = problem()
+    check(res, reference(mesh, p, kq, 63))
