@@ -3228,36 +3228,30 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
     CK(cudaMalloc(&t->d_err, sizeof(int)));
     CK(cudaMemset(t->d_err, 0, sizeof(int)));
     FG_LEGACY_FENCE();
-    // element map: validate, colour (no two elements of a colour share a DOF),
-    // sort by colour (the caller's order within a colour), transpose to [nl][E]
+    // element map: validate, transpose to [nl][E], CSR of element-local slots per DOF
     std::vector<int32_t> h(n_elem * nl);
     CK(cudaMemcpy(h.data(), elem_dofs, sizeof(int32_t) * h.size(), cudaMemcpyDefault));
+    std::vector<int32_t> soa(h.size());
+    std::vector<int64_t> offs(n_dofs + 1, 0);
     for (int64_t e = 0; e < n_elem; ++e)
         for (int i = 0; i < nl; ++i) {
             const int32_t d = h[e * nl + i];
             if (d < 0 || d >= n_dofs || (i < 4 && d >= n_nodes))
                 return fail(FG_BOUNDS, "element %lld local DOF %d out of range", (long long)e, i);
+            soa[(int64_t)i * n_elem + e] = d;
+            ++offs[d + 1];
         }
-    std::vector<uint8_t> colour;
-    const int ncol = hex_colour(n_elem, nl, n_dofs, h, colour);
-    if (ncol < 0) return fail(FG_UNSUPPORTED, "element colouring needs more than 64 colours");
-    t->col.ncol = ncol;
-    std::fill(std::begin(t->col.start), std::end(t->col.start), (int64_t)0);
-    for (uint8_t c : colour) ++t->col.start[c + 1];
-    for (int c = 0; c < ncol; ++c) t->col.start[c + 1] += t->col.start[c];
-    std::vector<int32_t> eid(n_elem), soa(h.size());
+    for (int64_t d = 0; d < n_dofs; ++d) offs[d + 1] += offs[d];
+    std::vector<int32_t> slots(offs[n_dofs]);
     {
-        std::vector<int64_t> pos(t->col.start, t->col.start + ncol);
-        for (int64_t e = 0; e < n_elem; ++e) eid[pos[colour[e]]++] = (int32_t)e;
+        std::vector<int64_t> pos(offs.begin(), offs.end() - 1);
+        for (int64_t e = 0; e < n_elem; ++e)  // (e, i) ascending within each DOF
+            for (int i = 0; i < nl; ++i) slots[pos[h[e * nl + i]]++] = (int32_t)(e * nl + i);
     }
-    for (int i = 0; i < nl; ++i)
-        for (int64_t s2 = 0; s2 < n_elem; ++s2) soa[(int64_t)i * n_elem + s2] = h[(int64_t)eid[s2] * nl + i];
-    if ((rc = tet_upload(&t->dofs, soa.data(), soa.size())) || (rc = tet_upload(&t->eid, eid.data(), eid.size())) ||
+    if ((rc = tet_upload(&t->dofs, soa.data(), soa.size())) || (rc = tet_upload(&t->offs, offs.data(), offs.size())) ||
+        (rc = tet_upload(&t->slots, slots.data(), slots.size())) ||
         (rc = tet_upload(&t->coords, coords, (size_t)n_nodes * 3)))
         return rc;
-    CK(cudaMalloc(&t->bar, 2 * sizeof(unsigned)));
-    CK(cudaMemset(t->bar, 0, 2 * sizeof(unsigned)));
-    FG_LEGACY_FENCE();
     if (ess && (rc = tet_upload(&t->ess, ess, (size_t)n_dofs))) return rc;
     // rule tables
     std::vector<double> pts, w;
@@ -3280,6 +3274,7 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
     CK(cudaMalloc(&t->G, sizeof(double) * 6 * n_elem));
     if (kind & 2) CK(cudaMalloc(&t->sk, sizeof(double) * t->nq * n_elem));
     if (kind & 1) CK(cudaMalloc(&t->sm, sizeof(double) * t->nq * n_elem));
+    CK(cudaMalloc(&t->Ye, sizeof(double) * nl * n_elem));
     const TetArgs A = tet_args(t);
     const int eb = (int)std::min<int64_t>((n_elem + 255) / 256, 148 * 16);
     tet_setup_kernel<<<eb, 256, 0, t->stream>>>(A, nl, t->coords, d_w, d_kq, kappa_const, d_rq, rho_const, c_mass,
@@ -3337,33 +3332,8 @@ FG_API int fg_tet_apply(fg_tet *t, const double *x, double *y, int accumulate, i
     int rc;
     if ((rc = tet_launch_apply(t, xd, yd, accumulate, constrained, 0))) return rc;
     if (mem == FG_HOST) CK(cudaMemcpyAsync(y, yd, nb, cudaMemcpyDeviceToHost, t->stream));
-    return tet_check(t);
-}
-
-FG_API int fg_tet_apply_native(fg_tet *t, const double *x, double *y, int accumulate, int constrained) {
-    if (!t || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
-    if (constrained && !t->ess) return fail(FG_INVALID_ARGUMENT, "constrained apply needs the essential mask");
-    std::lock_guard<std::mutex> lk(t->mu);
-    CK(cudaSetDevice(t->device));
-    return tet_launch_apply(t, x, y, accumulate, constrained, 0);
-}
-
-FG_API int fg_tet_set_stream(fg_tet *t, void *stream) {
-    if (!t) return fail(FG_INVALID_ARGUMENT, "NULL operator");
-    std::lock_guard<std::mutex> lk(t->mu);
-    CK(cudaSetDevice(t->device));
     CK(cudaStreamSynchronize(t->stream));
-    if (t->own_stream) cudaStreamDestroy(t->stream);
-    t->own_stream = false;
-    t->stream = reinterpret_cast<cudaStream_t>(stream);
     return FG_OK;
-}
-
-FG_API int fg_tet_check(fg_tet *t) {
-    if (!t) return fail(FG_INVALID_ARGUMENT, "NULL operator");
-    std::lock_guard<std::mutex> lk(t->mu);
-    CK(cudaSetDevice(t->device));
-    return tet_check(t);
 }
 
 FG_API int fg_tet_diagonal(fg_tet *t, double *d, int constrained, int mem) {
@@ -3380,7 +3350,8 @@ FG_API int fg_tet_diagonal(fg_tet *t, double *d, int constrained, int mem) {
     int rc;
     if ((rc = tet_launch_apply(t, nullptr, dd, 0, constrained, 1))) return rc;
     if (mem == FG_HOST) CK(cudaMemcpyAsync(d, dd, sizeof(double) * t->N, cudaMemcpyDeviceToHost, t->stream));
-    return tet_check(t);
+    CK(cudaStreamSynchronize(t->stream));
+    return FG_OK;
 }
 
 }  // extern "C"

@@ -13,19 +13,17 @@ struct fg_tet {
     int device = 0;
     int p = 1, nl = 4, kind = 2;
     int64_t E = 0, N = 0, n_nodes = 0;
-    int32_t *dofs = nullptr;  // [nl][E], elements sorted by colour
-    int32_t *eid = nullptr;   // [E] sorted -> caller element
-    double *G = nullptr, *sk = nullptr, *sm = nullptr, *coords = nullptr;
+    int32_t *dofs = nullptr;  // [nl][E]
+    double *G = nullptr, *sk = nullptr, *sm = nullptr, *Ye = nullptr, *coords = nullptr;
     double *qp = nullptr, *phi = nullptr, *grad = nullptr;  // rule tables (device)
     std::vector<double> h_phi, h_grad;                       // rule tables (host, kernel parameters)
     int nq = 0;
-    TetColours col{};          // colour ranges of the sorted elements
-    unsigned *bar = nullptr;   // grid-barrier counters of the coloured apply
+    int64_t *offs = nullptr;
+    int32_t *slots = nullptr;
     uint8_t *ess = nullptr;
     double *xh = nullptr, *yh = nullptr;  // device copies for host-memory calls
     int *d_err = nullptr;
     cudaStream_t stream = nullptr;
-    bool own_stream = true;
     std::mutex mu;
 };
 
@@ -179,7 +177,6 @@ static TetArgs tet_args(const fg_tet *t) {
     A.sk = t->sk;
     A.sm = t->sm;
     A.ess = t->ess;
-    A.eid = t->eid;
     A.R = TetRule{t->nq, t->phi, t->grad};
     return A;
 }
@@ -188,11 +185,11 @@ static void tet_free(fg_tet *t) {
     if (!t) return;
     cudaSetDevice(t->device);
     if (t->stream) cudaStreamSynchronize(t->stream);
-    void *ptrs[] = {t->dofs, t->eid, t->G, t->sk, t->sm, t->coords, t->qp, t->phi, t->grad,
-                    t->bar, t->ess, t->xh, t->yh, t->d_err};
+    void *ptrs[] = {t->dofs, t->G, t->sk, t->sm, t->Ye, t->coords, t->qp, t->phi, t->grad,
+                    t->offs, t->slots, t->ess, t->xh, t->yh, t->d_err};
     for (void *q : ptrs)
         if (q) cudaFree(q);
-    if (t->stream && t->own_stream) cudaStreamDestroy(t->stream);
+    if (t->stream) cudaStreamDestroy(t->stream);
     delete t;
 }
 
@@ -203,64 +200,36 @@ template <typename T> static int tet_upload(T **dst, const T *src, size_t n) {
     return FG_OK;
 }
 
-// One cooperative launch of the coloured apply, as many blocks as can be
-// resident at once (at most one per 128 elements).
 template <int NL, int MQ>
-static int tet_launch_t(fg_tet *t, const TetArgs &A, const double *x, double *y, int accumulate, int constrained,
-                        int diag) {
+static void tet_launch_t(fg_tet *t, const TetArgs &A, int eb, const double *x, int constrained, int diag) {
     TetTab<NL, MQ> R{};
     for (int q = 0; q < t->nq; ++q)
         for (int i = 0; i < NL; ++i) {
             R.phi[q][i] = t->h_phi[(size_t)q * NL + i];
             for (int c = 0; c < 3; ++c) R.grad[q][i][c] = t->h_grad[((size_t)q * NL + i) * 3 + c];
         }
-    auto kern = tet_apply_coloured_kernel<NL, MQ>;
-    static int per_sm[64];  // resident blocks per SM, per device
-    if (t->device < 0 || t->device >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", t->device);
-    if (!per_sm[t->device]) {
-        int b = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 128, 0));
-        per_sm[t->device] = std::max(b, 1);
-    }
-    int sms = 0;
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t->device));
-    const int64_t want = std::max<int64_t>((std::max(t->E, t->N) + 127) / 128, 1);
-    const int blocks = (int)std::min<int64_t>((int64_t)per_sm[t->device] * sms, want);
-    const TetColours &C = t->col;
-    unsigned *bar = t->bar;
-    int *err = t->d_err;
-    void *args[] = {(void *)&A, (void *)&R, (void *)&C, (void *)&x, (void *)&y, (void *)&accumulate,
-                    (void *)&constrained, (void *)&diag, (void *)&bar, (void *)&err};
-    CK(cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), dim3(128), args, 0, t->stream));
-    return FG_OK;
+    tet_apply_kernel<NL, MQ><<<eb, 128, 0, t->stream>>>(A, R, x, t->Ye, constrained, diag);
 }
 
 static int tet_launch_apply(fg_tet *t, const double *x, double *y, int accumulate, int constrained, int diag) {
     const TetArgs A = tet_args(t);
+    const int eb = (int)std::min<int64_t>((t->E + 127) / 128, 148 * 16);
     const bool small = t->nq <= 4;
-    int rc;
-    if (t->p == 1) rc = small ? tet_launch_t<4, 4>(t, A, x, y, accumulate, constrained, diag)
-                              : tet_launch_t<4, TET_MAXQ>(t, A, x, y, accumulate, constrained, diag);
-    else if (t->p == 2) rc = small ? tet_launch_t<10, 4>(t, A, x, y, accumulate, constrained, diag)
-                                   : tet_launch_t<10, TET_MAXQ>(t, A, x, y, accumulate, constrained, diag);
-    else rc = small ? tet_launch_t<20, 4>(t, A, x, y, accumulate, constrained, diag)
-                    : tet_launch_t<20, TET_MAXQ>(t, A, x, y, accumulate, constrained, diag);
-    return rc;
-}
-
-// Device-side error of the last applies: a grid barrier that ran out
-// (FG_DEVICE_TIMEOUT; the barrier counters are cleared for the next launch) or
-// a degenerate element at set-up (FG_BOUNDS).  Synchronises the stream.
-static int tet_check(fg_tet *t) {
-    int herr = 0;
-    CK(cudaMemcpyAsync(&herr, t->d_err, sizeof(int), cudaMemcpyDeviceToHost, t->stream));
-    CK(cudaStreamSynchronize(t->stream));
-    if (!herr) return FG_OK;
-    CK(cudaMemsetAsync(t->d_err, 0, sizeof(int), t->stream));
-    CK(cudaMemsetAsync(t->bar, 0, 2 * sizeof(unsigned), t->stream));
-    CK(cudaStreamSynchronize(t->stream));
-    if (herr & FG_DERR_TIMEOUT) return fail(FG_DEVICE_TIMEOUT, "a grid barrier of the tet apply timed out");
-    return fail(FG_BOUNDS, "device-side bounds error");
+    if (t->p == 1) {
+        if (small) tet_launch_t<4, 4>(t, A, eb, x, constrained, diag);
+        else tet_launch_t<4, TET_MAXQ>(t, A, eb, x, constrained, diag);
+    } else if (t->p == 2) {
+        if (small) tet_launch_t<10, 4>(t, A, eb, x, constrained, diag);
+        else tet_launch_t<10, TET_MAXQ>(t, A, eb, x, constrained, diag);
+    } else {
+        if (small) tet_launch_t<20, 4>(t, A, eb, x, constrained, diag);
+        else tet_launch_t<20, TET_MAXQ>(t, A, eb, x, constrained, diag);
+    }
+    const int db = (int)std::min<int64_t>((t->N + 255) / 256, 148 * 16);
+    tet_scatter_kernel<<<db, 256, 0, t->stream>>>(A, t->offs, t->slots, t->Ye, diag ? nullptr : x, y, accumulate,
+                                                  constrained);
+    CK(cudaGetLastError());
+    return FG_OK;
 }
 
 }  // namespace fg

@@ -1,23 +1,22 @@
 // tet_kernels.cuh -- partial-assembly operator on unstructured tetrahedra
 // (TetP1 / TetP2), the element path of crates/assembly/src/partial.rs on Tet4.
 //
-// Data layout (elements sorted by colour, element-major structure of arrays,
-// one coalesced load per component across a warp of consecutive elements):
+// Data layout (element-major structure of arrays, one coalesced load per
+// component across a warp of consecutive elements):
 //   dofs [nl][E]  int32 element-to-DOF map (first 4 = vertex nodes)
 //   G    [6][E]   |det J| J^-1 J^-T (symmetric: xx xy xz yy yz zz), constant
 //                 per element (affine map)
 //   sk   [nq][E]  w_q kappa_q c_k          (diffusion)
 //   sm   [nq][E]  w_q |det J| rho_q c_m    (mass)
-//   eid  [E]      the caller's index of each sorted element
+//   Ye   [E][nl]  element-local results (scratch; element-major so that the
+//                 slots of one DOF, which come from nearby elements, share sectors)
 // Per quadrature point the reference computes grad_phys = J^-T grad_ref and
 // y_i += w |det J| kappa (grad u . grad phi_i); with the affine map this is
 // y_i += (w kappa) grad_ref phi_i . G grad_ref u, which the apply evaluates.
 //
-// Scatter without float atomics: the elements are coloured so that no two
-// elements of a colour share a DOF.  One cooperative launch walks the colours
-// in order with a grid barrier between them, and each element adds its result
-// into y directly: every DOF receives its contributions in colour order, the
-// same sums every run, with no element-result round trip through HBM.
+// Scatter without float atomics: the transpose of the element-to-DOF map is a
+// CSR list per DOF of element-local slots (e*nl + i) in increasing (e, i); one
+// thread per DOF sums its slots in that order (deterministic).
 #pragma once
 #include "fg_common.cuh"
 
@@ -38,14 +37,7 @@ struct TetArgs {
     const double *G;           // [6][E]
     const double *sk, *sm;     // [nq][E]
     const uint8_t *ess;        // [N] or null
-    const int32_t *eid;        // [E] sorted -> caller element
     TetRule R;
-};
-
-// Colour ranges of the sorted elements (at most 64 colours).
-struct TetColours {
-    int64_t start[65];
-    int ncol;
 };
 
 // one thread per element: geometry and the per-point scalars
@@ -55,7 +47,6 @@ __global__ void tet_setup_kernel(TetArgs A, int nl, const double *__restrict__ c
                                  double *G, double *sk, double *sm, int *err) {
     const int64_t E = A.E;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t ec = A.eid[e];  // the caller's element (coefficient tables)
         const double *x0 = coords + 3 * (int64_t)A.dofs[e];
         double J[3][3];
         for (int c = 0; c < 3; ++c) {
@@ -83,8 +74,8 @@ __global__ void tet_setup_kernel(TetArgs A, int nl, const double *__restrict__ c
             G[(int64_t)k * E + e] = ad * (inv[m][0] * inv[n][0] + inv[m][1] * inv[n][1] + inv[m][2] * inv[n][2]);
         }
         for (int q = 0; q < A.R.nq; ++q) {
-            if (A.kind & 2) sk[(int64_t)q * E + e] = qw[q] * (kappa_q ? kappa_q[ec * A.R.nq + q] : kappa_c) * c_k;
-            if (A.kind & 1) sm[(int64_t)q * E + e] = qw[q] * ad * (rho_q ? rho_q[ec * A.R.nq + q] : rho_c) * c_m;
+            if (A.kind & 2) sk[(int64_t)q * E + e] = qw[q] * (kappa_q ? kappa_q[e * A.R.nq + q] : kappa_c) * c_k;
+            if (A.kind & 1) sm[(int64_t)q * E + e] = qw[q] * ad * (rho_q ? rho_q[e * A.R.nq + q] : rho_c) * c_m;
         }
         (void)nl;
     }
@@ -98,97 +89,88 @@ template <int NL, int MQ> struct TetTab {
     double grad[MQ][NL][3];
 };
 
-// ye = (A_e x_e) (diag = 0) or the element diagonal (diag = 1) of element e
+// Ye[e][i] = (A_e x_e)_i (diag = 0) or (A_e)_ii (diag = 1), one thread per element
 template <int NL, int MQ>
-__device__ __forceinline__ void tet_element(const TetArgs &A, const TetTab<NL, MQ> &R, const double *__restrict__ x,
-                                            int64_t e, int constrained, int diag, double (&ye)[NL]) {
+__global__ void __launch_bounds__(128) tet_apply_kernel(TetArgs A, const __grid_constant__ TetTab<NL, MQ> R,
+                                                        const double *__restrict__ x, double *__restrict__ Ye,
+                                                        int constrained, int diag) {
     const int64_t E = A.E;
     const int nq = A.R.nq;
-    double xe[NL];
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        double xe[NL], ye[NL];
 #pragma unroll
-    for (int i = 0; i < NL; ++i) {
-        ye[i] = 0.0;
-        xe[i] = 0.0;
-        if (!diag) {
-            const int32_t d = __ldg(A.dofs + (int64_t)i * E + e);
-            xe[i] = (constrained && A.ess && A.ess[d]) ? 0.0 : __ldg(x + d);
-        }
-    }
-    double g[6] = {0, 0, 0, 0, 0, 0};
-    if (A.kind & 2)
-#pragma unroll
-        for (int k = 0; k < 6; ++k) g[k] = __ldg(A.G + (int64_t)k * E + e);
-    for (int q = 0; q < nq; ++q) {
-        if (A.kind & 2) {
-            const double s = __ldg(A.sk + (int64_t)q * E + e);
+        for (int i = 0; i < NL; ++i) {
+            ye[i] = 0.0;
+            xe[i] = 0.0;
             if (!diag) {
-                double gu[3] = {0, 0, 0};
+                const int32_t d = __ldg(A.dofs + (int64_t)i * E + e);
+                xe[i] = (constrained && A.ess && A.ess[d]) ? 0.0 : __ldg(x + d);
+            }
+        }
+        double g[6] = {0, 0, 0, 0, 0, 0};
+        if (A.kind & 2)
 #pragma unroll
-                for (int j = 0; j < NL; ++j)
+            for (int k = 0; k < 6; ++k) g[k] = __ldg(A.G + (int64_t)k * E + e);
+        for (int q = 0; q < nq; ++q) {
+            if (A.kind & 2) {
+                const double s = __ldg(A.sk + (int64_t)q * E + e);
+                if (!diag) {
+                    double gu[3] = {0, 0, 0};
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) gu[c] += xe[j] * R.grad[q][j][c];
-                const double v0 = s * (g[0] * gu[0] + g[1] * gu[1] + g[2] * gu[2]);
-                const double v1 = s * (g[1] * gu[0] + g[3] * gu[1] + g[4] * gu[2]);
-                const double v2 = s * (g[2] * gu[0] + g[4] * gu[1] + g[5] * gu[2]);
+                    for (int j = 0; j < NL; ++j)
 #pragma unroll
-                for (int i = 0; i < NL; ++i)
-                    ye[i] += R.grad[q][i][0] * v0 + R.grad[q][i][1] * v1 + R.grad[q][i][2] * v2;
-            } else {
+                        for (int c = 0; c < 3; ++c) gu[c] += xe[j] * R.grad[q][j][c];
+                    const double v0 = s * (g[0] * gu[0] + g[1] * gu[1] + g[2] * gu[2]);
+                    const double v1 = s * (g[1] * gu[0] + g[3] * gu[1] + g[4] * gu[2]);
+                    const double v2 = s * (g[2] * gu[0] + g[4] * gu[1] + g[5] * gu[2]);
 #pragma unroll
-                for (int i = 0; i < NL; ++i) {
-                    const double a = R.grad[q][i][0], b = R.grad[q][i][1], c = R.grad[q][i][2];
-                    ye[i] += s * (g[0] * a * a + g[3] * b * b + g[5] * c * c +
-                                  2.0 * (g[1] * a * b + g[2] * a * c + g[4] * b * c));
+                    for (int i = 0; i < NL; ++i)
+                        ye[i] += R.grad[q][i][0] * v0 + R.grad[q][i][1] * v1 + R.grad[q][i][2] * v2;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < NL; ++i) {
+                        const double a = R.grad[q][i][0], b = R.grad[q][i][1], c = R.grad[q][i][2];
+                        ye[i] += s * (g[0] * a * a + g[3] * b * b + g[5] * c * c +
+                                      2.0 * (g[1] * a * b + g[2] * a * c + g[4] * b * c));
+                    }
+                }
+            }
+            if (A.kind & 1) {
+                const double m = __ldg(A.sm + (int64_t)q * E + e);
+                if (!diag) {
+                    double u = 0.0;
+#pragma unroll
+                    for (int j = 0; j < NL; ++j) u += R.phi[q][j] * xe[j];
+                    const double t = m * u;
+#pragma unroll
+                    for (int i = 0; i < NL; ++i) ye[i] += R.phi[q][i] * t;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < NL; ++i) ye[i] += m * R.phi[q][i] * R.phi[q][i];
                 }
             }
         }
-        if (A.kind & 1) {
-            const double m = __ldg(A.sm + (int64_t)q * E + e);
-            if (!diag) {
-                double u = 0.0;
+        double *dst = Ye + e * NL;
 #pragma unroll
-                for (int j = 0; j < NL; ++j) u += R.phi[q][j] * xe[j];
-                const double t = m * u;
-#pragma unroll
-                for (int i = 0; i < NL; ++i) ye[i] += R.phi[q][i] * t;
-            } else {
-#pragma unroll
-                for (int i = 0; i < NL; ++i) ye[i] += m * R.phi[q][i] * R.phi[q][i];
-            }
-        }
+        for (int i = 0; i < NL; ++i) dst[i] = ye[i];
     }
 }
 
-// The whole apply in one cooperative launch: y = (accumulate ? y : 0) + the
-// identity rows of the essential DOFs of a constrained call (x, or 1 for the
-// diagonal); then the colours in order, a grid barrier after each, every
-// element adding its result into its non-essential DOFs.  y is read at L2
-// (__ldcg): another SM may have written the DOF in an earlier colour.
-template <int NL, int MQ>
-__global__ void __launch_bounds__(128) tet_apply_coloured_kernel(TetArgs A, const __grid_constant__ TetTab<NL, MQ> R,
-                                                                 const __grid_constant__ TetColours C,
-                                                                 const double *__restrict__ x, double *y,
-                                                                 int accumulate, int constrained, int diag,
-                                                                 unsigned *bar, int *err) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (int64_t d = t0; d < A.N; d += stride) {
-        double v = accumulate ? y[d] : 0.0;
-        if (constrained && A.ess && A.ess[d]) v += diag ? 1.0 : x[d];
-        y[d] = v;
-    }
-    bool ok = true;
-    for (int c = 0; c < C.ncol; ++c) {
-        grid_barrier(bar, err, ok);
-        for (int64_t e = C.start[c] + t0; e < C.start[c + 1]; e += stride) {
-            double ye[NL];
-            tet_element<NL, MQ>(A, R, x, e, constrained, diag, ye);
-#pragma unroll
-            for (int i = 0; i < NL; ++i) {
-                const int32_t d = __ldg(A.dofs + (int64_t)i * A.E + e);
-                if (!(constrained && A.ess && A.ess[d])) y[d] = __ldcg(y + d) + ye[i];
-            }
+// y_d (+)= sum of the element-local slots of DOF d in (e, i) order; on
+// essential DOFs of a constrained call the identity row: y_d (+)= x_d (apply)
+// or 1 (diagonal, x null)
+__global__ void tet_scatter_kernel(TetArgs A, const int64_t *__restrict__ offs, const int32_t *__restrict__ slots,
+                                   const double *__restrict__ Ye, const double *__restrict__ x,
+                                   double *__restrict__ y, int accumulate, int constrained) {
+    for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < A.N; d += (int64_t)gridDim.x * blockDim.x) {
+        double s;
+        if (constrained && A.ess && A.ess[d]) {
+            s = x ? x[d] : 1.0;
+        } else {
+            s = 0.0;
+            for (int64_t k = offs[d]; k < offs[d + 1]; ++k) s += Ye[slots[k]];
         }
+        y[d] = accumulate ? y[d] + s : s;
     }
 }
 
@@ -198,7 +180,7 @@ __global__ void tet_qp_coords_kernel(TetArgs A, const double *__restrict__ coord
     const int nq = A.R.nq;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < A.E * nq; t += (int64_t)gridDim.x * blockDim.x) {
         const int q = (int)(t % nq);
-        const int64_t e = t / nq;  // sorted element; the output is in the caller's element order
+        const int64_t e = t / nq;
         const double *x0 = coords + 3 * (int64_t)A.dofs[e];
         const double *xi = qp + 3 * q;
         for (int r = 0; r < 3; ++r) {
@@ -207,7 +189,7 @@ __global__ void tet_qp_coords_kernel(TetArgs A, const double *__restrict__ coord
                 const double *xc = coords + 3 * (int64_t)A.dofs[(int64_t)(c + 1) * A.E + e];
                 s += (xc[r] - x0[r]) * xi[c];
             }
-            xyz[3 * ((int64_t)A.eid[e] * nq + q) + r] = s;
+            xyz[3 * t + r] = s;
         }
     }
 }

@@ -413,10 +413,8 @@ FG_API int fg_lumped_apply(const double *diag, const double *x, double *y, int64
  * [E][nq] at the rule's points (fg_tet_quadrature_points) or NULL for the
  * constants; ess: essential-DOF mask [n_dofs] (boundary_dofs) or NULL.  TetP3
  * element maps: [E][20] as build_p3_tet (dof_manager.rs:484-600).  All
- * arrays in host or device memory.  The scatter is coloured: elements that
- * share no DOF form a colour, the colours run in order inside one launch, and
- * each DOF sums its element contributions in colour order (no float atomics,
- * the same sums every run). */
+ * arrays in host or device memory.  The scatter is the transpose of the
+ * element map summed in a fixed order (no float atomics). */
 typedef struct fg_tet fg_tet;
 FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64_t n_elem,
                          const int32_t *elem_dofs, int64_t n_dofs, int kind, double c_mass, double c_diff,
@@ -433,15 +431,6 @@ FG_API int fg_tet_quadrature_points(fg_tet *op, double *xyz, int mem);
 FG_API int fg_tet_apply(fg_tet *op, const double *x, double *y, int accumulate, int constrained, int mem);
 /* Jacobi diagonal (1 on essential DOFs when constrained). */
 FG_API int fg_tet_diagonal(fg_tet *op, double *d, int constrained, int mem);
-/* fg_tet_apply on device vectors, asynchronous on the handle's stream (no
- * host synchronisation; fg_tet_check reports device-side errors). */
-FG_API int fg_tet_apply_native(fg_tet *op, const double *x, double *y, int accumulate, int constrained);
-/* Run on the caller's CUDA stream (cudaStream_t) instead of the handle's own. */
-FG_API int fg_tet_set_stream(fg_tet *op, void *stream);
-/* Synchronise the handle's stream; FG_DEVICE_TIMEOUT if a grid barrier of the
- * coloured apply ran out (the apply walks the element colours in one
- * cooperative launch with bounded barriers between them). */
-FG_API int fg_tet_check(fg_tet *op);
 
 /* Limit of each device-side wait of this handle's apply kernels for a copy
  * into shared memory (default 1 s; seconds <= 0 restores it, at most 60 s).
