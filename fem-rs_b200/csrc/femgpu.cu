@@ -3336,6 +3336,33 @@ FG_API int fg_tet_apply(fg_tet *t, const double *x, double *y, int accumulate, i
     return FG_OK;
 }
 
+FG_API int fg_tet_apply_native(fg_tet *t, const double *x, double *y, int accumulate, int constrained) {
+    if (!t || !x || !y) return fail(FG_INVALID_ARGUMENT, "NULL argument");
+    if (constrained && !t->ess) return fail(FG_INVALID_ARGUMENT, "constrained apply needs the essential mask");
+    std::lock_guard<std::mutex> lk(t->mu);
+    CK(cudaSetDevice(t->device));
+    return tet_launch_apply(t, x, y, accumulate, constrained, 0);
+}
+
+FG_API int fg_tet_set_stream(fg_tet *t, void *stream) {
+    if (!t) return fail(FG_INVALID_ARGUMENT, "NULL operator");
+    std::lock_guard<std::mutex> lk(t->mu);
+    CK(cudaSetDevice(t->device));
+    CK(cudaStreamSynchronize(t->stream));
+    if (t->own_stream) cudaStreamDestroy(t->stream);
+    t->own_stream = false;
+    t->stream = reinterpret_cast<cudaStream_t>(stream);
+    return FG_OK;
+}
+
+FG_API int fg_tet_check(fg_tet *t) {
+    if (!t) return fail(FG_INVALID_ARGUMENT, "NULL operator");
+    std::lock_guard<std::mutex> lk(t->mu);
+    CK(cudaSetDevice(t->device));
+    CK(cudaStreamSynchronize(t->stream));
+    return FG_OK;
+}
+
 FG_API int fg_tet_diagonal(fg_tet *t, double *d, int constrained, int mem) {
     if (!t || !d) return fail(FG_INVALID_ARGUMENT, "NULL argument");
     if (mem != FG_HOST && mem != FG_DEVICE) return fail(FG_INVALID_ARGUMENT, "bad mem %d", mem);

@@ -24,6 +24,7 @@ struct fg_tet {
     double *xh = nullptr, *yh = nullptr;  // device copies for host-memory calls
     int *d_err = nullptr;
     cudaStream_t stream = nullptr;
+    bool own_stream = true;
     std::mutex mu;
 };
 
@@ -189,7 +190,7 @@ static void tet_free(fg_tet *t) {
                     t->offs, t->slots, t->ess, t->xh, t->yh, t->d_err};
     for (void *q : ptrs)
         if (q) cudaFree(q);
-    if (t->stream) cudaStreamDestroy(t->stream);
+    if (t->stream && t->own_stream) cudaStreamDestroy(t->stream);
     delete t;
 }
 

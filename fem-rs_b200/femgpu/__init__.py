@@ -47,7 +47,8 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply", "fg_op_set_tile",
            "fg_op_tile", "fg_batch_autotune", "fg_tet_create", "fg_tet_destroy", "fg_tet_ndofs", "fg_tet_nq",
            "fg_tet_quadrature_points", "fg_tet_apply", "fg_tet_diagonal", "fg_op_set_wait_limit",
-           "fg_op_create_hex", "fg_op_colours", "fg_vec_dots", "fg_vec_pcg_update", "fg_vec_pupdate")
+           "fg_op_create_hex", "fg_op_colours", "fg_vec_dots", "fg_vec_pcg_update", "fg_vec_pupdate",
+           "fg_tet_apply_native", "fg_tet_set_stream", "fg_tet_check")
 
 
 class FgMesh(C.Structure):
@@ -154,6 +155,9 @@ def lib():
         L.fg_vec_dots.argtypes = [vp, i64, i, vp, vp, vp]
         L.fg_vec_pcg_update.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp]
         L.fg_vec_pupdate.argtypes = [vp, vp, vp, vp, vp]
+        L.fg_tet_apply_native.argtypes = [vp, vp, vp, i, i]
+        L.fg_tet_set_stream.argtypes = [vp, vp]
+        L.fg_tet_check.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -783,6 +787,16 @@ class TetOperator:
         d = np.zeros(self.n)
         _check(lib().fg_tet_diagonal(self._h, d.ctypes.data, int(constrained), HOST))
         return d
+
+    def apply_native(self, x_ptr, y_ptr, accumulate=False, constrained=True):
+        """y (+)= A x on device pointers, asynchronous on the handle's stream."""
+        _check(lib().fg_tet_apply_native(self._h, x_ptr, y_ptr, int(accumulate), int(constrained)))
+
+    def set_stream(self, stream_ptr):
+        _check(lib().fg_tet_set_stream(self._h, stream_ptr))
+
+    def check(self):
+        _check(lib().fg_tet_check(self._h))
 
 
 def _mesh_struct(nx, ny, nz, vcoord):

@@ -431,6 +431,13 @@ FG_API int fg_tet_quadrature_points(fg_tet *op, double *xyz, int mem);
 FG_API int fg_tet_apply(fg_tet *op, const double *x, double *y, int accumulate, int constrained, int mem);
 /* Jacobi diagonal (1 on essential DOFs when constrained). */
 FG_API int fg_tet_diagonal(fg_tet *op, double *d, int constrained, int mem);
+/* fg_tet_apply on device vectors, asynchronous on the handle's stream (no
+ * host synchronisation). */
+FG_API int fg_tet_apply_native(fg_tet *op, const double *x, double *y, int accumulate, int constrained);
+/* Run on the caller's CUDA stream (cudaStream_t) instead of the handle's own. */
+FG_API int fg_tet_set_stream(fg_tet *op, void *stream);
+/* Synchronise the handle's stream. */
+FG_API int fg_tet_check(fg_tet *op);
 
 /* Limit of each device-side wait of this handle's apply kernels for a copy
  * into shared memory (default 1 s; seconds <= 0 restores it, at most 60 s).
