@@ -246,6 +246,8 @@ struct fg_op {
     double *qa64 = nullptr;
     float *qa32 = nullptr;
     int *d_err = nullptr;
+    unsigned *bar = nullptr;  // grid-barrier counters of the fused PCG iteration kernel
+    bool fused_pcg = true;    // one cooperative launch per Jacobi-PCG iteration (FG_FUSED_PCG=0: three)
     uint64_t wait_ns = 0;  // limit of the apply kernels' device-side waits (0: 1 s)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -285,6 +287,7 @@ static void free_op(fg_op *op) {
     if (op->sd_w) cudaFree(op->sd_w);
     if (op->qa32) cudaFree(op->qa32);
     if (op->st) cudaFree(op->st);
+    if (op->bar) cudaFree(op->bar);
     if (op->d_err) cudaFree(op->d_err);
     if (op->ev0) cudaEventDestroy(op->ev0);
     if (op->ev1) cudaEventDestroy(op->ev1);
@@ -563,6 +566,8 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
         op->nn_overlap = !(o && o[0] == '0');
         const char *f = std::getenv("FG_FUSED_FIXUP");
         op->fused_fixup = f && f[0] == '1';
+        const char *fp = std::getenv("FG_FUSED_PCG");
+        op->fused_pcg = !(fp && fp[0] == '0');
     }
     if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)))
         return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
@@ -680,6 +685,7 @@ static int check_device_error(fg_op *op) {
     CK(cudaStreamSynchronize(op->stream));
     if (herr) {
         cudaMemsetAsync(op->d_err, 0, sizeof(int), op->stream);
+        if (op->bar) cudaMemsetAsync(op->bar, 0, 2 * sizeof(unsigned), op->stream);  // after a barrier timeout
         if (herr & FG_DERR_TIMEOUT) return fail(FG_DEVICE_TIMEOUT, "device-side wait timed out");
         return fail(FG_BOUNDS, "device-side bounds error");
     }
@@ -1064,6 +1070,43 @@ static int run_chunk(fg_op *op, ChunkGraph &cg, int key, int iters, const std::f
     return FG_OK;
 }
 
+// The vector work of one Jacobi-PCG (or operator-CG) iteration as one
+// cooperative launch (k_pcg_fused_jacobi); returns 1 when the device cannot
+// hold all VEC_GRID blocks at once (the caller then uses the three kernels).
+template <typename T> static int launch_pcg_fused(fg_op *op, const PcgBufs<T> &B, bool *used) {
+    *used = false;
+    if (!op->fused_pcg) return FG_OK;
+    static int fits[64];  // per device: 1 fits, -1 does not, 0 not yet known
+    if (op->device < 0 || op->device >= 64) return FG_OK;
+    auto kern = k_pcg_fused_jacobi<T>;
+    if (!fits[op->device]) {
+        int per_sm = 0, sms = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, VEC_THREADS, 0));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, op->device));
+        fits[op->device] = per_sm * sms >= VEC_GRID ? 1 : -1;
+    }
+    if (fits[op->device] < 0) return FG_OK;
+    if (!op->bar) {
+        CK(cudaMalloc(&op->bar, 2 * sizeof(unsigned)));
+        CK(cudaMemset(op->bar, 0, 2 * sizeof(unsigned)));
+        FG_LEGACY_FENCE();
+    }
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(VEC_GRID);
+    lc.blockDim = dim3(VEC_THREADS);
+    lc.stream = op->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    T *x = const_cast<T *>(B.x), *r = B.r, *p = B.p, *z = B.z;
+    CK(cudaLaunchKernelEx(&lc, kern, op->Nn, x, r, p, (const T *)B.ap, B.dinv, z, op->partials, B.st, op->bar,
+                          op->d_err));
+    *used = true;
+    return FG_OK;
+}
+
 template <typename T>
 static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebCoef *cc,
                    int max_iter, int check_interval, bool x_zero, SolverState *h,
@@ -1092,6 +1135,11 @@ static int pcg_run(fg_op *op, const PcgBufs<T> &B, bool jacobi_like, const ChebC
     auto iteration = [&]() -> int {
         int r2;
         if ((r2 = apply_native_t<T>(op, B.qd, B.face, B.p, B.ap, 0, 1, skip))) return r2;
+        if (!cheb) {
+            bool used = false;
+            if ((r2 = launch_pcg_fused<T>(op, B, &used))) return r2;
+            if (used) return FG_OK;
+        }
         k_pcg_pap<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(n, B.p, B.ap, op->partials, B.st);
         k_pcg_update<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(
             n, B.x, B.r, B.p, B.ap, B.dinv, B.z, cheb ? 0 : 1, op->partials, B.st);

@@ -156,6 +156,41 @@ __device__ __forceinline__ void wait_stage(uint64_t *bar, uint32_t parity, int *
 __device__ __forceinline__ void drain_stages(uint64_t *bars, int depth, int waited, int issued) {
     for (int j = waited; j < issued; ++j) mbar_wait(&bars[j % depth], (j / depth) & 1, nullptr);
 }
+// Grid-wide barrier of a cooperative launch (every block resident at once),
+// with a time limit.  bar[0] counts arrivals, bar[1] is the generation; the
+// last block to arrive resets the count and advances the generation.  A block
+// whose wait runs out sets FG_DERR_TIMEOUT, clears `ok` and from then on only
+// arrives (never waits), so the launch ends within about one limit; the host
+// then reports the timeout and clears bar[] before the next launch.
+__device__ __forceinline__ void grid_barrier(unsigned *bar, int *err, bool &ok,
+                                             uint64_t limit_ns = 1000000000ull) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok_s = ok ? 1 : 0;
+        volatile unsigned *gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else if (ok_s) {
+            const uint64_t t0 = globaltimer_ns();
+            while (*gen == g) {
+                if (globaltimer_ns() - t0 > limit_ns) {
+                    if (err) atomicOr(err, FG_DERR_TIMEOUT);
+                    ok_s = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    ok = ok_s != 0;
+}
 // 1-D bulk copy global -> shared, completing on an mbarrier (sizes/addresses
 // must be multiples of 16 bytes).
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,

@@ -211,6 +211,8 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
     {
         const char *e = std::getenv("FG_SOLVER_GRAPHS");
         op->graphs = !(e && e[0] == '0');
+        const char *fp = std::getenv("FG_FUSED_PCG");
+        op->fused_pcg = !(fp && fp[0] == '0');
     }
     if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)) ||
         cudaMalloc(&op->st, sizeof(SolverState)) != cudaSuccess ||

@@ -229,6 +229,118 @@ __global__ void __launch_bounds__(VEC_THREADS) k_pcg_update(int64_t n, T *__rest
     }
 }
 
+// ---- one PCG iteration's vector work in one cooperative launch -----------
+// The block partials of a reduction, then a grid barrier, then every block
+// sums all partials in the order grid_sum's last block uses, so every block
+// holds the same totals, bit for bit those of the separate kernels.
+template <int NV>
+__device__ __forceinline__ void all_blocks_sum(double (&v)[NV], double *partials, unsigned *bar, int *err,
+                                               bool &ok, double (&tot)[NV]) {
+    __shared__ double sm[NV * (VEC_THREADS / 32)];
+    __shared__ double tb[NV];
+    block_sum<NV>(v, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) partials[blockIdx.x * NV + k] = v[k];
+    }
+    grid_barrier(bar, err, ok);
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += VEC_THREADS)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[b * NV + k]);
+    block_sum<NV>(acc, sm);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) tb[k] = acc[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) tot[k] = tb[k];
+}
+
+// k_pcg_pap + k_pcg_update (Jacobi: z = dinv r) + k_pcg_pupdate of one
+// iteration in one launch with two grid barriers: p.Ap and alpha, the x / r /
+// z update with r.r and r.z, the stopping test, beta and p = z + beta p --
+// the iteration of par_solve_pcg_jacobi (crates/parallel/src/par_solver.rs:
+// 296-330) and of solve_cg_operator (dinv = 1, its own stopping rule).  The
+// state is read by every block at entry and written by block 0 only; the two
+// reductions use separate partial regions.  Same values as the separate kernels.
+template <typename T>
+__global__ void __launch_bounds__(VEC_THREADS) k_pcg_fused_jacobi(int64_t n, T *__restrict__ x, T *__restrict__ r,
+                                                                  T *__restrict__ p, const T *__restrict__ ap,
+                                                                  const T *__restrict__ dinv, T *__restrict__ z,
+                                                                  double *partials, SolverState *st, unsigned *bar,
+                                                                  int *err) {
+    if (st->done) return;
+    const double rz0 = st->rz, bnorm = st->bnorm, rtol = st->rtol, atol = st->atol, stop_abs = st->stop_abs;
+    const int iter0 = st->iter, max_iter = st->max_iter, cgop = st->cgop;
+    bool ok = true;
+    double v1[1] = {0.0};
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> pv = ld4(p, q), av = ld4(ap, q);
+        FG_K4 v1[0] += (double)pv.a[k] * (double)av.a[k];
+    }
+    double pap[1];
+    all_blocks_sum<1>(v1, partials, bar, err, ok, pap);
+    if (fabs(pap[0]) < (cgop ? 1e-32 : 1e-30)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            st->pap = pap[0];
+            st->breakdown = 1;
+            st->done = 1;
+        }
+        return;
+    }
+    const double alpha_d = rz0 / pap[0];
+    const T alpha = (T)alpha_d;
+    double v2[2] = {0.0, 0.0};
+    FG_VEC4_LOOP(q, n) {
+        V4<T> xv = ld4(x, q), rv = ld4(r, q), zv;
+        const V4<T> pv = ld4(p, q), av = ld4(ap, q), dv = ld4(dinv, q);
+        FG_K4 {
+            xv.a[k] += alpha * pv.a[k];
+            rv.a[k] = rv.a[k] - alpha * av.a[k];
+            v2[0] += (double)rv.a[k] * (double)rv.a[k];
+            zv.a[k] = dv.a[k] * rv.a[k];
+            v2[1] += (double)rv.a[k] * (double)zv.a[k];
+        }
+        st4(x, q, xv);
+        st4(r, q, rv);
+        st4(z, q, zv);
+    }
+    double tot[2];
+    all_blocks_sum<2>(v2, partials + 2 * VEC_GRID, bar, err, ok, tot);
+    const double rn = sqrt(tot[0]);
+    const double res = cgop ? rn : rn / bnorm;
+    const bool converged = cgop ? rn <= stop_abs : (res < rtol || rn < atol);
+    const bool stop = converged || iter0 + 1 >= max_iter;
+    const double beta_d = tot[1] / rz0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->pap = pap[0];
+        st->alpha = alpha_d;
+        st->iter = iter0 + 1;
+        st->rr = tot[0];
+        st->res = res;
+        if (converged) {
+            st->converged = 1;
+            st->done = 1;
+        } else if (stop) {
+            st->done = 1;
+        } else {
+            st->beta = beta_d;
+            st->rz = tot[1];
+        }
+    }
+    if (stop) return;
+    const T beta = (T)beta_d;
+    FG_VEC4_LOOP(q, n) {
+        const V4<T> zv = ld4(z, q);
+        V4<T> pv = ld4(p, q);
+        FG_K4 pv.a[k] = zv.a[k] + beta * pv.a[k];
+        st4(p, q, pv);
+    }
+}
+
 // rz_new = r.z ; beta = rz_new / rz ; rz = rz_new   (non-Jacobi preconditioners)
 template <typename T>
 __global__ void __launch_bounds__(VEC_THREADS) k_pcg_rz(int64_t n, const T *__restrict__ r,
