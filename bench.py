@@ -590,6 +590,66 @@ def run_tet(dev, peak):
     return out
 
 
+def box_as_hex_mesh(n, p):
+    """The unit-cube n^3 box of order p handed over as an unstructured Hex8 mesh:
+    node coordinates, HexQ1-ordered connectivity and tensor-order element DOF
+    maps (order 1: DOF = node), in lexicographic element order."""
+    m = n + 1
+    k, j, i = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
+    coords = np.stack([i / n, j / n, k / n], axis=-1).reshape(-1, 3)
+    ez, ey, ex = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    ex, ey, ez = ex.ravel(), ey.ravel(), ez.ravel()
+    corners = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+    conn = np.stack([((ez + c) * m + ey + b) * m + ex + a for a, b, c in corners], axis=1).astype(np.uint32)
+    if p == 1:
+        return coords, conn, None
+    s = n * p + 1
+    q = p + 1
+    loc = [(a, b, c) for c in range(q) for b in range(q) for a in range(q)]
+    maps = np.stack([((ez * p + c) * s + ey * p + b) * s + ex * p + a for a, b, c in loc], axis=1).astype(np.uint32)
+    return coords, conn, maps
+
+
+def run_hex_unstructured(n, p, kq, steps, peak, dev):
+    """The same operator as the headline apply built through the unstructured
+    Hex8 constructor (the drop-in for a caller's own mesh and DofManager
+    numbering; coloured scatter), against the structured fast path."""
+    import torch
+
+    import femgpu
+
+    coords, conn, maps = box_as_hex_mesh(n, p)
+    N = (n * p + 1) ** 3
+    sn = n * p + 1
+    ids = np.arange(N).reshape(sn, sn, sn)
+    ess = np.unique(np.concatenate([ids[[0, -1]].ravel(), ids[:, [0, -1]].ravel(), ids[:, :, [0, -1]].ravel()]))
+    t0 = time.perf_counter()
+    op = femgpu.HexMeshOperator(p, coords, conn, elem_dofs=maps, n_dofs=N, kappa=kq.reshape(n ** 3, -1),
+                                ess_dofs=ess.astype(np.uint32))
+    t_setup = time.perf_counter() - t0
+    stream = torch.cuda.current_stream(dev)
+    op.set_stream(stream.cuda_stream)
+    x = torch.from_numpy(op.to_native(np.random.default_rng(3).standard_normal(N))).to(dev)
+    y = torch.zeros_like(x)
+    for _ in range(3):
+        op.apply_native(x.data_ptr(), y.data_ptr())
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(steps):
+        op.apply_native(x.data_ptr(), y.data_ptr())
+    g1.record(stream)
+    torch.cuda.synchronize()
+    op.check()
+    ms = g0.elapsed_time(g1) / steps
+    E, q3 = n ** 3, (p + 1) ** 3
+    nbytes = 6 * q3 * E * 8 + q3 * E * 4 + 2 * N * 8  # qdata + element map + x, y
+    out = {"ms": round(ms, 4), "gdof_s": round(N / (ms / 1e3) / 1e9, 3), "frac": round(nbytes / (ms / 1e3) / 1e9 / peak, 4),
+           "colours": op.colours, "setup_s": round(t_setup, 2)}
+    op.close()
+    return out
+
+
 def run_ex1():
     """mfem_ex1 on 24^3 Q1: source form, PCG-Jacobi rtol 1e-10, L2 error, on the GPU."""
     import torch
@@ -718,7 +778,7 @@ def main():
     ap.add_argument("--workload", default="q2_128", choices=sorted(WORKLOADS))
     ap.add_argument("--detail", default=None, help="file for the full record (default: gpurun_out/bench_detail.json "
                                                    "if that folder exists)")
-    for opt in ("solve", "q3", "cpu", "heat", "batch", "tet", "ex1"):
+    for opt in ("solve", "q3", "cpu", "heat", "batch", "tet", "ex1", "hex"):
         ap.add_argument(f"--no-{opt}", action="store_true")
     ap.add_argument("--mode", default=None, choices=["replicas", "sharded"],
                     help="multi-GPU form (default: replicas for 1 GPU, sharded for more)")
@@ -833,6 +893,8 @@ def main():
         op3.close()
         del kq3
 
+    hexu = None if args.no_hex else run_hex_unstructured(n, p, kq, args.steps, peak, dev)
+
     heat = None
     if not args.no_heat:
         heat, detail["heat"] = run_heat(rank, args.heat_steps, stream)
@@ -883,6 +945,7 @@ def main():
             "solve": solve,
             "apply": variants,
             "q3_64": q3,
+            "hex_unstructured": hexu,
             "heat": heat,
             "batch": batch,
             "tet": tet,
