@@ -7,7 +7,9 @@
 #pragma once
 #include "hex_kernels.cuh"
 
-template <int P> struct HexBS { static constexpr int v = P == 3 ? 64 : 128; };
+// Warps per CTA, stages of the per-warp quadrature-data ring, CTAs per SM
+// the register allocation must allow (shared memory allows 5 at Q2 FP64).
+template <int P> struct HexCfg { static constexpr int WARPS = 2, S = P == 3 ? 2 : 3, MINB = P == 3 ? 4 : 5; };
 
 template <typename T>
 static HexApply<T> hex_args(fg_op *op, const T *qd, const T *x, T *y, int constrained, const int *skip) {
@@ -21,18 +23,28 @@ static HexApply<T> hex_args(fg_op *op, const T *qd, const T *x, T *y, int constr
     A.y = y;
     A.constrained = constrained;
     A.skip = skip;
+    A.err = op->d_err;
+    A.wait_ns = op->wait_ns;
     return A;
 }
 
 template <int P, int OPK, typename T>
 static int hex_apply_t(fg_op *op, HexApply<T> A) {
-    constexpr int BS = HexBS<P>::v;
+    constexpr int WARPS = HexCfg<P>::WARPS, S = HexCfg<P>::S, BS = WARPS * 32;
+    using SM = HexSmem<P, OPK, T, WARPS, S>;
+    auto kern = hex_apply_kernel<P, OPK, T, WARPS, S, HexCfg<P>::MINB>;
+    static std::atomic<bool> attr_set[64];  // per device, set once
+    if (op->device < 0 || op->device >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", op->device);
+    if (!attr_set[op->device].load(std::memory_order_acquire)) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
+        attr_set[op->device].store(true, std::memory_order_release);
+    }
     for (size_t c = 0; c + 1 < op->u_col.size(); ++c) {
         A.e0 = op->u_col[c];
         A.e1 = op->u_col[c + 1];
-        const int64_t n = A.e1 - A.e0;
+        const int64_t n = A.e1 - A.e0;  // a multiple of 32
         if (n <= 0) continue;
-        hex_apply_kernel<P, OPK, T, BS><<<(unsigned)((n + BS - 1) / BS), BS, 0, op->stream>>>(A);
+        kern<<<(unsigned)((n + BS - 1) / BS), BS, SM::bytes, op->stream>>>(A);
         CK(cudaGetLastError());
     }
     return FG_OK;
@@ -161,17 +173,21 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
     std::vector<uint8_t> colour;
     const int ncol = hex_colour(E, nl, N, lexmap, colour);
     if (ncol < 0) return fail(FG_UNSUPPORTED, "element colouring needs more than 64 colours");
-    // elements sorted by colour (stable: the caller's order within a colour)
-    std::vector<int64_t> start((size_t)ncol + 1, 0);
-    for (uint8_t c : colour) ++start[(size_t)c + 1];
-    for (int c = 0; c < ncol; ++c) start[(size_t)c + 1] += start[(size_t)c];
-    std::vector<int32_t> eid((size_t)E), sdofs((size_t)E * nl);
+    // elements sorted by colour (stable: the caller's order within a colour),
+    // each colour padded to whole 32-element chunks (padding: eid -1, map -1)
+    std::vector<int64_t> count((size_t)ncol, 0), start((size_t)ncol + 1, 0);
+    for (uint8_t c : colour) ++count[c];
+    for (int c = 0; c < ncol; ++c) start[(size_t)c + 1] = start[(size_t)c] + (count[(size_t)c] + 31) / 32 * 32;
+    const int64_t Ep = start[(size_t)ncol];
+    if (Ep >= ((int64_t)1 << 31)) return fail(FG_INVALID_ARGUMENT, "more than 2^31 padded elements");
+    std::vector<int32_t> eid((size_t)Ep, -1), sdofs((size_t)Ep * nl, -1);
     {
         std::vector<int64_t> pos(start.begin(), start.end() - 1);
         for (int64_t e = 0; e < E; ++e) eid[(size_t)pos[colour[(size_t)e]]++] = (int32_t)e;
     }
     for (int k = 0; k < nl; ++k)
-        for (int64_t s = 0; s < E; ++s) sdofs[(size_t)k * E + s] = lexmap[(size_t)eid[(size_t)s] * nl + k];
+        for (int64_t s = 0; s < Ep; ++s)
+            if (eid[(size_t)s] >= 0) sdofs[(size_t)k * Ep + s] = lexmap[(size_t)eid[(size_t)s] * nl + k];
     std::vector<uint8_t> mask((size_t)N, 0);
     if (n_ess > 0) {
         std::vector<uint32_t> h_ess((size_t)n_ess);
@@ -191,7 +207,7 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
     op->kind = kind;
     op->p = order;
     op->unstr = true;
-    op->u_E = E;
+    op->u_E = Ep;
     op->u_col = start;
     op->N = N;
     // native vectors: one row of the N plain values padded with zeros to a
@@ -230,7 +246,7 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
 
     // quadrature data
     const int NC = kind == FG_MASS ? 1 : (kind == FG_DIFF ? 6 : 7);
-    op->qsize = E * Q3 * NC;
+    op->qsize = Ep * Q3 * NC;
     if ((rc = alloc_vec(&op->qd, op->qsize))) return bail(rc);
     int32_t *d_eid = nullptr;
     uint32_t *d_conn = nullptr;
@@ -242,8 +258,8 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
         if (d_kq) cudaFree(d_kq);
         if (d_rq) cudaFree(d_rq);
     };
-    bool up_ok = !cudaMalloc(&d_eid, sizeof(int32_t) * E) &&
-                 !cudaMemcpy(d_eid, eid.data(), sizeof(int32_t) * E, cudaMemcpyHostToDevice) &&
+    bool up_ok = !cudaMalloc(&d_eid, sizeof(int32_t) * Ep) &&
+                 !cudaMemcpy(d_eid, eid.data(), sizeof(int32_t) * Ep, cudaMemcpyHostToDevice) &&
                  !cudaMalloc(&d_conn, sizeof(uint32_t) * E * 8) &&
                  !cudaMemcpy(d_conn, h_conn.data(), sizeof(uint32_t) * E * 8, cudaMemcpyHostToDevice) &&
                  !cudaMalloc(&d_xyz, sizeof(double) * 3 * n_nodes) &&
@@ -259,7 +275,7 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
         return bail(fail(FG_CUDA_ERROR, "upload of the mesh and coefficients failed"));
     }
     HexSetup S{};
-    S.E = E;
+    S.E = Ep;
     S.eid = d_eid;
     S.conn = d_conn;
     S.coords = d_xyz;

@@ -4,13 +4,18 @@
 // Hex8 geometry of crates/assembly/src/assembler.rs:96-143, for any element
 // connectivity and any DOF numbering (a DofManager's element maps).
 //
-// Data layout (elements sorted by colour, element-major structure of arrays,
-// so a warp of consecutive elements reads each entry in one coalesced load):
+// Data layout.  Elements are sorted by colour and every colour is padded to a
+// whole number of 32-element chunks (padding elements have map entries -1 and
+// zero quadrature data); a warp works on one chunk.
 //   dofs [nl][E]         int32 element-to-DOF map, local DOF (c,b,a) at
-//                        k = (c*D + b)*D + a (tensor order on the reference cube)
-//   qd   [Q^3*NC][E]     quadrature data of point pt = (qy*Q + qx)*Q + qz,
-//                        component c at (pt*NC + c)*E + e: 6 symmetric
-//                        w|detJ| kappa J^-1 J^-T and/or w|detJ| rho
+//                        k = (c*D + b)*D + a (tensor order on the reference cube);
+//                        element-major, so a warp reads each entry in one load
+//   qd                   quadrature data in each warp's consumption order:
+//                        [chunk][col = qy*Q + qx][qz][comp][lane], comp the 6
+//                        symmetric w|detJ| kappa J^-1 J^-T and/or w|detJ| rho.
+//                        One column of a chunk is a contiguous stage, streamed
+//                        into a per-warp ring of shared-memory stages by 1-D bulk
+//                        copies on mbarriers (bounded waits, drained on timeout)
 //   ess  [N]             essential-DOF mask (constrained applies)
 //
 // Scatter without float atomics: the elements are coloured so that no two
@@ -29,16 +34,24 @@
 namespace fg {
 
 template <typename T> struct HexApply {
-    int64_t E, N;          // elements, DOFs
-    int64_t e0, e1;        // element range of this launch (one colour)
+    int64_t E, N;          // elements (padded to whole chunks), DOFs
+    int64_t e0, e1;        // element range of this launch (one colour, whole chunks)
     const int32_t *dofs;   // [nl][E]
-    const T *qd;           // [Q^3*NC][E]
+    const T *qd;           // per-chunk streams (layout above)
     const uint8_t *ess;    // [N] or null
     const T *x;            // null: diagonal
     T *y;
     int constrained;
     const int *skip;       // if non-null and *skip != 0 the kernel returns at once
+    int *err;              // device error word
+    uint64_t wait_ns;      // limit of each wait for a stage (0: 1 s)
 };
+
+// Index of component `comp` of quadrature point (col, qz) of element e.
+template <int P, int OPK> __host__ __device__ inline int64_t hex_qd_index(int64_t e, int col, int qz, int comp) {
+    constexpr int Q = P + 1, NC = NComp<OPK>::v;
+    return (((e >> 5) * (Q * Q) + col) * Q + qz) * (NC * 32) + comp * 32 + (e & 31);
+}
 
 // y = (accumulate ? y : 0) + (identity rows of the essential DOFs of a
 // constrained call: x, or 1 for the diagonal); the colour launches add the
@@ -53,27 +66,66 @@ __global__ void hex_init_kernel(const HexApply<T> A, int accumulate) {
     }
 }
 
-template <int P, int OPK, typename T, int BS>
-__global__ void __launch_bounds__(BS) hex_apply_kernel(const HexApply<T> A) {
-    constexpr int D = P + 1, Q = P + 1, NL = D * D * D, NC = NComp<OPK>::v;
+template <int P, int OPK, typename T, int WARPS, int S> struct HexSmem {
+    static constexpr int Q = P + 1, NL = (P + 1) * (P + 1) * (P + 1), BS = WARPS * 32;
+    static constexpr int STAGE = Q * NComp<OPK>::v * 32;  // elements of one column stage
+    static constexpr int off_x = WARPS * S * STAGE * (int)sizeof(T);
+    static constexpr int off_b = round_up(off_x + NL * BS * (int)sizeof(T), 8);
+    static constexpr int bytes = off_b + WARPS * S * 8;
+};
+
+template <int P, int OPK, typename T, int WARPS, int S, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) hex_apply_kernel(const HexApply<T> A) {
+    constexpr int D = P + 1, Q = P + 1, NL = D * D * D, NC = NComp<OPK>::v, BS = WARPS * 32;
     constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
     constexpr int QH = (P == 3 && sizeof(T) == 8) ? 2 : Q;  // half slabs bound the Q3 FP64 state
+    constexpr int COLS = Q * Q;
+    using SM = HexSmem<P, OPK, T, WARPS, S>;
+    constexpr int STAGE = SM::STAGE;
+    constexpr uint32_t QBYTES = (uint32_t)(STAGE * sizeof(T));
     using TB = Tab<T>;
-    __shared__ T xs[NL * BS];
+    extern __shared__ __align__(128) unsigned char hex_smem[];
     if (A.skip && *A.skip) return;
-    const int64_t e = A.e0 + (int64_t)blockIdx.x * BS + threadIdx.x;
-    if (e >= A.e1) return;
+    T *ring = reinterpret_cast<T *>(hex_smem);
+    T *xs = reinterpret_cast<T *>(hex_smem + SM::off_x);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(hex_smem + SM::off_b);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
     const int64_t E = A.E;
-    const int tid = threadIdx.x;
-    // gather (E) with the essential columns masked
+    const int64_t chunk = A.e0 / 32 + (int64_t)blockIdx.x * WARPS + warp;
+    const bool wvalid = chunk * 32 < A.e1;
+    const int64_t e = chunk * 32 + lane;
+    const uint64_t wlim = A.wait_ns ? A.wait_ns : 1000000000ull;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < WARPS * S; ++i) mbar_init(&bars[i], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (!wvalid) return;
+    T *qsw = ring + warp * S * STAGE;
+    uint64_t *qbw = bars + warp * S;
+    const T *qdw = A.qd + chunk * COLS * STAGE;
+    int q_issued = 0, q_waited = 0;
+    if (lane == 0) {
+        for (int j = 0; j < S && j < COLS; ++j) {
+            mbar_arrive_expect_tx(&qbw[j], QBYTES);
+            bulk_g2s(qsw + j * STAGE, qdw + (int64_t)j * STAGE, QBYTES, &qbw[j]);
+            q_issued = j + 1;
+        }
+    }
+    // gather (E) with the essential columns masked; padding elements hold -1
+    const bool evalid = __ldg(A.dofs + e) >= 0;
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
-        const int32_t d = __ldg(A.dofs + (int64_t)k * E + e);
-        const bool ess = A.constrained && A.ess && A.ess[d];
-        xs[k * BS + tid] = ess ? T(0) : __ldg(A.x + d);
+        T v = T(0);
+        if (evalid) {
+            const int32_t d = __ldg(A.dofs + (int64_t)k * E + e);
+            const bool ess = A.constrained && A.ess && A.ess[d];
+            v = ess ? T(0) : __ldg(A.x + d);
+        }
+        xs[k * BS + tid] = v;
     }
     auto uval = [&](int c, int b, int a) -> T { return xs[((c * D + b) * D + a) * BS + tid]; };
-    auto qdv = [&](int pt, int comp) -> T { return __ldg(A.qd + ((int64_t)pt * NC + comp) * E + e); };
+    bool ok = true;
     T out[D][D][D];
 #pragma unroll
     for (int c = 0; c < D; ++c)
@@ -126,11 +178,13 @@ __global__ void __launch_bounds__(BS) hex_apply_kernel(const HexApply<T> A) {
             }
 #pragma unroll
             for (int k = 0; k < QH; ++k) {
-                const int col = qy * Q + h0 + k;
+                const int j = qy * Q + h0 + k;  // column = stream stage
+                const int st = j % S;
+                wait_stage(&qbw[st], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
+                const T *qc = qsw + st * STAGE + lane;
                 T vx[Q], vy[Q], vz[Q], vu[Q];
 #pragma unroll
                 for (int qz = 0; qz < Q; ++qz) {
-                    const int pt = col * Q + qz;
                     T gx = 0, gy = 0, gz = 0, ui = 0;
 #pragma unroll
                     for (int c = 0; c < D; ++c) {
@@ -141,15 +195,22 @@ __global__ void __launch_bounds__(BS) hex_apply_kernel(const HexApply<T> A) {
                         }
                         if (HM) ui += TB::B(P, qz, c) * C0[c][k];
                     }
+                    const T *qq = qc + qz * (NC * 32);
                     vx[qz] = vy[qz] = vz[qz] = vu[qz] = T(0);
                     if (HK) {
-                        const T d0 = qdv(pt, 0), d1 = qdv(pt, 1), d2 = qdv(pt, 2), d3 = qdv(pt, 3),
-                                d4 = qdv(pt, 4), d5 = qdv(pt, 5);
+                        const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
                         vx[qz] = d0 * gx + d1 * gy + d2 * gz;
                         vy[qz] = d1 * gx + d3 * gy + d4 * gz;
                         vz[qz] = d2 * gx + d4 * gy + d5 * gz;
                     }
-                    if (HM) vu[qz] = qdv(pt, HK ? 6 : 0) * ui;
+                    if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
+                }
+                __syncwarp();
+                if (lane == 0 && ok && j + S < COLS) {
+                    fence_proxy_async();
+                    mbar_arrive_expect_tx(&qbw[st], QBYTES);
+                    bulk_g2s(qsw + st * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[st]);
+                    q_issued = j + S + 1;
                 }
 #pragma unroll
                 for (int c = 0; c < D; ++c) {
@@ -197,6 +258,9 @@ __global__ void __launch_bounds__(BS) hex_apply_kernel(const HexApply<T> A) {
             }
         }
     }
+    // after a timeout: wait out the copies still in flight before the CTA exits
+    if (!ok && lane == 0) drain_stages(qbw, S, q_waited, q_issued);
+    if (!evalid) return;
     // E^T: add into the non-essential DOFs (no other element of this colour
     // touches them)
 #pragma unroll
@@ -219,7 +283,7 @@ __global__ void __launch_bounds__(128) hex_diag_kernel(const HexApply<double> A)
     constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
     using TB = Tab<double>;
     const int64_t e = A.e0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= A.e1) return;
+    if (e >= A.e1 || __ldg(A.dofs + e) < 0) return;
     const int64_t E = A.E;
     double out[D][D][D];
 #pragma unroll
@@ -231,10 +295,9 @@ __global__ void __launch_bounds__(128) hex_diag_kernel(const HexApply<double> A)
     for (int qy = 0; qy < Q; ++qy)
         for (int qx = 0; qx < Q; ++qx)
             for (int qz = 0; qz < Q; ++qz) {
-                const int pt = (qy * Q + qx) * Q + qz;
                 double d[7];
 #pragma unroll
-                for (int k = 0; k < NC; ++k) d[k] = __ldg(A.qd + ((int64_t)pt * NC + k) * E + e);
+                for (int k = 0; k < NC; ++k) d[k] = __ldg(A.qd + hex_qd_index<P, OPK>(e, qy * Q + qx, qz, k));
 #pragma unroll
                 for (int c = 0; c < D; ++c)
 #pragma unroll
@@ -273,8 +336,8 @@ __global__ void __launch_bounds__(128) hex_diag_kernel(const HexApply<double> A)
 // conn[eid*8 .. +8] in HexQ1 order; kappa_q / rho_q are indexed by the
 // caller's element and the tensor point (qz, qy, qx).
 struct HexSetup {
-    int64_t E;
-    const int32_t *eid;     // [E] sorted -> caller element
+    int64_t E;              // padded element count
+    const int32_t *eid;     // [E] sorted -> caller element, -1 for padding
     const uint32_t *conn;   // [E][8]
     const double *coords;   // [n_nodes][3]
     const double *kappa_q, *rho_q;
@@ -293,6 +356,12 @@ __global__ void hex_setup_kernel(const HexSetup S, T *__restrict__ qd) {
         const int q = (int)(t % Q3);  // tensor point index (qz, qy, qx), qx fastest
         const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
         const int64_t e = S.eid[s];
+        if (e < 0) {  // padding element: zero data
+            if (HK)
+                for (int k = 0; k < 6; ++k) qd[hex_qd_index<P, OPK>(s, qy * Q + qx, qz, k)] = (T)0;
+            if (HM) qd[hex_qd_index<P, OPK>(s, qy * Q + qx, qz, HK ? 6 : 0)] = (T)0;
+            continue;
+        }
         double xv[8][3];
         for (int k = 0; k < 8; ++k) {
             const int64_t v = S.conn[e * 8 + k];
@@ -306,10 +375,10 @@ __global__ void hex_setup_kernel(const HexSetup S, T *__restrict__ qd) {
         const double rho = S.rho_q ? S.rho_q[e * Q3 + q] : S.rho_c;
         double D[6], m;
         if (!hex_point_qdata(xv, xi, w, kap, S.c_k, rho, S.c_m, D, m) && S.err) atomicOr(S.err, FG_DERR_BOUNDS);
-        const int pt = (qy * Q + qx) * Q + qz;
         if (HK)
-            for (int k = 0; k < 6; ++k) qd[((int64_t)pt * NC + k) * S.E + s] = (T)D[k];
-        if (HM) qd[((int64_t)pt * NC + (HK ? 6 : 0)) * S.E + s] = (T)m;
+            for (int k = 0; k < 6; ++k) qd[hex_qd_index<P, OPK>(s, qy * Q + qx, qz, k)] = (T)D[k];
+        if (HM) qd[hex_qd_index<P, OPK>(s, qy * Q + qx, qz, HK ? 6 : 0)] = (T)m;
+        (void)NC;
     }
 }
 
