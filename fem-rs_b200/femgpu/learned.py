@@ -220,6 +220,10 @@ def main():
             "steps_per_field": args.steps_per_field, "batch": args.batch, "lr": args.lr,
             "first_loss": float(np.mean(hist[:k])), "final_loss": float(np.mean(hist[-k:])),
             "train_s": t_train, "params": net.num_params, "channels": list(net.channels)}
+    if args.init and seeds:  # fine-tuned from earlier weights
+        meta["init_from"] = {"file": os.path.basename(args.init),
+                             **{k: init_meta[k] for k in ("train_fields", "first_seed", "steps_per_field", "lr")
+                                if k in init_meta}}
     if seeds:
         save(net, args.out, meta)
     elif init_meta is not None:  # evaluation of stored weights
