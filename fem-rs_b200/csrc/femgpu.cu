@@ -248,10 +248,14 @@ struct fg_op {
     int *d_err = nullptr;
     unsigned *bar = nullptr;  // grid-barrier counters of the fused PCG iteration kernel
     bool fused_pcg = true;    // one cooperative launch per Jacobi-PCG iteration (FG_FUSED_PCG=0: three)
+    bool pipelined = true;    // host-memory applies pipelined over z ranges (FG_PIPELINED_APPLY=0: not)
     uint64_t wait_ns = 0;  // limit of the apply kernels' device-side waits (0: 1 s)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t cap_stream = nullptr;  // private stream for CUDA-graph capture
+    // pipelined host-memory applies: upload and download streams, per-range events
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    std::vector<cudaEvent_t> ev_in, ev_out;
     bool graphs = true;                 // replay solver chunks as CUDA graphs
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -293,6 +297,10 @@ static void free_op(fg_op *op) {
     if (op->ev1) cudaEventDestroy(op->ev1);
     if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
     if (op->cap_stream) cudaStreamDestroy(op->cap_stream);
+    if (op->s_in) cudaStreamDestroy(op->s_in);
+    if (op->s_out) cudaStreamDestroy(op->s_out);
+    for (cudaEvent_t e : op->ev_in) cudaEventDestroy(e);
+    for (cudaEvent_t e : op->ev_out) cudaEventDestroy(e);
     if (op->nn_stream) cudaStreamDestroy(op->nn_stream);
     if (op->nn_ev_r) cudaEventDestroy(op->nn_ev_r);
     if (op->nn_ev_n) cudaEventDestroy(op->nn_ev_n);
@@ -328,7 +336,8 @@ template <> struct TmapType<float> { static constexpr CUtensorMapDataType v = CU
 
 template <int P, int OPK, typename T, int FMT>
 static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const T *x, T *y,
-                          int accumulate, const int *skip, unsigned *fixcnt = nullptr) {
+                          int accumulate, const int *skip, unsigned *fixcnt = nullptr, int item0 = 0,
+                          int nitems = -1) {
     using C = KC<P, T>;
     static_assert(C::WY == KCfg<P>::WY, "FP32 and FP64 share the item tiling");
     constexpr int S = FMT == 0 ? C::S : 2;  // affine format: one element layer per stage
@@ -350,8 +359,8 @@ static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const 
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return fail(FG_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
-    ApplyArgs<T> A{g, qd, y, face, accumulate, op->d_err, skip, fixcnt, op->wait_ns};
-    kern<<<g.n_items(), C::WY * 32, SM::bytes, op->stream>>>(tmap, A);
+    ApplyArgs<T> A{g, qd, y, face, accumulate, op->d_err, skip, fixcnt, op->wait_ns, item0};
+    kern<<<nitems < 0 ? g.n_items() : nitems, C::WY * 32, SM::bytes, op->stream>>>(tmap, A);
     CK(cudaGetLastError());
     return FG_OK;
 }
@@ -362,20 +371,20 @@ template <> const float *qdata_of<float>(fg_op *op) { return op->fmt ? op->qa32 
 
 template <int P, typename T>
 static int launch_apply_p(fg_op *op, const Grid &g, const T *, T *face, const T *x, T *y,
-                          int accumulate, const int *skip, unsigned *fixcnt) {
+                          int accumulate, const int *skip, unsigned *fixcnt, int item0 = 0, int nitems = -1) {
     const T *qd = qdata_of<T>(op);
     if (!qd) return fail(FG_INVALID_ARGUMENT, "quadrature data for this precision/format not built");
     if (op->fmt == 0) {
         switch (op->kind) {
-        case FG_MASS: return launch_apply_t<P, 1, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
-        case FG_DIFF: return launch_apply_t<P, 2, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
-        default: return launch_apply_t<P, 3, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
+        case FG_MASS: return launch_apply_t<P, 1, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt, item0, nitems);
+        case FG_DIFF: return launch_apply_t<P, 2, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt, item0, nitems);
+        default: return launch_apply_t<P, 3, T, 0>(op, g, qd, face, x, y, accumulate, skip, fixcnt, item0, nitems);
         }
     }
     switch (op->kind) {
-    case FG_MASS: return launch_apply_t<P, 1, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
-    case FG_DIFF: return launch_apply_t<P, 2, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
-    default: return launch_apply_t<P, 3, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt);
+    case FG_MASS: return launch_apply_t<P, 1, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt, item0, nitems);
+    case FG_DIFF: return launch_apply_t<P, 2, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt, item0, nitems);
+    default: return launch_apply_t<P, 3, T, 1>(op, g, qd, face, x, y, accumulate, skip, fixcnt, item0, nitems);
     }
 }
 
@@ -568,6 +577,8 @@ FG_API int fg_op_create(const fg_mesh *mesh, int order, int nq1d, int kind, doub
         op->fused_fixup = f && f[0] == '1';
         const char *fp = std::getenv("FG_FUSED_PCG");
         op->fused_pcg = !(fp && fp[0] == '0');
+        const char *pp = std::getenv("FG_PIPELINED_APPLY");
+        op->pipelined = !(pp && pp[0] == '0');
     }
     if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)))
         return bail(fail(FG_CUDA_ERROR, "cudaMalloc failed"));
@@ -747,6 +758,92 @@ static int from_native(fg_op *op, double *dst, const double *src, int mem) {
     return from_native_t<double>(op, dst, src, mem);
 }
 
+// y = A x for host vectors on a box, pipelined over ranges of item layers in
+// z: the upload of range r+1's DOF planes, the apply and fix-up of range r and
+// the download of range r-1's finished planes run at the same time (PCIe moves
+// data both ways at once).  Range r's items need the planes [A_r, A_{r+1}]
+// (A_r = first plane of its item layers); its fix-up completes the planes
+// [A_r, A_{r+1}), whose owners are its items (plane A_{r+1} belongs to the next
+// range, which adds this range's face partials in its own fix-up).  Upload
+// chunk r holds the planes (A_r, A_{r+1}] (chunk 0 from plane 0), so range r
+// can start once chunks 0..r have arrived.  The staging buffer holds x planes
+// on the way in and y planes on the way out: a y range is packed only after
+// the x planes it overlaps were repacked, and uploads never touch it again.
+static int apply_host_pipelined(fg_op *op, const double *x, double *y, int constrained) {
+    Grid g = op->g;
+    g.ess = constrained ? op->ess_tags : 0;
+    const int R = std::min(g.ntz, 8);
+    double *st = nullptr;
+    int rc = stage_of(op, &st);
+    if (rc) return rc;
+    if (!op->s_in) {
+        CK(cudaStreamCreateWithFlags(&op->s_in, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&op->s_out, cudaStreamNonBlocking));
+    }
+    while ((int)op->ev_in.size() < R) {
+        cudaEvent_t a, b;
+        CK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+        op->ev_in.push_back(a);
+        op->ev_out.push_back(b);
+    }
+    const int SZe = g.TZ * g.p;
+    const int64_t plane = (int64_t)g.NI * g.NJ;  // plain values per DOF plane
+    const size_t sp = sizeof(double) * g.NIp, spl = sizeof(double) * g.NI;
+    std::vector<int> t0(R + 1), A(R + 1);
+    for (int r = 0; r <= R; ++r) t0[r] = (int)((int64_t)g.ntz * r / R);
+    for (int r = 0; r < R; ++r) A[r] = t0[r] * SZe;
+    A[R] = g.NK - 1;
+    // the caller's stream has to see the handle's earlier work first
+    CK(cudaEventRecord(op->ev_out[0], op->stream));
+    CK(cudaStreamWaitEvent(op->s_in, op->ev_out[0], 0));
+    for (int r = 0; r < R; ++r) {  // uploads, in order on the upload stream
+        const int lo = r == 0 ? 0 : A[r] + 1, hi = A[r + 1] + 1;
+        CK(cudaMemcpyAsync(st + lo * plane, x + lo * plane, sizeof(double) * plane * (hi - lo),
+                           cudaMemcpyHostToDevice, op->s_in));
+        CK(cudaEventRecord(op->ev_in[r], op->s_in));
+    }
+    const int items_per_layer = g.ntx * g.nty;
+    for (int r = 0; r < R; ++r) {
+        const int lo = r == 0 ? 0 : A[r] + 1, hi = A[r + 1] + 1;
+        CK(cudaStreamWaitEvent(op->stream, op->ev_in[r], 0));
+        CK(cudaMemcpy2DAsync(op->xs + (int64_t)lo * g.NJ * g.NIp, sp, st + lo * plane, spl, spl,
+                             (size_t)g.NJ * (hi - lo), cudaMemcpyDeviceToDevice, op->stream));
+        const int i0 = t0[r] * items_per_layer, ni = (t0[r + 1] - t0[r]) * items_per_layer;
+        switch (op->p) {
+        case 1: rc = launch_apply_p<1, double>(op, g, op->qd, op->face, op->xs, op->ys, 0, nullptr, nullptr, i0, ni); break;
+        case 2: rc = launch_apply_p<2, double>(op, g, op->qd, op->face, op->xs, op->ys, 0, nullptr, nullptr, i0, ni); break;
+        default: rc = launch_apply_p<3, double>(op, g, op->qd, op->face, op->xs, op->ys, 0, nullptr, nullptr, i0, ni); break;
+        }
+        if (rc) return rc;
+        // fix-up of the planes this range owns
+        const int Ka = A[r], Kb = r == R - 1 ? g.NK : A[r + 1];
+        int pl0 = 0, npl = 0;
+        for (int pl = 0; pl < g.ntz - 1; ++pl) {
+            const int K = (pl + 1) * SZe;
+            if (K >= Ka && K < Kb) {
+                if (!npl) pl0 = pl;
+                ++npl;
+            }
+        }
+        const int rows = (g.ntx - 1 + g.nty - 1) * (Kb - Ka) + npl * g.NJ;
+        if (rows > 0) {
+            fixup_range_kernel<double><<<rows, 128, 0, op->stream>>>(g, op->ys, op->face, Ka, Kb, pl0);
+            CK(cudaGetLastError());
+        }
+        CK(cudaMemcpy2DAsync(st + Ka * plane, spl, op->ys + (int64_t)Ka * g.NJ * g.NIp, sp, spl,
+                             (size_t)g.NJ * (Kb - Ka), cudaMemcpyDeviceToDevice, op->stream));
+        CK(cudaEventRecord(op->ev_out[r], op->stream));
+        CK(cudaStreamWaitEvent(op->s_out, op->ev_out[r], 0));
+        CK(cudaMemcpyAsync(y + Ka * plane, st + Ka * plane, sizeof(double) * plane * (Kb - Ka),
+                           cudaMemcpyDeviceToHost, op->s_out));
+    }
+    // the handle's stream ends after the last download
+    CK(cudaEventRecord(op->ev_in[0], op->s_out));
+    CK(cudaStreamWaitEvent(op->stream, op->ev_in[0], 0));
+    return FG_OK;
+}
+
 extern "C" {
 
 FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, int constrained,
@@ -756,6 +853,10 @@ FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, in
     std::lock_guard<std::mutex> lk(op->mu);
     CK(cudaSetDevice(op->device));
     int rc;
+    if (mem == FG_HOST && !accumulate && !op->unstr && !op->fused_fixup && op->g.ntz >= 2 && op->pipelined) {
+        if ((rc = apply_host_pipelined(op, x, y, constrained))) return rc;
+        return check_device_error(op);
+    }
     if ((rc = to_native(op, op->xs, x, mem))) return rc;
     if (accumulate && (rc = to_native(op, op->ys, y, mem))) return rc;
     if ((rc = apply_native(op, op->xs, op->ys, accumulate, constrained, nullptr))) return rc;

@@ -70,6 +70,7 @@ template <typename T> struct ApplyArgs {
     unsigned *fixcnt; // non-null: fix-up fused into the apply (per-item arrival counters, all zero
                       // between launches); null: fixup_kernel runs after the apply
     uint64_t wait_ns; // limit of each wait for a copy into shared memory; 0: 1 s
+    int item0;        // first item of this launch (block b works on item item0 + b)
 };
 
 template <typename T, int P>
@@ -857,7 +858,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
 template <int P, int OPK, typename T, int WY, int S, int MINB, int FMT = 0>
 __global__ void __launch_bounds__(WY * 32, MINB)
     pa_apply_kernel(const __grid_constant__ CUtensorMap xmap, const ApplyArgs<T> A) {
-    pa_apply_body<P, OPK, T, WY, S, FMT>(&xmap, A, blockIdx.x);
+    pa_apply_body<P, OPK, T, WY, S, FMT>(&xmap, A, A.item0 + blockIdx.x);
 }
 
 // Batched operators (many independent instances of the same order, kind and
@@ -1143,6 +1144,28 @@ __global__ void __launch_bounds__(128) fixup_kernel(const Grid g, T *__restrict_
                                                     const T *__restrict__ face, const int *skip) {
     if (skip && *skip) return;
     fixup_row<T>(g, blockIdx.x, y, face);
+}
+
+// Fix-up of the shared DOFs owned by the DOF planes [Ka, Kb): the x- and
+// y-plane rows of those planes and the z-plane rows of the item-layer
+// boundaries pl0 .. pl0 + npl - 1 inside the range, in fixup_row's numbering
+// (used when an apply is run one range of item layers at a time).
+template <typename T>
+__global__ void __launch_bounds__(128) fixup_range_kernel(const Grid g, T *__restrict__ y,
+                                                          const T *__restrict__ face, int Ka, int Kb, int pl0) {
+    const int nk = Kb - Ka;
+    const int rx = (g.ntx - 1) * nk, ry = (g.nty - 1) * nk;
+    int b = blockIdx.x, r;
+    if (b < rx) {
+        r = (b / nk) * g.NK + Ka + b % nk;
+    } else if (b < rx + ry) {
+        b -= rx;
+        r = (g.ntx - 1) * g.NK + (b / nk) * g.NK + Ka + b % nk;
+    } else {
+        b -= rx + ry;
+        r = (g.ntx - 1) * g.NK + (g.nty - 1) * g.NK + (pl0 + b / g.NJ) * g.NJ + b % g.NJ;
+    }
+    fixup_row<T>(g, r, y, face);
 }
 
 // Batched fix-up: blockIdx.y = instance; blocks stride over the instance's

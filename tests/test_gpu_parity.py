@@ -244,3 +244,23 @@ def test_cg_operator_stopping_rule_matches_oracle(rtol, atol):
     res0 = femgpu.solve_cg_operator(N, N, op, b, x.copy(),
                                     femgpu.SolverConfig(rtol=0.0, atol=2.0 * res.final_residual))
     assert res0.converged and res0.iterations == 0
+
+
+@pytest.mark.parametrize("p,shape", [(1, (70, 9, 40)), (2, (40, 9, 37)), (3, (33, 5, 26)), (2, (128, 16, 64))])
+def test_pipelined_host_apply_is_bit_identical(p, shape, monkeypatch):
+    """fg_op_apply on host vectors runs in z ranges of item layers (upload of the
+    next range, apply and fix-up of this one, download of the finished planes
+    overlapped); the sums are those of the one-launch apply, bit for bit."""
+    need_gpu()
+    mesh, coef, op = make_pair(shape, p, femgpu.MASS_DIFF, seed=3, c_m=0.4, c_k=1.2)
+    monkeypatch.setenv("FG_PIPELINED_APPLY", "0")
+    _, _, ref = make_pair(shape, p, femgpu.MASS_DIFF, seed=3, c_m=0.4, c_k=1.2)
+    monkeypatch.delenv("FG_PIPELINED_APPLY")
+    assert op.tile[2] < shape[2]  # more than one item layer: the pipelined path runs
+    x = np.random.default_rng(8).normal(size=mesh.ndofs)
+    for constrained in (False, True):
+        for _ in range(2):
+            assert np.array_equal(op.matvec(x, constrained=constrained), ref.matvec(x, constrained=constrained))
+    assert relerr(op.matvec(x, constrained=True), O.apply_constrained(mesh, coef, O.ess_mask(mesh), x)) <= RTOL
+    op.close()
+    ref.close()
