@@ -198,7 +198,10 @@ FG_API int fg_op_set_stream(fg_op *op, void *stream);
  * (mem = FG_HOST) or device (FG_DEVICE) memory.  Synchronous.  Host vectors
  * go through a device staging buffer of n_dofs values that the first
  * host-memory call allocates; page-locked host memory runs the copies at full
- * PCIe rate. */
+ * PCIe rate.  With host vectors, accumulate = 0 and more than one layer of
+ * work items in z, the call is pipelined over z ranges: the upload of the
+ * next range's DOF planes, the apply of this range and the download of the
+ * planes it finished run at the same time (the same sums as one launch). */
 FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, int constrained,
                        int mem);
 
