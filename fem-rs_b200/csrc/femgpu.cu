@@ -772,7 +772,7 @@ static int from_native(fg_op *op, double *dst, const double *src, int mem) {
 static int apply_host_pipelined(fg_op *op, const double *x, double *y, int constrained) {
     Grid g = op->g;
     g.ess = constrained ? op->ess_tags : 0;
-    const int R = std::min(g.ntz, 8);
+    const int R = std::min(g.ntz, 16);
     double *st = nullptr;
     int rc = stage_of(op, &st);
     if (rc) return rc;
