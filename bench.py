@@ -580,13 +580,19 @@ def run_tet(dev, peak):
         top.check()
         dt = g0.elapsed_time(g1) / 1e3 / reps
         E, nl, nqt = dofs.shape[0], dofs.shape[1], top.nq
-        # algorithmic bytes: element map, geometry, per-point scalars, x gathered once, y written once
-        ab = E * (nl * 4 + 6 * 8 + nqt * 8) + nd * (8 + 8)
-        out[f"p{tp}_n{tn}"] = {"elements": int(E), "dofs": int(nd), "ms": round(dt * 1e3, 4),
-                               "gdof_s": round(nd / dt / 1e9, 3), "frac_algorithmic": round(ab / dt / 1e9 / peak, 4)}
+        # algorithmic bytes of the diffusion apply in the moment form: element map (int32), geometry G
+        # (6 doubles), diffusion moments (10 doubles for P2, 1 for P1), x read once, y written once;
+        # the point form would read nq point scalars instead of the moments
+        nmom = 10 if tp == 2 else 1
+        ab = E * (nl * 4 + 6 * 8 + nmom * 8) + nd * (8 + 8)
+        ab_pt = E * (nl * 4 + 6 * 8 + nqt * 8) + nd * (8 + 8)
+        out[f"p{tp}_n{tn}"] = {"elements": int(E), "dofs": int(nd), "points": int(nqt), "ms": round(dt * 1e3, 4),
+                               "gdof_s": round(nd / dt / 1e9, 3), "frac_algorithmic": round(ab / dt / 1e9 / peak, 4),
+                               "point_form_bytes_per_s_frac": round(ab_pt / dt / 1e9 / peak, 4)}
         top.close()
         del xt, yt
-    out["timing"] = "CUDA events over 20 asynchronous applies (element kernel + CSR scatter kernel each)"
+    out["timing"] = ("CUDA events over 20 asynchronous applies (chunk kernel + shared-DOF kernel each); "
+                     "diffusion in the moment form")
     return out
 
 

@@ -3377,30 +3377,63 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
     CK(cudaMalloc(&t->d_err, sizeof(int)));
     CK(cudaMemset(t->d_err, 0, sizeof(int)));
     FG_LEGACY_FENCE();
-    // element map: validate, transpose to [nl][E], CSR of element-local slots per DOF
+    // element map: validate, transpose to [nl][E]; chunk order and chunk DOF lists
     std::vector<int32_t> h(n_elem * nl);
     CK(cudaMemcpy(h.data(), elem_dofs, sizeof(int32_t) * h.size(), cudaMemcpyDefault));
+    std::vector<double> hc((size_t)n_nodes * 3);
+    CK(cudaMemcpy(hc.data(), coords, sizeof(double) * hc.size(), cudaMemcpyDefault));
     std::vector<int32_t> soa(h.size());
-    std::vector<int64_t> offs(n_dofs + 1, 0);
     for (int64_t e = 0; e < n_elem; ++e)
         for (int i = 0; i < nl; ++i) {
             const int32_t d = h[e * nl + i];
             if (d < 0 || d >= n_dofs || (i < 4 && d >= n_nodes))
                 return fail(FG_BOUNDS, "element %lld local DOF %d out of range", (long long)e, i);
             soa[(int64_t)i * n_elem + e] = d;
-            ++offs[d + 1];
         }
-    for (int64_t d = 0; d < n_dofs; ++d) offs[d + 1] += offs[d];
-    std::vector<int32_t> slots(offs[n_dofs]);
-    {
-        std::vector<int64_t> pos(offs.begin(), offs.end() - 1);
-        for (int64_t e = 0; e < n_elem; ++e)  // (e, i) ascending within each DOF
-            for (int i = 0; i < nl; ++i) slots[pos[h[e * nl + i]]++] = (int32_t)(e * nl + i);
+    t->CE = order == 3 ? 256 : 512;
+    if (const char *ev = std::getenv("FG_TET_CHUNK")) {
+        const int v = std::atoi(ev);
+        if (v >= 32 && v <= 1024 && v * nl <= 65536) t->CE = v;
     }
-    if ((rc = tet_upload(&t->dofs, soa.data(), soa.size())) || (rc = tet_upload(&t->offs, offs.data(), offs.size())) ||
-        (rc = tet_upload(&t->slots, slots.data(), slots.size())) ||
+    if (const char *ev = std::getenv("FG_TET_WIDE")) t->wide = std::atoi(ev) != 0;
+    TetChunkPlan plan;
+    tet_plan_chunks(h, hc, n_elem, n_dofs, nl, t->CE, plan);
+    t->n_chunks = (int)((n_elem + t->CE - 1) / t->CE);
+    t->max_nu = plan.max_nu;
+    if (tet_chunk_smem(nl, t->CE, t->max_nu) > 227 * 1024)
+        return fail(FG_UNSUPPORTED, "tet chunk of %d elements needs too much shared memory", t->CE);
+    t->n_shared = (int64_t)plan.sh_dof.size();
+    t->n_part = plan.sh_off.back();
+    if ((rc = tet_upload(&t->dofs, soa.data(), soa.size())) ||
+        (rc = tet_upload(&t->cu_slots, plan.cu_slots.data(), plan.cu_slots.size())) ||
+        (rc = tet_upload(&t->cu_off, plan.cu_off.data(), plan.cu_off.size())) ||
+        (rc = tet_upload(&t->cu_dof, plan.cu_dof.data(), plan.cu_dof.size())) ||
+        (rc = tet_upload(&t->cu_pid, plan.cu_pid.data(), plan.cu_pid.size())) ||
+        (rc = tet_upload(&t->cu_soff, plan.cu_soff.data(), plan.cu_soff.size())) ||
+        (rc = tet_upload(&t->sh_dof, plan.sh_dof.data(), plan.sh_dof.size())) ||
+        (rc = tet_upload(&t->sh_off, plan.sh_off.data(), plan.sh_off.size())) ||
         (rc = tet_upload(&t->coords, coords, (size_t)n_nodes * 3)))
         return rc;
+    CK(cudaMalloc(&t->part, sizeof(double) * std::max<int64_t>(t->n_part, 1)));
+    {   // element map and essential local DOFs in the chunk order
+        std::vector<int32_t> ed(h.size());
+        std::vector<uint8_t> he;
+        if (ess) {
+            he.resize(n_dofs);
+            CK(cudaMemcpy(he.data(), ess, n_dofs, cudaMemcpyDefault));
+        }
+        std::vector<uint32_t> em(ess ? n_elem : 0, 0u);
+        for (int64_t n = 0; n < n_elem; ++n) {
+            const int64_t e = plan.perm[n];
+            for (int i = 0; i < nl; ++i) {
+                const int32_t d = h[e * nl + i];
+                ed[(int64_t)i * n_elem + n] = d;
+                if (ess && he[d]) em[n] |= 1u << i;
+            }
+        }
+        if ((rc = tet_upload(&t->edof, ed.data(), ed.size()))) return rc;
+        if (ess && (rc = tet_upload(&t->emsk, em.data(), em.size()))) return rc;
+    }
     if (ess && (rc = tet_upload(&t->ess, ess, (size_t)n_dofs))) return rc;
     // rule tables
     std::vector<double> pts, w;
@@ -3420,14 +3453,36 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
     struct FT { double **a, **b; ~FT() { if (*a) cudaFree(*a); if (*b) cudaFree(*b); } } ft{&tk, &tr};
     if (kappa_q) { if ((rc = tet_upload(&tk, kappa_q, (size_t)n_elem * t->nq))) return rc; d_kq = tk; }
     if (rho_q) { if ((rc = tet_upload(&tr, rho_q, (size_t)n_elem * t->nq))) return rc; d_rq = tr; }
+    // geometry and point scalars in the caller's order, then the chunk order
+    // and the diffusion moments (P1: S00 G, P2: 10)
+    double *G0 = nullptr, *sk0 = nullptr, *sm0 = nullptr;
+    int32_t *d_perm = nullptr;
+    struct FS { double **a, **b, **c; int32_t **d;
+        ~FS() { if (*a) cudaFree(*a); if (*b) cudaFree(*b); if (*c) cudaFree(*c); if (*d) cudaFree(*d); } }
+        fs{&G0, &sk0, &sm0, &d_perm};
+    CK(cudaMalloc(&G0, sizeof(double) * 6 * n_elem));
     CK(cudaMalloc(&t->G, sizeof(double) * 6 * n_elem));
-    if (kind & 2) CK(cudaMalloc(&t->sk, sizeof(double) * t->nq * n_elem));
-    if (kind & 1) CK(cudaMalloc(&t->sm, sizeof(double) * t->nq * n_elem));
-    CK(cudaMalloc(&t->Ye, sizeof(double) * nl * n_elem));
-    const TetArgs A = tet_args(t);
+    if (kind & 2) {
+        CK(cudaMalloc(&sk0, sizeof(double) * t->nq * n_elem));
+        CK(cudaMalloc(&t->sk, sizeof(double) * t->nq * n_elem));
+    }
+    if (kind & 1) {
+        CK(cudaMalloc(&sm0, sizeof(double) * t->nq * n_elem));
+        CK(cudaMalloc(&t->sm, sizeof(double) * t->nq * n_elem));
+    }
+    const int nmom = (kind & 2) ? (order == 1 ? 6 : (order == 2 ? 10 : 0)) : 0;
+    if (nmom) CK(cudaMalloc(&t->Sm, sizeof(double) * nmom * n_elem));
+    if ((rc = tet_upload(&d_perm, plan.perm.data(), plan.perm.size()))) return rc;
+    TetArgs A = tet_args(t);
+    A.G = G0;
+    A.sk = sk0;
+    A.sm = sm0;
     const int eb = (int)std::min<int64_t>((n_elem + 255) / 256, 148 * 16);
     tet_setup_kernel<<<eb, 256, 0, t->stream>>>(A, nl, t->coords, d_w, d_kq, kappa_const, d_rq, rho_const, c_mass,
-                                                c_diff, t->G, t->sk, t->sm, t->d_err);
+                                                c_diff, G0, sk0, sm0, t->d_err);
+    CK(cudaGetLastError());
+    tet_permute_kernel<<<eb, 256, 0, t->stream>>>(n_elem, t->nq, kind, nmom, d_perm, t->qp, G0, sk0, sm0, t->G,
+                                                  t->sk, t->sm, t->Sm);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(t->stream));
     int herr = 0;

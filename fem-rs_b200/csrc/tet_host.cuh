@@ -13,13 +13,20 @@ struct fg_tet {
     int device = 0;
     int p = 1, nl = 4, kind = 2;
     int64_t E = 0, N = 0, n_nodes = 0;
-    int32_t *dofs = nullptr;  // [nl][E]
-    double *G = nullptr, *sk = nullptr, *sm = nullptr, *Ye = nullptr, *coords = nullptr;
+    int32_t *dofs = nullptr;  // [nl][E] caller's element order (setup, quadrature points)
+    double *G = nullptr, *sk = nullptr, *sm = nullptr, *Sm = nullptr, *coords = nullptr;  // chunk order
     double *qp = nullptr, *phi = nullptr, *grad = nullptr;  // rule tables (device)
     std::vector<double> h_phi, h_grad;                       // rule tables (host, kernel parameters)
     int nq = 0;
-    int64_t *offs = nullptr;
-    int32_t *slots = nullptr;
+    // chunked scatter
+    int CE = 0, max_nu = 0, n_chunks = 0, wide = 0;  // wide: 512-thread CTAs for the P2 moment form
+    int64_t n_shared = 0, n_part = 0;
+    int32_t *edof = nullptr;   // [nl][E] chunk order
+    uint32_t *emsk = nullptr;  // [E] chunk order
+    uint16_t *cu_slots = nullptr;
+    int32_t *cu_off = nullptr, *cu_dof = nullptr, *cu_pid = nullptr, *cu_soff = nullptr;
+    int32_t *sh_dof = nullptr, *sh_off = nullptr;
+    double *part = nullptr;
     uint8_t *ess = nullptr;
     double *xh = nullptr, *yh = nullptr;  // device copies for host-memory calls
     int *d_err = nullptr;
@@ -182,12 +189,38 @@ static TetArgs tet_args(const fg_tet *t) {
     return A;
 }
 
+static TetChunk tet_chunk_args(const fg_tet *t) {
+    TetChunk C{};
+    C.E = t->E;
+    C.N = t->N;
+    C.CE = t->CE;
+    C.max_nu = t->max_nu;
+    C.G = t->G;
+    C.Sm = t->Sm;
+    C.sk = t->sk;
+    C.sm = t->sm;
+    C.edof = t->edof;
+    C.emsk = t->emsk;
+    C.cu_off = t->cu_off;
+    C.cu_dof = t->cu_dof;
+    C.cu_pid = t->cu_pid;
+    C.cu_soff = t->cu_soff;
+    C.cu_slots = t->cu_slots;
+    C.part = t->part;
+    C.sh_dof = t->sh_dof;
+    C.sh_off = t->sh_off;
+    C.ess = t->ess;
+    C.n_shared = t->n_shared;
+    return C;
+}
+
 static void tet_free(fg_tet *t) {
     if (!t) return;
     cudaSetDevice(t->device);
     if (t->stream) cudaStreamSynchronize(t->stream);
-    void *ptrs[] = {t->dofs, t->G, t->sk, t->sm, t->Ye, t->coords, t->qp, t->phi, t->grad,
-                    t->offs, t->slots, t->ess, t->xh, t->yh, t->d_err};
+    void *ptrs[] = {t->dofs, t->G, t->sk, t->sm, t->Sm, t->coords, t->qp, t->phi, t->grad, t->edof, t->emsk, t->cu_slots,
+                    t->cu_off, t->cu_dof, t->cu_pid, t->cu_soff, t->sh_dof, t->sh_off, t->part, t->ess, t->xh,
+                    t->yh, t->d_err};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (t->stream && t->own_stream) cudaStreamDestroy(t->stream);
@@ -201,34 +234,132 @@ template <typename T> static int tet_upload(T **dst, const T *src, size_t n) {
     return FG_OK;
 }
 
-template <int NL, int MQ>
-static void tet_launch_t(fg_tet *t, const TetArgs &A, int eb, const double *x, int constrained, int diag) {
-    TetTab<NL, MQ> R{};
-    for (int q = 0; q < t->nq; ++q)
-        for (int i = 0; i < NL; ++i) {
-            R.phi[q][i] = t->h_phi[(size_t)q * NL + i];
-            for (int c = 0; c < 3; ++c) R.grad[q][i][c] = t->h_grad[((size_t)q * NL + i) * 3 + c];
+// Morton key of a point in the box [lo, lo + ext): 21 bits per axis, interleaved
+static uint64_t tet_morton(const double *p, const double *lo, const double *ext) {
+    uint64_t key = 0;
+    uint32_t v[3];
+    for (int a = 0; a < 3; ++a) {
+        double f = ext[a] > 0.0 ? (p[a] - lo[a]) / ext[a] : 0.0;
+        f = std::min(std::max(f, 0.0), 1.0);
+        v[a] = (uint32_t)std::min<double>(f * 2097152.0, 2097151.0);
+    }
+    for (int b = 20; b >= 0; --b)
+        for (int a = 0; a < 3; ++a) key = (key << 1) | ((v[a] >> b) & 1u);
+    return key;
+}
+
+// Element order and chunk DOF lists.  h = element map [E][nl] (caller's order);
+// perm[n] = the caller's element at position n of the chunk order.
+struct TetChunkPlan {
+    std::vector<int32_t> perm, cu_off, cu_dof, cu_pid, cu_soff, sh_dof, sh_off;
+    std::vector<uint16_t> cu_slots;
+    int max_nu = 0;
+};
+
+static void tet_plan_chunks(const std::vector<int32_t> &h, const std::vector<double> &coords, int64_t E,
+                            int64_t N, int nl, int CE, TetChunkPlan &P) {
+    // Morton order of the element centroids (vertex nodes = first 4 local DOFs)
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    std::vector<double> cen((size_t)E * 3);
+    for (int64_t e = 0; e < E; ++e)
+        for (int a = 0; a < 3; ++a) {
+            double s = 0.0;
+            for (int v = 0; v < 4; ++v) s += coords[3 * (size_t)h[e * nl + v] + a];
+            cen[3 * e + a] = 0.25 * s;
+            lo[a] = std::min(lo[a], cen[3 * e + a]);
+            hi[a] = std::max(hi[a], cen[3 * e + a]);
         }
-    tet_apply_kernel<NL, MQ><<<eb, 128, 0, t->stream>>>(A, R, x, t->Ye, constrained, diag);
+    const double ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+    std::vector<uint64_t> key(E);
+    for (int64_t e = 0; e < E; ++e) key[e] = tet_morton(&cen[3 * e], lo, ext);
+    P.perm.resize(E);
+    for (int64_t e = 0; e < E; ++e) P.perm[e] = (int32_t)e;
+    std::stable_sort(P.perm.begin(), P.perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    // per chunk: its DOFs (ascending), their local slots (ascending), the local map
+    const int64_t nch = (E + CE - 1) / CE;
+    P.cu_off.assign(nch + 1, 0);
+    P.cu_slots.reserve((size_t)E * nl);
+    std::vector<int32_t> nchk(N, 0);
+    std::vector<std::pair<int32_t, int32_t>> pr;
+    for (int64_t c = 0; c < nch; ++c) {
+        const int64_t e0 = c * CE;
+        const int ne = (int)std::min<int64_t>(CE, E - e0);
+        pr.clear();
+        for (int el = 0; el < ne; ++el)
+            for (int i = 0; i < nl; ++i) pr.push_back({h[(int64_t)P.perm[e0 + el] * nl + i], i * CE + el});
+        std::sort(pr.begin(), pr.end());
+        int nu = 0;
+        for (size_t k = 0; k < pr.size(); ++k) {
+            if (k == 0 || pr[k].first != pr[k - 1].first) {
+                P.cu_dof.push_back(pr[k].first);
+                P.cu_soff.push_back((int32_t)P.cu_slots.size());
+                ++nchk[pr[k].first];
+                ++nu;
+            }
+            P.cu_slots.push_back((uint16_t)pr[k].second);
+        }
+        P.cu_off[c + 1] = P.cu_off[c] + nu;
+        P.max_nu = std::max(P.max_nu, nu);
+    }
+    P.cu_soff.push_back((int32_t)P.cu_slots.size());
+    // DOFs not owned by exactly one chunk: partial ranges in chunk order
+    std::vector<int32_t> base(N, -1);
+    P.sh_off.push_back(0);
+    for (int64_t d = 0; d < N; ++d)
+        if (nchk[d] != 1) {
+            base[d] = P.sh_off.back();
+            P.sh_dof.push_back((int32_t)d);
+            P.sh_off.push_back(P.sh_off.back() + nchk[d]);
+        }
+    P.cu_pid.resize(P.cu_dof.size());
+    for (size_t u = 0; u < P.cu_dof.size(); ++u) {  // chunks in order, so partials land in chunk order
+        const int32_t d = P.cu_dof[u];
+        P.cu_pid[u] = nchk[d] == 1 ? -1 : base[d]++;
+    }
+}
+
+template <int NL, int MQ, bool MOM, int BT>
+static int tet_launch_t(fg_tet *t, const TetChunk &C, const double *x, double *y, int accumulate, int constrained,
+                        int diag) {
+    TetTab<NL, MQ> R{};
+    if (!MOM)
+        for (int q = 0; q < t->nq; ++q)
+            for (int i = 0; i < NL; ++i) {
+                R.phi[q][i] = t->h_phi[(size_t)q * NL + i];
+                for (int c = 0; c < 3; ++c) R.grad[q][i][c] = t->h_grad[((size_t)q * NL + i) * 3 + c];
+            }
+    const size_t smem = tet_chunk_smem(NL, t->CE, t->max_nu);
+    if (smem > 48 * 1024)
+        CK(cudaFuncSetAttribute(tet_chunk_kernel<NL, MQ, MOM, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+    tet_chunk_kernel<NL, MQ, MOM, BT><<<t->n_chunks, BT, smem, t->stream>>>(C, t->kind, t->nq, R, x, y, accumulate,
+                                                                            constrained, diag);
+    return FG_OK;
 }
 
 static int tet_launch_apply(fg_tet *t, const double *x, double *y, int accumulate, int constrained, int diag) {
-    const TetArgs A = tet_args(t);
-    const int eb = (int)std::min<int64_t>((t->E + 127) / 128, 148 * 16);
+    const TetChunk C = tet_chunk_args(t);
     const bool small = t->nq <= 4;
+    const bool mom = !diag && t->kind == 2 && t->p <= 2;
+    int rc;
     if (t->p == 1) {
-        if (small) tet_launch_t<4, 4>(t, A, eb, x, constrained, diag);
-        else tet_launch_t<4, TET_MAXQ>(t, A, eb, x, constrained, diag);
+        if (mom) rc = tet_launch_t<4, 1, true, 256>(t, C, x, y, accumulate, constrained, diag);
+        else if (small) rc = tet_launch_t<4, 4, false, 256>(t, C, x, y, accumulate, constrained, diag);
+        else rc = tet_launch_t<4, TET_MAXQ, false, 256>(t, C, x, y, accumulate, constrained, diag);
     } else if (t->p == 2) {
-        if (small) tet_launch_t<10, 4>(t, A, eb, x, constrained, diag);
-        else tet_launch_t<10, TET_MAXQ>(t, A, eb, x, constrained, diag);
+        if (mom && t->wide) rc = tet_launch_t<10, 1, true, 512>(t, C, x, y, accumulate, constrained, diag);
+        else if (mom) rc = tet_launch_t<10, 1, true, 256>(t, C, x, y, accumulate, constrained, diag);
+        else if (small) rc = tet_launch_t<10, 4, false, 256>(t, C, x, y, accumulate, constrained, diag);
+        else rc = tet_launch_t<10, TET_MAXQ, false, 256>(t, C, x, y, accumulate, constrained, diag);
     } else {
-        if (small) tet_launch_t<20, 4>(t, A, eb, x, constrained, diag);
-        else tet_launch_t<20, TET_MAXQ>(t, A, eb, x, constrained, diag);
+        if (small) rc = tet_launch_t<20, 4, false, 256>(t, C, x, y, accumulate, constrained, diag);
+        else rc = tet_launch_t<20, TET_MAXQ, false, 256>(t, C, x, y, accumulate, constrained, diag);
     }
-    const int db = (int)std::min<int64_t>((t->N + 255) / 256, 148 * 16);
-    tet_scatter_kernel<<<db, 256, 0, t->stream>>>(A, t->offs, t->slots, t->Ye, diag ? nullptr : x, y, accumulate,
-                                                  constrained);
+    if (rc) return rc;
+    if (t->n_shared) {
+        const int db = (int)std::min<int64_t>((t->n_shared + 255) / 256, 148 * 16);
+        tet_shared_kernel<<<db, 256, 0, t->stream>>>(C, diag ? nullptr : x, y, accumulate, constrained, diag);
+    }
     CK(cudaGetLastError());
     return FG_OK;
 }

@@ -150,3 +150,49 @@ def test_tet_rejects_bad_input():
     op = femgpu.TetOperator(1, coords, dofs, nd)
     with pytest.raises(femgpu.SolverError):
         op.matvec(np.ones(nd), constrained=True)  # no essential mask given
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("kind", [femgpu.DIFF, femgpu.MASS_DIFF])
+@pytest.mark.parametrize("chunk", [32, 96, None])
+def test_tet_chunk_plans_on_shuffled_mesh(p, kind, chunk, monkeypatch):
+    """The chunked scatter with many chunks (most DOFs shared between chunks):
+    elements given in a random order, DOFs renumbered at random, two DOFs that
+    no element touches, an arbitrary essential list; apply, accumulate and
+    diagonal against the oracle, and bit-for-bit repeatable."""
+    need_gpu()
+    if chunk:
+        monkeypatch.setenv("FG_TET_CHUNK", str(chunk))
+    else:
+        monkeypatch.delenv("FG_TET_CHUNK", raising=False)
+    coords, dofs, nd, _ = space(6 if p < 3 else 4, p, seed=11 + p)
+    rng = np.random.default_rng(100 * p + kind)
+    n_nodes = coords.shape[0]
+    # vertex DOFs must stay the nodes 0..n_nodes-1: permute the nodes and the other DOFs separately
+    pn = rng.permutation(n_nodes)
+    po = n_nodes + rng.permutation(nd - n_nodes)
+    newid = np.concatenate([pn, po])
+    coords2 = np.empty_like(coords)
+    coords2[pn] = coords
+    dofs2 = newid[dofs][rng.permutation(dofs.shape[0])].astype(np.int32)
+    nd2 = nd + 2
+    mask = np.zeros(nd2, dtype=np.uint8)
+    mask[rng.choice(nd, size=nd // 7, replace=False)] = 1
+    mask[nd] = 1  # an untouched essential DOF
+    qo = 2 * p
+    nq = len(O.tet_rule(qo)[1])
+    kq = np.exp(rng.normal(size=dofs2.shape[0] * nq))
+    op = femgpu.TetOperator(p, coords2, dofs2, nd2, kind=kind, kappa=kq, c_mass=0.9, c_diff=1.1,
+                            quad_order=qo, ess=mask)
+    sp = O.TetSpace(p, coords2, dofs2, nd2, mask)
+    coef = O.Coef(kind, c_m=0.9, c_k=1.1, kappa_q=kq)
+    x = rng.standard_normal(nd2)
+    for constrained in (False, True):
+        ref = O.tet_pa_apply(sp, coef, x, qo, constrained)
+        y = op.matvec(x, constrained)
+        assert rel(y, ref) <= 1e-12, (constrained, rel(y, ref))
+        y2 = np.full(nd2, 0.5)
+        op.apply(x, y2, constrained)
+        assert rel(y2, ref + 0.5) <= 1e-12
+        assert rel(op.diagonal(constrained), O.tet_diagonal(sp, coef, qo, constrained)) <= 1e-12
+    assert np.array_equal(op.matvec(x, True), op.matvec(x, True))
