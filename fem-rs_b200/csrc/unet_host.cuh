@@ -221,7 +221,7 @@ static void launch_restrict(fg_unet *u, const TView &in, const Vol &Vf, TView ou
 static int unet_forward(fg_unet *u) {
     UnetBufs &b = u->buf;
     const int C0 = u->C0, C1 = u->C1, C2 = u->C2;
-    int rc, blocks;
+    int rc;
     const TView x0{b.x0, 2, 0}, a0{b.a0, C0, 0}, h0{b.cat0, C1 + C0, C1}, x1{b.x1, C0, 0},
         a1{b.a1, C1, 0}, h1{b.cat1, C2 + C1, C2}, x2{b.x2, C1, 0}, a2{b.a2, C2, 0}, h2{b.h2, C2, 0},
         up1{b.cat1, C2 + C1, 0}, cat1{b.cat1, C2 + C1, 0}, g1{b.g1, C1, 0}, up0{b.cat0, C1 + C0, 0},
@@ -283,7 +283,7 @@ static int relu_bwd(fg_unet *u, TView dy, const TView &y, const Vol &V, int C) {
 static int unet_backward(fg_unet *u) {
     UnetBufs &b = u->buf;
     const int C0 = u->C0, C1 = u->C1, C2 = u->C2;
-    int rc, blocks;
+    int rc;
     const TView x0{b.x0, 2, 0}, a0{b.a0, C0, 0}, h0{b.cat0, C1 + C0, C1}, x1{b.x1, C0, 0},
         a1{b.a1, C1, 0}, h1{b.cat1, C2 + C1, C2}, x2{b.x2, C1, 0}, a2{b.a2, C2, 0}, h2{b.h2, C2, 0},
         cat1{b.cat1, C2 + C1, 0}, g1{b.g1, C1, 0}, cat0{b.cat0, C1 + C0, 0}, g0{b.g0, C0, 0};
