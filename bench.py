@@ -619,7 +619,7 @@ def box_as_hex_mesh(n, p):
 def run_hex_unstructured(n, p, kq, steps, peak, dev):
     """The same operator as the headline apply built through the unstructured
     Hex8 constructor (the drop-in for a caller's own mesh and DofManager
-    numbering; coloured scatter), against the structured fast path."""
+    numbering; chunked scatter), against the structured fast path."""
     import torch
 
     import femgpu
@@ -651,7 +651,7 @@ def run_hex_unstructured(n, p, kq, steps, peak, dev):
     E, q3 = n ** 3, (p + 1) ** 3
     nbytes = 6 * q3 * E * 8 + q3 * E * 4 + 2 * N * 8  # qdata + element map + x, y
     out = {"ms": round(ms, 4), "gdof_s": round(N / (ms / 1e3) / 1e9, 3), "frac": round(nbytes / (ms / 1e3) / 1e9 / peak, 4),
-           "colours": op.colours, "setup_s": round(t_setup, 2)}
+           "chunks": op.chunks, "setup_s": round(t_setup, 2)}
     op.close()
     return out
 

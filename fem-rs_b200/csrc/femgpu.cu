@@ -236,13 +236,18 @@ struct fg_op {
     struct NnTimes { int ir, fmt, degree; double plain_ms, learned_ms; };
     std::vector<NnTimes> nn_times;
     int fmt = 0;
-    // unstructured Hex8 mesh (fg_op_create_hex): element maps sorted by colour,
-    // colour starts, essential-DOF mask; vectors are plain (no pads)
+    // unstructured Hex8 mesh (fg_op_create_hex): element maps in the chunk
+    // order, the chunk scatter's lists, essential-DOF mask; vectors are plain
+    // (no pads)
     bool unstr = false;
-    int64_t u_E = 0;
-    std::vector<int64_t> u_col;
+    int64_t u_E = 0, u_chunks = 0, u_nshared = 0;
+    int u_max_nu = 0;
     int32_t *u_dofs = nullptr;
     uint8_t *u_ess = nullptr;
+    int32_t *u_cu_off = nullptr, *u_cu_dof = nullptr, *u_cu_pid = nullptr, *u_cu_soff = nullptr;
+    int32_t *u_sh_dof = nullptr, *u_sh_off = nullptr;
+    uint16_t *u_cu_slots = nullptr;
+    double *u_part = nullptr;  // partials of the shared DOFs (FP64 or FP32 applies)
     double *qa64 = nullptr;
     float *qa32 = nullptr;
     int *d_err = nullptr;
@@ -269,6 +274,12 @@ static void free_op(fg_op *op) {
     if (op->fixcnt) cudaFree(op->fixcnt);
     if (op->u_dofs) cudaFree(op->u_dofs);
     if (op->u_ess) cudaFree(op->u_ess);
+    {
+        void *u[] = {op->u_cu_off, op->u_cu_dof, op->u_cu_pid, op->u_cu_soff, op->u_sh_dof, op->u_sh_off,
+                     op->u_cu_slots, op->u_part};
+        for (void *q : u)
+            if (q) cudaFree(q);
+    }
     for (int k = 0; k < CHEB_MAXD; ++k) {
         if (op->cdk[k]) cudaFree(op->cdk[k]);
         if (op->cdk32[k]) cudaFree(op->cdk32[k]);
@@ -3396,14 +3407,15 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
         if (v >= 32 && v <= 1024 && v * nl <= 65536) t->CE = v;
     }
     if (const char *ev = std::getenv("FG_TET_WIDE")) t->wide = std::atoi(ev) != 0;
-    TetChunkPlan plan;
-    tet_plan_chunks(h, hc, n_elem, n_dofs, nl, t->CE, plan);
-    t->n_chunks = (int)((n_elem + t->CE - 1) / t->CE);
+    ChunkPlan plan;
+    std::vector<int32_t> perm;
+    tet_plan_chunks(h, hc, n_elem, n_dofs, nl, t->CE, perm, plan);
+    t->n_chunks = (int)plan.n_chunks;
     t->max_nu = plan.max_nu;
     if (tet_chunk_smem(nl, t->CE, t->max_nu) > 227 * 1024)
         return fail(FG_UNSUPPORTED, "tet chunk of %d elements needs too much shared memory", t->CE);
     t->n_shared = (int64_t)plan.sh_dof.size();
-    t->n_part = plan.sh_off.back();
+    t->n_part = plan.n_part;
     if ((rc = tet_upload(&t->dofs, soa.data(), soa.size())) ||
         (rc = tet_upload(&t->cu_slots, plan.cu_slots.data(), plan.cu_slots.size())) ||
         (rc = tet_upload(&t->cu_off, plan.cu_off.data(), plan.cu_off.size())) ||
@@ -3424,7 +3436,7 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
         }
         std::vector<uint32_t> em(ess ? n_elem : 0, 0u);
         for (int64_t n = 0; n < n_elem; ++n) {
-            const int64_t e = plan.perm[n];
+            const int64_t e = perm[n];
             for (int i = 0; i < nl; ++i) {
                 const int32_t d = h[e * nl + i];
                 ed[(int64_t)i * n_elem + n] = d;
@@ -3472,7 +3484,7 @@ FG_API int fg_tet_create(int order, int64_t n_nodes, const double *coords, int64
     }
     const int nmom = (kind & 2) ? (order == 1 ? 6 : (order == 2 ? 10 : 0)) : 0;
     if (nmom) CK(cudaMalloc(&t->Sm, sizeof(double) * nmom * n_elem));
-    if ((rc = tet_upload(&d_perm, plan.perm.data(), plan.perm.size()))) return rc;
+    if ((rc = tet_upload(&d_perm, perm.data(), perm.size()))) return rc;
     TetArgs A = tet_args(t);
     A.G = G0;
     A.sk = sk0;

@@ -1,18 +1,25 @@
 // hex_host.cuh -- host side of the unstructured Hex8 operator (fg_op_create_hex):
-// validation of the caller's mesh and DOF maps, the element colouring of the
+// validation of the caller's mesh and DOF maps, the element chunks of the
 // deterministic scatter, the quadrature-data build and the launches.  Included
 // by femgpu.cu after the fg_op handle; an operator built here is an ordinary
 // fg_op whose applies and diagonal go through hex_kernels.cuh, so fg_op_apply,
 // fg_op_diagonal and fg_pcg serve both mesh kinds.
 #pragma once
+#include "chunk_plan.h"
 #include "hex_kernels.cuh"
 
-// Warps per CTA, stages of the per-warp quadrature-data ring, CTAs per SM
-// the register allocation must allow (shared memory allows 5 at Q2 FP64).
-template <int P> struct HexCfg { static constexpr int WARPS = 2, S = P == 3 ? 2 : 3, MINB = P == 3 ? 4 : 5; };
+// Warps per CTA (a chunk is WARPS * 32 elements), stages of the per-warp
+// quadrature-data ring, CTAs per SM the register allocation must allow.
+template <int P> struct HexCfg {
+    static constexpr int WARPS = P == 3 ? 2 : 4, S = 2, MINB = P == 3 ? 4 : 3;
+};
+static int hex_chunk_size(int p) {
+    return 32 * (p == 1 ? HexCfg<1>::WARPS : p == 2 ? HexCfg<2>::WARPS : HexCfg<3>::WARPS);
+}
 
 template <typename T>
-static HexApply<T> hex_args(fg_op *op, const T *qd, const T *x, T *y, int constrained, const int *skip) {
+static HexApply<T> hex_args(fg_op *op, const T *qd, const T *x, T *y, int accumulate, int constrained,
+                            const int *skip) {
     HexApply<T> A{};
     A.E = op->u_E;
     A.N = op->N;
@@ -21,108 +28,111 @@ static HexApply<T> hex_args(fg_op *op, const T *qd, const T *x, T *y, int constr
     A.ess = op->u_ess;
     A.x = x;
     A.y = y;
+    A.accumulate = accumulate;
     A.constrained = constrained;
     A.skip = skip;
     A.err = op->d_err;
     A.wait_ns = op->wait_ns;
+    A.L.cu_off = op->u_cu_off;
+    A.L.cu_dof = op->u_cu_dof;
+    A.L.cu_pid = op->u_cu_pid;
+    A.L.cu_soff = op->u_cu_soff;
+    A.L.cu_slots = op->u_cu_slots;
+    A.L.part = op->u_part;
+    A.L.sh_dof = op->u_sh_dof;
+    A.L.sh_off = op->u_sh_off;
+    A.L.n_shared = op->u_nshared;
+    A.L.max_nu = op->u_max_nu;
     return A;
 }
 
+// Raise a kernel's dynamic shared-memory limit to `bytes` on this device (once
+// per size reached; set-up calls are serialised by the handle mutexes, and a
+// race only repeats the call).
+template <typename K> static int hex_smem_limit(K kern, int device, int bytes, std::atomic<int> *lim) {
+    if (device < 0 || device >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", device);
+    if (lim[device].load(std::memory_order_acquire) < bytes) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        lim[device].store(bytes, std::memory_order_release);
+    }
+    return FG_OK;
+}
+
 template <int P, int OPK, typename T>
-static int hex_apply_t(fg_op *op, HexApply<T> A) {
+static int hex_apply_t(fg_op *op, const HexApply<T> &A) {
     constexpr int WARPS = HexCfg<P>::WARPS, S = HexCfg<P>::S, BS = WARPS * 32;
     using SM = HexSmem<P, OPK, T, WARPS, S>;
     auto kern = hex_apply_kernel<P, OPK, T, WARPS, S, HexCfg<P>::MINB>;
-    static std::atomic<bool> attr_set[64];  // per device, set once
-    if (op->device < 0 || op->device >= 64) return fail(FG_CUDA_ERROR, "device id %d out of range", op->device);
-    if (!attr_set[op->device].load(std::memory_order_acquire)) {
-        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
-        attr_set[op->device].store(true, std::memory_order_release);
-    }
-    for (size_t c = 0; c + 1 < op->u_col.size(); ++c) {
-        A.e0 = op->u_col[c];
-        A.e1 = op->u_col[c + 1];
-        const int64_t n = A.e1 - A.e0;  // a multiple of 32
-        if (n <= 0) continue;
-        kern<<<(unsigned)((n + BS - 1) / BS), BS, SM::bytes, op->stream>>>(A);
-        CK(cudaGetLastError());
-    }
+    static std::atomic<int> lim[64];
+    const int bytes = SM::bytes(op->u_max_nu);
+    int rc;
+    if ((rc = hex_smem_limit(kern, op->device, bytes, lim))) return rc;
+    kern<<<(unsigned)op->u_chunks, BS, bytes, op->stream>>>(A);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
+template <typename T> static int hex_shared(fg_op *op, const HexApply<T> &A, int diag) {
+    if (!op->u_nshared) return FG_OK;
+    const int db = (int)std::min<int64_t>((op->u_nshared + 255) / 256, 148 * 16);
+    chunk_shared_kernel<T><<<db, 256, 0, op->stream>>>(A.L, A.ess, A.x, A.y, A.accumulate, A.constrained, diag,
+                                                       A.skip);
+    CK(cudaGetLastError());
     return FG_OK;
 }
 
 // y (+)= A x on native vectors of an unstructured operator (the plain values, then zero pads).
 template <typename T>
 static int hex_apply(fg_op *op, const T *qd, const T *x, T *y, int accumulate, int constrained, const int *skip) {
-    HexApply<T> A = hex_args<T>(op, qd, x, y, constrained, skip);
-    hex_init_kernel<T><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(A, accumulate);
-    CK(cudaGetLastError());
+    const HexApply<T> A = hex_args<T>(op, qd, x, y, accumulate, constrained, skip);
+    int rc;
     switch (op->p * 4 + op->kind) {
-    case 1 * 4 + 1: return hex_apply_t<1, 1, T>(op, A);
-    case 1 * 4 + 2: return hex_apply_t<1, 2, T>(op, A);
-    case 1 * 4 + 3: return hex_apply_t<1, 3, T>(op, A);
-    case 2 * 4 + 1: return hex_apply_t<2, 1, T>(op, A);
-    case 2 * 4 + 2: return hex_apply_t<2, 2, T>(op, A);
-    case 2 * 4 + 3: return hex_apply_t<2, 3, T>(op, A);
-    case 3 * 4 + 1: return hex_apply_t<3, 1, T>(op, A);
-    case 3 * 4 + 2: return hex_apply_t<3, 2, T>(op, A);
-    default: return hex_apply_t<3, 3, T>(op, A);
+    case 1 * 4 + 1: rc = hex_apply_t<1, 1, T>(op, A); break;
+    case 1 * 4 + 2: rc = hex_apply_t<1, 2, T>(op, A); break;
+    case 1 * 4 + 3: rc = hex_apply_t<1, 3, T>(op, A); break;
+    case 2 * 4 + 1: rc = hex_apply_t<2, 1, T>(op, A); break;
+    case 2 * 4 + 2: rc = hex_apply_t<2, 2, T>(op, A); break;
+    case 2 * 4 + 3: rc = hex_apply_t<2, 3, T>(op, A); break;
+    case 3 * 4 + 1: rc = hex_apply_t<3, 1, T>(op, A); break;
+    case 3 * 4 + 2: rc = hex_apply_t<3, 2, T>(op, A); break;
+    default: rc = hex_apply_t<3, 3, T>(op, A); break;
     }
+    return rc ? rc : hex_shared<T>(op, A, 0);
 }
 
-template <int P, int OPK> static int hex_diag_t(fg_op *op, HexApply<double> A) {
-    for (size_t c = 0; c + 1 < op->u_col.size(); ++c) {
-        A.e0 = op->u_col[c];
-        A.e1 = op->u_col[c + 1];
-        const int64_t n = A.e1 - A.e0;
-        if (n <= 0) continue;
-        hex_diag_kernel<P, OPK><<<(unsigned)((n + 127) / 128), 128, 0, op->stream>>>(A);
-        CK(cudaGetLastError());
-    }
+template <int P, int OPK> static int hex_diag_t(fg_op *op, const HexApply<double> &A) {
+    constexpr int BS = HexCfg<P>::WARPS * 32, NL = (P + 1) * (P + 1) * (P + 1);
+    auto kern = hex_diag_kernel<P, OPK, BS>;
+    static std::atomic<int> lim[64];
+    const int bytes = (int)(sizeof(double) * NL * BS + chunk_list_smem(NL, BS, op->u_max_nu));
+    int rc;
+    if ((rc = hex_smem_limit(kern, op->device, bytes, lim))) return rc;
+    kern<<<(unsigned)op->u_chunks, BS, bytes, op->stream>>>(A);
+    CK(cudaGetLastError());
     return FG_OK;
 }
 
 static int hex_diag(fg_op *op, double *y, int constrained) {
-    HexApply<double> A = hex_args<double>(op, op->qd, nullptr, y, constrained, nullptr);
-    hex_init_kernel<double><<<VEC_GRID, VEC_THREADS, 0, op->stream>>>(A, 0);
-    CK(cudaGetLastError());
+    const HexApply<double> A = hex_args<double>(op, op->qd, nullptr, y, 0, constrained, nullptr);
+    int rc;
     switch (op->p * 4 + op->kind) {
-    case 1 * 4 + 1: return hex_diag_t<1, 1>(op, A);
-    case 1 * 4 + 2: return hex_diag_t<1, 2>(op, A);
-    case 1 * 4 + 3: return hex_diag_t<1, 3>(op, A);
-    case 2 * 4 + 1: return hex_diag_t<2, 1>(op, A);
-    case 2 * 4 + 2: return hex_diag_t<2, 2>(op, A);
-    case 2 * 4 + 3: return hex_diag_t<2, 3>(op, A);
-    case 3 * 4 + 1: return hex_diag_t<3, 1>(op, A);
-    case 3 * 4 + 2: return hex_diag_t<3, 2>(op, A);
-    default: return hex_diag_t<3, 3>(op, A);
+    case 1 * 4 + 1: rc = hex_diag_t<1, 1>(op, A); break;
+    case 1 * 4 + 2: rc = hex_diag_t<1, 2>(op, A); break;
+    case 1 * 4 + 3: rc = hex_diag_t<1, 3>(op, A); break;
+    case 2 * 4 + 1: rc = hex_diag_t<2, 1>(op, A); break;
+    case 2 * 4 + 2: rc = hex_diag_t<2, 2>(op, A); break;
+    case 2 * 4 + 3: rc = hex_diag_t<2, 3>(op, A); break;
+    case 3 * 4 + 1: rc = hex_diag_t<3, 1>(op, A); break;
+    case 3 * 4 + 2: rc = hex_diag_t<3, 2>(op, A); break;
+    default: rc = hex_diag_t<3, 3>(op, A); break;
     }
+    return rc ? rc : hex_shared<double>(op, A, 1);
 }
 
 template <int P, int OPK> static void hex_setup_launch(fg_op *op, const HexSetup &S) {
     const int64_t total = S.E * (P + 1) * (P + 1) * (P + 1);
     const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
     hex_setup_kernel<P, OPK, double><<<blocks, 256, 0, op->stream>>>(S, op->qd);
-}
-
-// Greedy element colouring: no two elements of a colour share a DOF.  Per DOF
-// a 64-bit mask of the colours of the elements already placed on it; each
-// element takes the lowest colour none of its DOFs has.  Returns the number of
-// colours, or -1 if an element would need a 65th.
-static int hex_colour(int64_t E, int nl, int64_t N, const std::vector<int32_t> &ed, std::vector<uint8_t> &col) {
-    std::vector<uint64_t> used((size_t)N, 0);
-    col.assign((size_t)E, 0);
-    int ncol = 0;
-    for (int64_t e = 0; e < E; ++e) {
-        uint64_t forb = 0;
-        for (int k = 0; k < nl; ++k) forb |= used[(size_t)ed[(size_t)e * nl + k]];
-        if (forb == ~0ull) return -1;
-        int c = 0;
-        while (forb >> c & 1ull) ++c;
-        col[(size_t)e] = (uint8_t)c;
-        ncol = std::max(ncol, c + 1);
-        for (int k = 0; k < nl; ++k) used[(size_t)ed[(size_t)e * nl + k]] |= 1ull << c;
-    }
-    return ncol;
 }
 
 extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double *coords, int64_t n_elem,
@@ -170,24 +180,35 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
                     const int src = order == 1 ? (b ? (a ? 2 : 3) : (a ? 1 : 0)) + 4 * c : k;
                     lexmap[(size_t)e * nl + k] = (int32_t)h_map[(size_t)e * nl + src];
                 }
-    std::vector<uint8_t> colour;
-    const int ncol = hex_colour(E, nl, N, lexmap, colour);
-    if (ncol < 0) return fail(FG_UNSUPPORTED, "element colouring needs more than 64 colours");
-    // elements sorted by colour (stable: the caller's order within a colour),
-    // each colour padded to whole 32-element chunks (padding: eid -1, map -1)
-    std::vector<int64_t> count((size_t)ncol, 0), start((size_t)ncol + 1, 0);
-    for (uint8_t c : colour) ++count[c];
-    for (int c = 0; c < ncol; ++c) start[(size_t)c + 1] = start[(size_t)c] + (count[(size_t)c] + 31) / 32 * 32;
-    const int64_t Ep = start[(size_t)ncol];
-    if (Ep >= ((int64_t)1 << 31)) return fail(FG_INVALID_ARGUMENT, "more than 2^31 padded elements");
-    std::vector<int32_t> eid((size_t)Ep, -1), sdofs((size_t)Ep * nl, -1);
+    // elements in the Morton order of their vertex centroids, padded to whole
+    // 32-element groups (padding: eid -1, map -1), cut into chunks of the CTA size
+    const int CE = hex_chunk_size(order);
+    if (nl * CE > 65536) return fail(FG_UNSUPPORTED, "chunk of %d elements too large for 16-bit slots", CE);
+    std::vector<int32_t> perm;
     {
-        std::vector<int64_t> pos(start.begin(), start.end() - 1);
-        for (int64_t e = 0; e < E; ++e) eid[(size_t)pos[colour[(size_t)e]]++] = (int32_t)e;
+        std::vector<double> h_xyz((size_t)n_nodes * 3);
+        CK(cudaMemcpy(h_xyz.data(), coords, sizeof(double) * h_xyz.size(), cudaMemcpyDefault));
+        std::vector<double> cen((size_t)E * 3);
+        for (int64_t e = 0; e < E; ++e)
+            for (int a = 0; a < 3; ++a) {
+                double sum = 0.0;
+                for (int v = 0; v < 8; ++v) sum += h_xyz[3 * (size_t)h_conn[(size_t)e * 8 + v] + a];
+                cen[3 * (size_t)e + a] = 0.125 * sum;
+            }
+        morton_order(cen, E, perm);
     }
-    for (int k = 0; k < nl; ++k)
-        for (int64_t s = 0; s < Ep; ++s)
-            if (eid[(size_t)s] >= 0) sdofs[(size_t)k * Ep + s] = lexmap[(size_t)eid[(size_t)s] * nl + k];
+    const int64_t Ep = (E + 31) / 32 * 32;
+    std::vector<int32_t> eid((size_t)Ep, -1), smap((size_t)Ep * nl, -1), sdofs((size_t)Ep * nl, -1);
+    for (int64_t s = 0; s < E; ++s) {
+        eid[(size_t)s] = perm[(size_t)s];
+        for (int k = 0; k < nl; ++k) {
+            const int32_t d = lexmap[(size_t)perm[(size_t)s] * nl + k];
+            smap[(size_t)s * nl + k] = d;
+            sdofs[(size_t)k * Ep + s] = d;
+        }
+    }
+    ChunkPlan plan;
+    plan_chunk_lists(smap, Ep, N, nl, CE, plan);
     std::vector<uint8_t> mask((size_t)N, 0);
     if (n_ess > 0) {
         std::vector<uint32_t> h_ess((size_t)n_ess);
@@ -208,7 +229,9 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
     op->p = order;
     op->unstr = true;
     op->u_E = Ep;
-    op->u_col = start;
+    op->u_chunks = plan.n_chunks;
+    op->u_nshared = (int64_t)plan.sh_dof.size();
+    op->u_max_nu = plan.max_nu;
     op->N = N;
     // native vectors: one row of the N plain values padded with zeros to a
     // multiple of 4 (the solver's vector kernels work in 4-wide groups); no tiles
@@ -243,6 +266,19 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
         cudaMemcpy(op->u_dofs, sdofs.data(), sizeof(int32_t) * sdofs.size(), cudaMemcpyHostToDevice) ||
         cudaMalloc(&op->u_ess, (size_t)N) || cudaMemcpy(op->u_ess, mask.data(), (size_t)N, cudaMemcpyHostToDevice))
         return bail(fail(FG_CUDA_ERROR, "upload of the element maps failed"));
+    {
+        auto up = [](auto **dst, const auto &v) {
+            using V = typename std::remove_reference<decltype(v)>::type::value_type;
+            const size_t n = std::max<size_t>(v.size(), 1);
+            if (cudaMalloc(dst, sizeof(V) * n) != cudaSuccess) return false;
+            return v.empty() || cudaMemcpy(*dst, v.data(), sizeof(V) * v.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+        };
+        if (!up(&op->u_cu_off, plan.cu_off) || !up(&op->u_cu_dof, plan.cu_dof) || !up(&op->u_cu_pid, plan.cu_pid) ||
+            !up(&op->u_cu_soff, plan.cu_soff) || !up(&op->u_cu_slots, plan.cu_slots) ||
+            !up(&op->u_sh_dof, plan.sh_dof) || !up(&op->u_sh_off, plan.sh_off) ||
+            cudaMalloc(&op->u_part, sizeof(double) * std::max<int64_t>(plan.n_part, 1)) != cudaSuccess)
+            return bail(fail(FG_CUDA_ERROR, "upload of the chunk lists failed"));
+    }
 
     // quadrature data
     const int NC = kind == FG_MASS ? 1 : (kind == FG_DIFF ? 6 : 7);
@@ -312,7 +348,7 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
     return FG_OK;
 }
 
-extern "C" FG_API int fg_op_colours(const fg_op *op) {
+extern "C" FG_API int64_t fg_op_chunks(const fg_op *op) {
     if (!op) return fail(FG_INVALID_ARGUMENT, "NULL op");
-    return op->unstr ? (int)op->u_col.size() - 1 : 0;
+    return op->unstr ? op->u_chunks : 0;
 }

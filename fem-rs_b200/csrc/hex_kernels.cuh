@@ -4,47 +4,52 @@
 // Hex8 geometry of crates/assembly/src/assembler.rs:96-143, for any element
 // connectivity and any DOF numbering (a DofManager's element maps).
 //
-// Data layout.  Elements are sorted by colour and every colour is padded to a
-// whole number of 32-element chunks (padding elements have map entries -1 and
-// zero quadrature data); a warp works on one chunk.
+// Data layout.  Elements are put in a Morton order of their centroids and cut
+// into chunks of CE = WARPS * 32 elements, one CTA each (the last chunk padded
+// to whole 32-element warp groups: padding elements have map entries -1 and
+// zero quadrature data).
 //   dofs [nl][E]         int32 element-to-DOF map, local DOF (c,b,a) at
 //                        k = (c*D + b)*D + a (tensor order on the reference cube);
 //                        element-major, so a warp reads each entry in one load
 //   qd                   quadrature data in each warp's consumption order:
-//                        [chunk][col = qy*Q + qx][qz][comp][lane], comp the 6
+//                        [group][col = qy*Q + qx][qz][comp][lane], comp the 6
 //                        symmetric w|detJ| kappa J^-1 J^-T and/or w|detJ| rho.
-//                        One column of a chunk is a contiguous stage, streamed
-//                        into a per-warp ring of shared-memory stages by 1-D bulk
-//                        copies on mbarriers (bounded waits, drained on timeout)
+//                        One column of a 32-element group is a contiguous stage,
+//                        streamed into a per-warp ring of shared-memory stages by
+//                        1-D bulk copies on mbarriers (bounded waits, drained on
+//                        timeout)
 //   ess  [N]             essential-DOF mask (constrained applies)
 //
-// Scatter without float atomics: the elements are coloured so that no two
-// elements of a colour share a DOF; one launch per colour adds each element's
-// result into y directly.  Every DOF receives its element contributions in
-// colour order, so the sums are the same from run to run.
+// Scatter without float atomics and without an element-result array in HBM
+// (chunk_plan.h, chunk_scatter.cuh): a CTA puts its element results in shared
+// memory and sums each DOF of its chunk's list over the DOF's element slots in
+// a fixed order; a DOF owned by the chunk is stored, a DOF shared with other
+// chunks gets a partial that chunk_shared_kernel adds in chunk order.  The
+// sums are the same from run to run.
 //
 // Element math: slab sum factorisation (one qy slab of QH quadrature columns
 // at a time: y then x contraction of the element values, per column z, D, z^T,
 // then the transposed x and y into the element result).  The element values
 // are staged in shared memory, one column per thread.
 #pragma once
+#include "chunk_scatter.cuh"
 #include "fg_common.cuh"
 #include "pa_kernels.cuh"
 
 namespace fg {
 
 template <typename T> struct HexApply {
-    int64_t E, N;          // elements (padded to whole chunks), DOFs
-    int64_t e0, e1;        // element range of this launch (one colour, whole chunks)
+    int64_t E, N;          // elements (padded to whole 32-element groups), DOFs
     const int32_t *dofs;   // [nl][E]
-    const T *qd;           // per-chunk streams (layout above)
+    const T *qd;           // per-group streams (layout above)
     const uint8_t *ess;    // [N] or null
     const T *x;            // null: diagonal
     T *y;
-    int constrained;
+    int accumulate, constrained;
     const int *skip;       // if non-null and *skip != 0 the kernel returns at once
     int *err;              // device error word
     uint64_t wait_ns;      // limit of each wait for a stage (0: 1 s)
+    ChunkLists L;          // chunks of the CTA size
 };
 
 // Index of component `comp` of quadrature point (col, qz) of element e.
@@ -53,25 +58,20 @@ template <int P, int OPK> __host__ __device__ inline int64_t hex_qd_index(int64_
     return (((e >> 5) * (Q * Q) + col) * Q + qz) * (NC * 32) + comp * 32 + (e & 31);
 }
 
-// y = (accumulate ? y : 0) + (identity rows of the essential DOFs of a
-// constrained call: x, or 1 for the diagonal); the colour launches add the
-// element contributions to the other DOFs.
-template <typename T>
-__global__ void hex_init_kernel(const HexApply<T> A, int accumulate) {
-    if (A.skip && *A.skip) return;
-    for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < A.N; d += (int64_t)gridDim.x * blockDim.x) {
-        T v = accumulate ? A.y[d] : T(0);
-        if (A.constrained && A.ess && A.ess[d]) v += A.x ? A.x[d] : T(1);
-        A.y[d] = v;
-    }
-}
-
+// Shared memory (bytes): a region holding first the per-warp quadrature-data
+// rings and, after the element phase, the chunk's lists; the element values
+// (then results), one column per thread; the ring barriers.
 template <int P, int OPK, typename T, int WARPS, int S> struct HexSmem {
     static constexpr int Q = P + 1, NL = (P + 1) * (P + 1) * (P + 1), BS = WARPS * 32;
     static constexpr int STAGE = Q * NComp<OPK>::v * 32;  // elements of one column stage
-    static constexpr int off_x = WARPS * S * STAGE * (int)sizeof(T);
-    static constexpr int off_b = round_up(off_x + NL * BS * (int)sizeof(T), 8);
-    static constexpr int bytes = off_b + WARPS * S * 8;
+    static constexpr int RING = WARPS * S * STAGE * (int)sizeof(T);
+    static __host__ __device__ int region(int max_nu) {
+        const int l = (int)chunk_list_smem(NL, BS, max_nu);
+        return round_up(RING > l ? RING : l, 128);
+    }
+    static __host__ __device__ int off_x(int max_nu) { return region(max_nu); }
+    static __host__ __device__ int off_b(int max_nu) { return round_up(off_x(max_nu) + NL * BS * (int)sizeof(T), 8); }
+    static __host__ __device__ int bytes(int max_nu) { return off_b(max_nu) + WARPS * S * 8; }
 };
 
 template <int P, int OPK, typename T, int WARPS, int S, int MINB>
@@ -86,204 +86,211 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) hex_apply_kernel(const HexAp
     using TB = Tab<T>;
     extern __shared__ __align__(128) unsigned char hex_smem[];
     if (A.skip && *A.skip) return;
+    const int MU = A.L.max_nu;
     T *ring = reinterpret_cast<T *>(hex_smem);
-    T *xs = reinterpret_cast<T *>(hex_smem + SM::off_x);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(hex_smem + SM::off_b);
+    T *xs = reinterpret_cast<T *>(hex_smem + SM::off_x(MU));
+    uint64_t *bars = reinterpret_cast<uint64_t *>(hex_smem + SM::off_b(MU));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
     const int64_t E = A.E;
-    const int64_t chunk = A.e0 / 32 + (int64_t)blockIdx.x * WARPS + warp;
-    const bool wvalid = chunk * 32 < A.e1;
-    const int64_t e = chunk * 32 + lane;
+    const int64_t group = (int64_t)blockIdx.x * WARPS + warp;  // 32-element group of this warp
+    const bool wvalid = group * 32 < E;
+    const int64_t e = group * 32 + lane;
     const uint64_t wlim = A.wait_ns ? A.wait_ns : 1000000000ull;
     if (threadIdx.x == 0) {
         for (int i = 0; i < WARPS * S; ++i) mbar_init(&bars[i], 1);
         fence_barrier_init();
     }
     __syncthreads();
-    if (!wvalid) return;
     T *qsw = ring + warp * S * STAGE;
     uint64_t *qbw = bars + warp * S;
-    const T *qdw = A.qd + chunk * COLS * STAGE;
+    const T *qdw = A.qd + group * COLS * STAGE;
     int q_issued = 0, q_waited = 0;
-    if (lane == 0) {
-        for (int j = 0; j < S && j < COLS; ++j) {
-            mbar_arrive_expect_tx(&qbw[j], QBYTES);
-            bulk_g2s(qsw + j * STAGE, qdw + (int64_t)j * STAGE, QBYTES, &qbw[j]);
-            q_issued = j + 1;
-        }
-    }
-    // gather (E) with the essential columns masked; padding elements hold -1
-    const bool evalid = __ldg(A.dofs + e) >= 0;
-#pragma unroll
-    for (int k = 0; k < NL; ++k) {
-        T v = T(0);
-        if (evalid) {
-            const int32_t d = __ldg(A.dofs + (int64_t)k * E + e);
-            const bool ess = A.constrained && A.ess && A.ess[d];
-            v = ess ? T(0) : __ldg(A.x + d);
-        }
-        xs[k * BS + tid] = v;
-    }
-    auto uval = [&](int c, int b, int a) -> T { return xs[((c * D + b) * D + a) * BS + tid]; };
     bool ok = true;
-    T out[D][D][D];
-#pragma unroll
-    for (int c = 0; c < D; ++c)
-#pragma unroll
-        for (int b = 0; b < D; ++b)
-#pragma unroll
-            for (int a = 0; a < D; ++a) out[c][b][a] = T(0);
-#pragma unroll 1
-    for (int qy = 0; qy < Q; ++qy) {
-        T by[D], gyb[D];
-#pragma unroll
-        for (int k = 0; k < D; ++k) {
-            by[k] = TB::B(P, qy, k);
-            gyb[k] = TB::G(P, qy, k);
+    if (wvalid) {
+        if (lane == 0) {
+            for (int j = 0; j < S && j < COLS; ++j) {
+                mbar_arrive_expect_tx(&qbw[j], QBYTES);
+                bulk_g2s(qsw + j * STAGE, qdw + (int64_t)j * STAGE, QBYTES, &qbw[j]);
+                q_issued = j + 1;
+            }
         }
+        // gather (E) with the essential columns masked; padding elements hold -1
+        const bool evalid = __ldg(A.dofs + e) >= 0;
 #pragma unroll
-        for (int h0 = 0; h0 < Q; h0 += QH) {
-            T C0[D][QH], C1[D][QH], C2[D][QH];  // [c][qx - h0]
+        for (int k = 0; k < NL; ++k) {
+            T v = T(0);
+            if (evalid) {
+                const int32_t d = __ldg(A.dofs + (int64_t)k * E + e);
+                const bool ess = A.constrained && A.ess && A.ess[d];
+                v = ess ? T(0) : __ldg(A.x + d);
+            }
+            xs[k * BS + tid] = v;
+        }
+        auto uval = [&](int c, int b, int a) -> T { return xs[((c * D + b) * D + a) * BS + tid]; };
+        T out[D][D][D];
 #pragma unroll
-            for (int c = 0; c < D; ++c) {
-                T R[D], Rg[D];
+        for (int c = 0; c < D; ++c)
 #pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    T s0 = 0, s1 = 0;
+            for (int b = 0; b < D; ++b)
 #pragma unroll
-                    for (int b = 0; b < D; ++b) {
-                        const T u = uval(c, b, a);
-                        s0 += by[b] * u;
-                        if (HK) s1 += gyb[b] * u;
-                    }
-                    R[a] = s0;
-                    Rg[a] = s1;
-                }
+                for (int a = 0; a < D; ++a) out[c][b][a] = T(0);
+#pragma unroll 1
+        for (int qy = 0; qy < Q; ++qy) {
+            T by[D], gyb[D];
 #pragma unroll
-                for (int k = 0; k < QH; ++k) {
-                    const int qx = h0 + k;
-                    T t0 = 0, t1 = 0, t2 = 0;
-#pragma unroll
-                    for (int a = 0; a < D; ++a) {
-                        t0 += TB::B(P, qx, a) * R[a];
-                        if (HK) {
-                            t1 += TB::B(P, qx, a) * Rg[a];
-                            t2 += TB::G(P, qx, a) * R[a];
-                        }
-                    }
-                    C0[c][k] = t0;
-                    C1[c][k] = t1;
-                    C2[c][k] = t2;
-                }
+            for (int k = 0; k < D; ++k) {
+                by[k] = TB::B(P, qy, k);
+                gyb[k] = TB::G(P, qy, k);
             }
 #pragma unroll
-            for (int k = 0; k < QH; ++k) {
-                const int j = qy * Q + h0 + k;  // column = stream stage
-                const int st = j % S;
-                wait_stage(&qbw[st], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
-                const T *qc = qsw + st * STAGE + lane;
-                T vx[Q], vy[Q], vz[Q], vu[Q];
-#pragma unroll
-                for (int qz = 0; qz < Q; ++qz) {
-                    T gx = 0, gy = 0, gz = 0, ui = 0;
-#pragma unroll
-                    for (int c = 0; c < D; ++c) {
-                        if (HK) {
-                            gx += TB::B(P, qz, c) * C2[c][k];
-                            gy += TB::B(P, qz, c) * C1[c][k];
-                            gz += TB::G(P, qz, c) * C0[c][k];
-                        }
-                        if (HM) ui += TB::B(P, qz, c) * C0[c][k];
-                    }
-                    const T *qq = qc + qz * (NC * 32);
-                    vx[qz] = vy[qz] = vz[qz] = vu[qz] = T(0);
-                    if (HK) {
-                        const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
-                        vx[qz] = d0 * gx + d1 * gy + d2 * gz;
-                        vy[qz] = d1 * gx + d3 * gy + d4 * gz;
-                        vz[qz] = d2 * gx + d4 * gy + d5 * gz;
-                    }
-                    if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
-                }
-                __syncwarp();
-                if (lane == 0 && ok && j + S < COLS) {
-                    fence_proxy_async();
-                    mbar_arrive_expect_tx(&qbw[st], QBYTES);
-                    bulk_g2s(qsw + st * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[st]);
-                    q_issued = j + S + 1;
-                }
+            for (int h0 = 0; h0 < Q; h0 += QH) {
+                T C0[D][QH], C1[D][QH], C2[D][QH];  // [c][qx - h0]
 #pragma unroll
                 for (int c = 0; c < D; ++c) {
-                    T e0 = 0, e1 = 0, e2 = 0;
+                    T R[D], Rg[D];
 #pragma unroll
-                    for (int qz = 0; qz < Q; ++qz) {
-                        if (HK) {
-                            e2 += TB::B(P, qz, c) * vx[qz];
-                            e1 += TB::B(P, qz, c) * vy[qz];
-                            e0 += TB::G(P, qz, c) * vz[qz];
+                    for (int a = 0; a < D; ++a) {
+                        T s0 = 0, s1 = 0;
+#pragma unroll
+                        for (int b = 0; b < D; ++b) {
+                            const T u = uval(c, b, a);
+                            s0 += by[b] * u;
+                            if (HK) s1 += gyb[b] * u;
                         }
-                        if (HM) e0 += TB::B(P, qz, c) * vu[qz];
+                        R[a] = s0;
+                        Rg[a] = s1;
                     }
-                    C0[c][k] = e0;
-                    C1[c][k] = e1;
-                    C2[c][k] = e2;
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < D; ++c) {
-                T H0[D], H1[D];
-#pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    T s0 = 0, s1 = 0;
 #pragma unroll
                     for (int k = 0; k < QH; ++k) {
                         const int qx = h0 + k;
-                        s0 += TB::B(P, qx, a) * C0[c][k];
-                        if (HK) {
-                            s0 += TB::G(P, qx, a) * C2[c][k];
-                            s1 += TB::B(P, qx, a) * C1[c][k];
+                        T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            t0 += TB::B(P, qx, a) * R[a];
+                            if (HK) {
+                                t1 += TB::B(P, qx, a) * Rg[a];
+                                t2 += TB::G(P, qx, a) * R[a];
+                            }
                         }
+                        C0[c][k] = t0;
+                        C1[c][k] = t1;
+                        C2[c][k] = t2;
                     }
-                    H0[a] = s0;
-                    H1[a] = s1;
                 }
 #pragma unroll
-                for (int b = 0; b < D; ++b)
+                for (int k = 0; k < QH; ++k) {
+                    const int j = qy * Q + h0 + k;  // column = stream stage
+                    const int st = j % S;
+                    wait_stage(&qbw[st], (j / S) & 1, A.err, wlim, ok, q_waited, j + 1);
+                    const T *qc = qsw + st * STAGE + lane;
+                    T vx[Q], vy[Q], vz[Q], vu[Q];
+#pragma unroll
+                    for (int qz = 0; qz < Q; ++qz) {
+                        T gx = 0, gy = 0, gz = 0, ui = 0;
+#pragma unroll
+                        for (int c = 0; c < D; ++c) {
+                            if (HK) {
+                                gx += TB::B(P, qz, c) * C2[c][k];
+                                gy += TB::B(P, qz, c) * C1[c][k];
+                                gz += TB::G(P, qz, c) * C0[c][k];
+                            }
+                            if (HM) ui += TB::B(P, qz, c) * C0[c][k];
+                        }
+                        const T *qq = qc + qz * (NC * 32);
+                        vx[qz] = vy[qz] = vz[qz] = vu[qz] = T(0);
+                        if (HK) {
+                            const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
+                            vx[qz] = d0 * gx + d1 * gy + d2 * gz;
+                            vy[qz] = d1 * gx + d3 * gy + d4 * gz;
+                            vz[qz] = d2 * gx + d4 * gy + d5 * gz;
+                        }
+                        if (HM) vu[qz] = qq[(HK ? 6 : 0) * 32] * ui;
+                    }
+                    __syncwarp();
+                    if (lane == 0 && ok && j + S < COLS) {
+                        fence_proxy_async();
+                        mbar_arrive_expect_tx(&qbw[st], QBYTES);
+                        bulk_g2s(qsw + st * STAGE, qdw + (int64_t)(j + S) * STAGE, QBYTES, &qbw[st]);
+                        q_issued = j + S + 1;
+                    }
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        T e0 = 0, e1 = 0, e2 = 0;
+#pragma unroll
+                        for (int qz = 0; qz < Q; ++qz) {
+                            if (HK) {
+                                e2 += TB::B(P, qz, c) * vx[qz];
+                                e1 += TB::B(P, qz, c) * vy[qz];
+                                e0 += TB::G(P, qz, c) * vz[qz];
+                            }
+                            if (HM) e0 += TB::B(P, qz, c) * vu[qz];
+                        }
+                        C0[c][k] = e0;
+                        C1[c][k] = e1;
+                        C2[c][k] = e2;
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    T H0[D], H1[D];
 #pragma unroll
                     for (int a = 0; a < D; ++a) {
-                        T v = out[c][b][a] + by[b] * H0[a];
-                        if (HK) v += gyb[b] * H1[a];
-                        out[c][b][a] = v;
+                        T s0 = 0, s1 = 0;
+#pragma unroll
+                        for (int k = 0; k < QH; ++k) {
+                            const int qx = h0 + k;
+                            s0 += TB::B(P, qx, a) * C0[c][k];
+                            if (HK) {
+                                s0 += TB::G(P, qx, a) * C2[c][k];
+                                s1 += TB::B(P, qx, a) * C1[c][k];
+                            }
+                        }
+                        H0[a] = s0;
+                        H1[a] = s1;
                     }
+#pragma unroll
+                    for (int b = 0; b < D; ++b)
+#pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            T v = out[c][b][a] + by[b] * H0[a];
+                            if (HK) v += gyb[b] * H1[a];
+                            out[c][b][a] = v;
+                        }
+                }
             }
         }
-    }
-    // after a timeout: wait out the copies still in flight before the CTA exits
-    if (!ok && lane == 0) drain_stages(qbw, S, q_waited, q_issued);
-    if (!evalid) return;
-    // E^T: add into the non-essential DOFs (no other element of this colour
-    // touches them)
+        // the element result replaces the element values in the thread's own column
 #pragma unroll
-    for (int c = 0; c < D; ++c)
+        for (int c = 0; c < D; ++c)
 #pragma unroll
-        for (int b = 0; b < D; ++b)
+            for (int b = 0; b < D; ++b)
 #pragma unroll
-            for (int a = 0; a < D; ++a) {
-                const int32_t d = __ldg(A.dofs + (int64_t)((c * D + b) * D + a) * E + e);
-                if (!(A.constrained && A.ess && A.ess[d])) A.y[d] += out[c][b][a];
-            }
+                for (int a = 0; a < D; ++a) xs[((c * D + b) * D + a) * BS + tid] = out[c][b][a];
+        // after a timeout: wait out the copies still in flight
+        if (!ok && lane == 0) drain_stages(qbw, S, q_waited, q_issued);
+    }  // wvalid
+    // E^T: the chunk's DOF sums.  The lists are staged where the rings were; a
+    // CTA in which a wait timed out (error word set) stores nothing, so that no
+    // copy that is still late can land in the staged lists.
+    if (__syncthreads_or(!ok)) return;
+    ChunkStage st = chunk_stage_at(A.L, hex_smem);
+    chunk_stage_lists<BS>(A.L, blockIdx.x, st);
+    __syncthreads();
+    chunk_sums<T, BS>(A.L, st, xs, A.ess, A.x, A.y, A.accumulate, A.constrained, 0);
 }
 
-// Jacobi diagonal: element diagonal sum_q g_i^T D_q g_i (+ m_q phi_i^2) added
-// into the non-essential DOFs, one launch per colour (after hex_init_kernel
-// with x = null, which puts 1 on the essential DOFs of a constrained call).
-template <int P, int OPK>
-__global__ void __launch_bounds__(128) hex_diag_kernel(const HexApply<double> A) {
-    constexpr int D = P + 1, Q = P + 1, NC = NComp<OPK>::v;
+// Jacobi diagonal: element diagonal sum_q g_i^T D_q g_i (+ m_q phi_i^2), one
+// thread per element of a chunk of BS elements, summed per DOF by the chunk
+// scatter (1 on the essential DOFs of a constrained call).
+template <int P, int OPK, int BS>
+__global__ void __launch_bounds__(BS) hex_diag_kernel(const HexApply<double> A) {
+    constexpr int D = P + 1, Q = P + 1, NL = D * D * D, NC = NComp<OPK>::v;
     constexpr bool HM = (OPK & 1) != 0, HK = (OPK & 2) != 0;
     using TB = Tab<double>;
-    const int64_t e = A.e0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= A.e1 || __ldg(A.dofs + e) < 0) return;
+    extern __shared__ __align__(128) unsigned char hex_smem[];
+    double *ys = reinterpret_cast<double *>(hex_smem);  // [NL][BS]
+    const int tid = threadIdx.x;
+    const int64_t e = (int64_t)blockIdx.x * BS + tid;
     const int64_t E = A.E;
     double out[D][D][D];
 #pragma unroll
@@ -292,43 +299,46 @@ __global__ void __launch_bounds__(128) hex_diag_kernel(const HexApply<double> A)
         for (int b = 0; b < D; ++b)
 #pragma unroll
             for (int a = 0; a < D; ++a) out[c][b][a] = 0.0;
-    for (int qy = 0; qy < Q; ++qy)
-        for (int qx = 0; qx < Q; ++qx)
-            for (int qz = 0; qz < Q; ++qz) {
-                double d[7];
+    if (e < E && __ldg(A.dofs + e) >= 0) {
+        for (int qy = 0; qy < Q; ++qy)
+            for (int qx = 0; qx < Q; ++qx)
+                for (int qz = 0; qz < Q; ++qz) {
+                    double d[7];
 #pragma unroll
-                for (int k = 0; k < NC; ++k) d[k] = __ldg(A.qd + hex_qd_index<P, OPK>(e, qy * Q + qx, qz, k));
+                    for (int k = 0; k < NC; ++k) d[k] = __ldg(A.qd + hex_qd_index<P, OPK>(e, qy * Q + qx, qz, k));
 #pragma unroll
-                for (int c = 0; c < D; ++c)
+                    for (int c = 0; c < D; ++c)
 #pragma unroll
-                    for (int b = 0; b < D; ++b)
+                        for (int b = 0; b < D; ++b)
 #pragma unroll
-                        for (int a = 0; a < D; ++a) {
-                            const double Bx = TB::B(P, qx, a), By = TB::B(P, qy, b), Bz = TB::B(P, qz, c);
-                            double s = 0.0;
-                            if (HK) {
-                                const double gx = TB::G(P, qx, a) * By * Bz;
-                                const double gy = Bx * TB::G(P, qy, b) * Bz;
-                                const double gz = Bx * By * TB::G(P, qz, c);
-                                s = d[0] * gx * gx + d[3] * gy * gy + d[5] * gz * gz +
-                                    2.0 * (d[1] * gx * gy + d[2] * gx * gz + d[4] * gy * gz);
+                            for (int a = 0; a < D; ++a) {
+                                const double Bx = TB::B(P, qx, a), By = TB::B(P, qy, b), Bz = TB::B(P, qz, c);
+                                double s = 0.0;
+                                if (HK) {
+                                    const double gx = TB::G(P, qx, a) * By * Bz;
+                                    const double gy = Bx * TB::G(P, qy, b) * Bz;
+                                    const double gz = Bx * By * TB::G(P, qz, c);
+                                    s = d[0] * gx * gx + d[3] * gy * gy + d[5] * gz * gz +
+                                        2.0 * (d[1] * gx * gy + d[2] * gx * gz + d[4] * gy * gz);
+                                }
+                                if (HM) {
+                                    const double ph = Bx * By * Bz;
+                                    s += d[HK ? 6 : 0] * ph * ph;
+                                }
+                                out[c][b][a] += s;
                             }
-                            if (HM) {
-                                const double ph = Bx * By * Bz;
-                                s += d[HK ? 6 : 0] * ph * ph;
-                            }
-                            out[c][b][a] += s;
-                        }
-            }
+                }
+    }
 #pragma unroll
     for (int c = 0; c < D; ++c)
 #pragma unroll
         for (int b = 0; b < D; ++b)
 #pragma unroll
-            for (int a = 0; a < D; ++a) {
-                const int32_t d = __ldg(A.dofs + (int64_t)((c * D + b) * D + a) * E + e);
-                if (!(A.constrained && A.ess && A.ess[d])) A.y[d] += out[c][b][a];
-            }
+            for (int a = 0; a < D; ++a) ys[((c * D + b) * D + a) * BS + tid] = out[c][b][a];
+    ChunkStage st = chunk_stage_at(A.L, hex_smem + sizeof(double) * NL * BS);
+    chunk_stage_lists<BS>(A.L, blockIdx.x, st);
+    __syncthreads();
+    chunk_sums<double, BS>(A.L, st, ys, A.ess, nullptr, A.y, 0, A.constrained, 1);
 }
 
 // Quadrature-data setup of the unstructured mesh: one thread per (element,

@@ -7,6 +7,7 @@
 #include <mutex>
 #include <vector>
 
+#include "chunk_plan.h"
 #include "tet_kernels.cuh"
 
 struct fg_tet {
@@ -194,23 +195,23 @@ static TetChunk tet_chunk_args(const fg_tet *t) {
     C.E = t->E;
     C.N = t->N;
     C.CE = t->CE;
-    C.max_nu = t->max_nu;
     C.G = t->G;
     C.Sm = t->Sm;
     C.sk = t->sk;
     C.sm = t->sm;
     C.edof = t->edof;
     C.emsk = t->emsk;
-    C.cu_off = t->cu_off;
-    C.cu_dof = t->cu_dof;
-    C.cu_pid = t->cu_pid;
-    C.cu_soff = t->cu_soff;
-    C.cu_slots = t->cu_slots;
-    C.part = t->part;
-    C.sh_dof = t->sh_dof;
-    C.sh_off = t->sh_off;
     C.ess = t->ess;
-    C.n_shared = t->n_shared;
+    C.L.cu_off = t->cu_off;
+    C.L.cu_dof = t->cu_dof;
+    C.L.cu_pid = t->cu_pid;
+    C.L.cu_soff = t->cu_soff;
+    C.L.cu_slots = t->cu_slots;
+    C.L.part = t->part;
+    C.L.sh_dof = t->sh_dof;
+    C.L.sh_off = t->sh_off;
+    C.L.n_shared = t->n_shared;
+    C.L.max_nu = t->max_nu;
     return C;
 }
 
@@ -234,88 +235,23 @@ template <typename T> static int tet_upload(T **dst, const T *src, size_t n) {
     return FG_OK;
 }
 
-// Morton key of a point in the box [lo, lo + ext): 21 bits per axis, interleaved
-static uint64_t tet_morton(const double *p, const double *lo, const double *ext) {
-    uint64_t key = 0;
-    uint32_t v[3];
-    for (int a = 0; a < 3; ++a) {
-        double f = ext[a] > 0.0 ? (p[a] - lo[a]) / ext[a] : 0.0;
-        f = std::min(std::max(f, 0.0), 1.0);
-        v[a] = (uint32_t)std::min<double>(f * 2097152.0, 2097151.0);
-    }
-    for (int b = 20; b >= 0; --b)
-        for (int a = 0; a < 3; ++a) key = (key << 1) | ((v[a] >> b) & 1u);
-    return key;
-}
-
-// Element order and chunk DOF lists.  h = element map [E][nl] (caller's order);
-// perm[n] = the caller's element at position n of the chunk order.
-struct TetChunkPlan {
-    std::vector<int32_t> perm, cu_off, cu_dof, cu_pid, cu_soff, sh_dof, sh_off;
-    std::vector<uint16_t> cu_slots;
-    int max_nu = 0;
-};
-
+// Element order (Morton order of the centroids of the four vertex nodes, the
+// first four local DOFs) and the chunk DOF lists.  h = element map [E][nl] in
+// the caller's order; perm[n] = the caller's element at position n.
 static void tet_plan_chunks(const std::vector<int32_t> &h, const std::vector<double> &coords, int64_t E,
-                            int64_t N, int nl, int CE, TetChunkPlan &P) {
-    // Morton order of the element centroids (vertex nodes = first 4 local DOFs)
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                            int64_t N, int nl, int CE, std::vector<int32_t> &perm, ChunkPlan &P) {
     std::vector<double> cen((size_t)E * 3);
     for (int64_t e = 0; e < E; ++e)
         for (int a = 0; a < 3; ++a) {
             double s = 0.0;
             for (int v = 0; v < 4; ++v) s += coords[3 * (size_t)h[e * nl + v] + a];
             cen[3 * e + a] = 0.25 * s;
-            lo[a] = std::min(lo[a], cen[3 * e + a]);
-            hi[a] = std::max(hi[a], cen[3 * e + a]);
         }
-    const double ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
-    std::vector<uint64_t> key(E);
-    for (int64_t e = 0; e < E; ++e) key[e] = tet_morton(&cen[3 * e], lo, ext);
-    P.perm.resize(E);
-    for (int64_t e = 0; e < E; ++e) P.perm[e] = (int32_t)e;
-    std::stable_sort(P.perm.begin(), P.perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
-    // per chunk: its DOFs (ascending), their local slots (ascending), the local map
-    const int64_t nch = (E + CE - 1) / CE;
-    P.cu_off.assign(nch + 1, 0);
-    P.cu_slots.reserve((size_t)E * nl);
-    std::vector<int32_t> nchk(N, 0);
-    std::vector<std::pair<int32_t, int32_t>> pr;
-    for (int64_t c = 0; c < nch; ++c) {
-        const int64_t e0 = c * CE;
-        const int ne = (int)std::min<int64_t>(CE, E - e0);
-        pr.clear();
-        for (int el = 0; el < ne; ++el)
-            for (int i = 0; i < nl; ++i) pr.push_back({h[(int64_t)P.perm[e0 + el] * nl + i], i * CE + el});
-        std::sort(pr.begin(), pr.end());
-        int nu = 0;
-        for (size_t k = 0; k < pr.size(); ++k) {
-            if (k == 0 || pr[k].first != pr[k - 1].first) {
-                P.cu_dof.push_back(pr[k].first);
-                P.cu_soff.push_back((int32_t)P.cu_slots.size());
-                ++nchk[pr[k].first];
-                ++nu;
-            }
-            P.cu_slots.push_back((uint16_t)pr[k].second);
-        }
-        P.cu_off[c + 1] = P.cu_off[c] + nu;
-        P.max_nu = std::max(P.max_nu, nu);
-    }
-    P.cu_soff.push_back((int32_t)P.cu_slots.size());
-    // DOFs not owned by exactly one chunk: partial ranges in chunk order
-    std::vector<int32_t> base(N, -1);
-    P.sh_off.push_back(0);
-    for (int64_t d = 0; d < N; ++d)
-        if (nchk[d] != 1) {
-            base[d] = P.sh_off.back();
-            P.sh_dof.push_back((int32_t)d);
-            P.sh_off.push_back(P.sh_off.back() + nchk[d]);
-        }
-    P.cu_pid.resize(P.cu_dof.size());
-    for (size_t u = 0; u < P.cu_dof.size(); ++u) {  // chunks in order, so partials land in chunk order
-        const int32_t d = P.cu_dof[u];
-        P.cu_pid[u] = nchk[d] == 1 ? -1 : base[d]++;
-    }
+    morton_order(cen, E, perm);
+    std::vector<int32_t> smap((size_t)E * nl);
+    for (int64_t n = 0; n < E; ++n)
+        for (int i = 0; i < nl; ++i) smap[(size_t)n * nl + i] = h[(size_t)perm[n] * nl + i];
+    plan_chunk_lists(smap, E, N, nl, CE, P);
 }
 
 template <int NL, int MQ, bool MOM, int BT>
@@ -358,7 +294,8 @@ static int tet_launch_apply(fg_tet *t, const double *x, double *y, int accumulat
     if (rc) return rc;
     if (t->n_shared) {
         const int db = (int)std::min<int64_t>((t->n_shared + 255) / 256, 148 * 16);
-        tet_shared_kernel<<<db, 256, 0, t->stream>>>(C, diag ? nullptr : x, y, accumulate, constrained, diag);
+        chunk_shared_kernel<double><<<db, 256, 0, t->stream>>>(C.L, t->ess, diag ? nullptr : x, y, accumulate,
+                                                               constrained, diag, nullptr);
     }
     CK(cudaGetLastError());
     return FG_OK;

@@ -32,9 +32,11 @@
 // shared memory and sums, per DOF of its list, the element-local slots of
 // that DOF in increasing (local index, element) order.  A DOF whose elements all lie in the chunk is
 // stored directly; a DOF shared with other chunks gets one partial sum per
-// chunk, and tet_shared_kernel adds the partials of each such DOF in
-// increasing chunk order.  The result is deterministic.
+// chunk, and chunk_shared_kernel adds the partials of each such DOF in
+// increasing chunk order (chunk_plan.h, chunk_scatter.cuh).  The result is
+// deterministic.
 #pragma once
+#include "chunk_scatter.cuh"
 #include "fg_common.cuh"
 
 namespace fg {
@@ -61,21 +63,12 @@ struct TetArgs {
 struct TetChunk {
     int64_t E, N;
     int CE;                      // elements per chunk
-    int max_nu;                  // largest chunk DOF list
     const double *G, *Sm;        // [6][E], [10][E] (P1: [6][E] S00 G)
     const double *sk, *sm;       // [nq][E]
     const int32_t *edof;         // [nl][E]
     const uint32_t *emsk;        // [E] essential local DOFs (bit i), null if no essential list
-    const int32_t *cu_off;       // [n_chunks + 1] start of each chunk's DOF list
-    const int32_t *cu_dof;       // [U] global DOF
-    const int32_t *cu_pid;       // [U] partial slot of a shared DOF, -1 for a DOF owned by the chunk
-    const int32_t *cu_soff;      // [U + 1] start of each DOF's local slots
-    const uint16_t *cu_slots;    // [E nl] local slots i * CE + e_local, increasing per DOF
-    double *part;                // [n_part] partial sums of shared DOFs
-    const int32_t *sh_dof;       // [n_shared] DOFs not owned by one chunk (incl. DOFs of no element)
-    const int32_t *sh_off;       // [n_shared + 1] their partial ranges (in chunk order)
     const uint8_t *ess;          // [N] or null
-    int64_t n_shared;
+    ChunkLists L;
 };
 
 // one thread per element: geometry and the per-point scalars
@@ -266,12 +259,10 @@ __device__ __forceinline__ void tet_elem_moments(const double (&md)[TetMom<NL>::
     }
 }
 
-// Shared-memory plan of a chunk (bytes): element results, DOF ids, partial
-// ids, slot offsets (relative to the chunk), local slots.
+// Shared-memory plan of a chunk (bytes): element results, then the chunk's
+// lists.
 __host__ __device__ inline size_t tet_chunk_smem(int NL, int CE, int max_nu) {
-    const size_t a = sizeof(double) * (size_t)NL * CE;
-    const size_t b = sizeof(int32_t) * (3 * (size_t)max_nu + 1);
-    return a + ((b + sizeof(uint16_t) * (size_t)NL * CE + 15) & ~(size_t)15);
+    return sizeof(double) * (size_t)NL * CE + chunk_list_smem(NL, CE, max_nu);
 }
 
 // One CTA (BT threads) per chunk.  First the chunk's DOF list (ids, partial
@@ -289,24 +280,13 @@ __global__ void __launch_bounds__(BT, MOM ? (BT == 512 ? 2 : 3) : 1) tet_chunk_k
                                                                   double *__restrict__ y, int accumulate,
                                                                   int constrained, int diag) {
     extern __shared__ __align__(16) unsigned char tsm_raw[];
-    const int CE = C.CE, MU = C.max_nu;
+    const int CE = C.CE;
     double *ys = reinterpret_cast<double *>(tsm_raw);  // [NL][CE] element results
-    int32_t *sdof = reinterpret_cast<int32_t *>(ys + NL * CE);
-    int32_t *spid = sdof + MU;
-    int32_t *soff = spid + MU;                         // [MU + 1]
-    uint16_t *sslot = reinterpret_cast<uint16_t *>(soff + MU + 1);
+    ChunkStage S = chunk_stage_at(C.L, tsm_raw + sizeof(double) * NL * CE);
     const int c = blockIdx.x;
-    const int u0 = __ldg(C.cu_off + c), nu = __ldg(C.cu_off + c + 1) - u0;
-    const int s0 = __ldg(C.cu_soff + u0), ns = __ldg(C.cu_soff + u0 + nu) - s0;
     const int64_t e0 = (int64_t)c * CE;
     const int ne = (int)(C.E - e0 < CE ? C.E - e0 : CE);
-    for (int k = threadIdx.x; k < nu; k += BT) {
-        sdof[k] = __ldg(C.cu_dof + u0 + k);
-        spid[k] = __ldg(C.cu_pid + u0 + k);
-        soff[k] = __ldg(C.cu_soff + u0 + k) - s0;
-    }
-    if (threadIdx.x == 0) soff[nu] = ns;
-    for (int j = threadIdx.x; j < ns; j += BT) sslot[j] = __ldg(C.cu_slots + s0 + j);
+    chunk_stage_lists<BT>(C.L, c, S);
     const bool mask = constrained && C.emsk;
     for (int el = threadIdx.x; el < ne; el += BT) {
         const int64_t e = e0 + el;
@@ -328,32 +308,7 @@ __global__ void __launch_bounds__(BT, MOM ? (BT == 512 ? 2 : 3) : 1) tet_chunk_k
         for (int i = 0; i < NL; ++i) ys[i * CE + el] = ye[i];
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < nu; k += BT) {
-        double s = 0.0;
-        for (int j = soff[k]; j < soff[k + 1]; ++j) s += ys[sslot[j]];
-        const int32_t pid = spid[k];
-        if (pid >= 0) {
-            C.part[pid] = s;
-        } else {
-            const int32_t d = sdof[k];
-            if (constrained && C.ess && C.ess[d]) s = diag ? 1.0 : x[d];
-            y[d] = accumulate ? y[d] + s : s;
-        }
-    }
-}
-
-// DOFs not owned by a single chunk: the partials of their chunks in chunk order
-__global__ void tet_shared_kernel(const TetChunk C, const double *__restrict__ x, double *__restrict__ y,
-                                  int accumulate, int constrained, int diag) {
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < C.n_shared;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t d = C.sh_dof[k];
-        double s = 0.0;
-#pragma unroll 4
-        for (int j = C.sh_off[k]; j < C.sh_off[k + 1]; ++j) s += C.part[j];
-        if (constrained && C.ess && C.ess[d]) s = diag ? 1.0 : x[d];
-        y[d] = accumulate ? y[d] + s : s;
-    }
+    chunk_sums<double, BT>(C.L, S, ys, C.ess, x, y, accumulate, constrained, diag);
 }
 
 // Reorder the per-element data into the chunk order and form the diffusion

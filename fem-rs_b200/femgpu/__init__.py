@@ -47,7 +47,7 @@ EXPORTS = ("fg_cfg_default", "fg_last_error", "fg_op_create", "fg_op_destroy", "
            "fg_assemble_source", "fg_l2_error", "fg_lumped_mass", "fg_lumped_apply", "fg_op_set_tile",
            "fg_op_tile", "fg_batch_autotune", "fg_tet_create", "fg_tet_destroy", "fg_tet_ndofs", "fg_tet_nq",
            "fg_tet_quadrature_points", "fg_tet_apply", "fg_tet_diagonal", "fg_op_set_wait_limit",
-           "fg_op_create_hex", "fg_op_colours", "fg_vec_dots", "fg_vec_pcg_update", "fg_vec_pupdate",
+           "fg_op_create_hex", "fg_op_chunks", "fg_vec_dots", "fg_vec_pcg_update", "fg_vec_pupdate",
            "fg_tet_apply_native", "fg_tet_set_stream", "fg_tet_check")
 
 
@@ -151,7 +151,8 @@ def lib():
         L.fg_op_set_wait_limit.argtypes = [vp, d]
         L.fg_op_create_hex.argtypes = [i, i64, vp, i64, vp, vp, i64, i, d, d, vp, d, vp, d, vp, i64,
                                        C.POINTER(vp)]
-        L.fg_op_colours.argtypes = [vp]
+        L.fg_op_chunks.argtypes = [vp]
+        L.fg_op_chunks.restype = i64
         L.fg_vec_dots.argtypes = [vp, i64, i, vp, vp, vp]
         L.fg_vec_pcg_update.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp]
         L.fg_vec_pupdate.argtypes = [vp, vp, vp, vp, vp]
@@ -426,8 +427,9 @@ class HexMeshOperator(PAOperator):
     reference cube, local DOF (c, b, a) at (c*(p+1) + b)*(p+1) + a);
     ``kappa`` / ``rho``: scalar or (E, (p+1)^3) at the tensor Gauss points;
     ``ess_dofs``: the essential-DOF list (boundary_dofs, constraints.rs:53-60).
-    Native vectors are the plain numbering padded with zeros to a multiple of 4.  The scatter is a
-    coloured element loop (no float atomics, same sums every run).
+    Native vectors are the plain numbering padded with zeros to a multiple of 4.  The scatter works on
+    Morton-ordered element chunks with the DOF sums in shared memory (no float atomics, same sums every
+    run).
     """
 
     def __init__(self, order, coords, conn, elem_dofs=None, n_dofs=None, kind=DIFF, kappa=1.0, rho=1.0,
@@ -461,9 +463,9 @@ class HexMeshOperator(PAOperator):
         self.NI, self.NJ, self.NK, self.NIp = (int(v) for v in dims)
 
     @property
-    def colours(self):
-        """Element colours of the deterministic scatter (one launch each)."""
-        return int(lib().fg_op_colours(self._h))
+    def chunks(self):
+        """Element chunks of the deterministic scatter (one CTA each)."""
+        return int(lib().fg_op_chunks(self._h))
 
 
 class PADiffusionOperator(PAOperator):

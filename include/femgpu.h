@@ -169,15 +169,20 @@ FG_API void fg_op_destroy(fg_op *op);
  * CHEBYSHEV; FP64 and FG_FP32_IR) work as for a box; entry points that need
  * the box's lattice or tiles (affine format, tiles, batches, SDIRK-2, the
  * learned correction, the no-alloc apply) return FG_UNSUPPORTED.  The scatter
- * is coloured: elements that share no DOF form a colour and each colour is
- * one launch adding into y (no float atomics; the same sums every run). */
+ * is chunked: elements in a Morton order form chunks of one CTA each, whose DOF
+ * sums are formed in shared memory in a fixed order; DOFs shared between chunks
+ * add their chunk partials in chunk order (no float atomics; the same sums
+ * every run). */
 FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double *coords, int64_t n_elem,
                             const uint32_t *conn, const uint32_t *elem_dofs, int64_t n_dofs, int kind,
                             double c_mass, double c_diff, const double *kappa_q, double kappa_const,
                             const double *rho_q, double rho_const, const uint32_t *ess_dofs, int64_t n_ess,
                             fg_op **out);
-/* Element colours of an operator from fg_op_create_hex (0 for a box). */
-FG_API int fg_op_colours(const fg_op *op);
+/* Element chunks of an operator from fg_op_create_hex (0 for a box): the
+ * elements in a Morton order of their centroids, one CTA per chunk, each
+ * chunk's DOF sums formed in shared memory (no float atomics, no colour
+ * passes). */
+FG_API int64_t fg_op_chunks(const fg_op *op);
 
 /* MatFreeOperator::n_dofs / LinearOperator::{nrows,ncols}. */
 FG_API int64_t fg_op_ndofs(const fg_op *op);
