@@ -244,6 +244,7 @@ struct fg_op {
     int u_max_nu = 0;
     int32_t *u_dofs = nullptr;
     uint8_t *u_ess = nullptr;
+    uint64_t *u_emsk = nullptr;  // [E] essential local DOFs of each element (bit k)
     int32_t *u_cu_off = nullptr, *u_cu_dof = nullptr, *u_cu_pid = nullptr, *u_cu_soff = nullptr;
     int32_t *u_sh_dof = nullptr, *u_sh_off = nullptr;
     uint16_t *u_cu_slots = nullptr;
@@ -275,7 +276,7 @@ static void free_op(fg_op *op) {
     if (op->u_dofs) cudaFree(op->u_dofs);
     if (op->u_ess) cudaFree(op->u_ess);
     {
-        void *u[] = {op->u_cu_off, op->u_cu_dof, op->u_cu_pid, op->u_cu_soff, op->u_sh_dof, op->u_sh_off,
+        void *u[] = {op->u_emsk, op->u_cu_off, op->u_cu_dof, op->u_cu_pid, op->u_cu_soff, op->u_sh_dof, op->u_sh_off,
                      op->u_cu_slots, op->u_part};
         for (void *q : u)
             if (q) cudaFree(q);

@@ -26,6 +26,7 @@ static HexApply<T> hex_args(fg_op *op, const T *qd, const T *x, T *y, int accumu
     A.dofs = op->u_dofs;
     A.qd = qd;
     A.ess = op->u_ess;
+    A.emsk = op->u_emsk;
     A.x = x;
     A.y = y;
     A.accumulate = accumulate;
@@ -273,7 +274,13 @@ extern "C" FG_API int fg_op_create_hex(int order, int64_t n_nodes, const double 
             if (cudaMalloc(dst, sizeof(V) * n) != cudaSuccess) return false;
             return v.empty() || cudaMemcpy(*dst, v.data(), sizeof(V) * v.size(), cudaMemcpyHostToDevice) == cudaSuccess;
         };
-        if (!up(&op->u_cu_off, plan.cu_off) || !up(&op->u_cu_dof, plan.cu_dof) || !up(&op->u_cu_pid, plan.cu_pid) ||
+        std::vector<uint64_t> em((size_t)Ep, 0ull);
+        for (int64_t s = 0; s < Ep; ++s)
+            for (int k = 0; k < nl; ++k) {
+                const int32_t d = smap[(size_t)s * nl + k];
+                if (d >= 0 && mask[(size_t)d]) em[(size_t)s] |= 1ull << k;
+            }
+        if (!up(&op->u_emsk, em) || !up(&op->u_cu_off, plan.cu_off) || !up(&op->u_cu_dof, plan.cu_dof) || !up(&op->u_cu_pid, plan.cu_pid) ||
             !up(&op->u_cu_soff, plan.cu_soff) || !up(&op->u_cu_slots, plan.cu_slots) ||
             !up(&op->u_sh_dof, plan.sh_dof) || !up(&op->u_sh_off, plan.sh_off) ||
             cudaMalloc(&op->u_part, sizeof(double) * std::max<int64_t>(plan.n_part, 1)) != cudaSuccess)

@@ -19,6 +19,8 @@
 //                        1-D bulk copies on mbarriers (bounded waits, drained on
 //                        timeout)
 //   ess  [N]             essential-DOF mask (constrained applies)
+//   emsk [E]             per element, bit k set: local DOF k is essential (the
+//                        gather masks with it instead of reading ess per DOF)
 //
 // Scatter without float atomics and without an element-result array in HBM
 // (chunk_plan.h, chunk_scatter.cuh): a CTA puts its element results in shared
@@ -43,6 +45,7 @@ template <typename T> struct HexApply {
     const int32_t *dofs;   // [nl][E]
     const T *qd;           // per-group streams (layout above)
     const uint8_t *ess;    // [N] or null
+    const uint64_t *emsk;  // [E] essential local DOFs (bit k), or null
     const T *x;            // null: diagonal
     T *y;
     int accumulate, constrained;
@@ -116,13 +119,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) hex_apply_kernel(const HexAp
         }
         // gather (E) with the essential columns masked; padding elements hold -1
         const bool evalid = __ldg(A.dofs + e) >= 0;
+        const uint64_t m = (A.constrained && A.emsk) ? __ldg(A.emsk + e) : 0ull;
 #pragma unroll
         for (int k = 0; k < NL; ++k) {
             T v = T(0);
             if (evalid) {
-                const int32_t d = __ldg(A.dofs + (int64_t)k * E + e);
-                const bool ess = A.constrained && A.ess && A.ess[d];
-                v = ess ? T(0) : __ldg(A.x + d);
+                const T xv = __ldg(A.x + __ldg(A.dofs + (int64_t)k * E + e));
+                v = ((m >> k) & 1ull) ? T(0) : xv;
             }
             xs[k * BS + tid] = v;
         }
