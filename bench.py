@@ -492,7 +492,10 @@ def run_heat(rank, steps, stream):
 
 def run_batch(rank, batch_n, dev):
     """256 uneven solves, n ~ U{8..48}, p ~ U{1,2,3}, own lognormal kappa
-    (sigma2 ~ U[0.25,2], ell ~ U[0.05,0.3]) and RHS M xi, FP32 mixed precision."""
+    (sigma2 ~ U[0.25,2], ell ~ U[0.05,0.3]) and RHS M xi, FP32 mixed precision.
+    Sequential and batched with the default tiles and full quadrature data,
+    then the autotuner's (format, tile) per group, sequential and batched again;
+    iterations are compared between the two tuned runs."""
     import femgpu
     from femgpu.fields import lognormal_kappa_q
 
@@ -531,10 +534,11 @@ def run_batch(rank, batch_n, dev):
     t_tune = time.perf_counter()
     tune = femgpu.batch_autotune(bops, reps=3)
     t_tune = time.perf_counter() - t_tune
-    t_seq, _ = sequential()  # tuned tiles: the batching gain alone
+    t_seq, seq_iters = sequential()  # tuned tiles and formats: the batching gain alone
     bxs = [np.zeros_like(v) for v in bbs]
     ok, bres = femgpu.batch_pcg(bops, bbs, bxs, cfgb, femgpu.PC_CHEBYSHEV)
     t_batch = bres[0].solve_ms / 1e3
+    dof_its = sum(int(o.n_dofs()) * int(r.iterations) for o, r in zip(bops, bres))
     for o in bops:
         o.close()
     summary = {"instances": len(bops), "total_dofs": total, "all_converged": bool(ok and ok0),
@@ -544,11 +548,13 @@ def run_batch(rank, batch_n, dev):
                "sequential_default_tiles_s": round(t_seq0, 3), "sequential_tuned_tiles_s": round(t_seq, 3),
                "batched_default_tiles_s": round(t_batch0, 3), "batched_tuned_s": round(t_batch, 3),
                "speedup_batching_same_tiles": round(t_seq / t_batch, 3),
-               "speedup_autotune_batched": round(t_batch0 / t_batch, 3)}
+               "speedup_autotune_batched": round(t_batch0 / t_batch, 3),
+               "affine_groups": sum(e["format"] == femgpu.QDATA_AFFINE for e in tune), "groups": len(tune)}
     detail = dict(summary, setup_s=t_setup, autotune_s=t_tune,
-                  dof_iterations_per_s=sum(o.n_dofs() * r.iterations for o, r in zip(bops, bres)) / t_batch,
+                  dof_iterations=dof_its, dof_iterations_per_s=dof_its / t_batch,
                   autotune=[{"order": e["order"], "size_class": e["size_class"], "instances": e["instances"],
-                             "tz": e["tz"], "us_per_candidate_tz": e["us"]} for e in tune])
+                             "format": "affine" if e["format"] == femgpu.QDATA_AFFINE else "full", "tz": e["tz"],
+                             "us_per_candidate_tz": e["us"], "us_other_format": e["us_other"]} for e in tune])
     return summary, detail
 
 

@@ -337,7 +337,13 @@ template <> struct KCfg32<1> { static constexpr int WY = 4, S = 6, MINB = 4; };
 #define FG_F32_Q2_S 4
 #endif
 template <> struct KCfg32<2> { static constexpr int WY = 4, S = FG_F32_Q2_S, MINB = 3; };
-template <> struct KCfg32<3> { static constexpr int WY = FG_Q3_WY, S = 3, MINB = 2; };
+#ifndef FG_F32_Q3_S  // FP32 Q3 qdata ring depth and CTAs/SM hint
+#define FG_F32_Q3_S 3
+#endif
+#ifndef FG_F32_Q3_MINB
+#define FG_F32_Q3_MINB 2
+#endif
+template <> struct KCfg32<3> { static constexpr int WY = FG_Q3_WY, S = FG_F32_Q3_S, MINB = FG_F32_Q3_MINB; };
 template <int P, typename T> struct KC;
 template <int P> struct KC<P, double> : KCfg<P> {};
 template <int P> struct KC<P, float> : KCfg32<P> {};
@@ -2063,17 +2069,18 @@ FG_API int fg_batch_autotune(fg_op *const *ops, int n, int reps, fg_tune_entry *
     int rc;
     for (int i = 0; i < n; ++i)
         if ((rc = ensure_solver_buffers(ops[i])) || (rc = ensure_fp32(ops[i]))) return rc;
-    // classes of (order, kind, format, size): elements <= 16^3, <= 32^3, larger
-    struct Cls { int p, kind, fmt, sc; std::vector<int> inst; };
+    // classes of (order, kind, size): elements <= 16^3, <= 32^3, larger; the
+    // quadrature-data format is a tuned dimension of each class
+    struct Cls { int p, kind, sc; std::vector<int> inst; };
     std::vector<Cls> cls;
     for (int i = 0; i < n; ++i) {
         const fg_op *o = ops[i];
         const int64_t E = (int64_t)o->g.nx * o->g.ny * o->g.nz;
         const int sc = E <= 4096 ? 0 : (E <= 32768 ? 1 : 2);
         auto it = std::find_if(cls.begin(), cls.end(), [&](const Cls &c) {
-            return c.p == o->p && c.kind == o->kind && c.fmt == o->fmt && c.sc == sc;
+            return c.p == o->p && c.kind == o->kind && c.sc == sc;
         });
-        if (it == cls.end()) { cls.push_back(Cls{o->p, o->kind, o->fmt, sc, {}}); it = cls.end() - 1; }
+        if (it == cls.end()) { cls.push_back(Cls{o->p, o->kind, sc, {}}); it = cls.end() - 1; }
         it->inst.push_back(i);
     }
     cudaStream_t bs;
@@ -2085,22 +2092,53 @@ FG_API int fg_batch_autotune(fg_op *const *ops, int n, int reps, fg_tune_entry *
         while (d * 2 <= tz && d * 2 <= o->g.nz) d *= 2;
         return d;
     };
+    // put every member of a class on format f; false if a member refuses the
+    // affine format (an element whose Jacobian is not constant)
+    auto set_format = [&](const Cls &c, int f, int &err) {
+        err = FG_OK;
+        for (int i : c.inst) {
+            fg_op *o = ops[i];
+            if (f == 1 && !o->qa64) {
+                const int r = build_affine<double>(o, &o->qa64);
+                if (r == FG_UNSUPPORTED) {
+                    t_last_status = FG_OK;  // a refusal here only removes the candidate
+                    for (int j : c.inst) ops[j]->fmt = 0;
+                    return false;
+                }
+                if (r) { err = r; return false; }
+            }
+            o->fmt = f;
+        }
+        return true;
+    };
     int count = 0;
     for (const Cls &c : cls) {
-        double us[FG_TUNE_CANDIDATES];
-        int best = -1;
+        double us[2][FG_TUNE_CANDIDATES];
+        int best_f = -1, best_k = -1;
         int maxnz = 1;
         for (int i : c.inst) maxnz = std::max(maxnz, ops[i]->g.nz);
-        for (int k = 0; k < FG_TUNE_CANDIDATES; ++k) {
-            us[k] = -1.0;
-            if (k > 0 && kTuneTZ[k] > maxnz) continue;  // same shapes as a smaller candidate
-            for (int i : c.inst)
-                if ((rc = set_tile_locked(ops[i], depth(ops[i], kTuneTZ[k])))) return rc;
-            if ((rc = time_batched_apply(ops, c.inst, bs, reps, &us[k]))) return rc;
-            if (best < 0 || us[k] < us[best]) best = k;
+        for (int f = 0; f < 2; ++f) {
+            for (int k = 0; k < FG_TUNE_CANDIDATES; ++k) us[f][k] = -1.0;
+            int err;
+            if (!set_format(c, f, err)) {
+                if (err) return err;
+                continue;
+            }
+            for (int k = 0; k < FG_TUNE_CANDIDATES; ++k) {
+                if (k > 0 && kTuneTZ[k] > maxnz) continue;  // same shapes as a smaller candidate
+                for (int i : c.inst)
+                    if ((rc = set_tile_locked(ops[i], depth(ops[i], kTuneTZ[k])))) return rc;
+                if ((rc = time_batched_apply(ops, c.inst, bs, reps, &us[f][k]))) return rc;
+                if (best_k < 0 || us[f][k] < us[best_f][best_k]) {
+                    best_f = f;
+                    best_k = k;
+                }
+            }
         }
+        int err;
+        if (!set_format(c, best_f, err)) return err ? err : fail(FG_CUDA_ERROR, "autotune: format lost");
         for (int i : c.inst) {
-            if ((rc = set_tile_locked(ops[i], depth(ops[i], kTuneTZ[best]))) || (rc = ensure_fp32(ops[i])))
+            if ((rc = set_tile_locked(ops[i], depth(ops[i], kTuneTZ[best_k]))) || (rc = ensure_fp32(ops[i])))
                 return rc;
             CK(cudaStreamSynchronize(ops[i]->stream));
         }
@@ -2110,9 +2148,12 @@ FG_API int fg_batch_autotune(fg_op *const *ops, int n, int reps, fg_tune_entry *
             e.kind = c.kind;
             e.size_class = c.sc;
             e.instances = (int)c.inst.size();
-            e.tz = kTuneTZ[best];
-            e.format = c.fmt;
-            for (int k = 0; k < FG_TUNE_CANDIDATES; ++k) e.us[k] = us[k];
+            e.tz = kTuneTZ[best_k];
+            e.format = best_f;
+            for (int k = 0; k < FG_TUNE_CANDIDATES; ++k) {
+                e.us[k] = us[best_f][k];
+                e.us_other[k] = us[1 - best_f][k];
+            }
         }
         ++count;
     }

@@ -74,7 +74,8 @@ TUNE_TZ = (1, 2, 4, 8, 16)
 
 class FgTuneEntry(C.Structure):
     _fields_ = [("order", C.c_int32), ("kind", C.c_int32), ("format", C.c_int32), ("size_class", C.c_int32),
-                ("instances", C.c_int32), ("tz", C.c_int32), ("us", C.c_double * len(TUNE_TZ))]
+                ("instances", C.c_int32), ("tz", C.c_int32), ("us", C.c_double * len(TUNE_TZ)),
+                ("us_other", C.c_double * len(TUNE_TZ))]
 
 
 class FgResult(C.Structure):
@@ -555,16 +556,19 @@ def batch_pcg(ops, bs, xs, cfg=None, precond=PC_CHEBYSHEV):
 
 
 def batch_autotune(ops, reps=5):
-    """Choose each batch class's item depth TZ by timing the batched FP32 apply
-    (fg_batch_autotune); the choice stays on the operators.  Returns one dict
-    per (order, kind, format, size class)."""
+    """Choose each batch class's quadrature-data format and item depth TZ by
+    timing the batched FP32 apply (fg_batch_autotune); the choice stays on the
+    operators.  Returns one dict per (order, kind, size class): ``format`` and
+    ``tz`` chosen, ``us`` the times per TZ in that format, ``us_other`` in the
+    other format (None: not tried)."""
     n = len(ops)
     hs = (C.c_void_p * n)(*[o.handle for o in ops])
     out = (FgTuneEntry * 64)()
     cnt = C.c_int()
     _check(lib().fg_batch_autotune(hs, n, int(reps), out, 64, C.byref(cnt)))
     return [dict(order=e.order, kind=e.kind, format=e.format, size_class=e.size_class, instances=e.instances,
-                 tz=e.tz, us={tz: (e.us[k] if e.us[k] >= 0 else None) for k, tz in enumerate(TUNE_TZ)})
+                 tz=e.tz, us={tz: (e.us[k] if e.us[k] >= 0 else None) for k, tz in enumerate(TUNE_TZ)},
+                 us_other={tz: (e.us_other[k] if e.us_other[k] >= 0 else None) for k, tz in enumerate(TUNE_TZ)})
             for e in out[:min(cnt.value, 64)]]
 
 

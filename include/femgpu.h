@@ -366,18 +366,24 @@ FG_API int fg_op_tile(const fg_op *op, int dims[3]);
 
 #define FG_TUNE_CANDIDATES 5 /* TZ = 1, 2, 4, 8, 16 */
 typedef struct {
-    int32_t order, kind, format;
+    int32_t order, kind;
+    int32_t format;      /* chosen quadrature-data format (FG_QDATA_FULL / FG_QDATA_AFFINE) */
     int32_t size_class;  /* 0: <= 16^3 elements, 1: <= 32^3, 2: larger */
     int32_t instances;   /* batch members in the class */
     int32_t tz;          /* chosen layers per item */
-    double us[FG_TUNE_CANDIDATES]; /* batched FP32 apply time per candidate, -1 = not tried */
+    double us[FG_TUNE_CANDIDATES];       /* batched FP32 apply time per TZ candidate in the chosen
+                                            format, -1 = not tried */
+    double us_other[FG_TUNE_CANDIDATES]; /* the same in the other format (-1: not tried, or the
+                                            affine format refused by a member's geometry) */
 } fg_tune_entry;
-/* Autotuner for fg_batch_pcg: instances are grouped by (order, kind, qdata
- * format, size class); for each group every candidate TZ (clamped per
- * instance to the largest power of two <= nz) is applied to all members, the
- * group's batched FP32 apply (one launch + fix-up) is timed over `reps`
- * launches with CUDA events, and the fastest is kept on the operators.
- * Results per group in out[0 .. min(*n_out, max_out)). */
+/* Autotuner for fg_batch_pcg: instances are grouped by (order, kind, size
+ * class); for each group every candidate (quadrature-data format, TZ) -- the
+ * affine format only when every member's elements have constant Jacobians;
+ * TZ clamped per instance to the largest power of two <= nz -- is applied to
+ * all members, the group's batched FP32 apply (one launch + fix-up) is timed
+ * over `reps` launches with CUDA events, and the fastest pair is kept on the
+ * operators (the FP64 reliable-update applies of the mixed solve use the same
+ * format).  Results per group in out[0 .. min(*n_out, max_out)). */
 FG_API int fg_batch_autotune(fg_op *const *ops, int n, int reps, fg_tune_entry *out, int max_out,
                              int *n_out);
 

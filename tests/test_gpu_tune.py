@@ -87,7 +87,11 @@ def test_autotune_then_batch_solve():
     assert sum(e["instances"] for e in table) == len(ops)
     for e in table:
         tried = {tz: t for tz, t in e["us"].items() if t is not None}
+        other = [t for t in e["us_other"].items() if t[1] is not None]
         assert e["tz"] in tried and tried[e["tz"]] == min(tried.values())
+        assert not other or tried[e["tz"]] <= min(t for _, t in other)
+        assert e["format"] in (femgpu.QDATA_FULL, femgpu.QDATA_AFFINE)
+        assert other  # box meshes: both formats were timed
     for op in ops:
         assert op.tile[2] in femgpu.TUNE_TZ
     xs = [np.zeros_like(b) for b in bs]
@@ -96,3 +100,44 @@ def test_autotune_then_batch_solve():
     for x, xs1, r in zip(xs, singles, res):
         assert r.true_residual <= 1e-8
         assert rel(x, xs1) <= 1e-7
+
+
+def test_autotune_keeps_full_format_when_a_member_is_not_affine():
+    """A class with one distorted mesh (a moved interior vertex): the affine
+    candidate is refused for the whole class, the tuner keeps the full format
+    there and the batched solve still matches the single solves; an all-box
+    class of another order may still move to the affine format."""
+    need_gpu()
+    rng = np.random.default_rng(5)
+    cfg = femgpu.SolverConfig(rtol=1e-8, max_iter=5000, precision=femgpu.FP32_IR, check_interval=5)
+    ops, bs, singles = [], [], []
+    for i, (n, p, distort) in enumerate([(8, 2, False), (9, 2, True), (10, 1, False), (7, 1, False)]):
+        mesh = (n, n, n)
+        if distort:
+            k, j, ii = np.meshgrid(np.arange(n + 1), np.arange(n + 1), np.arange(n + 1), indexing="ij")
+            v = np.stack([ii / n, j / n, k / n], axis=-1).astype(np.float64)
+            v[n // 2, n // 2, n // 2] += 0.3 / n
+            mesh = dict(nx=n, ny=n, nz=n, vcoord=v.reshape(-1, 3))
+        op = femgpu.PADiffusionOperator(mesh, p, kappa=lognormal_kappa_q(n, n, n, p, seed=500 + i))
+        b = rng.standard_normal(op.n_dofs())
+        b3 = b.reshape(op.NK, op.NJ, op.NI)
+        b3[[0, -1]], b3[:, [0, -1]], b3[:, :, [0, -1]] = 0.0, 0.0, 0.0
+        x = np.zeros_like(b)
+        assert op.pcg(b, x, cfg, femgpu.PC_CHEBYSHEV).converged
+        ops.append(op)
+        bs.append(b)
+        singles.append(x)
+    table = femgpu.batch_autotune(ops, reps=2)
+    q2 = [e for e in table if e["order"] == 2]
+    assert len(q2) == 1 and q2[0]["format"] == femgpu.QDATA_FULL
+    assert all(t is None for t in q2[0]["us_other"].values())
+    q1 = [e for e in table if e["order"] == 1]
+    assert q1 and all(any(t is not None for t in e["us_other"].values()) for e in q1)
+    xs = [np.zeros_like(b) for b in bs]
+    ok, res = femgpu.batch_pcg(ops, bs, xs, cfg, femgpu.PC_CHEBYSHEV)
+    assert ok
+    for x, x1, r in zip(xs, singles, res):
+        assert r.true_residual <= 1e-8
+        assert rel(x, x1) <= 1e-7
+    for op in ops:
+        op.close()
