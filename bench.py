@@ -490,6 +490,47 @@ def run_heat(rank, steps, stream):
     return summary, detail
 
 
+def measure_pcie(nbytes, dev, reps=5):
+    """Pinned host <-> device copy bandwidth (GB/s) for buffers of `nbytes`:
+    host-to-device alone, device-to-host alone, and both at once on two
+    streams (total bytes of both directions / time), CUDA events."""
+    import torch
+
+    n = nbytes // 8
+    hs = torch.empty(n, dtype=torch.float64).pin_memory()
+    hd = torch.empty(n, dtype=torch.float64).pin_memory()
+    d_in = torch.empty(n, dtype=torch.float64, device=dev)
+    d_out = torch.zeros(n, dtype=torch.float64, device=dev)
+    s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def timed(fn_list):
+        for _ in range(2):
+            for st, fn in fn_list:
+                with torch.cuda.stream(st):
+                    fn()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in fn_list]
+        start = torch.cuda.Event(enable_timing=True)
+        start.record(fn_list[0][0])
+        for (st, fn), (a, b) in zip(fn_list, ev):
+            st.wait_event(start)
+            a.record(st)
+            with torch.cuda.stream(st):
+                for _ in range(reps):
+                    fn()
+            b.record(st)
+        torch.cuda.synchronize()
+        return max(start.elapsed_time(b) for _, b in ev) / 1e3
+
+    h2d = lambda: d_in.copy_(hs, non_blocking=True)
+    d2h = lambda: hd.copy_(d_out, non_blocking=True)
+    t_h = timed([(s1, h2d)])
+    t_d = timed([(s2, d2h)])
+    t_b = timed([(s1, h2d), (s2, d2h)])
+    return {"h2d_gbs": round(nbytes * reps / t_h / 1e9, 2), "d2h_gbs": round(nbytes * reps / t_d / 1e9, 2),
+            "both_directions_gbs": round(2 * nbytes * reps / t_b / 1e9, 2), "bytes": int(nbytes)}
+
+
 def run_batch(rank, batch_n, dev):
     """256 uneven solves, n ~ U{8..48}, p ~ U{1,2,3}, own lognormal kappa
     (sigma2 ~ U[0.25,2], ell ~ U[0.05,0.3]) and RHS M xi, FP32 mixed precision.
@@ -881,6 +922,9 @@ def main():
     te_ms = max_over_ranks(f0.elapsed_time(f1), world, dev)
     e2e_val = whole_job_gdofs(world, N, k_e2e, te_ms)
     _ = float(yh[0])
+    # the PCIe ceiling of the e2e step: N doubles each way, both directions at once
+    pcie = measure_pcie(N * 8, dev)
+    e2e_ideal_ms = 2 * N * 8 / (pcie["both_directions_gbs"] * 1e9) * 1e3
 
     detail = {}
     variants = time_apply_variants(op, n, p, x, args.steps, peak, stream)
@@ -950,7 +994,8 @@ def main():
                          "frac_no_map": bytes_nomap / per_apply_s / 1e9 / peak,
                          "kernel": "pa_apply_kernel + fixup_kernel (timed together per apply)"},
             "e2e": {"value": e2e_val, "unit": "GDOF/s", "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
-                    "steps": k_e2e},
+                    "steps": k_e2e, "ms_per_step": te_ms / k_e2e, "pcie": pcie,
+                    "pcie_bound_ms": e2e_ideal_ms, "frac_of_pcie": e2e_ideal_ms / (te_ms / k_e2e)},
             "gpu_launches": launches_per_apply * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
