@@ -743,6 +743,16 @@ template <typename T> static int stage_of(fg_op *op, T **st) {
     *st = reinterpret_cast<T *>(op->stage);
     return FG_OK;
 }
+// rows x w values between pitches sp and dp (elements) on `s`, by k_repitch
+template <typename T>
+static int repitch(const T *src, int64_t sp, T *dst, int64_t dp, int w, int64_t rows, cudaStream_t s) {
+    if (rows <= 0) return FG_OK;
+    const int64_t blocks = std::min<int64_t>((rows + 7) / 8, 148 * 16);
+    k_repitch<T><<<(unsigned)blocks, 256, 0, s>>>(src, sp, dst, dp, w, rows);
+    CK(cudaGetLastError());
+    return FG_OK;
+}
+
 template <typename T> static int to_native_t(fg_op *op, T *dst, const T *src, int mem) {
     const Grid &g = op->g;
     if (mem == FG_HOST) {
@@ -752,9 +762,7 @@ template <typename T> static int to_native_t(fg_op *op, T *dst, const T *src, in
         CK(cudaMemcpyAsync(st, src, sizeof(T) * op->N, cudaMemcpyHostToDevice, op->stream));
         src = st;
     }
-    CK(cudaMemcpy2DAsync(dst, sizeof(T) * g.NIp, src, sizeof(T) * g.NI, sizeof(T) * g.NI,
-                         (size_t)g.NJ * g.NK, cudaMemcpyDeviceToDevice, op->stream));
-    return FG_OK;
+    return repitch<T>(src, g.NI, dst, g.NIp, g.NI, (int64_t)g.NJ * g.NK, op->stream);
 }
 template <typename T> static int from_native_t(fg_op *op, T *dst, const T *src, int mem) {
     const Grid &g = op->g;
@@ -763,8 +771,8 @@ template <typename T> static int from_native_t(fg_op *op, T *dst, const T *src, 
         int rc = stage_of(op, &out);
         if (rc) return rc;
     }
-    CK(cudaMemcpy2DAsync(out, sizeof(T) * g.NI, src, sizeof(T) * g.NIp, sizeof(T) * g.NI,
-                         (size_t)g.NJ * g.NK, cudaMemcpyDeviceToDevice, op->stream));
+    int rc;
+    if ((rc = repitch<T>(src, g.NIp, out, g.NI, g.NI, (int64_t)g.NJ * g.NK, op->stream))) return rc;
     if (mem == FG_HOST)
         CK(cudaMemcpyAsync(dst, out, sizeof(T) * op->N, cudaMemcpyDeviceToHost, op->stream));
     return FG_OK;
@@ -790,7 +798,12 @@ static int from_native(fg_op *op, double *dst, const double *src, int mem) {
 static int apply_host_pipelined(fg_op *op, const double *x, double *y, int constrained) {
     Grid g = op->g;
     g.ess = constrained ? op->ess_tags : 0;
-    const int R = std::min(g.ntz, 16);
+    static const int max_ranges = [] {  // FG_PIPE_RANGES: z ranges of the pipeline (default 16)
+        const char *e = std::getenv("FG_PIPE_RANGES");
+        const int v = e ? std::atoi(e) : 16;
+        return v >= 1 && v <= 256 ? v : 16;
+    }();
+    const int R = std::min(g.ntz, max_ranges);
     double *st = nullptr;
     int rc = stage_of(op, &st);
     if (rc) return rc;
@@ -807,7 +820,6 @@ static int apply_host_pipelined(fg_op *op, const double *x, double *y, int const
     }
     const int SZe = g.TZ * g.p;
     const int64_t plane = (int64_t)g.NI * g.NJ;  // plain values per DOF plane
-    const size_t sp = sizeof(double) * g.NIp, spl = sizeof(double) * g.NI;
     std::vector<int> t0(R + 1), A(R + 1);
     for (int r = 0; r <= R; ++r) t0[r] = (int)((int64_t)g.ntz * r / R);
     for (int r = 0; r < R; ++r) A[r] = t0[r] * SZe;
@@ -825,8 +837,9 @@ static int apply_host_pipelined(fg_op *op, const double *x, double *y, int const
     for (int r = 0; r < R; ++r) {
         const int lo = r == 0 ? 0 : A[r] + 1, hi = A[r + 1] + 1;
         CK(cudaStreamWaitEvent(op->stream, op->ev_in[r], 0));
-        CK(cudaMemcpy2DAsync(op->xs + (int64_t)lo * g.NJ * g.NIp, sp, st + lo * plane, spl, spl,
-                             (size_t)g.NJ * (hi - lo), cudaMemcpyDeviceToDevice, op->stream));
+        if ((rc = repitch<double>(st + lo * plane, g.NI, op->xs + (int64_t)lo * g.NJ * g.NIp, g.NIp, g.NI,
+                                  (int64_t)g.NJ * (hi - lo), op->stream)))
+            return rc;
         const int i0 = t0[r] * items_per_layer, ni = (t0[r + 1] - t0[r]) * items_per_layer;
         switch (op->p) {
         case 1: rc = launch_apply_p<1, double>(op, g, op->qd, op->face, op->xs, op->ys, 0, nullptr, nullptr, i0, ni); break;
@@ -849,8 +862,9 @@ static int apply_host_pipelined(fg_op *op, const double *x, double *y, int const
             fixup_range_kernel<double><<<rows, 128, 0, op->stream>>>(g, op->ys, op->face, Ka, Kb, pl0);
             CK(cudaGetLastError());
         }
-        CK(cudaMemcpy2DAsync(st + Ka * plane, spl, op->ys + (int64_t)Ka * g.NJ * g.NIp, sp, spl,
-                             (size_t)g.NJ * (Kb - Ka), cudaMemcpyDeviceToDevice, op->stream));
+        if ((rc = repitch<double>(op->ys + (int64_t)Ka * g.NJ * g.NIp, g.NIp, st + Ka * plane, g.NI, g.NI,
+                                  (int64_t)g.NJ * (Kb - Ka), op->stream)))
+            return rc;
         CK(cudaEventRecord(op->ev_out[r], op->stream));
         CK(cudaStreamWaitEvent(op->s_out, op->ev_out[r], 0));
         CK(cudaMemcpyAsync(y + Ka * plane, st + Ka * plane, sizeof(double) * plane * (Kb - Ka),

@@ -663,6 +663,23 @@ __global__ void __launch_bounds__(VEC_THREADS) k_to_f32(int64_t n, const double 
     FG_VEC_LOOP(i, n) b[i] = (float)a[i];
 }
 
+// Rows of `w` values from a layout of row pitch `sp` to one of pitch `dp` (the
+// plain <-> padded native layouts): one warp per row, lanes across the row.
+// On the SMs, so that the copy engines stay free for the PCIe transfers of a
+// host-memory apply.
+template <typename T>
+__global__ void __launch_bounds__(256) k_repitch(const T *__restrict__ src, int64_t sp, T *__restrict__ dst,
+                                                 int64_t dp, int w, int64_t rows) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = wid; r < rows; r += nw) {
+        const T *s = src + r * sp;
+        T *d = dst + r * dp;
+        for (int c = lane; c < w; c += 32) d[c] = __ldg(s + c);
+    }
+}
+
 // ---- mixed-precision PCG with reliable updates -----------------------------
 // FP32 iterates (x_lo: correction since the last update, r_lo, p, z), FP64
 // solution x and FP64 dot products.  When ||r_lo|| has dropped by `delta`
