@@ -206,7 +206,9 @@ FG_API int fg_op_set_stream(fg_op *op, void *stream);
  * PCIe rate.  With host vectors, accumulate = 0 and more than one layer of
  * work items in z, the call is pipelined over z ranges: the upload of the
  * next range's DOF planes, the apply of this range and the download of the
- * planes it finished run at the same time (the same sums as one launch). */
+ * planes it finished run at the same time (the same sums as one launch).
+ * Environment: FG_PIPELINED_APPLY=0 selects the serial form; FG_PIPE_RANGES
+ * sets the number of z ranges (default 16, capped by the item layers). */
 FG_API int fg_op_apply(fg_op *op, const double *x, double *y, int accumulate, int constrained,
                        int mem);
 
