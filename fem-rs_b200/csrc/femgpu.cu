@@ -149,6 +149,37 @@ static int ensure_tables(int dev) {
     CK(cudaMemcpyToSymbol(c_GB32, GB, sizeof GB));
     CK(cudaMemcpyToSymbol(c_BG32, BG, sizeof BG));
     CK(cudaMemcpyToSymbol(c_BB32, BB, sizeof BB));
+    // Dq = G B^-1 per order (B inverted by Gauss-Jordan with partial pivoting, in FP64)
+    float DQ[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {};
+    for (int p = 1; p <= FG_MAXP; ++p) {
+        const int n = p + 1;
+        double a[4][8] = {};
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                a[i][j] = B[p - 1][i][j];
+                a[i][n + j] = i == j ? 1.0 : 0.0;
+            }
+        for (int c = 0; c < n; ++c) {
+            int piv = c;
+            for (int r = c + 1; r < n; ++r)
+                if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+            for (int j = 0; j < 2 * n; ++j) std::swap(a[c][j], a[piv][j]);
+            const double d = a[c][c];
+            for (int j = 0; j < 2 * n; ++j) a[c][j] /= d;
+            for (int r = 0; r < n; ++r)
+                if (r != c) {
+                    const double f = a[r][c];
+                    for (int j = 0; j < 2 * n; ++j) a[r][j] -= f * a[c][j];
+                }
+        }
+        for (int q = 0; q < n; ++q)
+            for (int k = 0; k < n; ++k) {
+                double v = 0.0;
+                for (int d = 0; d < n; ++d) v += G[p - 1][q][d] * a[d][n + k];
+                DQ[p - 1][q][k] = (float)v;
+            }
+    }
+    CK(cudaMemcpyToSymbol(c_DQ32, DQ, sizeof DQ));
     g_tables_ready[dev] = true;
     return FG_OK;
 }
@@ -336,7 +367,10 @@ template <> struct KCfg32<1> { static constexpr int WY = 4, S = 6, MINB = 4; };
 #ifndef FG_F32_Q2_S  // FP32 Q2 full-format qdata ring depth (stages of one quadrature column per warp)
 #define FG_F32_Q2_S 4
 #endif
-template <> struct KCfg32<2> { static constexpr int WY = 4, S = FG_F32_Q2_S, MINB = 3; };
+#ifndef FG_F32_Q2_MINB  // FP32 Q2 CTAs/SM hint
+#define FG_F32_Q2_MINB 3
+#endif
+template <> struct KCfg32<2> { static constexpr int WY = 4, S = FG_F32_Q2_S, MINB = FG_F32_Q2_MINB; };
 #ifndef FG_F32_Q3_S  // FP32 Q3 qdata ring depth and CTAs/SM hint
 #define FG_F32_Q3_S 3
 #endif
@@ -344,6 +378,20 @@ template <> struct KCfg32<2> { static constexpr int WY = 4, S = FG_F32_Q2_S, MIN
 #define FG_F32_Q3_MINB 2
 #endif
 template <> struct KCfg32<3> { static constexpr int WY = FG_Q3_WY, S = FG_F32_Q3_S, MINB = FG_F32_Q3_MINB; };
+#ifndef FG_F32_Q2_AS  // FP32 Q2 affine-format qdata ring depth (stages of one element layer per warp)
+#define FG_F32_Q2_AS 1
+#endif
+#ifndef FG_F32_Q2_AMINB  // FP32 Q2 affine-format CTAs/SM hint (the 1-deep ring leaves room for 5)
+#define FG_F32_Q2_AMINB 5
+#endif
+// ring depth of the affine format: one element layer per stage
+template <int P, typename T> constexpr int affine_stages() {
+    return (P == 2 && std::is_same<T, float>::value) ? FG_F32_Q2_AS : 2;
+}
+// CTAs/SM hint of an apply kernel
+template <int P, typename T, int FMT, int MINB> constexpr int apply_minb() {
+    return (FMT == 1 && P == 2 && std::is_same<T, float>::value) ? FG_F32_Q2_AMINB : MINB;
+}
 template <int P, typename T> struct KC;
 template <int P> struct KC<P, double> : KCfg<P> {};
 template <int P> struct KC<P, float> : KCfg32<P> {};
@@ -358,12 +406,12 @@ static int launch_apply_t(fg_op *op, const Grid &g, const T *qd, T *face, const 
                           int nitems = -1) {
     using C = KC<P, T>;
     static_assert(C::WY == KCfg<P>::WY, "FP32 and FP64 share the item tiling");
-    constexpr int S = FMT == 0 ? C::S : 2;  // affine format: one element layer per stage
+    constexpr int S = FMT == 0 ? C::S : affine_stages<P, T>();  // affine format: one element layer per stage
     using SM = ApplySmem<P, T, C::WY, S, stage_elems<P, OPK, FMT>() / 32>;
     // per device, set once; handles on several host threads may race here, and
     // setting the same attribute twice is harmless
     static std::atomic<bool> attr_set[64];
-    auto kern = pa_apply_kernel<P, OPK, T, C::WY, S, C::MINB, FMT>;
+    auto kern = pa_apply_kernel<P, OPK, T, C::WY, S, apply_minb<P, T, FMT, C::MINB>(), FMT>;
     if (!attr_set[op->device].load(std::memory_order_acquire)) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes));
         attr_set[op->device].store(true, std::memory_order_release);
@@ -1832,7 +1880,7 @@ static int pcg_core(fg_op *op, const fg_cfg &cfg, fg_result *res) {
 template <int P, typename T, int FMT>
 static int encode_xmap_t(const Grid &g, const T *x, CUtensorMap *tmap) {
     using C = KC<P, T>;
-    constexpr int S = FMT == 0 ? C::S : 2;
+    constexpr int S = FMT == 0 ? C::S : affine_stages<P, T>();
     using SM = ApplySmem<P, T, C::WY, S, 1>;
     cuuint64_t gdim[3] = {(cuuint64_t)g.NI, (cuuint64_t)g.NJ, (cuuint64_t)g.NK};
     cuuint64_t gstr[2] = {(cuuint64_t)g.NIp * sizeof(T), (cuuint64_t)g.NIp * g.NJ * sizeof(T)};
@@ -1863,9 +1911,9 @@ template <int P, int OPK, typename T, int FMT>
 static int launch_batched_t(cudaStream_t st, const BatchGroup &G, const ApplyArgs<T> *args,
                             const CUtensorMap *tm, int nslots, int slot) {
     using C = KC<P, T>;
-    constexpr int S = FMT == 0 ? C::S : 2;
+    constexpr int S = FMT == 0 ? C::S : affine_stages<P, T>();
     using SM = ApplySmem<P, T, C::WY, S, stage_elems<P, OPK, FMT>() / 32>;
-    auto kern = pa_apply_batched_kernel<P, OPK, T, C::WY, S, C::MINB, FMT>;
+    auto kern = pa_apply_batched_kernel<P, OPK, T, C::WY, S, apply_minb<P, T, FMT, C::MINB>(), FMT>;
     static std::atomic<bool> attr_set[64];
     int dev = 0;
     CK(cudaGetDevice(&dev));

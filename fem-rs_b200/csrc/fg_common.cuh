@@ -36,6 +36,9 @@ __constant__ float c_G32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 __constant__ float2 c_GB32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 __constant__ float2 c_BG32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 __constant__ float2 c_BB32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
+// collocated derivative at the Gauss points, Dq = G B^-1: the derivative at
+// point q of the degree-p polynomial through the values at the p+1 points
+__constant__ float c_DQ32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 
 template <typename T> struct Tab;
 template <> struct Tab<double> {
@@ -45,6 +48,7 @@ template <> struct Tab<double> {
 template <> struct Tab<float> {
     static __device__ __forceinline__ float B(int p, int q, int d) { return c_B32[p - 1][q][d]; }
     static __device__ __forceinline__ float G(int p, int q, int d) { return c_G32[p - 1][q][d]; }
+    static __device__ __forceinline__ float DQ(int p, int q, int k) { return c_DQ32[p - 1][q][k]; }
 };
 
 __host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
