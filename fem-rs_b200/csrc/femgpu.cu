@@ -151,6 +151,7 @@ static int ensure_tables(int dev) {
     CK(cudaMemcpyToSymbol(c_BB32, BB, sizeof BB));
     // Dq = G B^-1 per order (B inverted by Gauss-Jordan with partial pivoting, in FP64)
     float DQ[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {};
+    double DQd[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1] = {};
     for (int p = 1; p <= FG_MAXP; ++p) {
         const int n = p + 1;
         double a[4][8] = {};
@@ -177,9 +178,11 @@ static int ensure_tables(int dev) {
                 double v = 0.0;
                 for (int d = 0; d < n; ++d) v += G[p - 1][q][d] * a[d][n + k];
                 DQ[p - 1][q][k] = (float)v;
+                DQd[p - 1][q][k] = v;
             }
     }
     CK(cudaMemcpyToSymbol(c_DQ32, DQ, sizeof DQ));
+    CK(cudaMemcpyToSymbol(c_DQ64, DQd, sizeof DQd));
     g_tables_ready[dev] = true;
     return FG_OK;
 }

@@ -39,11 +39,13 @@ __constant__ float2 c_BB32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 // collocated derivative at the Gauss points, Dq = G B^-1: the derivative at
 // point q of the degree-p polynomial through the values at the p+1 points
 __constant__ float c_DQ32[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
+__constant__ double c_DQ64[FG_MAXP][FG_MAXP + 1][FG_MAXP + 1];
 
 template <typename T> struct Tab;
 template <> struct Tab<double> {
     static __device__ __forceinline__ double B(int p, int q, int d) { return c_B64[p - 1][q][d]; }
     static __device__ __forceinline__ double G(int p, int q, int d) { return c_G64[p - 1][q][d]; }
+    static __device__ __forceinline__ double DQ(int p, int q, int k) { return c_DQ64[p - 1][q][k]; }
 };
 template <> struct Tab<float> {
     static __device__ __forceinline__ float B(int p, int q, int d) { return c_B32[p - 1][q][d]; }

@@ -43,6 +43,9 @@
 #ifndef FG_F32_Q2_COLLOC  // FP32 Q2 diffusion: collocated-gradient form (1) or packed sum factorisation (0)
 #define FG_F32_Q2_COLLOC 1
 #endif
+#ifndef FG_F64_Q2A_COLLOC  // FP64 Q2 affine-format diffusion: collocated-gradient form (1) or sum factorisation (0)
+#define FG_F64_Q2A_COLLOC 1
+#endif
 #ifndef FG_F32_Q3_COLLOC  // FP32 Q3 affine-format diffusion: collocated-gradient form (1) or sum factorisation (0)
 #define FG_F32_Q3_COLLOC 1
 #endif
@@ -311,9 +314,10 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                                                   xb * SM::XB);
 
         T out[D][D][D];
-        if constexpr (std::is_same<T, float>::value && HK &&
-                      ((P == 2 && FG_F32_Q2_COLLOC) || (P == 3 && FMT == 1 && FG_F32_Q3_COLLOC))) {
-            // FP32 Q2 / Q3-affine diffusion (+ mass), collocated form: the element values are
+        if constexpr (HK && ((std::is_same<T, float>::value &&
+                               ((P == 2 && FG_F32_Q2_COLLOC) || (P == 3 && FMT == 1 && FG_F32_Q3_COLLOC))) ||
+                              (std::is_same<T, double>::value && P == 2 && FMT == 1 && FG_F64_Q2A_COLLOC))) {
+            // FP32 Q2 / Q3-affine and FP64 Q2-affine diffusion (+ mass), collocated form: the element values are
             // interpolated to the Gauss points (uq = (B x B x B) u), the gradient
             // at a point is the collocated derivative Dq = G B^-1 along the
             // point's three lines of uq, D is applied per point, the transposed
@@ -323,41 +327,41 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
             // 54 live values instead of 81; Q3 3648 instead of ~5700 FMAs with 128
             // live values (faster than the slab form on the affine format, slower
             // on the full format, where the slab form's smaller state wins).
-            using TBf = Tab<float>;
-            float uq[Q][Q][Q];  // [qz][qy][qx]
+            using TBf = Tab<T>;
+            T uq[Q][Q][Q];  // [qz][qy][qx]
             {
-                float u[D][D][D];
+                T u[D][D][D];
 #pragma unroll
                 for (int c = 0; c < D; ++c)
 #pragma unroll
                     for (int b = 0; b < D; ++b)
 #pragma unroll
                         for (int a = 0; a < D; ++a) {
-                            const float v = xt[(c * RY + warp * P + b) * XW + lane * P + a];
+                            const T v = xt[(c * RY + warp * P + b) * XW + lane * P + a];
                             const bool e = (a == 0 && fx0) || (a == P && fx1) || (b == 0 && fy0) ||
                                            (b == P && fy1) || (c == 0 && fz0) || (c == P && fz1);
-                            u[c][b][a] = e ? 0.f : v;
+                            u[c][b][a] = e ? T(0) : v;
                         }
-                float t1[D][D][Q];  // [c][b][qx]
+                T t1[D][D][Q];  // [c][b][qx]
 #pragma unroll
                 for (int c = 0; c < D; ++c)
 #pragma unroll
                     for (int b = 0; b < D; ++b)
 #pragma unroll
                         for (int qx = 0; qx < Q; ++qx) {
-                            float s0 = 0.f;
+                            T s0 = T(0);
 #pragma unroll
                             for (int a = 0; a < D; ++a) s0 += TBf::B(P, qx, a) * u[c][b][a];
                             t1[c][b][qx] = s0;
                         }
-                float t2[D][Q][Q];  // [c][qy][qx]
+                T t2[D][Q][Q];  // [c][qy][qx]
 #pragma unroll
                 for (int c = 0; c < D; ++c)
 #pragma unroll
                     for (int qy = 0; qy < Q; ++qy)
 #pragma unroll
                         for (int qx = 0; qx < Q; ++qx) {
-                            float s0 = 0.f;
+                            T s0 = T(0);
 #pragma unroll
                             for (int b = 0; b < D; ++b) s0 += TBf::B(P, qy, b) * t1[c][b][qx];
                             t2[c][qy][qx] = s0;
@@ -368,20 +372,20 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     for (int qy = 0; qy < Q; ++qy)
 #pragma unroll
                         for (int qx = 0; qx < Q; ++qx) {
-                            float s0 = 0.f;
+                            T s0 = T(0);
 #pragma unroll
                             for (int c = 0; c < D; ++c) s0 += TBf::B(P, qz, c) * t2[c][qy][qx];
                             uq[qz][qy][qx] = s0;
                         }
             }
-            float w[Q][Q][Q];
+            T w[Q][Q][Q];
 #pragma unroll
             for (int qz = 0; qz < Q; ++qz)
 #pragma unroll
                 for (int qy = 0; qy < Q; ++qy)
 #pragma unroll
-                    for (int qx = 0; qx < Q; ++qx) w[qz][qy][qx] = 0.f;
-            float Ge[6] = {0, 0, 0, 0, 0, 0};
+                    for (int qx = 0; qx < Q; ++qx) w[qz][qy][qx] = T(0);
+            T Ge[6] = {0, 0, 0, 0, 0, 0};
             const T *ql = nullptr;
             if (FMT == 1) {
                 const int j = lz, s = j % S;
@@ -401,25 +405,25 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     const T *qc = FMT == 0 ? qsw + s * STAGE : ql;
 #pragma unroll
                     for (int qz = 0; qz < Q; ++qz) {
-                        float gx = 0.f, gy = 0.f, gz = 0.f;
+                        T gx = T(0), gy = T(0), gz = T(0);
 #pragma unroll
                         for (int k = 0; k < Q; ++k) {
                             gx += TBf::DQ(P, qx, k) * uq[qz][qy][k];
                             gy += TBf::DQ(P, qy, k) * uq[qz][k][qx];
                             gz += TBf::DQ(P, qz, k) * uq[k][qy][qx];
                         }
-                        float vx, vy, vz, vu = 0.f;
+                        T vx, vy, vz, vu = T(0);
                         if (FMT == 0) {
                             const T *qq = qc + qz * (NC * 32) + lane;
-                            const float d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
+                            const T d0 = qq[0], d1 = qq[32], d2 = qq[64], d3 = qq[96], d4 = qq[128], d5 = qq[160];
                             vx = d0 * gx + d1 * gy + d2 * gz;
                             vy = d1 * gx + d3 * gy + d4 * gz;
                             vz = d2 * gx + d4 * gy + d5 * gz;
                             if (HM) vu = qq[6 * 32] * uq[qz][qy][qx];
                         } else {
                             const T *qq = qc + (NCE + (col * Q + qz) * NCQ) * 32 + lane;
-                            const float sk = qq[0];
-                            const float hx = sk * gx, hy = sk * gy, hz = sk * gz;
+                            const T sk = qq[0];
+                            const T hx = sk * gx, hy = sk * gy, hz = sk * gz;
                             vx = Ge[0] * hx + Ge[1] * hy + Ge[2] * hz;
                             vy = Ge[1] * hx + Ge[3] * hy + Ge[4] * hz;
                             vz = Ge[2] * hx + Ge[4] * hy + Ge[5] * hz;
@@ -454,26 +458,26 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                 }
             }
             {
-                float s1[D][Q][Q];  // [c][qy][qx]
+                T s1[D][Q][Q];  // [c][qy][qx]
 #pragma unroll
                 for (int c = 0; c < D; ++c)
 #pragma unroll
                     for (int qy = 0; qy < Q; ++qy)
 #pragma unroll
                         for (int qx = 0; qx < Q; ++qx) {
-                            float t = 0.f;
+                            T t = T(0);
 #pragma unroll
                             for (int qz = 0; qz < Q; ++qz) t += TBf::B(P, qz, c) * w[qz][qy][qx];
                             s1[c][qy][qx] = t;
                         }
-                float s2[D][D][Q];  // [c][b][qx]
+                T s2[D][D][Q];  // [c][b][qx]
 #pragma unroll
                 for (int c = 0; c < D; ++c)
 #pragma unroll
                     for (int b = 0; b < D; ++b)
 #pragma unroll
                         for (int qx = 0; qx < Q; ++qx) {
-                            float t = 0.f;
+                            T t = T(0);
 #pragma unroll
                             for (int qy = 0; qy < Q; ++qy) t += TBf::B(P, qy, b) * s1[c][qy][qx];
                             s2[c][b][qx] = t;
@@ -484,7 +488,7 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     for (int b = 0; b < D; ++b)
 #pragma unroll
                         for (int a = 0; a < D; ++a) {
-                            float t = 0.f;
+                            T t = T(0);
 #pragma unroll
                             for (int qx = 0; qx < Q; ++qx) t += TBf::B(P, qx, a) * s2[c][b][qx];
                             out[c][b][a] = t;
