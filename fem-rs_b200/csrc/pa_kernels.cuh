@@ -43,6 +43,9 @@
 #ifndef FG_F32_Q2_COLLOC  // FP32 Q2 diffusion: collocated-gradient form (1) or packed sum factorisation (0)
 #define FG_F32_Q2_COLLOC 1
 #endif
+#ifndef FG_Q1_COLLOC  // Q1 diffusion (FP32 both formats, FP64 affine): collocated-gradient form (1) or not (0)
+#define FG_Q1_COLLOC 1
+#endif
 #ifndef FG_F64_Q2A_COLLOC  // FP64 Q2 affine-format diffusion: collocated-gradient form (1) or sum factorisation (0)
 #define FG_F64_Q2A_COLLOC 1
 #endif
@@ -315,8 +318,10 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
 
         T out[D][D][D];
         if constexpr (HK && ((std::is_same<T, float>::value &&
-                               ((P == 2 && FG_F32_Q2_COLLOC) || (P == 3 && FMT == 1 && FG_F32_Q3_COLLOC))) ||
-                              (std::is_same<T, double>::value && P == 2 && FMT == 1 && FG_F64_Q2A_COLLOC))) {
+                               ((P == 1 && FG_Q1_COLLOC) || (P == 2 && FG_F32_Q2_COLLOC) ||
+                                (P == 3 && FMT == 1 && FG_F32_Q3_COLLOC))) ||
+                              (std::is_same<T, double>::value && FMT == 1 &&
+                               ((P == 1 && FG_Q1_COLLOC) || (P == 2 && FG_F64_Q2A_COLLOC))))) {
             // FP32 Q2 / Q3-affine and FP64 Q2-affine diffusion (+ mass), collocated form: the element values are
             // interpolated to the Gauss points (uq = (B x B x B) u), the gradient
             // at a point is the collocated derivative Dq = G B^-1 along the
