@@ -388,8 +388,15 @@ template <> struct KCfg32<3> { static constexpr int WY = FG_Q3_WY, S = FG_F32_Q3
 #define FG_F32_Q2_AMINB 5
 #endif
 // ring depth of the affine format: one element layer per stage
+#ifndef FG_F32_Q3_AS  // FP32 Q3 affine-format qdata ring depth (1: 4 CTAs per SM instead of 3)
+#define FG_F32_Q3_AS 1
+#endif
+#ifndef FG_AFFINE_AS  // affine-format qdata ring depth of the other orders and precisions
+#define FG_AFFINE_AS 2
+#endif
 template <int P, typename T> constexpr int affine_stages() {
-    return (P == 2 && std::is_same<T, float>::value) ? FG_F32_Q2_AS : 2;
+    return std::is_same<T, float>::value ? (P == 2 ? FG_F32_Q2_AS : (P == 3 ? FG_F32_Q3_AS : FG_AFFINE_AS))
+                                         : FG_AFFINE_AS;
 }
 // CTAs/SM hint of an apply kernel
 template <int P, typename T, int FMT, int MINB> constexpr int apply_minb() {
