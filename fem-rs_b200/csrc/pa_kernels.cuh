@@ -43,6 +43,9 @@
 #ifndef FG_F32_Q2_COLLOC  // FP32 Q2 diffusion: collocated-gradient form (1) or packed sum factorisation (0)
 #define FG_F32_Q2_COLLOC 1
 #endif
+#ifndef FG_F32_COLLOC_PACK  // FP32 collocated form: packed pairs in the interpolation passes (1) or scalar (0)
+#define FG_F32_COLLOC_PACK 1
+#endif
 #ifndef FG_Q1_COLLOC  // Q1 diffusion (FP32 both formats, FP64 affine): collocated-gradient form (1) or not (0)
 #define FG_Q1_COLLOC 1
 #endif
@@ -334,7 +337,84 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
             // on the full format, where the slab form's smaller state wins).
             using TBf = Tab<T>;
             T uq[Q][Q][Q];  // [qz][qy][qx]
-            {
+            if constexpr (std::is_same<T, float>::value && FG_F32_COLLOC_PACK) {
+                // x and y passes as packed pairs of DOF planes (c, c+1), loaded
+                // straight into register pairs; the z pass reads the halves in
+                // plane order.  Every lane does the scalar code's FMA in its
+                // order, so the result is the same bit for bit.
+                constexpr int NPC = D / 2;
+                float2 up[NPC][D][D];
+                float us[D][D];
+                auto ld = [&](int c, int b, int a) -> float {
+                    const float v = xt[(c * RY + warp * P + b) * XW + lane * P + a];
+                    const bool e = (a == 0 && fx0) || (a == P && fx1) || (b == 0 && fy0) || (b == P && fy1) ||
+                                   (c == 0 && fz0) || (c == P && fz1);
+                    return e ? 0.f : v;
+                };
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int a = 0; a < D; ++a) {
+#pragma unroll
+                        for (int cp = 0; cp < NPC; ++cp) up[cp][b][a] = make_float2(ld(2 * cp, b, a), ld(2 * cp + 1, b, a));
+                        if (D & 1) us[b][a] = ld(D - 1, b, a);
+                    }
+                float2 t1p[NPC][D][Q];
+                float t1s[D][Q];
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+#pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+#pragma unroll
+                        for (int cp = 0; cp < NPC; ++cp) {
+                            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int a = 0; a < D; ++a) acc = __ffma2_rn(c_BB32[P - 1][qx][a], up[cp][b][a], acc);
+                            t1p[cp][b][qx] = acc;
+                        }
+                        if (D & 1) {
+                            float s0 = 0.f;
+#pragma unroll
+                            for (int a = 0; a < D; ++a) s0 += TBf::B(P, qx, a) * us[b][a];
+                            t1s[b][qx] = s0;
+                        }
+                    }
+                float2 t2p[NPC][Q][Q];
+                float t2s[Q][Q];
+#pragma unroll
+                for (int qy = 0; qy < Q; ++qy)
+#pragma unroll
+                    for (int qx = 0; qx < Q; ++qx) {
+#pragma unroll
+                        for (int cp = 0; cp < NPC; ++cp) {
+                            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int b = 0; b < D; ++b) acc = __ffma2_rn(c_BB32[P - 1][qy][b], t1p[cp][b][qx], acc);
+                            t2p[cp][qy][qx] = acc;
+                        }
+                        if (D & 1) {
+                            float s0 = 0.f;
+#pragma unroll
+                            for (int b = 0; b < D; ++b) s0 += TBf::B(P, qy, b) * t1s[b][qx];
+                            t2s[qy][qx] = s0;
+                        }
+                    }
+#pragma unroll
+                for (int qz = 0; qz < Q; ++qz)
+#pragma unroll
+                    for (int qy = 0; qy < Q; ++qy)
+#pragma unroll
+                        for (int qx = 0; qx < Q; ++qx) {
+                            float s0 = 0.f;
+#pragma unroll
+                            for (int cp = 0; cp < NPC; ++cp) {
+                                s0 += TBf::B(P, qz, 2 * cp) * t2p[cp][qy][qx].x;
+                                s0 += TBf::B(P, qz, 2 * cp + 1) * t2p[cp][qy][qx].y;
+                            }
+                            if (D & 1) s0 += TBf::B(P, qz, D - 1) * t2s[qy][qx];
+                            uq[qz][qy][qx] = s0;
+                        }
+            } else {
                 T u[D][D][D];
 #pragma unroll
                 for (int c = 0; c < D; ++c)
@@ -383,13 +463,26 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                             uq[qz][qy][qx] = s0;
                         }
             }
+            // point field w: FP32 as pairs of adjacent qx (wp) and the last qx of an
+            // odd Q (ws), so the transposed z and y passes run packed; FP64 plain
+            constexpr int NPX = Q / 2;
             T w[Q][Q][Q];
+            float2 wp[Q][Q][NPX > 0 ? NPX : 1];
+            float ws[Q][Q];
+            auto W = [&](int qz, int qy, int qx) -> T & {
+                if constexpr (std::is_same<T, float>::value && FG_F32_COLLOC_PACK) {
+                    if (qx < 2 * NPX) return (qx & 1) ? wp[qz][qy][qx >> 1].y : wp[qz][qy][qx >> 1].x;
+                    return ws[qz][qy];
+                } else {
+                    return w[qz][qy][qx];
+                }
+            };
 #pragma unroll
             for (int qz = 0; qz < Q; ++qz)
 #pragma unroll
                 for (int qy = 0; qy < Q; ++qy)
 #pragma unroll
-                    for (int qx = 0; qx < Q; ++qx) w[qz][qy][qx] = T(0);
+                    for (int qx = 0; qx < Q; ++qx) W(qz, qy, qx) = T(0);
             T Ge[6] = {0, 0, 0, 0, 0, 0};
             const T *ql = nullptr;
             if (FMT == 1) {
@@ -436,11 +529,11 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                         }
 #pragma unroll
                         for (int k = 0; k < Q; ++k) {
-                            w[qz][qy][k] += TBf::DQ(P, qx, k) * vx;
-                            w[qz][k][qx] += TBf::DQ(P, qy, k) * vy;
-                            w[k][qy][qx] += TBf::DQ(P, qz, k) * vz;
+                            W(qz, qy, k) += TBf::DQ(P, qx, k) * vx;
+                            W(qz, k, qx) += TBf::DQ(P, qy, k) * vy;
+                            W(k, qy, qx) += TBf::DQ(P, qz, k) * vz;
                         }
-                        if (HM) w[qz][qy][qx] += vu;
+                        if (HM) W(qz, qy, qx) += vu;
                     }
                     if (FMT == 0) {
                         __syncwarp();
@@ -462,7 +555,64 @@ __device__ __forceinline__ void pa_apply_body(const CUtensorMap *xmap_ptr, const
                     q_issued = j + S + 1;
                 }
             }
-            {
+            if constexpr (std::is_same<T, float>::value && FG_F32_COLLOC_PACK) {
+                // transposed z and y passes packed over pairs of qx, then x from the halves
+                float2 s1p[D][Q][NPX > 0 ? NPX : 1];
+                float s1s[D][Q];
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+#pragma unroll
+                    for (int qy = 0; qy < Q; ++qy) {
+#pragma unroll
+                        for (int xp = 0; xp < NPX; ++xp) {
+                            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int qz = 0; qz < Q; ++qz) acc = __ffma2_rn(c_BB32[P - 1][qz][c], wp[qz][qy][xp], acc);
+                            s1p[c][qy][xp] = acc;
+                        }
+                        if (Q & 1) {
+                            float t = 0.f;
+#pragma unroll
+                            for (int qz = 0; qz < Q; ++qz) t += TBf::B(P, qz, c) * ws[qz][qy];
+                            s1s[c][qy] = t;
+                        }
+                    }
+                float2 s2p[D][D][NPX > 0 ? NPX : 1];
+                float s2s[D][D];
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+#pragma unroll
+                    for (int b = 0; b < D; ++b) {
+#pragma unroll
+                        for (int xp = 0; xp < NPX; ++xp) {
+                            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int qy = 0; qy < Q; ++qy) acc = __ffma2_rn(c_BB32[P - 1][qy][b], s1p[c][qy][xp], acc);
+                            s2p[c][b][xp] = acc;
+                        }
+                        if (Q & 1) {
+                            float t = 0.f;
+#pragma unroll
+                            for (int qy = 0; qy < Q; ++qy) t += TBf::B(P, qy, b) * s1s[c][qy];
+                            s2s[c][b] = t;
+                        }
+                    }
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+#pragma unroll
+                    for (int b = 0; b < D; ++b)
+#pragma unroll
+                        for (int a = 0; a < D; ++a) {
+                            float t = 0.f;
+#pragma unroll
+                            for (int xp = 0; xp < NPX; ++xp) {
+                                t += TBf::B(P, 2 * xp, a) * s2p[c][b][xp].x;
+                                t += TBf::B(P, 2 * xp + 1, a) * s2p[c][b][xp].y;
+                            }
+                            if (Q & 1) t += TBf::B(P, Q - 1, a) * s2s[c][b];
+                            out[c][b][a] = t;
+                        }
+            } else {
                 T s1[D][Q][Q];  // [c][qy][qx]
 #pragma unroll
                 for (int c = 0; c < D; ++c)
