@@ -1460,6 +1460,7 @@ template <typename T> static int nn_begin(fg_op *op, const T *r, const float **f
         op->stream = op->nn_stream;
     }
     u->stream = op->stream;
+    u->err = op->d_err;
     const int64_t nv = Vc.nvox();
     int blocks;
     grid_launch(nv, blocks);
@@ -2927,6 +2928,17 @@ static int unet_adam(fg_unet *u, float lr) {
     return FG_OK;
 }
 
+// Reads (and clears) the network's own device error word after a synchronised call.
+static int unet_check_err(fg_unet *u) {
+    int h = 0;
+    CK(cudaMemcpy(&h, u->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        CK(cudaMemset(u->d_err, 0, sizeof(int)));
+        return fail(FG_DEVICE_TIMEOUT, "device-side wait timed out in the network's convolution");
+    }
+    return FG_OK;
+}
+
 extern "C" {
 
 FG_API int fg_unet_create(const int channels[3], uint64_t seed, fg_unet **out) {
@@ -2944,6 +2956,13 @@ FG_API int fg_unet_create(const int channels[3], uint64_t seed, fg_unet **out) {
     fg_unet *u = new fg_unet();
     CK(cudaGetDevice(&u->device));
     u->C0 = c[0]; u->C1 = c[1]; u->C2 = c[2];
+    if (const char *e = std::getenv("FG_UNET_TC")) u->tc = std::atoi(e) != 0;
+    if (cudaMalloc(&u->d_err, sizeof(int)) != cudaSuccess || cudaMemset(u->d_err, 0, sizeof(int)) != cudaSuccess ||
+        conv_tc_init() != FG_OK) {
+        fg_unet_destroy(u);
+        return fail(FG_CUDA_ERROR, "network set-up failed");
+    }
+    u->err = u->d_err;
     const int cin[NLAYERS] = {2, c[0], c[0], c[1], c[1], c[2], c[2] + c[1], c[1] + c[0], c[0]};
     const int cout[NLAYERS] = {c[0], c[0], c[1], c[1], c[2], c[2], c[1], c[0], 8};
     for (int l = 0; l < NLAYERS; ++l) {
@@ -2965,6 +2984,7 @@ FG_API void fg_unet_destroy(fg_unet *u) {
     }
     unet_free_bufs(u->buf);
     if (u->wflip) cudaFree(u->wflip);
+    if (u->d_err) cudaFree(u->d_err);
     delete u;
 }
 
@@ -2997,6 +3017,7 @@ FG_API int fg_unet_forward(fg_unet *u, const float *in, int B, int Z, int Y, int
     if (!u || !in || !out || B < 1) return fail(FG_INVALID_ARGUMENT, "bad arguments");
     CK(cudaSetDevice(u->device));
     u->stream = nullptr;
+    u->err = u->d_err;
     int rc;
     if ((rc = unet_ensure_bufs(u, B, Z, Y, X)) || (rc = unet_load_input(u, in, mem)) || (rc = unet_forward(u)))
         return rc;
@@ -3012,7 +3033,7 @@ FG_API int fg_unet_forward(fg_unet *u, const float *in, int B, int Z, int Y, int
         cudaFree(tmp);
     }
     CK(cudaDeviceSynchronize());
-    return FG_OK;
+    return unet_check_err(u);
 }
 
 // Loss and gradients of the mean squared error between output channel 0 and
@@ -3022,12 +3043,13 @@ FG_API int fg_unet_loss_grad(fg_unet *u, const float *in, const float *target, i
     if (!u || !in || !target || B < 1) return fail(FG_INVALID_ARGUMENT, "bad arguments");
     CK(cudaSetDevice(u->device));
     u->stream = nullptr;
+    u->err = u->d_err;
     int rc;
     if ((rc = unet_ensure_bufs(u, B, Z, Y, X)) || (rc = unet_load_input(u, in, mem)) ||
         (rc = unet_load_target(u, target, mem)) || (rc = unet_loss_grad(u, loss)))
         return rc;
     CK(cudaDeviceSynchronize());
-    return FG_OK;
+    return unet_check_err(u);
 }
 
 // One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss of the batch.
@@ -3237,6 +3259,7 @@ FG_API int fg_unet_train_energy(fg_unet *u, fg_op *op, const double *d_res, int 
     int rc;
     if ((rc = ensure_solver_buffers(op))) return rc;
     u->stream = op->stream;
+    u->err = op->d_err;
     const Vol Vc = nn_coarse_vol(op);
     if ((rc = unet_ensure_bufs(u, B, Vc.Z, Vc.Y, Vc.X))) return rc;
     const int64_t nv = Vc.nvox(), n = op->Nn;

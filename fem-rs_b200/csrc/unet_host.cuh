@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "unet_kernels.cuh"
+#include "unet_tc.cuh"
 
 namespace fg {
 
@@ -55,6 +56,9 @@ struct fg_unet {
     size_t wflip_n = 0;
     int step = 0;
     cudaStream_t stream = nullptr;
+    int tc = 0;            // FG_UNET_TC=1: convolutions on tcgen05 where the shapes allow (default mma.sync)
+    int *d_err = nullptr;  // the network's own device error word
+    int *err = nullptr;    // error word the convolutions report to (d_err, or the solving operator's)
 };
 
 namespace fg {
@@ -170,10 +174,51 @@ static int conv_fwd_ks(fg_unet *u, const TView &in, const Vol &V, const __nv_bfl
     return FG_OK;
 }
 
-// K split chosen so that about 148 x 32 warps are in flight
+template <int NPAD>
+static void conv_tc_launch(fg_unet *u, const TView &in, const Vol &V, const __nv_bfloat16 *w, int cin, int cinp,
+                           int kp, int cout, const float *bias, TView out, int relu) {
+    const int blocks = (int)((V.nvox() + 127) / 128);
+    int G, S;
+    conv_tc_plan(NPAD, cinp, blocks, G, S);
+    conv3_fwd_tc_kernel<NPAD><<<blocks, 128, conv_tc_smem_bytes(NPAD, cinp, G, S), u->stream>>>(
+        in, V, cin, cinp, w, kp, cout, bias, out, relu, G, S, u->err);
+}
+
+// Shapes the tcgen05 convolution takes: channel counts multiples of 8 (the
+// 2-channel input layer stays on mma.sync), 16-byte aligned channel views.
+static bool conv_tc_ok(const fg_unet *u, const TView &in, const TView &out, int cin, int cout, int kp) {
+    return u->tc && cin % 8 == 0 && cout % 8 == 0 && cout <= 64 && (cin + 15) / 16 * 16 <= TC_MAX_CINP &&
+           in.cs % 8 == 0 && in.co % 8 == 0 && out.cs % 8 == 0 && out.co % 8 == 0 && kp % 16 == 0;
+}
+
+// Every tcgen05 convolution instance may use up to TC_SMEM_MAX bytes of
+// dynamic shared memory (set once per network, outside any stream capture).
+static int conv_tc_init() {
+    CK(cudaFuncSetAttribute(conv3_fwd_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+    CK(cudaFuncSetAttribute(conv3_fwd_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+    CK(cudaFuncSetAttribute(conv3_fwd_tc_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+    CK(cudaFuncSetAttribute(conv3_fwd_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+    return FG_OK;
+}
+
+// mma.sync with the K split chosen so that about 148 x 32 warps are in
+// flight; tcgen05 instead where the network asks for it and the shapes allow
+// (on the B200 the mma.sync kernels measured faster at every volume from 9^3
+// to 2 x 65^3, forward and backward)
 static int conv_fwd(fg_unet *u, const ConvLayer &l, const TView &in, const Vol &V, const __nv_bfloat16 *w,
                     int cin, int cout, int kp, const float *bias, TView out, int relu) {
     (void)l;
+    if (conv_tc_ok(u, in, out, cin, cout, kp)) {
+        const int cinp = (cin + 15) / 16 * 16;
+        switch ((cout + 15) / 16) {
+        case 1: conv_tc_launch<16>(u, in, V, w, cin, cinp, kp, cout, bias, out, relu); break;
+        case 2: conv_tc_launch<32>(u, in, V, w, cin, cinp, kp, cout, bias, out, relu); break;
+        case 3: conv_tc_launch<48>(u, in, V, w, cin, cinp, kp, cout, bias, out, relu); break;
+        default: conv_tc_launch<64>(u, in, V, w, cin, cinp, kp, cout, bias, out, relu); break;
+        }
+        CK(cudaGetLastError());
+        return FG_OK;
+    }
     const int64_t tiles = (V.nvox() + 15) / 16;
     if (tiles >= 148 * 32) return conv_fwd_ks<1>(u, in, V, w, cin, cout, kp, bias, out, relu);
     if (tiles >= 148 * 16) return conv_fwd_ks<2>(u, in, V, w, cin, cout, kp, bias, out, relu);

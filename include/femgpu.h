@@ -316,7 +316,12 @@ FG_API int fg_sdirk2(fg_op *stiff, fg_op *stage, double *u, double dt, int n_ste
  * coarsened L = 1..4 times from an operator's DOF lattice (equispaced nodes
  * of any order form a uniform lattice; full-weighting R, trilinear P); with
  * FG_PC_CHEB_NN, fg_pcg runs flexible CG with
- * z = Chebyshev(r) + s 8^L P^L(UNet(R^L r / s, R^L log kappa)), s = rms(R^L r). */
+ * z = Chebyshev(r) + s 8^L P^L(UNet(R^L r / s, R^L log kappa)), s = rms(R^L r).
+ * The convolutions run on the BF16 tensor cores through mma.sync.  Environment,
+ * read by fg_unet_create: FG_UNET_TC=1 moves that network's forward and
+ * input-gradient convolutions with channel counts that are multiples of 8 to
+ * tcgen05 (accumulators in tensor memory); the mma.sync kernels measured
+ * faster on the B200 at every volume from 9^3 to 2 x 65^3. */
 typedef struct fg_unet fg_unet;
 FG_API int fg_unet_create(const int channels[3], uint64_t seed, fg_unet **out);
 FG_API void fg_unet_destroy(fg_unet *net);

@@ -74,6 +74,53 @@ def test_training_reduces_loss():
     assert last < 0.5 * l0, (l0, last)
 
 
+@pytest.mark.parametrize("channels,shape,grads", [
+    ((16, 32, 48), (2, 9, 13, 9), True),
+    ((16, 32, 48), (1, 33, 33, 33), True),   # the network volume of the 128^3 Q2 learned solve
+    ((16, 64, 16), (1, 17, 13, 9), True),    # 64 output channels
+    ((32, 48, 64), (1, 17, 13, 9), False),   # 112 input channels (its backward needs a 112-channel
+                                             # input gradient, which neither path supports)
+    ((8, 16, 32), (3, 9, 9, 13), False),     # 24-channel input (K padded to 32; its backward needs a
+                                             # 24-channel input gradient, which mma.sync does not support)
+    ((8, 8, 8), (2, 13, 9, 9), True),        # 8-channel layers (K padded to 16)
+])
+def test_tcgen05_convolutions_match_mma_sync(channels, shape, grads, monkeypatch):
+    """The convolutions on tcgen05 (TMEM accumulators; FG_UNET_TC=1) against
+    the mma.sync kernels (the default) on the same weights and input: the
+    forward output, the loss and every layer's weight and bias gradient (the
+    input gradients run the same convolution with flipped weights).  Both
+    accumulate BF16 products in FP32, in different orders, so they agree to
+    BF16 rounding: 1e-2 relative for the output and loss, 5e-2 for the
+    gradients, the tolerances used against the reference above."""
+    need_gpu()
+    rng = np.random.default_rng(7)
+    inp = rng.standard_normal(shape + (2,)).astype(np.float32)
+    tgt = rng.standard_normal(shape).astype(np.float32)
+    monkeypatch.setenv("FG_UNET_TC", "0")
+    legacy = femgpu.UNet(channels=channels, seed=11)
+    monkeypatch.setenv("FG_UNET_TC", "1")
+    tc = femgpu.UNet(channels=channels, seed=11)
+    out_l, out_t = legacy.forward(inp), tc.forward(inp)
+    assert np.all(np.isfinite(out_t))
+    assert rel(out_t, out_l) <= 1e-2, rel(out_t, out_l)
+    if not grads:
+        return
+    loss_l, loss_t = legacy.loss_grad(inp, tgt), tc.loss_grad(inp, tgt)
+    assert abs(loss_t - loss_l) <= 1e-2 * abs(loss_l), (loss_t, loss_l)
+    g_l, g_t = legacy.get_grads(), tc.get_grads()
+    assert g_l.shape == g_t.shape
+    c0, c1, c2 = channels
+    shapes = [(2, c0), (c0, c0), (c0, c1), (c1, c1), (c1, c2), (c2, c2), (c2 + c1, c1), (c1 + c0, c0), (c0, 8)]
+    o = 0
+    for li, (ci, co) in enumerate(shapes):
+        nw = co * 27 * ci
+        for part, sl in (("W", slice(o, o + nw)), ("b", slice(o + nw, o + nw + co))):
+            e = rel(g_t[sl], g_l[sl])
+            assert e <= 5e-2, (li, part, e)
+        o += nw + co
+    assert o == g_t.size
+
+
 def _q1_problem(n, seed, p=1):
     kq = lognormal_kappa_q(n, n, n, p, seed=seed)
     mesh = O.Mesh(n, n, n, p)
